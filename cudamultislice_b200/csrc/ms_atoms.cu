@@ -1,0 +1,355 @@
+// ms_atoms.cu -- bit-exact atom binning and the potential-build kernels.
+#include <cmath>
+
+#include "ms_atoms.cuh"
+
+namespace ms {
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Atom binning.  atombin2 (U.cu:277-303) computes, per atom and in FP32,
+//   bidx = floor((x - minx) / (maxx - minx) * 50), bidy likewise,
+//   zid  = floor((maxz - z) / 1);
+// the reference host code then gathers the atoms into a CSR ordered
+// slice -> y-bin -> x-bin, stable in input order (U.cu:1444-1525).  Here the
+// whole index is built on the device: keys + counts, exclusive scan, scatter,
+// a per-bin insertion sort that restores input order, and a gather that
+// stores positions shifted by the box minimum.  Every rounding is explicit
+// (no FMA contraction), so bins agree bit for bit with the host definition.
+// ---------------------------------------------------------------------------
+__global__ void k_bin_keys(const float* __restrict__ x, const float* __restrict__ y,
+                           const float* __restrict__ z, int n, Box b, int nz,
+                           int* __restrict__ key, int* __restrict__ count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float qx = fdiv_x(fsub_x(x[i], b.MinX), fsub_x(b.MaxX, b.MinX));
+  const float qy = fdiv_x(fsub_x(y[i], b.MinY), fsub_x(b.MaxY, b.MinY));
+  int bx = (int)floorf(fmul_x(qx, (float)kBins));
+  int by = (int)floorf(fmul_x(qy, (float)kBins));
+  int bz = (int)floorf(fdiv_x(fsub_x(b.MaxZ, z[i]), 1.0f));
+  // The +-2 A box padding keeps imported atoms in range; displaced thermal
+  // positions are clamped to the edge bins.
+  bx = min(max(bx, 0), kBins - 1);
+  by = min(max(by, 0), kBins - 1);
+  bz = min(max(bz, 0), nz - 1);
+  const int k = bz * kBins2 + by * kBins + bx;
+  key[i] = k;
+  atomicAdd(count + k, 1);
+}
+
+__global__ void k_scatter(const int* __restrict__ key, int n, int* __restrict__ cursor,
+                          int* __restrict__ idx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  idx[atomicAdd(cursor + key[i], 1)] = i;
+}
+
+// Restores input order inside each bin (bins hold a handful of atoms).
+__global__ void k_sort_bins(const int* __restrict__ off, int nbins, int* __restrict__ idx) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbins) return;
+  const int s = off[b], e = off[b + 1];
+  for (int i = s + 1; i < e; ++i) {
+    const int v = idx[i];
+    int j = i - 1;
+    while (j >= s && idx[j] > v) {
+      idx[j + 1] = idx[j];
+      --j;
+    }
+    idx[j + 1] = v;
+  }
+}
+
+__global__ void k_gather(const int* __restrict__ idx, int n, const int* __restrict__ Z,
+                         const float* __restrict__ x, const float* __restrict__ y,
+                         const float* __restrict__ z, Box b, float4* __restrict__ out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const int i = idx[j];
+  out[j] = make_float4(fsub_x(x[i], b.MinX), fsub_x(y[i], b.MinY), fsub_x(z[i], b.MinZ),
+                       __int_as_float(Z[i]));
+}
+
+// ---- exclusive scan of int counts (nbins) into offsets (nbins + 1) ----
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* s_warp, int* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) s_warp[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    int w = (lane < (int)(blockDim.x >> 5)) ? s_warp[lane] : 0;
+    int wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += t;
+    }
+    s_warp[lane] = wi - w;
+    if (lane == 31) s_warp[32] = wi;
+  }
+  __syncthreads();
+  const int r = s_warp[warp] + incl - v;
+  *total = s_warp[32];
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const int* __restrict__ in, int n,
+                                                             int* __restrict__ out, int* __restrict__ tile_sums) {
+  __shared__ int s_warp[33];
+  const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  int v[kScanItems], sum = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    v[k] = (base + k < n) ? in[base + k] : 0;
+    sum += v[k];
+  }
+  int total;
+  int run = block_exclusive_scan(sum, s_warp, &total);
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    if (base + k < n) out[base + k] = run;
+    run += v[k];
+  }
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+// Single block: exclusive scan of the tile sums in place; writes the grand total.
+__global__ void __launch_bounds__(kScanThreads) k_scan_sums(int* __restrict__ sums, int ntiles,
+                                                            int* __restrict__ total_out) {
+  __shared__ int s_warp[33];
+  int carry = 0;
+  for (int base = 0; base < ntiles; base += kScanThreads) {
+    const int i = base + threadIdx.x;
+    const int v = (i < ntiles) ? sums[i] : 0;
+    int total;
+    const int ex = block_exclusive_scan(v, s_warp, &total);
+    if (i < ntiles) sums[i] = carry + ex;
+    carry += total;
+  }
+  if (threadIdx.x == 0) *total_out = carry;
+}
+
+__global__ void k_scan_add(int* __restrict__ out, int n, const int* __restrict__ tile_sums) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] += tile_sums[i / kScanTile];
+}
+
+// ---------------------------------------------------------------------------
+// Potential build.  One CTA covers a 32 x 8 pixel tile (the reference's
+// thread-block shape).  The atoms that can reach the tile (xy bins within
+// sqrt(5) A plus one bin of margin, z-bins of the window) form a list of
+// contiguous CSR segments; the CTA stages them in shared memory in chunks and
+// every thread accumulates its pixel with the reference's exact cut-off
+// r^2 < 5 A^2 evaluated in non-contracted FP32.
+// ---------------------------------------------------------------------------
+constexpr int kTX = 32, kTY = 8, kPotThreads = kTX * kTY;
+constexpr int kChunk = 256;
+constexpr int kMaxSeg = 512;
+
+// v(r) of vatom (U.cu:160-193) from precomputed per-Z coefficients:
+// c[0..2] = 150.4121417 a_i, c[3..5] = 2 pi sqrt(b_i) log2(e),
+// c[6..8] = 266.5157269 c_i d_i^-1.5, c[9..11] = pi^2 / d_i log2(e).
+__device__ __forceinline__ float vatom_f(const float* __restrict__ c, float r2) {
+  float r = sqrtf(fabsf(r2));
+  if (r < 0.25f) r = 0.25f;
+  const float rinv = __frcp_rn(r);
+  const float L = c[0] * exp2f(-c[3] * r) + c[1] * exp2f(-c[4] * r) + c[2] * exp2f(-c[5] * r);
+  const float rr = r * r;
+  const float G = c[6] * exp2f(-c[9] * rr) + c[7] * exp2f(-c[10] * rr) + c[8] * exp2f(-c[11] * rr);
+  return L * rinv + G;
+}
+
+// K0 of bessk0 (U.cu:77-111): the small-argument series (which cancels) in FP64,
+// the asymptotic branch in FP32.
+__device__ __forceinline__ float bessk0_f(float x) {
+  const float ax = fabsf(x);
+  if (ax > 2.0f) {
+    const float t = 2.0f / ax;
+    float s = 0.00053208f;
+    s = s * t - 0.00251540f;
+    s = s * t + 0.00587872f;
+    s = s * t - 0.01062446f;
+    s = s * t + 0.02189568f;
+    s = s * t - 0.07832358f;
+    s = s * t + 1.25331414f;
+    return expf(-ax) * s * rsqrtf(ax);
+  }
+  if (ax > 0.0f) {
+    const double xd = ax, h = xd / 2.0, x2 = h * h;
+    double s = 0.00000740;
+    s = s * x2 + 0.00010750;
+    s = s * x2 + 0.00262698;
+    s = s * x2 + 0.03488590;
+    s = s * x2 + 0.23069756;
+    s = s * x2 + 0.42278420;
+    s = s * x2 - 0.57721566;
+    double t = xd / 3.75;
+    t = t * t;
+    double i0 = 0.0045813;
+    i0 = i0 * t + 0.0360768;
+    i0 = i0 * t + 0.2659732;
+    i0 = i0 * t + 1.2067492;
+    i0 = i0 * t + 3.0899424;
+    i0 = i0 * t + 3.5156229;
+    i0 = i0 * t + 1.0;
+    return (float)(-log(h) * i0 + s);
+  }
+  return 1.0e20f;
+}
+
+// vz(r) of vzatom2 (U.cu:119-152): c[12..14] = 300.8242834 a_i,
+// c[15..17] = 2 pi sqrt(b_i), c[18..20] = 150.4121417 c_i / d_i,
+// c[21..23] = pi^2 / d_i log2(e).
+__device__ __forceinline__ float vzatom2_f(const float* __restrict__ c, float r2) {
+  float r = sqrtf(fabsf(r2));
+  if (r < 0.25f) r = 0.25f;
+  const float L = c[12] * bessk0_f(c[15] * r) + c[13] * bessk0_f(c[16] * r) + c[14] * bessk0_f(c[17] * r);
+  const float rr = r * r;
+  const float G = c[18] * exp2f(-c[21] * rr) + c[19] * exp2f(-c[22] * rr) + c[20] * exp2f(-c[23] * rr);
+  return L + G;
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a) {
+  constexpr int NSUB = (KIND == POT_CONVENTIONAL) ? 20 : 1;
+  __shared__ float4 s_at[kChunk];
+  __shared__ float s_coef[103 * kCoefPerZ];
+  __shared__ int s_start[kMaxSeg];
+  __shared__ int s_pref[kMaxSeg + 1];
+  __shared__ int s_warp[33];
+
+  for (int i = threadIdx.x; i < 103 * kCoefPerZ; i += kPotThreads) s_coef[i] = a.coef[i];
+
+  const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
+  const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY;
+  const int x = x0 + tx, y = y0 + ty;
+  const bool inside = (x < a.nx) && (y < a.ny);
+
+  // pixel position, rounded exactly as the host definition (no FMA)
+  const float px = fadd_x(a.xoff, fmul_x((float)x, a.ps));
+  const float py = fadd_x(a.yoff, fmul_x((float)y, a.ps));
+
+  // candidate bins of the tile (conservative: sqrt(5) + one bin)
+  const float xlo = a.xoff + x0 * a.ps - 2.2361f, xhi = a.xoff + (x0 + kTX - 1) * a.ps + 2.2361f;
+  const float ylo = a.yoff + y0 * a.ps - 2.2361f, yhi = a.yoff + (y0 + kTY - 1) * a.ps + 2.2361f;
+  const int bxl = max((int)floorf(xlo / a.bw_x) - 1, 0);
+  const int bxh = min((int)floorf(xhi / a.bw_x) + 1, kBins - 1);
+  const int byl = max((int)floorf(ylo / a.bw_y) - 1, 0);
+  const int byh = min((int)floorf(yhi / a.bw_y) + 1, kBins - 1);
+  const int nyb = byh - byl + 1;
+
+  float acc = 0.0f;
+  if (bxl <= bxh && byl <= byh && a.kt <= a.kb) {
+    const int kstep = max(kMaxSeg / nyb, 1);
+    for (int kg = a.kt; kg <= a.kb; kg += kstep) {
+      const int kend = min(kg + kstep - 1, a.kb);
+      const int nseg = (kend - kg + 1) * nyb;
+      // segment lengths and their exclusive prefix
+      int len0 = 0, len1 = 0, st0 = 0, st1 = 0;
+      const int s0 = threadIdx.x, s1 = threadIdx.x + kPotThreads;
+      if (s0 < nseg) {
+        const int k = kg + s0 / nyb, j = byl + s0 % nyb;
+        const int b = k * kBins2 + j * kBins;
+        st0 = a.off[b + bxl];
+        len0 = a.off[b + bxh + 1] - st0;
+      }
+      if (s1 < nseg) {
+        const int k = kg + s1 / nyb, j = byl + s1 % nyb;
+        const int b = k * kBins2 + j * kBins;
+        st1 = a.off[b + bxl];
+        len1 = a.off[b + bxh + 1] - st1;
+      }
+      int total;
+      const int ex = block_exclusive_scan(len0 + len1, s_warp, &total);
+      if (s0 < nseg) { s_start[s0] = st0; s_pref[s0] = ex; }
+      if (s1 < nseg) { s_start[s1] = st1; s_pref[s1] = ex + len0; }
+      if (threadIdx.x == 0) s_pref[nseg] = total;
+      __syncthreads();
+
+      for (int base = 0; base < total; base += kChunk) {
+        const int cnt = min(kChunk, total - base);
+        if (threadIdx.x < cnt) {
+          const int gidx = base + threadIdx.x;
+          int lo = 0, hi = nseg - 1;  // last segment with s_pref <= gidx
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (s_pref[mid] <= gidx) lo = mid; else hi = mid - 1;
+          }
+          s_at[threadIdx.x] = a.atoms[s_start[lo] + (gidx - s_pref[lo])];
+        }
+        __syncthreads();
+        for (int i = 0; i < cnt; ++i) {
+          const float4 at = s_at[i];
+          const float dx = fsub_x(px, at.x), dy = fsub_x(py, at.y);
+          const float dxy = fadd_x(fmul_x(dx, dx), fmul_x(dy, dy));
+          if (!(dxy < 5.0f)) continue;
+          const float* c = s_coef + (__float_as_int(at.w) - 1) * kCoefPerZ;
+          if constexpr (KIND == POT_PROJECTED) {
+            const int slab = (int)floorf(fdiv_x(fsub_x(a.top, at.z), a.slab_dz));
+            if (slab == a.slab) acc += vzatom2_f(c, dxy);
+          } else {
+#pragma unroll
+            for (int m = 0; m < NSUB; ++m) {
+              const float dz = fsub_x(a.zsub[m], at.z);
+              const float r2 = fadd_x(dxy, fmul_x(dz, dz));
+              if (r2 < 5.0f) acc += a.wsub * vatom_f(c, r2);
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+  }
+  if (inside) a.V[(long long)y * a.nx + x] = acc;
+}
+
+}  // namespace
+
+size_t bin_scratch_blocks(int nbins) { return (size_t)(nbins + kScanTile - 1) / kScanTile + 1; }
+
+cudaError_t build_atom_index(const int* dZ, const float* dx, const float* dy, const float* dz, int n,
+                             const Box& box, int nz, AtomIndex& out, BinScratch& scr, cudaStream_t s) {
+  const int nbins = nz * kBins2;
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(scr.cursor, 0, sizeof(int) * nbins, s)) != cudaSuccess) return e;
+  const int tb = 256;
+  k_bin_keys<<<(n + tb - 1) / tb, tb, 0, s>>>(dx, dy, dz, n, box, nz, scr.key, scr.cursor);
+  // offsets = exclusive scan of the counts; off[nbins] = n
+  const int ntiles = (nbins + kScanTile - 1) / kScanTile;
+  k_scan_tiles<<<ntiles, kScanThreads, 0, s>>>(scr.cursor, nbins, out.off, scr.blocksum);
+  k_scan_sums<<<1, kScanThreads, 0, s>>>(scr.blocksum, ntiles, out.off + nbins);
+  k_scan_add<<<(nbins + tb - 1) / tb, tb, 0, s>>>(out.off, nbins, scr.blocksum);
+  if ((e = cudaMemcpyAsync(scr.cursor, out.off, sizeof(int) * nbins, cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
+    return e;
+  k_scatter<<<(n + tb - 1) / tb, tb, 0, s>>>(scr.key, n, scr.cursor, scr.idx);
+  k_sort_bins<<<(nbins + tb - 1) / tb, tb, 0, s>>>(out.off, nbins, scr.idx);
+  k_gather<<<(n + tb - 1) / tb, tb, 0, s>>>(scr.idx, n, dZ, dx, dy, dz, box, out.atoms);
+  out.n = n;
+  out.nz = nz;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_potential(const PotArgs& a, int kind, cudaStream_t s) {
+  dim3 grid((a.nx + kTX - 1) / kTX, (a.ny + kTY - 1) / kTY);
+  switch (kind) {
+    case POT_CONVENTIONAL: k_potential<POT_CONVENTIONAL><<<grid, kPotThreads, 0, s>>>(a); break;
+    case POT_FD: k_potential<POT_FD><<<grid, kPotThreads, 0, s>>>(a); break;
+    case POT_PROJECTED: k_potential<POT_PROJECTED><<<grid, kPotThreads, 0, s>>>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace ms

@@ -1,0 +1,60 @@
+// ms_atoms.cuh -- atom index (bit-exact binning) and projected-potential build.
+#pragma once
+#include <cuda_runtime.h>
+#include "ms_common.cuh"
+
+namespace ms {
+
+// Box as computed by LoadAtomFile (U.cu:1350-1355).
+struct Box {
+  float MaxX, MinX, MaxY, MinY, MaxZ, MinZ;
+};
+
+// Device atom index: atoms sorted slice -> y-bin -> x-bin, stable in input
+// order, positions shifted by the box minimum (U.cu:1444-1525).
+struct AtomIndex {
+  float4* atoms;   // (x, y, z, Z as int bits), shifted frame
+  int* off;        // CSR offsets, nz * 2500 + 1
+  int n;           // atoms
+  int nz;          // 1-A z-bins
+};
+
+// Scratch for building the index (all sized by n or by the bin count).
+struct BinScratch {
+  int* key;      // n
+  int* idx;      // n
+  int* cursor;   // nbins
+  int* blocksum; // scan partials
+};
+
+size_t bin_scratch_blocks(int nbins);
+cudaError_t build_atom_index(const int* dZ, const float* dx, const float* dy, const float* dz, int n,
+                             const Box& box, int nz, AtomIndex& out, BinScratch& scr, cudaStream_t s);
+
+// Per-Z coefficients of vatom / vzatom2 derived from one fparams row on the
+// host in FP64: 12 floats for vatom, then 12 for vzatom2 (see engine).
+constexpr int kCoefPerZ = 24;
+
+enum PotKind : int { POT_CONVENTIONAL = 0, POT_FD = 1, POT_PROJECTED = 2 };
+
+struct PotArgs {
+  const float4* atoms;
+  const int* off;
+  const float* coef;     // [103][kCoefPerZ]
+  float* V;              // [ny][nx] output (V*A, not yet exponentiated)
+  int nx, ny, nz;
+  float ps, xoff, yoff;  // pixel (x,y) sits at (xoff + x*ps, yoff + y*ps) in the shifted frame
+  float bw_x, bw_y;      // bin widths (MaxX-MinX)/50, (MaxY-MinY)/50
+  int kt, kb;            // inclusive z-bin window
+  int nsub;              // sub-planes (20 conventional, 1 finite difference)
+  float zsub[20];        // sub-plane z (shifted frame), FP32 as the reference
+  float wsub;            // weight per sub-plane
+  // projected mode: atoms with floorf((top - z)/dz) == slab
+  float top, slab_dz;
+  int slab;
+  long long batch_stride_V;
+};
+
+cudaError_t launch_potential(const PotArgs& a, int kind, cudaStream_t s);
+
+}  // namespace ms

@@ -1,0 +1,1480 @@
+// ms_engine.cu -- host engine and C ABI of the B200 multislice library.
+//
+// ms::Engine is the B200-native counterpart of the reference class
+// UnmanagedMultisliceSimulation (GUI Simulation/unmanagedGUISimulation.cuh:62-200,
+// GUI Simulation/UnmanagedGUISimulation.cu = "U.cu").  Set-up scalars that the
+// reference computes on the host in FP32 (wavelength, interaction constant,
+// finite-difference step, frequencies, kmax, slice planes) are computed here
+// with the same FP32 operations in the same order, so the engine solves exactly
+// the reference's problem; the heavy numerics run in the CUDA kernels of
+// ms_atoms.cu (binning, potentials), ms_slice.cu (fused slice passes) and
+// ms_pointwise.cu (plain path, finite differences, probe, read-out).
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/mslice.h"
+#include "ms_atoms.cuh"
+#include "ms_philox.h"
+#include "ms_pointwise.cuh"
+#include "ms_slice.cuh"
+
+// Inside Engine members: return an ms_status with the message set.
+#define MS_TRY(expr)                                    \
+  do {                                                  \
+    cudaError_t _e = (expr);                            \
+    if (_e != cudaSuccess) return cuda_fail(_e, #expr); \
+  } while (0)
+#define MS_TRY_FFT(expr)                                                                 \
+  do {                                                                                   \
+    cufftResult _r = (expr);                                                             \
+    if (_r != CUFFT_SUCCESS) return fail(MS_ERR_CUDA, std::string("cuFFT failed: ") + #expr); \
+  } while (0)
+
+namespace ms {
+
+// ---------------------------------------------------------------------------
+// small utilities
+// ---------------------------------------------------------------------------
+struct Status {
+  int code;
+  std::string msg;
+};
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t resize(size_t count) {
+    if (count == n && p) return cudaSuccess;
+    release();
+    if (count == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return e;
+    }
+    n = count;
+    return cudaSuccess;
+  }
+};
+
+// Element symbols for Z = 1..103 (the rows of fparams.dat).
+static const char* const kElements[103] = {
+    "H",  "He", "Li", "Be", "B",  "C",  "N",  "O",  "F",  "Ne", "Na", "Mg", "Al", "Si", "P",  "S",  "Cl", "Ar",
+    "K",  "Ca", "Sc", "Ti", "V",  "Cr", "Mn", "Fe", "Co", "Ni", "Cu", "Zn", "Ga", "Ge", "As", "Se", "Br", "Kr",
+    "Rb", "Sr", "Y",  "Zr", "Nb", "Mo", "Tc", "Ru", "Rh", "Pd", "Ag", "Cd", "In", "Sn", "Sb", "Te", "I",  "Xe",
+    "Cs", "Ba", "La", "Ce", "Pr", "Nd", "Pm", "Sm", "Eu", "Gd", "Tb", "Dy", "Ho", "Er", "Tm", "Yb", "Lu", "Hf",
+    "Ta", "W",  "Re", "Os", "Ir", "Pt", "Au", "Hg", "Tl", "Pb", "Bi", "Po", "At", "Rn", "Fr", "Ra", "Ac", "Th",
+    "Pa", "U",  "Np", "Pu", "Am", "Cm", "Bk", "Cf", "Es", "Fm", "Md", "No", "Lr"};
+
+// GetZNum U.cu:1188-1243: the reference knows 25 symbols; any other maps to 1.
+static int znum(const std::string& s, bool full) {
+  static const int ref_known[] = {1, 2, 3, 4, 5, 6, 7, 8, 9, 11, 12, 14, 15, 16, 17, 20, 24, 35, 26, 38, 44, 57, 62, 73, 74};
+  if (full) {
+    for (int z = 1; z <= 103; ++z)
+      if (s == kElements[z - 1]) return z;
+    return 1;
+  }
+  for (int z : ref_known)
+    if (s == kElements[z - 1]) return z;
+  return 1;
+}
+
+// ---------------------------------------------------------------------------
+// Engine
+// ---------------------------------------------------------------------------
+class Engine {
+ public:
+  explicit Engine(int device) : device_(device) {}
+  ~Engine() {
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    if (have_plan_) cufftDestroy(plan_);
+    if (ev0_) cudaEventDestroy(ev0_);
+    if (ev1_) cudaEventDestroy(ev1_);
+    if (stream_) cudaStreamDestroy(stream_);
+  }
+
+  std::string err;
+  long long launches = 0;
+
+  int init() {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(MS_ERR_CUDA, "no CUDA device available");
+    if (device_ < 0 || device_ >= ndev) return fail(MS_ERR_INVALID, "device index out of range");
+    MS_TRY(cudaSetDevice(device_));
+    MS_TRY(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    MS_TRY(cudaEventCreate(&ev0_));
+    MS_TRY(cudaEventCreate(&ev1_));
+    return MS_OK;
+  }
+
+  // ---- options ----
+  int set_option(int opt, int value) {
+    switch (opt) {
+      case MS_OPT_SLICE_PATH:
+        if (value != 0 && value != 1) return fail(MS_ERR_INVALID, "slice path must be 0 (fused) or 1 (plain)");
+        force_plain_ = value == 1;
+        invalidate_graph();
+        return MS_OK;
+      case MS_OPT_ELEMENT_TABLE:
+        if (value != 0 && value != 1) return fail(MS_ERR_INVALID, "element table must be 0 or 1");
+        full_table_ = value == 1;
+        return MS_OK;
+      case MS_OPT_POTENTIAL:
+        if (value != 0 && value != 1) return fail(MS_ERR_INVALID, "potential mode must be 0 or 1");
+        pot_mode_ = value;
+        stack_valid_ = false;
+        invalidate_graph();
+        return MS_OK;
+      default:
+        return fail(MS_ERR_INVALID, "unknown option");
+    }
+  }
+
+  // ---- structure ----
+  int import_atoms(const char* path) {
+    if (!path) return fail(MS_ERR_INVALID, "null path");
+    std::ifstream in(path);
+    if (!in) return fail(MS_ERR_IO, std::string("cannot open structure file ") + path);
+    int n = 0;
+    if (!(in >> n) || n <= 0) return fail(MS_ERR_IO, "structure file: bad atom count");
+    std::string line;
+    std::getline(in, line);
+    std::getline(in, line);  // comment line
+    std::vector<int> Z(n);
+    std::vector<float> x(n), y(n), z(n);
+    for (int i = 0; i < n; ++i) {
+      std::string sym;
+      if (!(in >> sym >> x[i] >> y[i] >> z[i])) return fail(MS_ERR_IO, "structure file: truncated atom list");
+      Z[i] = znum(sym, full_table_);
+    }
+    return set_atoms(Z.data(), x.data(), y.data(), z.data(), n);
+  }
+
+  int set_atoms(const int* Z, const float* x, const float* y, const float* z, int n) {
+    if (n <= 0 || !Z || !x || !y || !z) return fail(MS_ERR_INVALID, "no atoms");
+    for (int i = 0; i < n; ++i) {
+      if (Z[i] < 1 || Z[i] > 103) return fail(MS_ERR_INVALID, "atomic number out of range 1..103");
+      if (!std::isfinite(x[i]) || !std::isfinite(y[i]) || !std::isfinite(z[i]))
+        return fail(MS_ERR_INVALID, "non-finite atom position");
+    }
+    hZ_.assign(Z, Z + n);
+    hx_.assign(x, x + n);
+    hy_.assign(y, y + n);
+    hz_.assign(z, z + n);
+    // bounding box as LoadAtomFile (U.cu:1326-1355): extreme atoms, +-2 A in FP32
+    size_t mx = 0, mnx = 0, my = 0, mny = 0, mz = 0, mnz = 0;
+    for (size_t i = 1; i < hx_.size(); ++i) {
+      if (hx_[i] > hx_[mx]) mx = i;
+      if (hy_[i] > hy_[my]) my = i;
+      if (hz_[i] > hz_[mz]) mz = i;
+      if (hx_[i] < hx_[mnx]) mnx = i;
+      if (hy_[i] < hy_[mny]) mny = i;
+      if (hz_[i] < hz_[mnz]) mnz = i;
+    }
+    box_.MaxX = hx_[mx] + 2;
+    box_.MinX = hx_[mnx] - 2;
+    box_.MaxY = hy_[my] + 2;
+    box_.MinY = hy_[mny] - 2;
+    box_.MaxZ = hz_[mz] + 2;
+    box_.MinZ = hz_[mnz] - 2;
+    have_atoms_ = true;
+    have_index_ = false;
+    stack_valid_ = false;
+    invalidate_graph();
+    return MS_OK;
+  }
+
+  int upload_binned(bool tds, uint64_t seed, uint32_t pass, float sigma) {
+    if (!have_atoms_) return fail(MS_ERR_STATE, "no atoms: call ms_import_atoms or ms_set_atoms first");
+    const int n = (int)hx_.size();
+    std::vector<float> x = hx_, y = hy_, z = hz_;
+    if (tds) {
+      if (!(sigma >= 0) || !std::isfinite(sigma)) return fail(MS_ERR_INVALID, "bad thermal displacement sigma");
+      tds_displace(hx_.data(), hy_.data(), hz_.data(), n, seed, pass, sigma, x.data(), y.data(), z.data());
+    }
+    // nSlices = ceil((MaximumZ-MinimumZ)/dz), dz = 1 (U.cu:1409-1411)
+    int nz = (int)std::ceil((box_.MaxZ - box_.MinZ) / (float)1);
+    nz += (nz == 0);
+    const int nbins = nz * kBins2;
+    MS_TRY(d_Zin_.resize(n));
+    MS_TRY(d_xin_.resize(n));
+    MS_TRY(d_yin_.resize(n));
+    MS_TRY(d_zin_.resize(n));
+    MS_TRY(d_atoms_.resize(n));
+    MS_TRY(d_off_.resize(nbins + 1));
+    MS_TRY(d_key_.resize(n));
+    MS_TRY(d_idx_.resize(n));
+    MS_TRY(d_cursor_.resize(nbins));
+    MS_TRY(d_blocksum_.resize(bin_scratch_blocks(nbins)));
+    MS_TRY(cudaMemcpyAsync(d_Zin_.p, hZ_.data(), sizeof(int) * n, cudaMemcpyHostToDevice, stream_));
+    MS_TRY(cudaMemcpyAsync(d_xin_.p, x.data(), sizeof(float) * n, cudaMemcpyHostToDevice, stream_));
+    MS_TRY(cudaMemcpyAsync(d_yin_.p, y.data(), sizeof(float) * n, cudaMemcpyHostToDevice, stream_));
+    MS_TRY(cudaMemcpyAsync(d_zin_.p, z.data(), sizeof(float) * n, cudaMemcpyHostToDevice, stream_));
+    AtomIndex idx{d_atoms_.p, d_off_.p, 0, 0};
+    BinScratch scr{d_key_.p, d_idx_.p, d_cursor_.p, d_blocksum_.p};
+    MS_TRY(build_atom_index(d_Zin_.p, d_xin_.p, d_yin_.p, d_zin_.p, n, box_, nz, idx, scr, stream_));
+    launches += 8;
+    MS_TRY(cudaStreamSynchronize(stream_));
+    natoms_ = n;
+    nzb_ = nz;
+    have_index_ = true;
+    stack_valid_ = false;
+    invalidate_graph();
+    return MS_OK;
+  }
+
+  // fparams.dat, U.cu:1718-1747: rows of 12 numbers, row Z-1.
+  int get_parameterisation(const char* path) {
+    if (!path) return fail(MS_ERR_INVALID, "null path");
+    std::ifstream in(path);
+    if (!in) return fail(MS_ERR_IO, std::string("cannot open parameterisation file ") + path);
+    std::vector<double> fp;
+    double v[12];
+    while (fp.size() < 103 * 12) {
+      int k = 0;
+      for (; k < 12; ++k)
+        if (!(in >> v[k])) break;
+      if (k < 12) break;
+      fp.insert(fp.end(), v, v + 12);
+    }
+    if (fp.empty()) return fail(MS_ERR_IO, "parameterisation file holds no complete row");
+    nrows_fp_ = (int)(fp.size() / 12);
+    for (double d : fp)
+      if (!std::isfinite(d)) return fail(MS_ERR_IO, "parameterisation file holds a non-finite value");
+    // Per-Z coefficients in FP64, rounded once (layout in ms_atoms.cu).
+    const double pi = 3.141592654, log2e = 1.4426950408889634;
+    std::vector<float> coef(103 * kCoefPerZ, 0.0f);
+    for (int r = 0; r < nrows_fp_; ++r) {
+      const double* f = &fp[r * 12];
+      float* c = &coef[r * kCoefPerZ];
+      bool ok = true;
+      for (int i = 0; i < 3; ++i) {
+        const double a = f[2 * i], b = f[2 * i + 1], cc = f[6 + 2 * i], d = f[7 + 2 * i];
+        if (!(b >= 0) || !(d > 0)) { ok = false; break; }
+        c[i] = (float)(150.4121417 * a);
+        c[3 + i] = (float)(2.0 * pi * std::sqrt(b) * log2e);
+        c[6 + i] = (float)(266.5157269 * cc * std::pow(d, -1.5));
+        c[9 + i] = (float)(pi * pi / d * log2e);
+        c[12 + i] = (float)(300.8242834 * a);
+        c[15 + i] = (float)(2.0 * pi * std::sqrt(b));
+        c[18 + i] = (float)(150.4121417 * cc / d);
+        c[21 + i] = (float)(pi * pi / d * log2e);
+      }
+      if (!ok) return fail(MS_ERR_IO, "parameterisation row with b < 0 or d <= 0");
+    }
+    MS_TRY(d_coef_.resize(coef.size()));
+    MS_TRY(cudaMemcpy(d_coef_.p, coef.data(), sizeof(float) * coef.size(), cudaMemcpyHostToDevice));
+    have_fp_ = true;
+    stack_valid_ = false;
+    invalidate_graph();
+    return MS_OK;
+  }
+
+  int apply_microscope(float kV, float df, float A2, float phi2, float Cs, float beta, float delta, float ap) {
+    const float v[8] = {kV, df, A2, phi2, Cs, beta, delta, ap};
+    for (float f : v)
+      if (!std::isfinite(f)) return fail(MS_ERR_INVALID, "non-finite microscope parameter");
+    if (!(kV > 0)) return fail(MS_ERR_INVALID, "accelerating voltage must be positive");
+    kV_ = kV; df_ = df; A2_ = A2; phi2_ = phi2; Cs_ = Cs; beta_ = beta; delta_ = delta; aperture_ = ap;
+    have_micro_ = true;
+    return MS_OK;
+  }
+
+  // SetCalculationVariables U.cu:1763-1875 (stem = false) and
+  // STEMSetCalculationVariables U.cu:2567-2670 (stem = true).
+  int set_calc(float ps, float df, int nx, int ny, float sizeZ, float xoff, float yoff, bool stem) {
+    if (!have_micro_) return fail(MS_ERR_STATE, "microscope parameters not applied");
+    if (!have_atoms_) return fail(MS_ERR_STATE, "no atoms");
+    if (nx < 2 || ny < 2 || nx > 16384 || ny > 16384) return fail(MS_ERR_INVALID, "grid size out of range 2..16384");
+    if (!(ps > 0) || !std::isfinite(ps) || !std::isfinite(df) || !std::isfinite(xoff) || !std::isfinite(yoff))
+      return fail(MS_ERR_INVALID, "bad pixel size, defocus or offset");
+    nx_ = nx; ny_ = ny; ps_ = ps; df_ = df; stem_ = stem;
+    xoff_ = stem ? 0.0f : xoff;
+    yoff_ = stem ? 0.0f : yoff;
+    const float ksizex = ps * nx, ksizey = ps * ny;
+    const float Pi = 3.1415926f;
+    const float V = kV_;
+    const float echarge = 1.6e-019f;
+    wavel_ = 6.63e-034f * 3e+008f / std::sqrt((echarge * V * 1000 * (2 * 9.11e-031f * 9e+016f + echarge * V * 1000))) *
+             1e+010f;
+    sigma2_ = (2 * Pi / (wavel_ * V * 1000)) *
+              ((9.11e-031f * 9e+016f + echarge * V * 1000) / (2 * 9.11e-031f * 9e+016f + echarge * V * 1000));
+    const float V2 = V * 1000;
+    const float fnkx = (float)nx, fnky = (float)ny;
+    const float p1 = fnkx / (2 * ksizex), p2 = fnky / (2 * ksizey);
+    const float p12 = p1 * p1, p22 = p2 * p2;
+    const float ke2 = (.666666f) * (p12 + p22);
+    const float qA = (ke2 * ke2 * 16 * Pi * Pi * Pi * Pi) - (32 * Pi * Pi * Pi * ke2 * sigma2_ * V2 / wavel_) +
+                     (16 * Pi * Pi * sigma2_ * sigma2_ * V2 * V2 / (wavel_ * wavel_));
+    const float qB = 16 * Pi * Pi * (ke2 - (sigma2_ * V2 / (Pi * wavel_)) - (1 / (4 * wavel_ * wavel_)));
+    const float qC = 3;
+    const float disc = qB * qB - 4 * qA * qC;
+    float msd = (-qB + std::sqrt(disc)) / (2 * qA);
+    msd = (float)(0.99 * (double)std::sqrt(msd));
+    if (stem && msd > 0.06) msd = (float)0.06;
+    int nFD = (int)std::ceil(sizeZ / msd);
+    nFD += (nFD == 0);
+    fd_stable_ = disc >= 0 && msd > 0 && std::isfinite(msd);
+    dzFD_ = msd;
+    nFD_ = fd_stable_ ? nFD : -1;
+    lbz_ = (int)std::ceil(std::sqrt(5.0f) / (float)1);  // consts[2], U.cu:1859
+    have_calc_ = true;
+    have_freq_ = false;
+    have_waves_ = false;
+    stack_valid_ = false;
+    invalidate_graph();
+    return MS_OK;
+  }
+
+  // PreCalculateFrequencies U.cu:1877-1964 (the unused doubled grids are not built).
+  int precalc() {
+    if (!have_calc_) return fail(MS_ERR_STATE, "calculation variables not set");
+    const int nx = nx_, ny = ny_;
+    const float ksizex = ps_ * nx, ksizey = ps_ * ny;
+    const int imidx = (int)std::floor(nx / 2 + 0.5), imidy = (int)std::floor(ny / 2 + 0.5);
+    hkx_.resize(nx);
+    hky_.resize(ny);
+    for (int i = 1; i <= nx; ++i) hkx_[i - 1] = ((i - 1) > imidx) ? ((i - 1) - nx) / ksizex : (i - 1) / ksizex;
+    for (int i = 1; i <= ny; ++i) hky_[i - 1] = ((i - 1) > imidy) ? ((i - 1) - ny) / ksizey : (i - 1) / ksizey;
+    const float kmaxx = (float)std::pow((double)(hkx_[imidx - 1] * 1 / 2), 2);
+    const float kmaxy = (float)std::pow((double)(hky_[imidy - 1] * 1 / 2), 2);
+    kmax_ = std::sqrt((kmaxy <= kmaxx) ? kmaxy : kmaxx);
+    const size_t N = (size_t)nx * ny;
+    MS_TRY(d_kx_.resize(nx));
+    MS_TRY(d_ky_.resize(ny));
+    MS_TRY(cudaMemcpy(d_kx_.p, hkx_.data(), sizeof(float) * nx, cudaMemcpyHostToDevice));
+    MS_TRY(cudaMemcpy(d_ky_.p, hky_.data(), sizeof(float) * ny, cudaMemcpyHostToDevice));
+    // wave buffers
+    MS_TRY(d_psi0_.resize(N));
+    MS_TRY(d_psi_.resize(N));
+    MS_TRY(d_psim_.resize(N));
+    MS_TRY(d_t1_.resize(N));
+    MS_TRY(d_t2_.resize(N));
+    MS_TRY(d_V_.resize(N));
+    MS_TRY(d_f_.resize(N));
+    MS_TRY(d_grad_.resize(N));
+    MS_TRY(d_partial_.resize(1024 + 8));
+    // cuFFT plan for the plain path, as U.cu:1961 (ny rows of nx)
+    if (have_plan_) {
+      cufftDestroy(plan_);
+      have_plan_ = false;
+    }
+    if (cufftPlan2d(&plan_, ny, nx, CUFFT_C2C) != CUFFT_SUCCESS) return fail(MS_ERR_CUDA, "cufftPlan2d failed");
+    if (cufftSetStream(plan_, stream_) != CUFFT_SUCCESS) return fail(MS_ERR_CUDA, "cufftSetStream failed");
+    have_plan_ = true;
+    fused_ok_ = fused_supported(nx, ny);
+    if (fused_ok_) {
+      std::vector<float2> tw(std::max(nx, ny));
+      MS_TRY(d_twx_.resize(nx));
+      MS_TRY(d_twy_.resize(ny));
+      make_twiddles(nx, tw.data());
+      MS_TRY(cudaMemcpy(d_twx_.p, tw.data(), sizeof(float2) * nx, cudaMemcpyHostToDevice));
+      make_twiddles(ny, tw.data());
+      MS_TRY(cudaMemcpy(d_twy_.p, tw.data(), sizeof(float2) * ny, cudaMemcpyHostToDevice));
+    }
+    prop_dz_ = -1.0f;
+    have_freq_ = true;
+    have_waves_ = false;
+    stack_valid_ = false;
+    invalidate_graph();
+    return MS_OK;
+  }
+
+  // ---- wavefunctions ----
+  int init_waves(float conv_dz) {
+    if (!have_freq_) return fail(MS_ERR_STATE, "frequencies not precalculated");
+    if (conv_dz > 0 && !std::isfinite(conv_dz)) return fail(MS_ERR_INVALID, "bad slice thickness");
+    const float dz = conv_dz > 0 ? conv_dz : 1.0f;  // U.cu:1968 / U.cu:2005
+    if (dz != convdz_) {
+      stack_valid_ = false;
+      invalidate_graph();
+    }
+    convdz_ = dz;
+    const Grid2 g{nx_, ny_};
+    MS_TRY(pw_fill(d_psi0_.p, g, make_float2(1.f, 0.f), stream_, &launches));
+    return finish_init();
+  }
+
+  int stem_init_waves(int px, int py) {
+    if (!have_freq_) return fail(MS_ERR_STATE, "frequencies not precalculated");
+    const Grid2 g{nx_, ny_};
+    const float apert = (float)((double)aperture_ * 0.001 / (double)wavel_);
+    MS_TRY(pw_probe(d_t1_.p, d_kx_.p, d_ky_.p, px, py, apert, ps_, df_, Cs_, wavel_, g, stream_, &launches));
+    // unnormalised inverse FFT (U.cu:2693), then divide by sum |psi| (U.cu:2698-2705)
+    MS_TRY_FFT(cufftExecC2C(plan_, d_t1_.p, d_psi0_.p, CUFFT_INVERSE));
+    MS_TRY(pw_sum_abs(d_psi0_.p, (long long)nx_ * ny_, d_partial_.p, d_partial_.p + 1024, stream_, &launches));
+    double l1 = 0;
+    MS_TRY(cudaMemcpyAsync(&l1, d_partial_.p + 1024, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    MS_TRY(cudaStreamSynchronize(stream_));
+    if (!(l1 > 0)) return fail(MS_ERR_NUMERIC, "probe is empty (aperture smaller than one frequency pixel)");
+    MS_TRY(pw_scale(d_psi0_.p, (float)(1.0 / l1), g, stream_, &launches));
+    return finish_init();
+  }
+
+  int set_fd_dz(float dz) {
+    if (!have_calc_) return fail(MS_ERR_STATE, "calculation variables not set");
+    if (!(dz > 0) || !std::isfinite(dz)) return fail(MS_ERR_INVALID, "bad finite-difference step");
+    dzFD_ = dz;
+    int n = (int)std::ceil((box_.MaxZ - box_.MinZ) / dz);
+    nFD_ = n + (n == 0);
+    fd_stable_ = true;
+    return MS_OK;
+  }
+
+  // ---- steps ----
+  int step_conventional(int it) {
+    if (!have_waves_) return fail(MS_ERR_STATE, "wavefunctions not initialised");
+    if (it < 1) return fail(MS_ERR_INVALID, "iteration counts from 1");
+    if (int rc = require_potential_inputs()) return rc;
+    const float* V = nullptr;
+    if (stack_valid_ && it <= nstack_) {
+      V = d_stack_.p + (size_t)(it - 1) * nx_ * ny_;
+    } else {
+      if (int rc = potential_slice(pot_mode_ == 1 ? POT_PROJECTED : POT_CONVENTIONAL, it, d_V_.p)) return rc;
+      V = d_V_.p;
+    }
+    return transmit_propagate(V, it == 1);
+  }
+
+  int step_fd(int it) {
+    if (!have_waves_) return fail(MS_ERR_STATE, "wavefunctions not initialised");
+    if (it < 1) return fail(MS_ERR_INVALID, "iteration counts from 1");
+    if (!fd_stable_) return fail(MS_ERR_NUMERIC, "no stable finite-difference step for these conditions");
+    if (int rc = require_potential_inputs()) return rc;
+    if (int rc = ensure_real()) return rc;
+    const Grid2 g{nx_, ny_};
+    const float nf = 1.0f / std::sqrt((float)(nx_ * ny_));
+    // V at the plane, band-limited (U.cu:2053-2063)
+    if (int rc = potential_slice(POT_FD, it, d_f_.p)) return rc;
+    MS_TRY(pw_real_to_complex(d_f_.p, d_t1_.p, g, stream_, &launches));
+    MS_TRY_FFT(cufftExecC2C(plan_, d_t1_.p, d_t2_.p, CUFFT_FORWARD));
+    MS_TRY(pw_bandlimit(d_t2_.p, d_kx_.p, d_ky_.p, kmax_, nf * nf, g, stream_, &launches));
+    MS_TRY_FFT(cufftExecC2C(plan_, d_t2_.p, d_t1_.p, CUFFT_INVERSE));  // t1 = band-limited V
+    // spectral Laplacian of psi (U.cu:2066-2069)
+    MS_TRY_FFT(cufftExecC2C(plan_, d_psi_.p, d_t2_.p, CUFFT_FORWARD));
+    MS_TRY(pw_laplacian(d_t2_.p, d_kx_.p, d_ky_.p, nf * nf, g, stream_, &launches));
+    MS_TRY_FFT(cufftExecC2C(plan_, d_t2_.p, d_grad_.p, CUFFT_INVERSE));  // grad
+    // three-level update (U.cu:2073) into t2
+    MS_TRY(pw_fd_update(d_grad_.p, d_psim_.p, d_t2_.p, d_psi_.p, d_t1_.p, sigma2_, wavel_, dzFD_, g, stream_,
+                        &launches));
+    // band-limit psi+ (U.cu:2075-2078)
+    MS_TRY_FFT(cufftExecC2C(plan_, d_t2_.p, d_t1_.p, CUFFT_FORWARD));
+    MS_TRY(pw_bandlimit(d_t1_.p, d_kx_.p, d_ky_.p, kmax_, nf * nf, g, stream_, &launches));
+    MS_TRY_FFT(cufftExecC2C(plan_, d_t1_.p, d_t2_.p, CUFFT_INVERSE));
+    // rotate psi- <- psi <- psi+ (U.cu:2081-2082) by swapping buffers
+    std::swap(d_psim_.p, d_psi_.p);  // psim = old psi
+    std::swap(d_psi_.p, d_t2_.p);    // psi = psi+
+    invalidate_graph();
+    return MS_OK;
+  }
+
+  // ---- queries ----
+  int get_slices(bool conventional, int* out) {
+    if (!have_atoms_) return fail(MS_ERR_STATE, "no atoms");
+    if (conventional) {
+      *out = (int)std::ceil((box_.MaxZ - box_.MinZ) / convdz_);  // ManagedMultislice.cpp:108
+    } else {
+      if (!have_calc_) return fail(MS_ERR_STATE, "calculation variables not set");
+      if (!fd_stable_) return fail(MS_ERR_NUMERIC, "no stable finite-difference step for these conditions");
+      *out = nFD_;
+    }
+    return MS_OK;
+  }
+
+  // ---- read-out ----
+  int get_exit_wave(bool stem_view) {
+    if (!have_waves_) return fail(MS_ERR_STATE, "wavefunctions not initialised");
+    if (int rc = ensure_real()) return rc;
+    const size_t N = (size_t)nx_ * ny_;
+    ew_.resize(N);
+    if (stem_view) {
+      // GetSTEMExitWave U.cu:2180-2229: centred FFT(psi)
+      const Grid2 g{nx_, ny_};
+      MS_TRY_FFT(cufftExecC2C(plan_, d_psi_.p, d_t1_.p, CUFFT_FORWARD));
+      MS_TRY(pw_centre(d_t1_.p, d_t2_.p, g, stream_, &launches));
+      MS_TRY(cudaMemcpyAsync(ew_.data(), d_t2_.p, N * sizeof(float2), cudaMemcpyDeviceToHost, stream_));
+    } else {
+      MS_TRY(cudaMemcpyAsync(ew_.data(), d_psi_.p, N * sizeof(float2), cudaMemcpyDeviceToHost, stream_));
+    }
+    MS_TRY(cudaStreamSynchronize(stream_));
+    float mn = INFINITY, mx = -INFINITY;
+    for (const float2& v : ew_) {
+      const float a = std::sqrt(v.x * v.x + v.y * v.y);
+      mn = std::min(mn, a);
+      mx = std::max(mx, a);
+    }
+    ew_min_ = mn;
+    ew_max_ = mx;
+    have_ew_ = true;
+    return MS_OK;
+  }
+
+  int free_exit_wave() {
+    ew_.clear();
+    ew_.shrink_to_fit();
+    have_ew_ = false;
+    return MS_OK;
+  }
+
+  int ew_value(int x, int y, int which, float* out) {
+    if (!have_ew_) return fail(MS_ERR_STATE, "exit wave not fetched (ms_get_exit_wave)");
+    if (x < 0 || y < 0 || x >= nx_ || y >= ny_) return fail(MS_ERR_INVALID, "pixel index out of range");
+    const float2 v = ew_[(size_t)y * nx_ + x];
+    *out = which == 0 ? std::sqrt(v.x * v.x + v.y * v.y) : which == 1 ? v.x : v.y;
+    return MS_OK;
+  }
+
+  int copy_exit_wave(float* dst) {
+    if (!have_waves_) return fail(MS_ERR_STATE, "wavefunctions not initialised");
+    if (!dst) return fail(MS_ERR_INVALID, "null destination");
+    if (int rc = ensure_real()) return rc;
+    MS_TRY(cudaMemcpyAsync(dst, d_psi_.p, sizeof(float2) * nx_ * ny_, cudaMemcpyDeviceToHost, stream_));
+    MS_TRY(cudaStreamSynchronize(stream_));
+    return MS_OK;
+  }
+
+  int alloc_tds() {
+    if (!have_freq_) return fail(MS_ERR_STATE, "frequencies not precalculated");
+    MS_TRY(d_tds_.resize((size_t)nx_ * ny_));
+    MS_TRY(cudaMemsetAsync(d_tds_.p, 0, sizeof(float) * nx_ * ny_, stream_));
+    have_tds_ = true;
+    return MS_OK;
+  }
+
+  // AddTDSWaves U.cu:2734-2766: tds += |centre(FFT(psi))|, unnormalised FFT.
+  int add_tds() {
+    if (!have_waves_) return fail(MS_ERR_STATE, "wavefunctions not initialised");
+    if (!have_tds_) return fail(MS_ERR_STATE, "TDS buffer not allocated (ms_alloc_tds)");
+    const Grid2 g{nx_, ny_};
+    if (use_fused() && domain_ == 1) {
+      PassBArgs b = passb_args(d_psi_.p, d_psi_.p);
+      b.acc = d_tds_.p;
+      b.scale = (float)nx_;  // FFT_rows(psi) = nx * X for the row-frequency state X
+      MS_TRY(launch_pass_b(b, B_CBED, 1, stream_));
+      ++launches;
+    } else if (use_fused()) {
+      PassAArgs a = passa_args(d_psi_.p, d_t1_.p);
+      MS_TRY(launch_pass_a(a, A_FWD, 1, stream_));
+      PassBArgs b = passb_args(d_t1_.p, d_t1_.p);
+      b.acc = d_tds_.p;
+      b.scale = 1.0f;
+      MS_TRY(launch_pass_b(b, B_CBED, 1, stream_));
+      launches += 2;
+    } else {
+      MS_TRY_FFT(cufftExecC2C(plan_, d_psi_.p, d_t1_.p, CUFFT_FORWARD));
+      MS_TRY(pw_centre_abs_acc(d_t1_.p, d_tds_.p, 1.0f, g, stream_, &launches));
+    }
+    tds_host_valid_ = false;
+    return MS_OK;
+  }
+
+  int tds_host() {
+    if (!have_tds_) return fail(MS_ERR_STATE, "TDS buffer not allocated (ms_alloc_tds)");
+    if (tds_host_valid_) return MS_OK;
+    htds_.resize((size_t)nx_ * ny_);
+    MS_TRY(cudaMemcpyAsync(htds_.data(), d_tds_.p, sizeof(float) * htds_.size(), cudaMemcpyDeviceToHost, stream_));
+    MS_TRY(cudaStreamSynchronize(stream_));
+    tds_host_valid_ = true;
+    return MS_OK;
+  }
+
+  int tds_query(int which, int x, int y, float* out) {
+    if (int rc = tds_host()) return rc;
+    if (which == 0) {
+      // GetTDSMin U.cu:2768-2777
+      float m = FLT_MAX_;
+      for (float v : htds_) m = std::min(m, v);
+      *out = m;
+    } else if (which == 1) {
+      // GetTDSMax U.cu:2778-2787 (starts from FLT_MIN as the reference)
+      float m = 1.17549435e-38f;
+      for (float v : htds_) m = std::max(m, v);
+      *out = m;
+    } else {
+      if (x < 0 || y < 0 || x >= nx_ || y >= ny_) return fail(MS_ERR_INVALID, "pixel index out of range");
+      *out = htds_[(size_t)y * nx_ + x];
+    }
+    return MS_OK;
+  }
+
+  int copy_tds(float* dst) {
+    if (!dst) return fail(MS_ERR_INVALID, "null destination");
+    if (int rc = tds_host()) return rc;
+    std::memcpy(dst, htds_.data(), sizeof(float) * htds_.size());
+    return MS_OK;
+  }
+
+  int alloc_host_image() {
+    if (!have_freq_) return fail(MS_ERR_STATE, "frequencies not precalculated");
+    image_.assign((size_t)nx_ * ny_, 0.0f);
+    have_image_buf_ = true;
+    return MS_OK;
+  }
+
+  // SimulateImage U.cu:2311-2343 (deterministic part).
+  int simulate_image() {
+    if (!have_waves_) return fail(MS_ERR_STATE, "wavefunctions not initialised");
+    if (!have_image_buf_) alloc_host_image();
+    const Grid2 g{nx_, ny_};
+    const size_t N = (size_t)nx_ * ny_;
+    const float wavel = wavel_, objap = aperture_;
+    const float objap2 = (((objap * 0.001f) / wavel) * ((objap * 0.001f) / wavel));
+    const double beta = (double)(beta_ / 1000);
+    if (use_fused()) {
+      PassBArgs b;
+      float2* src = d_psi_.p;
+      float scale = 1.0f / (float)N;
+      if (domain_ == 0) {
+        PassAArgs a = passa_args(d_psi_.p, d_t1_.p);
+        MS_TRY(launch_pass_a(a, A_FWD, 1, stream_));
+        ++launches;
+        src = d_t1_.p;
+      } else {
+        scale = (float)nx_ / (float)N;  // FFT_rows(psi) = nx * X
+      }
+      b = passb_args(src, d_t2_.p);
+      b.ctf = CtfParams{(double)wavel, (double)Cs_, (double)df_, (double)A2_, (double)phi2_, 0.0, 0.0, beta,
+                        (double)delta_, objap2};
+      b.scale = scale;
+      MS_TRY(launch_pass_b(b, B_CTF, 1, stream_));
+      PassAArgs a = passa_args(d_t2_.p, nullptr);
+      a.out_f = d_f_.p;
+      a.scale = 1.0f;
+      MS_TRY(launch_pass_a(a, A_INV | A_INTENSITY, 1, stream_));
+      launches += 2;
+    } else {
+      if (int rc = ensure_real()) return rc;
+      MS_TRY_FFT(cufftExecC2C(plan_, d_psi_.p, d_t1_.p, CUFFT_FORWARD));
+      MS_TRY(pw_ctf(d_t1_.p, d_kx_.p, d_ky_.p, wavel, Cs_, df_, A2_, phi2_, beta, delta_, objap2, 1.0f / (float)N, g,
+                    stream_, &launches));
+      MS_TRY_FFT(cufftExecC2C(plan_, d_t1_.p, d_t2_.p, CUFFT_INVERSE));
+      MS_TRY(pw_abs2(d_t2_.p, d_f_.p, 1.0f, g, stream_, &launches));
+    }
+    MS_TRY(cudaMemcpyAsync(image_.data(), d_f_.p, sizeof(float) * N, cudaMemcpyDeviceToHost, stream_));
+    MS_TRY(cudaStreamSynchronize(stream_));
+    float mn = INFINITY, mx = -INFINITY;
+    for (float v : image_) {
+      mn = std::min(mn, v);
+      mx = std::max(mx, v);
+    }
+    im_min_ = mn;
+    im_max_ = mx;
+    have_image_ = true;
+    return MS_OK;
+  }
+
+  int im_value(int x, int y, float* out) {
+    if (!have_image_) return fail(MS_ERR_STATE, "image not simulated (ms_simulate_image)");
+    if (x < 0 || y < 0 || x >= nx_ || y >= ny_) return fail(MS_ERR_INVALID, "pixel index out of range");
+    *out = image_[(size_t)y * nx_ + x];
+    return MS_OK;
+  }
+
+  // RMS contrast over a sub-rectangle (U.cu:2453-2491 computes it over the
+  // top-left 512 x 512 with cublasSasum; the rectangle is given here).
+  int image_contrast(int t, int l, int b, int r, float* out) {
+    if (!have_image_) return fail(MS_ERR_STATE, "image not simulated (ms_simulate_image)");
+    if (t < 0 || l < 0 || b > ny_ || r > nx_ || t >= b || l >= r) return fail(MS_ERR_INVALID, "bad rectangle");
+    double s = 0, s2 = 0;
+    const double n = (double)(b - t) * (r - l);
+    for (int y = t; y < b; ++y)
+      for (int x = l; x < r; ++x) s += image_[(size_t)y * nx_ + x];
+    const double mean = s / n;
+    for (int y = t; y < b; ++y)
+      for (int x = l; x < r; ++x) {
+        const double d = image_[(size_t)y * nx_ + x] - mean;
+        s2 += d * d;
+      }
+    *out = (float)std::sqrt(s2 / n);
+    return MS_OK;
+  }
+
+  int copy_image(float* dst) {
+    if (!have_image_) return fail(MS_ERR_STATE, "image not simulated (ms_simulate_image)");
+    if (!dst) return fail(MS_ERR_INVALID, "null destination");
+    std::memcpy(dst, image_.data(), sizeof(float) * image_.size());
+    return MS_OK;
+  }
+
+  int annular(float inner, float outer, double* out) {
+    if (!have_waves_) return fail(MS_ERR_STATE, "wavefunctions not initialised");
+    if (!(inner >= 0) || !(outer > inner)) return fail(MS_ERR_INVALID, "need 0 <= inner < outer");
+    if (int rc = ensure_real()) return rc;
+    const Grid2 g{nx_, ny_};
+    MS_TRY_FFT(cufftExecC2C(plan_, d_psi_.p, d_t1_.p, CUFFT_FORWARD));
+    const float kin = (inner * 0.001f) / wavel_, kout = (outer * 0.001f) / wavel_;
+    MS_TRY(pw_annular(d_t1_.p, d_kx_.p, d_ky_.p, kin * kin, kout * kout, 1.0 / ((double)nx_ * ny_), g, d_partial_.p,
+                      d_partial_.p + 1024, stream_, &launches));
+    MS_TRY(cudaMemcpyAsync(out, d_partial_.p + 1024, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    MS_TRY(cudaStreamSynchronize(stream_));
+    return MS_OK;
+  }
+
+  // ---- whole-run entry points ----
+  int build_stack(int* nslices) {
+    if (int rc = require_potential_inputs()) return rc;
+    int S = 0;
+    if (int rc = get_slices(true, &S)) return rc;
+    if (S < 1) return fail(MS_ERR_INVALID, "structure has no slices");
+    if (!stack_valid_ || nstack_ != S) {
+      const size_t N = (size_t)nx_ * ny_;
+      MS_TRY(d_stack_.resize(N * S));
+      for (int it = 1; it <= S; ++it)
+        if (int rc = potential_slice(pot_mode_ == 1 ? POT_PROJECTED : POT_CONVENTIONAL, it, d_stack_.p + (it - 1) * N))
+          return rc;
+      MS_TRY(cudaStreamSynchronize(stream_));
+      nstack_ = S;
+      stack_valid_ = true;
+      invalidate_graph();
+    }
+    if (nslices) *nslices = S;
+    return MS_OK;
+  }
+
+  int run_conventional(int* nslices) {
+    if (!have_waves_) return fail(MS_ERR_STATE, "wavefunctions not initialised");
+    int S = 0;
+    if (int rc = build_stack(&S)) return rc;
+    if (int rc = ensure_prop_tables(convdz_)) return rc;
+    if (use_fused()) {
+      if (!graph_exec_ || graph_S_ != S) {
+        invalidate_graph();
+        MS_TRY(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        int rc = MS_OK;
+        for (int it = 1; it <= S && rc == MS_OK; ++it) rc = enqueue_fused_step(d_stack_.p + (size_t)(it - 1) * nx_ * ny_, it == 1);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(stream_, &graph);
+        if (rc != MS_OK) {
+          if (graph) cudaGraphDestroy(graph);
+          return rc;
+        }
+        if (e != cudaSuccess) return fail(MS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&graph_exec_, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+          graph_exec_ = nullptr;
+          return fail(MS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        }
+        graph_S_ = S;
+      }
+      MS_TRY(cudaGraphLaunch(graph_exec_, stream_));
+      launches += 2LL * S;
+      domain_ = 1;
+    } else {
+      for (int it = 1; it <= S; ++it)
+        if (int rc = transmit_propagate(d_stack_.p + (size_t)(it - 1) * nx_ * ny_, it == 1)) return rc;
+    }
+    MS_TRY(cudaStreamSynchronize(stream_));
+    if (nslices) *nslices = S;
+    return MS_OK;
+  }
+
+  int time_slices(int steps, int reps, float* total_ms, float* row_ms, float* col_ms) {
+    if (!have_waves_) return fail(MS_ERR_STATE, "wavefunctions not initialised");
+    if (steps < 1 || reps < 1 || steps > 100000) return fail(MS_ERR_INVALID, "need 1 <= steps <= 100000, reps >= 1");
+    int S = 0;
+    if (int rc = build_stack(&S)) return rc;
+    if (int rc = ensure_prop_tables(convdz_)) return rc;
+    const size_t N = (size_t)nx_ * ny_;
+    MS_TRY(cudaStreamSynchronize(stream_));
+    // whole steps, back to back
+    MS_TRY(cudaEventRecord(ev0_, stream_));
+    for (int r = 0; r < reps; ++r)
+      for (int k = 0; k < steps; ++k)
+        if (int rc = transmit_propagate(d_stack_.p + (size_t)(k % S) * N, k == 0)) return rc;
+    MS_TRY(cudaEventRecord(ev1_, stream_));
+    MS_TRY(cudaEventSynchronize(ev1_));
+    MS_TRY(cudaEventElapsedTime(total_ms, ev0_, ev1_));
+    *row_ms = *col_ms = 0.0f;
+    if (use_fused()) {
+      // the same sequence with an event between every pass: per-launch averages
+      std::vector<cudaEvent_t> ev(2 * steps + 1, nullptr);
+      int rc = MS_OK;
+      for (auto& e : ev)
+        if (cudaEventCreate(&e) != cudaSuccess) rc = fail(MS_ERR_CUDA, "cudaEventCreate failed");
+      if (rc == MS_OK) {
+        cudaEventRecord(ev[0], stream_);
+        for (int k = 0; k < steps && rc == MS_OK; ++k) {
+          PassAArgs a = passa_args(k == 0 ? d_psi0_.p : d_psi_.p, d_psi_.p);
+          a.V = d_stack_.p + (size_t)(k % S) * N;
+          cudaError_t e1 = launch_pass_a(a, k == 0 ? (A_MULT_T | A_FWD) : (A_INV | A_MULT_T | A_FWD), 1, stream_);
+          cudaEventRecord(ev[2 * k + 1], stream_);
+          cudaError_t e2 = launch_pass_b(passb_args(d_psi_.p, d_psi_.p), B_PROPAGATE, 1, stream_);
+          cudaEventRecord(ev[2 * k + 2], stream_);
+          if (e1 != cudaSuccess || e2 != cudaSuccess) rc = cuda_fail(e1 != cudaSuccess ? e1 : e2, "timed pass launch");
+        }
+        launches += 2LL * steps;
+        domain_ = 1;
+        if (cudaEventSynchronize(ev[2 * steps]) != cudaSuccess && rc == MS_OK) rc = fail(MS_ERR_CUDA, "event sync");
+        double ta = 0, tb = 0;
+        for (int k = 0; k < steps && rc == MS_OK; ++k) {
+          float m1 = 0, m2 = 0;
+          cudaEventElapsedTime(&m1, ev[2 * k], ev[2 * k + 1]);
+          cudaEventElapsedTime(&m2, ev[2 * k + 1], ev[2 * k + 2]);
+          ta += m1;
+          tb += m2;
+        }
+        *row_ms = (float)(ta / steps);
+        *col_ms = (float)(tb / steps);
+      }
+      for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
+      if (rc != MS_OK) return rc;
+    }
+    return MS_OK;
+  }
+
+  int fft2_host(const float* in, float* out, int nx, int ny, int sign) {
+    if (!fused_supported(nx, ny)) return fail(MS_ERR_UNSUPPORTED, "grid not supported by the fused FFT passes");
+    const size_t N = (size_t)nx * ny;
+    DevBuf<float2> buf, tw1, tw2;
+    MS_TRY(buf.resize(N));
+    MS_TRY(tw1.resize(nx));
+    MS_TRY(tw2.resize(ny));
+    std::vector<float2> tw(std::max(nx, ny));
+    make_twiddles(nx, tw.data());
+    MS_TRY(cudaMemcpy(tw1.p, tw.data(), sizeof(float2) * nx, cudaMemcpyHostToDevice));
+    make_twiddles(ny, tw.data());
+    MS_TRY(cudaMemcpy(tw2.p, tw.data(), sizeof(float2) * ny, cudaMemcpyHostToDevice));
+    MS_TRY(cudaMemcpy(buf.p, in, sizeof(float2) * N, cudaMemcpyHostToDevice));
+    PassAArgs a{};
+    a.in = buf.p; a.out = buf.p; a.tw = tw1.p; a.nx = nx; a.ny = ny; a.scale = 1.0f;
+    PassBArgs b{};
+    b.in = buf.p; b.out = buf.p; b.tw = tw2.p; b.nx = nx; b.ny = ny; b.scale = 1.0f;
+    MS_TRY(launch_pass_a(a, sign < 0 ? A_FWD : A_INV, 1, stream_));
+    MS_TRY(launch_pass_b(b, sign < 0 ? B_FWD_ONLY : B_INV_ONLY, 1, stream_));
+    launches += 2;
+    MS_TRY(cudaMemcpyAsync(out, buf.p, sizeof(float2) * N, cudaMemcpyDeviceToHost, stream_));
+    MS_TRY(cudaStreamSynchronize(stream_));
+    return MS_OK;
+  }
+
+  // ---- inspection ----
+  int binned_counts(int* n, int* nz) {
+    if (!have_index_) return fail(MS_ERR_STATE, "atoms not binned");
+    *n = natoms_;
+    *nz = nzb_;
+    return MS_OK;
+  }
+
+  int copy_binned(int* off, int* Z, float* x, float* y, float* z) {
+    if (!have_index_) return fail(MS_ERR_STATE, "atoms not binned");
+    std::vector<float4> at(natoms_);
+    MS_TRY(cudaMemcpy(at.data(), d_atoms_.p, sizeof(float4) * natoms_, cudaMemcpyDeviceToHost));
+    MS_TRY(cudaMemcpy(off, d_off_.p, sizeof(int) * ((size_t)nzb_ * kBins2 + 1), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < natoms_; ++i) {
+      x[i] = at[i].x;
+      y[i] = at[i].y;
+      z[i] = at[i].z;
+      int zz;
+      std::memcpy(&zz, &at[i].w, sizeof(int));
+      Z[i] = zz;
+    }
+    return MS_OK;
+  }
+
+  int copy_potential(int kind, int it, float* dst) {
+    if (int rc = require_potential_inputs()) return rc;
+    if (it < 1) return fail(MS_ERR_INVALID, "iteration counts from 1");
+    if (kind < 0 || kind > 2) return fail(MS_ERR_INVALID, "unknown potential kind");
+    if (int rc = potential_slice(kind, it, d_f_.p)) return rc;
+    MS_TRY(cudaMemcpyAsync(dst, d_f_.p, sizeof(float) * nx_ * ny_, cudaMemcpyDeviceToHost, stream_));
+    MS_TRY(cudaStreamSynchronize(stream_));
+    return MS_OK;
+  }
+
+  // ---- simple accessors ----
+  int device() const { return device_; }
+  const Box& box() const { return box_; }
+  bool have_atoms() const { return have_atoms_; }
+  float kmax() const { return kmax_; }
+  bool have_freq() const { return have_freq_; }
+  int nx() const { return nx_; }
+  int ny() const { return ny_; }
+  float ew_min() const { return ew_min_; }
+  float ew_max() const { return ew_max_; }
+  bool have_ew() const { return have_ew_; }
+  float im_min() const { return im_min_; }
+  float im_max() const { return im_max_; }
+  bool have_image() const { return have_image_; }
+
+  int fail(int code, const std::string& m) {
+    err = m;
+    return code;
+  }
+
+ private:
+  static constexpr float FLT_MAX_ = 3.40282347e+38f;
+
+  int cuda_fail(cudaError_t e, const char* what) {
+    err = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? MS_ERR_NOMEM : MS_ERR_CUDA;
+  }
+
+  bool use_fused() const { return fused_ok_ && !force_plain_; }
+
+
+  void invalidate_graph() {
+    if (graph_exec_) {
+      cudaGraphExecDestroy(graph_exec_);
+      graph_exec_ = nullptr;
+    }
+    graph_S_ = -1;
+  }
+
+  int require_potential_inputs() {
+    if (!have_index_) return fail(MS_ERR_STATE, "atoms not binned (ms_upload_binned_atoms)");
+    if (!have_fp_) return fail(MS_ERR_STATE, "parameterisation not loaded (ms_get_parameterisation)");
+    if (!have_freq_) return fail(MS_ERR_STATE, "frequencies not precalculated");
+    for (int z : hZ_)
+      if (z > nrows_fp_) return fail(MS_ERR_INVALID, "an atom's Z has no row in the parameterisation table");
+    return MS_OK;
+  }
+
+  // Common tail of the initialisers: psi- = psi0, and the second level for
+  // finite differences psi = IFFT(P(dzFD) FFT(psi0)) / N (U.cu:1984-1993).
+  int finish_init() {
+    const Grid2 g{nx_, ny_};
+    const size_t N = (size_t)nx_ * ny_;
+    MS_TRY(cudaMemcpyAsync(d_psim_.p, d_psi0_.p, sizeof(float2) * N, cudaMemcpyDeviceToDevice, stream_));
+    const float nf = 1.0f / std::sqrt((float)(nx_ * ny_));
+    MS_TRY(pw_props(d_kx_.p, d_ky_.p, dzFD_, wavel_, kmax_, d_t2_.p, g, stream_, &launches));
+    MS_TRY_FFT(cufftExecC2C(plan_, d_psi0_.p, d_t1_.p, CUFFT_FORWARD));
+    MS_TRY(pw_cmul(d_t1_.p, d_t2_.p, d_t1_.p, nf, g, stream_, &launches));
+    MS_TRY_FFT(cufftExecC2C(plan_, d_t1_.p, d_psi_.p, CUFFT_INVERSE));
+    MS_TRY(pw_scale(d_psi_.p, nf, g, stream_, &launches));
+    MS_TRY(cudaStreamSynchronize(stream_));
+    domain_ = 0;
+    have_waves_ = true;
+    prop_dz_ = -1.0f;
+    return MS_OK;
+  }
+
+  // Propagator factors for the fused column pass: P(kx,ky) = px[kx] * py[ky]
+  // with px = exp(-i pi dz lambda kx^2) / N and py = exp(-i pi dz lambda ky^2),
+  // phases in FP64 (CreatePropsKernel U.cu:399-428 uses pi = 3.14159265).
+  int ensure_prop_tables(float dz) {
+    if (dz == prop_dz_ && d_px_.p) return MS_OK;
+    std::vector<float2> px(nx_), py(ny_);
+    const double invN = 1.0 / ((double)nx_ * ny_);
+    for (int i = 0; i < nx_; ++i) {
+      const double ph = 3.14159265 * (double)dz * (double)wavel_ * (double)hkx_[i] * (double)hkx_[i];
+      px[i] = make_float2((float)(std::cos(ph) * invN), (float)(-std::sin(ph) * invN));
+    }
+    for (int j = 0; j < ny_; ++j) {
+      const double ph = 3.14159265 * (double)dz * (double)wavel_ * (double)hky_[j] * (double)hky_[j];
+      py[j] = make_float2((float)std::cos(ph), (float)(-std::sin(ph)));
+    }
+    MS_TRY(d_px_.resize(nx_));
+    MS_TRY(d_py_.resize(ny_));
+    MS_TRY(cudaMemcpy(d_px_.p, px.data(), sizeof(float2) * nx_, cudaMemcpyHostToDevice));
+    MS_TRY(cudaMemcpy(d_py_.p, py.data(), sizeof(float2) * ny_, cudaMemcpyHostToDevice));
+    prop_dz_ = dz;
+    // plain path: full propagator array, as CreatePropsKernel
+    MS_TRY(d_P_.resize((size_t)nx_ * ny_));
+    MS_TRY(pw_props(d_kx_.p, d_ky_.p, dz, wavel_, kmax_, d_P_.p, Grid2{nx_, ny_}, stream_, &launches));
+    return MS_OK;
+  }
+
+  PassAArgs passa_args(const float2* in, float2* out) {
+    PassAArgs a{};
+    a.in = in; a.out = out; a.tw = d_twx_.p; a.nx = nx_; a.ny = ny_;
+    a.sigma = sigma2_; a.scale = 1.0f;
+    return a;
+  }
+  PassBArgs passb_args(const float2* in, float2* out) {
+    PassBArgs b{};
+    b.in = in; b.out = out; b.tw = d_twy_.p; b.px = d_px_.p; b.py = d_py_.p;
+    b.kx = d_kx_.p; b.ky = d_ky_.p; b.kmax = kmax_; b.nx = nx_; b.ny = ny_; b.scale = 1.0f;
+    return b;
+  }
+
+  // Enqueue one fused conventional step on the stream (no host sync, no
+  // allocation or copy: safe inside stream capture once the propagator
+  // tables exist).
+  int enqueue_fused_step(const float* V, bool first) {
+    // iteration 1 starts from the initial wave (real space); later ones from
+    // the current wave in whichever domain it is held
+    PassAArgs a = passa_args(first ? d_psi0_.p : d_psi_.p, d_psi_.p);
+    a.V = V;
+    const int fl = (first || domain_ == 0) ? (A_MULT_T | A_FWD) : (A_INV | A_MULT_T | A_FWD);
+    MS_TRY(launch_pass_a(a, fl, 1, stream_));
+    MS_TRY(launch_pass_b(passb_args(d_psi_.p, d_psi_.p), B_PROPAGATE, 1, stream_));
+    domain_ = 1;
+    return MS_OK;
+  }
+
+  // transmission + propagation of one conventional slice with potential V.
+  int transmit_propagate(const float* V, bool first) {
+    if (int rc = ensure_prop_tables(convdz_)) return rc;
+    if (use_fused()) {
+      if (int rc = enqueue_fused_step(V, first)) return rc;
+      launches += 2;
+      return MS_OK;
+    }
+    // plain path: the reference's launch sequence (U.cu:2101-2122)
+    if (int rc = ensure_real()) return rc;
+    const Grid2 g{nx_, ny_};
+    const float nf = 1.0f / std::sqrt((float)(nx_ * ny_));
+    MS_TRY(pw_transmission(V, sigma2_, d_t2_.p, g, stream_, &launches));
+    MS_TRY(pw_cmul(d_t2_.p, first ? d_psi0_.p : d_psi_.p, d_t1_.p, 1.0f, g, stream_, &launches));
+    MS_TRY_FFT(cufftExecC2C(plan_, d_t1_.p, d_t2_.p, CUFFT_FORWARD));
+    MS_TRY(pw_cmul(d_t2_.p, d_P_.p, d_t1_.p, nf, g, stream_, &launches));
+    MS_TRY_FFT(cufftExecC2C(plan_, d_t1_.p, d_psi_.p, CUFFT_INVERSE));
+    MS_TRY(pw_scale(d_psi_.p, nf, g, stream_, &launches));
+    domain_ = 0;
+    return MS_OK;
+  }
+
+  int ensure_real() {
+    if (domain_ == 0) return MS_OK;
+    PassAArgs a = passa_args(d_psi_.p, d_psi_.p);
+    MS_TRY(launch_pass_a(a, A_INV, 1, stream_));
+    ++launches;
+    domain_ = 0;
+    return MS_OK;
+  }
+
+  // Potential of one slice into out (ny x nx floats).
+  int potential_slice(int kind, int it, float* out) {
+    PotArgs a{};
+    a.atoms = d_atoms_.p;
+    a.off = d_off_.p;
+    a.coef = d_coef_.p;
+    a.V = out;
+    a.nx = nx_;
+    a.ny = ny_;
+    a.nz = nzb_;
+    a.ps = ps_;
+    a.bw_x = (box_.MaxX - box_.MinX) / kBins;
+    a.bw_y = (box_.MaxY - box_.MinY) / kBins;
+    const float top = box_.MaxZ - box_.MinZ;
+    if (kind == POT_CONVENTIONAL) {
+      // binnedAtomPKernel3 U.cu:582-653 launched at U.cu:2101 with z = top - convdz*it
+      const float z = box_.MaxZ - box_.MinZ - convdz_ * it;
+      const int K = (int)std::floor((box_.MaxZ - box_.MinZ - z) / (float)1);
+      a.kt = std::max(K - lbz_, 0);
+      a.kb = std::min(K + lbz_, nzb_ - 1);
+      a.xoff = xoff_;
+      a.yoff = yoff_;
+      a.nsub = 20;
+      for (int m = 1; m <= 20; ++m) a.zsub[m - 1] = z - m * convdz_ / 20.0f;
+      a.wsub = convdz_ / 20.0f;
+    } else if (kind == POT_FD) {
+      // binnedAtomPKernelFD U.cu:883-946 at z = top - dzFD*it, no offsets
+      const float z = box_.MaxZ - box_.MinZ - dzFD_ * it;
+      const int K = (int)std::floor((box_.MaxZ - box_.MinZ - z) / (float)1);
+      a.kt = std::max(K - lbz_, 0);
+      a.kb = std::min(K + lbz_, nzb_ - 1);
+      a.xoff = 0.0f;
+      a.yoff = 0.0f;
+      a.nsub = 1;
+      a.zsub[0] = z;
+      a.wsub = 1.0f;
+    } else {
+      // projected slab it: depth in [(it-1) dz, it dz)
+      a.xoff = xoff_;
+      a.yoff = yoff_;
+      a.top = top;
+      a.slab_dz = convdz_;
+      a.slab = it - 1;
+      a.kt = std::max((int)std::floor((it - 1) * convdz_) - 1, 0);
+      a.kb = std::min((int)std::floor(it * convdz_) + 1, nzb_ - 1);
+    }
+    MS_TRY(launch_potential(a, kind, stream_));
+    ++launches;
+    return MS_OK;
+  }
+
+  static void tds_displace(const float* x, const float* y, const float* z, int n, uint64_t seed, uint32_t pass,
+                           float sigma, float* xo, float* yo, float* zo) {
+    const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    const double twopi = 6.283185307179586;
+    for (int a = 0; a < n; ++a) {
+      uint32_t ctr[4] = {(uint32_t)a, pass, 0x5EEDu, 0u}, r[4];
+      philox4x32_10(ctr, key, r);
+      double u[4];
+      for (int j = 0; j < 4; ++j) u[j] = ((double)r[j] + 0.5) * 2.3283064365386963e-10;
+      const double m0 = std::sqrt(-2.0 * std::log(u[0])), m1 = std::sqrt(-2.0 * std::log(u[2]));
+      xo[a] = (float)((double)x[a] + (double)sigma * m0 * std::cos(twopi * u[1]));
+      yo[a] = (float)((double)y[a] + (double)sigma * m0 * std::sin(twopi * u[1]));
+      zo[a] = (float)((double)z[a] + (double)sigma * m1 * std::cos(twopi * u[3]));
+    }
+  }
+
+  // state
+  int device_;
+  cudaStream_t stream_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  bool force_plain_ = false, full_table_ = false;
+  int pot_mode_ = 0;
+  // structure
+  std::vector<int> hZ_;
+  std::vector<float> hx_, hy_, hz_;
+  Box box_{};
+  bool have_atoms_ = false, have_index_ = false;
+  int natoms_ = 0, nzb_ = 0;
+  DevBuf<int> d_Zin_, d_off_, d_key_, d_idx_, d_cursor_, d_blocksum_;
+  DevBuf<float> d_xin_, d_yin_, d_zin_;
+  DevBuf<float4> d_atoms_;
+  // table
+  DevBuf<float> d_coef_;
+  int nrows_fp_ = 0;
+  bool have_fp_ = false;
+  // microscope
+  float kV_ = 0, df_ = 0, A2_ = 0, phi2_ = 0, Cs_ = 0, beta_ = 0, delta_ = 0, aperture_ = 0;
+  bool have_micro_ = false;
+  // calculation
+  int nx_ = 0, ny_ = 0, nFD_ = 0, lbz_ = 3;
+  float ps_ = 0, xoff_ = 0, yoff_ = 0, wavel_ = 0, sigma2_ = 0, dzFD_ = 0, kmax_ = 0, convdz_ = 1.0f;
+  bool stem_ = false, have_calc_ = false, have_freq_ = false, fd_stable_ = false, fused_ok_ = false;
+  std::vector<float> hkx_, hky_;
+  DevBuf<float> d_kx_, d_ky_;
+  DevBuf<float2> d_twx_, d_twy_, d_px_, d_py_, d_P_;
+  float prop_dz_ = -1.0f;
+  cufftHandle plan_ = 0;
+  bool have_plan_ = false;
+  // waves
+  DevBuf<float2> d_psi0_, d_psi_, d_psim_, d_t1_, d_t2_, d_grad_;
+  DevBuf<float> d_V_, d_f_, d_tds_, d_stack_;
+  DevBuf<double> d_partial_;
+  int domain_ = 0;  // 0 real space, 1 row-frequency state of the fused passes
+  bool have_waves_ = false, stack_valid_ = false, have_tds_ = false, tds_host_valid_ = false;
+  int nstack_ = 0;
+  cudaGraphExec_t graph_exec_ = nullptr;
+  int graph_S_ = -1;
+  // host read-out
+  std::vector<float2> ew_;
+  float ew_min_ = 0, ew_max_ = 0;
+  bool have_ew_ = false;
+  std::vector<float> image_, htds_;
+  float im_min_ = 0, im_max_ = 0;
+  bool have_image_ = false, have_image_buf_ = false;
+};
+
+}  // namespace ms
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+struct ms_sim {
+  ms::Engine* e;
+};
+
+namespace {
+thread_local std::string g_create_error;
+
+template <class F>
+ms_status guarded(ms_sim* s, F&& f) {
+  if (!s || !s->e) return MS_ERR_INVALID;
+  try {
+    if (cudaSetDevice(s->e->device()) != cudaSuccess) return s->e->fail(MS_ERR_CUDA, "cudaSetDevice failed");
+    return f(*s->e);
+  } catch (const std::bad_alloc&) {
+    return s->e->fail(MS_ERR_NOMEM, "host allocation failed");
+  } catch (const std::exception& ex) {
+    return s->e->fail(MS_ERR_INVALID, ex.what());
+  }
+}
+
+ms_status out_check(ms_sim* s, const void* p) {
+  if (!p) return s && s->e ? s->e->fail(MS_ERR_INVALID, "null output pointer") : MS_ERR_INVALID;
+  return MS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+const char* ms_version(void) { return "cudamultislice_b200 0.1 (sm_100a)"; }
+
+ms_status ms_create(int device, ms_sim** out) {
+  if (!out) return MS_ERR_INVALID;
+  *out = nullptr;
+  ms_sim* s = nullptr;
+  try {
+    s = new ms_sim{new ms::Engine(device)};
+  } catch (const std::bad_alloc&) {
+    g_create_error = "host allocation failed";
+    return MS_ERR_NOMEM;
+  }
+  const int rc = s->e->init();
+  if (rc != MS_OK) {
+    g_create_error = s->e->err;
+    delete s->e;
+    delete s;
+    return rc;
+  }
+  *out = s;
+  return MS_OK;
+}
+
+ms_status ms_destroy(ms_sim* s) {
+  if (!s) return MS_ERR_INVALID;
+  delete s->e;
+  delete s;
+  return MS_OK;
+}
+
+const char* ms_last_error(const ms_sim* s) {
+  if (!s || !s->e) return g_create_error.c_str();
+  return s->e->err.c_str();
+}
+
+ms_status ms_set_option(ms_sim* s, int option, int value) {
+  return guarded(s, [&](ms::Engine& e) { return e.set_option(option, value); });
+}
+ms_status ms_import_atoms(ms_sim* s, const char* path) {
+  return guarded(s, [&](ms::Engine& e) { return e.import_atoms(path); });
+}
+ms_status ms_set_atoms(ms_sim* s, const int* Z, const float* x, const float* y, const float* z, int n) {
+  return guarded(s, [&](ms::Engine& e) { return e.set_atoms(Z, x, y, z, n); });
+}
+ms_status ms_upload_binned_atoms(ms_sim* s) {
+  return guarded(s, [&](ms::Engine& e) { return e.upload_binned(false, 0, 0, 0.0f); });
+}
+ms_status ms_upload_binned_atoms_tds(ms_sim* s, uint64_t seed, uint32_t pass, float sigma) {
+  return guarded(s, [&](ms::Engine& e) { return e.upload_binned(true, seed, pass, sigma); });
+}
+ms_status ms_get_parameterisation(ms_sim* s, const char* path) {
+  return guarded(s, [&](ms::Engine& e) { return e.get_parameterisation(path); });
+}
+ms_status ms_apply_microscope_parameters(ms_sim* s, float kV, float df, float A2, float phi2, float Cs, float beta,
+                                         float delta, float aperture) {
+  return guarded(s, [&](ms::Engine& e) { return e.apply_microscope(kV, df, A2, phi2, Cs, beta, delta, aperture); });
+}
+ms_status ms_set_calculation_variables(ms_sim* s, float ps, float df, int nx, int ny, float sx, float sy, float sz,
+                                       float xoff, float yoff) {
+  (void)sx;
+  (void)sy;
+  return guarded(s, [&](ms::Engine& e) { return e.set_calc(ps, df, nx, ny, sz, xoff, yoff, false); });
+}
+ms_status ms_stem_set_calculation_variables(ms_sim* s, float ps, float df, int nx, int ny, float sx, float sy,
+                                            float sz) {
+  (void)sx;
+  (void)sy;
+  return guarded(s, [&](ms::Engine& e) { return e.set_calc(ps, df, nx, ny, sz, 0.0f, 0.0f, true); });
+}
+ms_status ms_precalculate_frequencies(ms_sim* s) {
+  return guarded(s, [&](ms::Engine& e) { return e.precalc(); });
+}
+ms_status ms_initialise_wavefunctions(ms_sim* s) {
+  return guarded(s, [&](ms::Engine& e) { return e.init_waves(-1.0f); });
+}
+ms_status ms_initialise_wavefunctions_dz(ms_sim* s, float dz) {
+  return guarded(s, [&](ms::Engine& e) {
+    if (!(dz > 0)) return e.fail(MS_ERR_INVALID, "slice thickness must be positive");
+    return e.init_waves(dz);
+  });
+}
+ms_status ms_stem_initialise_wavefunctions(ms_sim* s, int px, int py) {
+  return guarded(s, [&](ms::Engine& e) { return e.stem_init_waves(px, py); });
+}
+ms_status ms_set_fd_dz(ms_sim* s, float dz) {
+  return guarded(s, [&](ms::Engine& e) { return e.set_fd_dz(dz); });
+}
+ms_status ms_multislice_step_fd(ms_sim* s, int it) {
+  return guarded(s, [&](ms::Engine& e) { return e.step_fd(it); });
+}
+ms_status ms_multislice_step_conventional(ms_sim* s, int it) {
+  return guarded(s, [&](ms::Engine& e) { return e.step_conventional(it); });
+}
+ms_status ms_get_size_x(ms_sim* s, float* out) {
+  if (ms_status r = out_check(s, out)) return r;
+  return guarded(s, [&](ms::Engine& e) {
+    if (!e.have_atoms()) return e.fail(MS_ERR_STATE, "no atoms");
+    *out = e.box().MaxX - e.box().MinX;
+    return (int)MS_OK;
+  });
+}
+ms_status ms_get_size_y(ms_sim* s, float* out) {
+  if (ms_status r = out_check(s, out)) return r;
+  return guarded(s, [&](ms::Engine& e) {
+    if (!e.have_atoms()) return e.fail(MS_ERR_STATE, "no atoms");
+    *out = e.box().MaxY - e.box().MinY;
+    return (int)MS_OK;
+  });
+}
+ms_status ms_get_size_z(ms_sim* s, float* out) {
+  if (ms_status r = out_check(s, out)) return r;
+  return guarded(s, [&](ms::Engine& e) {
+    if (!e.have_atoms()) return e.fail(MS_ERR_STATE, "no atoms");
+    *out = e.box().MaxZ - e.box().MinZ;
+    return (int)MS_OK;
+  });
+}
+ms_status ms_get_slices(ms_sim* s, int conventional, int* out) {
+  if (ms_status r = out_check(s, out)) return r;
+  return guarded(s, [&](ms::Engine& e) { return e.get_slices(conventional != 0, out); });
+}
+ms_status ms_get_kmax(ms_sim* s, float* out) {
+  if (ms_status r = out_check(s, out)) return r;
+  return guarded(s, [&](ms::Engine& e) {
+    if (!e.have_freq()) return e.fail(MS_ERR_STATE, "frequencies not precalculated");
+    *out = e.kmax();
+    return (int)MS_OK;
+  });
+}
+ms_status ms_get_exit_wave(ms_sim* s) {
+  return guarded(s, [&](ms::Engine& e) { return e.get_exit_wave(false); });
+}
+ms_status ms_get_stem_exit_wave(ms_sim* s) {
+  return guarded(s, [&](ms::Engine& e) { return e.get_exit_wave(true); });
+}
+ms_status ms_free_exit_wave(ms_sim* s) {
+  return guarded(s, [&](ms::Engine& e) { return e.free_exit_wave(); });
+}
+ms_status ms_get_ew_value_abs(ms_sim* s, int x, int y, float* out) {
+  if (ms_status r = out_check(s, out)) return r;
+  return guarded(s, [&](ms::Engine& e) { return e.ew_value(x, y, 0, out); });
+}
+ms_status ms_get_ew_value_re(ms_sim* s, int x, int y, float* out) {
+  if (ms_status r = out_check(s, out)) return r;
+  return guarded(s, [&](ms::Engine& e) { return e.ew_value(x, y, 1, out); });
+}
+ms_status ms_get_ew_value_im(ms_sim* s, int x, int y, float* out) {
+  if (ms_status r = out_check(s, out)) return r;
+  return guarded(s, [&](ms::Engine& e) { return e.ew_value(x, y, 2, out); });
+}
+ms_status ms_get_ew_min(ms_sim* s, float* out) {
+  if (ms_status r = out_check(s, out)) return r;
+  return guarded(s, [&](ms::Engine& e) {
+    if (!e.have_ew()) return e.fail(MS_ERR_STATE, "exit wave not fetched (ms_get_exit_wave)");
+    *out = e.ew_min();
+    return (int)MS_OK;
+  });
+}
+ms_status ms_get_ew_max(ms_sim* s, float* out) {
+  if (ms_status r = out_check(s, out)) return r;
+  return guarded(s, [&](ms::Engine& e) {
+    if (!e.have_ew()) return e.fail(MS_ERR_STATE, "exit wave not fetched (ms_get_exit_wave)");
+    *out = e.ew_max();
+    return (int)MS_OK;
+  });
+}
+ms_status ms_alloc_tds(ms_sim* s) {
+  return guarded(s, [&](ms::Engine& e) { return e.alloc_tds(); });
+}
+ms_status ms_add_tds_waves(ms_sim* s) {
+  return guarded(s, [&](ms::Engine& e) { return e.add_tds(); });
+}
+ms_status ms_get_tds_min(ms_sim* s, float* out) {
+  if (ms_status r = out_check(s, out)) return r;
+  return guarded(s, [&](ms::Engine& e) { return e.tds_query(0, 0, 0, out); });
+}
+ms_status ms_get_tds_max(ms_sim* s, float* out) {
+  if (ms_status r = out_check(s, out)) return r;
+  return guarded(s, [&](ms::Engine& e) { return e.tds_query(1, 0, 0, out); });
+}
+ms_status ms_get_tds_val(ms_sim* s, int x, int y, float* out) {
+  if (ms_status r = out_check(s, out)) return r;
+  return guarded(s, [&](ms::Engine& e) { return e.tds_query(2, x, y, out); });
+}
+ms_status ms_alloc_host_image(ms_sim* s) {
+  return guarded(s, [&](ms::Engine& e) { return e.alloc_host_image(); });
+}
+ms_status ms_simulate_image(ms_sim* s, float dose) {
+  (void)dose;
+  return guarded(s, [&](ms::Engine& e) { return e.simulate_image(); });
+}
+ms_status ms_get_im_value(ms_sim* s, int x, int y, float* out) {
+  if (ms_status r = out_check(s, out)) return r;
+  return guarded(s, [&](ms::Engine& e) { return e.im_value(x, y, out); });
+}
+ms_status ms_get_im_min(ms_sim* s, float* out) {
+  if (ms_status r = out_check(s, out)) return r;
+  return guarded(s, [&](ms::Engine& e) {
+    if (!e.have_image()) return e.fail(MS_ERR_STATE, "image not simulated (ms_simulate_image)");
+    *out = e.im_min();
+    return (int)MS_OK;
+  });
+}
+ms_status ms_get_im_max(ms_sim* s, float* out) {
+  if (ms_status r = out_check(s, out)) return r;
+  return guarded(s, [&](ms::Engine& e) {
+    if (!e.have_image()) return e.fail(MS_ERR_STATE, "image not simulated (ms_simulate_image)");
+    *out = e.im_max();
+    return (int)MS_OK;
+  });
+}
+ms_status ms_get_image_contrast(ms_sim* s, int t, int l, int b, int r, float* out) {
+  if (ms_status rr = out_check(s, out)) return rr;
+  return guarded(s, [&](ms::Engine& e) { return e.image_contrast(t, l, b, r, out); });
+}
+ms_status ms_copy_exit_wave(ms_sim* s, float* dst) {
+  return guarded(s, [&](ms::Engine& e) { return e.copy_exit_wave(dst); });
+}
+ms_status ms_copy_image(ms_sim* s, float* dst) {
+  return guarded(s, [&](ms::Engine& e) { return e.copy_image(dst); });
+}
+ms_status ms_copy_tds(ms_sim* s, float* dst) {
+  return guarded(s, [&](ms::Engine& e) { return e.copy_tds(dst); });
+}
+ms_status ms_get_grid(ms_sim* s, int* nx, int* ny) {
+  if (ms_status r = out_check(s, nx)) return r;
+  if (ms_status r = out_check(s, ny)) return r;
+  return guarded(s, [&](ms::Engine& e) {
+    if (!e.have_freq()) return e.fail(MS_ERR_STATE, "frequencies not precalculated");
+    *nx = e.nx();
+    *ny = e.ny();
+    return (int)MS_OK;
+  });
+}
+ms_status ms_build_potential_stack(ms_sim* s, int* nslices) {
+  return guarded(s, [&](ms::Engine& e) { return e.build_stack(nslices); });
+}
+ms_status ms_run_conventional(ms_sim* s, int* nslices) {
+  return guarded(s, [&](ms::Engine& e) { return e.run_conventional(nslices); });
+}
+ms_status ms_annular_detector(ms_sim* s, float inner, float outer, double* out) {
+  if (ms_status r = out_check(s, out)) return r;
+  return guarded(s, [&](ms::Engine& e) { return e.annular(inner, outer, out); });
+}
+ms_status ms_get_binned_counts(ms_sim* s, int* n, int* nz) {
+  if (ms_status r = out_check(s, n)) return r;
+  if (ms_status r = out_check(s, nz)) return r;
+  return guarded(s, [&](ms::Engine& e) { return e.binned_counts(n, nz); });
+}
+ms_status ms_copy_binned(ms_sim* s, int* off, int* Z, float* x, float* y, float* z) {
+  if (!off || !Z || !x || !y || !z) return s && s->e ? s->e->fail(MS_ERR_INVALID, "null destination") : MS_ERR_INVALID;
+  return guarded(s, [&](ms::Engine& e) { return e.copy_binned(off, Z, x, y, z); });
+}
+ms_status ms_copy_potential_slice(ms_sim* s, int kind, int it, float* dst) {
+  if (ms_status r = out_check(s, dst)) return r;
+  return guarded(s, [&](ms::Engine& e) { return e.copy_potential(kind, it, dst); });
+}
+ms_status ms_fft2(ms_sim* s, const float* in, float* out, int nx, int ny, int sign) {
+  if (!in || !out) return s && s->e ? s->e->fail(MS_ERR_INVALID, "null buffer") : MS_ERR_INVALID;
+  return guarded(s, [&](ms::Engine& e) { return e.fft2_host(in, out, nx, ny, sign); });
+}
+ms_status ms_time_slices(ms_sim* s, int steps, int reps, float* total, float* row, float* col) {
+  if (!total || !row || !col) return s && s->e ? s->e->fail(MS_ERR_INVALID, "null output") : MS_ERR_INVALID;
+  return guarded(s, [&](ms::Engine& e) { return e.time_slices(steps, reps, total, row, col); });
+}
+ms_status ms_get_launch_count(ms_sim* s, long long* out) {
+  if (ms_status r = out_check(s, out)) return r;
+  return guarded(s, [&](ms::Engine& e) {
+    *out = e.launches;
+    return (int)MS_OK;
+  });
+}
+
+}  // extern "C"

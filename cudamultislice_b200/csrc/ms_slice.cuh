@@ -1,0 +1,66 @@
+// ms_slice.cuh -- launch interface of the fused slice-step passes.
+//
+// One slice step psi <- IFFT2(P * FFT2(t * psi)) / N is split into two
+// line-local passes, because IFFT2 = IFFT_rows o IFFT_cols and consecutive
+// steps meet row-to-row:
+//   pass A (rows):    [IFFT_row] -> x t = exp(i sigma V) -> FFT_row
+//   pass B (columns): FFT_col -> x P(k)/N (band-limited) -> IFFT_col
+// Between steps the wave stays in the "row-frequency" domain; a final pass A
+// with only IFFT_row returns it to real space.  Each pass reads and writes the
+// wave once (8 MB at 1024^2: L2-resident on B200) and pass A streams V.
+#pragma once
+#include <cuda_runtime.h>
+#include "ms_common.cuh"
+
+namespace ms {
+
+enum PassAFlags : int { A_INV = 1, A_MULT_T = 2, A_FWD = 4, A_INTENSITY = 8 };
+enum PassBMode : int {
+  B_FWD_ONLY = 0,    // FFT_col
+  B_INV_ONLY = 1,    // IFFT_col
+  B_PROPAGATE = 2,   // FFT_col, x Px*Py (band-limited), IFFT_col
+  B_CTF = 3,         // FFT_col, x CTF(k)/N (objective aperture), IFFT_col
+  B_CBED = 4,        // FFT_col, accumulate |.| fftshifted into a float map
+};
+
+struct PassAArgs {
+  const float2* in;   // wave read (may alias out)
+  float2* out;        // wave written
+  float* out_f;       // intensity output (A_INTENSITY), else unused
+  const float* V;     // potential slice [ny][nx] (A_MULT_T)
+  float sigma;        // interaction constant
+  float scale;        // applied to the result of the line (1 = none)
+  const float2* tw;   // twiddle table for nx
+  int nx, ny;
+  long long batch_stride_wave;  // elements between instances (blockIdx.y)
+  long long batch_stride_V;
+};
+
+struct CtfParams {
+  double wavel, Cs, df, A2, phi2, A3, phi3, beta, delta;  // beta in rad
+  float objap2;                                          // FP32 aperture decision
+};
+
+struct PassBArgs {
+  const float2* in;
+  float2* out;
+  float* acc;          // B_CBED accumulation map [ny][nx]
+  const float2* tw;    // twiddle table for ny
+  const float2* px;    // propagator factor per column (scaled 1/N)
+  const float2* py;    // propagator factor per row
+  const float* kx;     // FP32 reference frequencies (decisions)
+  const float* ky;
+  float kmax;
+  CtfParams ctf;
+  float scale;         // B_CTF: factor on the weight; B_CBED: factor on |.|
+  int nx, ny;
+  long long batch_stride_wave;
+};
+
+bool fused_supported(int nx, int ny);
+cudaError_t launch_pass_a(const PassAArgs& a, int flags, int batch, cudaStream_t s);
+cudaError_t launch_pass_b(const PassBArgs& a, int mode, int batch, cudaStream_t s);
+// forward twiddle table W_N^{r*i}, r < P, i < E, as [r][i]
+void make_twiddles(int n, float2* host_out);
+
+}  // namespace ms

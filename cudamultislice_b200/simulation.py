@@ -1,0 +1,285 @@
+"""Python mirror of the reference's simulation API over the C ABI.
+
+``ManagedMultisliceSimulation`` has the method list of the reference's .NET
+wrapper (GUI Simulation/GUI Simulation.h:17-59, ManagedMultislice.cpp), so a
+script written against the reference's call sequence runs unchanged:
+
+    sim = ManagedMultisliceSimulation()
+    sim.ImportAtoms("structure.xyz")
+    sim.UploadBinnedAtoms()
+    sim.GetParameterisation("fparams.dat")
+    sim.ApplyMicroscopeParameters(kV, df, A2, phi2, Cs, beta, delta, aperture)
+    sim.SetCalculationVariables(ps, df, nx, ny, sim.GetSizeX(), sim.GetSizeY(), sim.GetSizeZ(), xoff, yoff)
+    sim.PreCalculateFrequencies()
+    sim.InitialiseWavefunctions(dz)
+    for i in range(1, sim.GetSlices(True) + 1):
+        sim.MultisliceStepConventional(i)
+    sim.GetExitWave()
+
+Every call goes to ``libmslice_b200.so`` (hand-written sm_100a kernels); there
+is no CPU implementation behind it.  Errors raise ``MultisliceError`` with the
+library's message instead of being ignored.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import MultisliceError, lib
+
+_p = C.c_void_p
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class ManagedMultisliceSimulation:
+    """One engine handle (ms_sim) on one GPU."""
+
+    SLICE_PATH_FUSED = 0
+    SLICE_PATH_PLAIN = 1
+
+    def __init__(self, device: int = 0):
+        self._L = lib()
+        h = C.c_void_p()
+        rc = self._L.ms_create(int(device), C.byref(h))
+        if rc != 0:
+            raise MultisliceError(rc, self._L.ms_last_error(None).decode())
+        self._h = h
+        self.nx = self.ny = 0
+
+    # ---- lifecycle ----
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.ms_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _chk(self, rc: int):
+        if rc != 0:
+            raise MultisliceError(rc, self._L.ms_last_error(self._h).decode())
+
+    def _f(self, fn, *args) -> float:
+        out = C.c_float()
+        self._chk(fn(self._h, *args, C.byref(out)))
+        return out.value
+
+    # ---- options ----
+    def SetSlicePath(self, path: int):
+        self._chk(self._L.ms_set_option(self._h, 0, int(path)))
+
+    def SetElementTable(self, full: bool):
+        self._chk(self._L.ms_set_option(self._h, 1, int(bool(full))))
+
+    def SetPotentialMode(self, projected: bool):
+        self._chk(self._L.ms_set_option(self._h, 2, int(bool(projected))))
+
+    # ---- structure ----
+    def ImportAtoms(self, filename: str):
+        self._chk(self._L.ms_import_atoms(self._h, filename.encode()))
+
+    def SetAtoms(self, Z, x, y, z):
+        Z = np.ascontiguousarray(Z, np.int32)
+        x, y, z = (np.ascontiguousarray(a, np.float32) for a in (x, y, z))
+        if not (Z.size == x.size == y.size == z.size):
+            raise ValueError("Z, x, y, z must have the same length")
+        self._chk(self._L.ms_set_atoms(self._h, _ptr(Z), _ptr(x), _ptr(y), _ptr(z), Z.size))
+
+    def UploadBinnedAtoms(self):
+        self._chk(self._L.ms_upload_binned_atoms(self._h))
+
+    def UploadBinnedAtomsTDS(self, seed: int = 0x5EED2026, pas: int = 0, sigma: float = 0.075):
+        self._chk(self._L.ms_upload_binned_atoms_tds(self._h, int(seed), int(pas), float(sigma)))
+
+    def GetParameterisation(self, path: str):
+        self._chk(self._L.ms_get_parameterisation(self._h, path.encode()))
+
+    # ---- set-up ----
+    def ApplyMicroscopeParameters(self, Voltage, defocus, Mod2f, Arg2f, spherical, B, D, obj):
+        self._chk(self._L.ms_apply_microscope_parameters(
+            self._h, Voltage, defocus, Mod2f, Arg2f, spherical, B, D, obj))
+
+    def SetCalculationVariables(self, PixelScaleIn, defocus, resX, resY, SizeX, SizeY, SizeZ,
+                                blockoffsetx=0.0, blockoffsety=0.0):
+        self._chk(self._L.ms_set_calculation_variables(
+            self._h, PixelScaleIn, defocus, int(resX), int(resY), SizeX, SizeY, SizeZ, blockoffsetx, blockoffsety))
+        self.nx, self.ny = int(resX), int(resY)
+
+    def STEMSetCalculationVariables(self, PixelScaleIn, defocus, resX, resY, SizeX, SizeY, SizeZ):
+        self._chk(self._L.ms_stem_set_calculation_variables(
+            self._h, PixelScaleIn, defocus, int(resX), int(resY), SizeX, SizeY, SizeZ))
+        self.nx, self.ny = int(resX), int(resY)
+
+    def PreCalculateFrequencies(self):
+        self._chk(self._L.ms_precalculate_frequencies(self._h))
+
+    def InitialiseWavefunctions(self, dz: float | None = None):
+        if dz is None:
+            self._chk(self._L.ms_initialise_wavefunctions(self._h))
+        else:
+            self._chk(self._L.ms_initialise_wavefunctions_dz(self._h, float(dz)))
+
+    def STEMInitialiseWavefunctions(self, posx: int, posy: int):
+        self._chk(self._L.ms_stem_initialise_wavefunctions(self._h, int(posx), int(posy)))
+
+    def SetFDdz(self, dz: float):
+        self._chk(self._L.ms_set_fd_dz(self._h, float(dz)))
+
+    # ---- steps ----
+    def MultisliceStepFD(self, iteration: int):
+        self._chk(self._L.ms_multislice_step_fd(self._h, int(iteration)))
+
+    def MultisliceStepConventional(self, iteration: int):
+        self._chk(self._L.ms_multislice_step_conventional(self._h, int(iteration)))
+
+    # ---- queries ----
+    def GetSizeX(self) -> float:
+        return self._f(self._L.ms_get_size_x)
+
+    def GetSizeY(self) -> float:
+        return self._f(self._L.ms_get_size_y)
+
+    def GetSizeZ(self) -> float:
+        return self._f(self._L.ms_get_size_z)
+
+    def GetSlices(self, conventional: bool) -> int:
+        out = C.c_int()
+        self._chk(self._L.ms_get_slices(self._h, int(bool(conventional)), C.byref(out)))
+        return out.value
+
+    def GetKmax(self) -> float:
+        return self._f(self._L.ms_get_kmax)
+
+    # ---- read-out ----
+    def GetExitWave(self):
+        self._chk(self._L.ms_get_exit_wave(self._h))
+
+    def GetSTEMExitWave(self):
+        self._chk(self._L.ms_get_stem_exit_wave(self._h))
+
+    def FreeExitWave(self):
+        self._chk(self._L.ms_free_exit_wave(self._h))
+
+    def GetEWValueAbs(self, x, y) -> float:
+        return self._f(self._L.ms_get_ew_value_abs, int(x), int(y))
+
+    def GetEWValueRe(self, x, y) -> float:
+        return self._f(self._L.ms_get_ew_value_re, int(x), int(y))
+
+    def GetEWValueIm(self, x, y) -> float:
+        return self._f(self._L.ms_get_ew_value_im, int(x), int(y))
+
+    def GetEWMin(self) -> float:
+        return self._f(self._L.ms_get_ew_min)
+
+    def GetEWMax(self) -> float:
+        return self._f(self._L.ms_get_ew_max)
+
+    def AllocTDS(self):
+        self._chk(self._L.ms_alloc_tds(self._h))
+
+    def AddTDSWaves(self):
+        self._chk(self._L.ms_add_tds_waves(self._h))
+
+    def GetTDSMin(self) -> float:
+        return self._f(self._L.ms_get_tds_min)
+
+    def GetTDSMax(self) -> float:
+        return self._f(self._L.ms_get_tds_max)
+
+    def GetTDSVal(self, x, y) -> float:
+        return self._f(self._L.ms_get_tds_val, int(x), int(y))
+
+    def AllocHostImage(self):
+        self._chk(self._L.ms_alloc_host_image(self._h))
+
+    def SimulateImage(self, doseperpix: float = 0.0):
+        self._chk(self._L.ms_simulate_image(self._h, float(doseperpix)))
+
+    def GetImValue(self, x, y) -> float:
+        return self._f(self._L.ms_get_im_value, int(x), int(y))
+
+    def GetImMin(self) -> float:
+        return self._f(self._L.ms_get_im_min)
+
+    def GetImMax(self) -> float:
+        return self._f(self._L.ms_get_im_max)
+
+    def GetImageContrast(self, t, l, b, r) -> float:
+        return self._f(self._L.ms_get_image_contrast, int(t), int(l), int(b), int(r))
+
+    # ---- bulk and batched (new) ----
+    def ExitWave(self) -> np.ndarray:
+        out = np.zeros((self.ny, self.nx), np.complex64)
+        self._chk(self._L.ms_copy_exit_wave(self._h, _ptr(out)))
+        return out
+
+    def Image(self) -> np.ndarray:
+        out = np.zeros((self.ny, self.nx), np.float32)
+        self._chk(self._L.ms_copy_image(self._h, _ptr(out)))
+        return out
+
+    def TDS(self) -> np.ndarray:
+        out = np.zeros((self.ny, self.nx), np.float32)
+        self._chk(self._L.ms_copy_tds(self._h, _ptr(out)))
+        return out
+
+    def BuildPotentialStack(self) -> int:
+        out = C.c_int()
+        self._chk(self._L.ms_build_potential_stack(self._h, C.byref(out)))
+        return out.value
+
+    def RunConventional(self) -> int:
+        out = C.c_int()
+        self._chk(self._L.ms_run_conventional(self._h, C.byref(out)))
+        return out.value
+
+    def AnnularDetector(self, inner_mrad: float, outer_mrad: float) -> float:
+        out = C.c_double()
+        self._chk(self._L.ms_annular_detector(self._h, float(inner_mrad), float(outer_mrad), C.byref(out)))
+        return out.value
+
+    # ---- inspection ----
+    def Binned(self):
+        n, nz = C.c_int(), C.c_int()
+        self._chk(self._L.ms_get_binned_counts(self._h, C.byref(n), C.byref(nz)))
+        off = np.zeros(nz.value * 2500 + 1, np.int32)
+        Z = np.zeros(n.value, np.int32)
+        x, y, z = (np.zeros(n.value, np.float32) for _ in range(3))
+        self._chk(self._L.ms_copy_binned(self._h, _ptr(off), _ptr(Z), _ptr(x), _ptr(y), _ptr(z)))
+        return off, Z, x, y, z
+
+    def PotentialSlice(self, kind: int, iteration: int) -> np.ndarray:
+        out = np.zeros((self.ny, self.nx), np.float32)
+        self._chk(self._L.ms_copy_potential_slice(self._h, int(kind), int(iteration), _ptr(out)))
+        return out
+
+    def FFT2(self, a: np.ndarray, sign: int = -1) -> np.ndarray:
+        a = np.ascontiguousarray(a, np.complex64)
+        out = np.zeros_like(a)
+        ny, nx = a.shape
+        self._chk(self._L.ms_fft2(self._h, _ptr(a), _ptr(out), nx, ny, int(sign)))
+        return out
+
+    def TimeSlices(self, steps: int, reps: int = 1):
+        t, a, b = C.c_float(), C.c_float(), C.c_float()
+        self._chk(self._L.ms_time_slices(self._h, int(steps), int(reps), C.byref(t), C.byref(a), C.byref(b)))
+        return t.value, a.value, b.value
+
+    def LaunchCount(self) -> int:
+        out = C.c_longlong()
+        self._chk(self._L.ms_get_launch_count(self._h, C.byref(out)))
+        return out.value

@@ -1,0 +1,207 @@
+/*
+ * mslice.h -- C ABI of the B200 multislice engine (libmslice_b200.so).
+ *
+ * This is the drop-in boundary for the reference's simulation class
+ * UnmanagedMultisliceSimulation (GUI Simulation/unmanagedGUISimulation.cuh:62-200,
+ * implemented in GUI Simulation/UnmanagedGUISimulation.cu, "U.cu" below), which
+ * the reference exposes to .NET through ManagedMultisliceSimulation
+ * (GUI Simulation/GUI Simulation.h:17-59, GUI Simulation/ManagedMultislice.cpp).
+ * Each reference method has one entry point here, with the same argument
+ * meaning and units, in the same call order:
+ *
+ *   import/set atoms -> upload binned atoms -> get parameterisation ->
+ *   apply microscope parameters -> set calculation variables ->
+ *   precalculate frequencies -> initialise wavefunctions ->
+ *   step x S -> get exit wave -> (simulate image / add TDS waves)
+ *
+ * Conventions (differences from the reference are deliberate and listed):
+ *  - Every function returns ms_status; MS_OK is 0.  The message of the last
+ *    failure is ms_last_error().  (The reference reports no errors and calls
+ *    exit(1) on a missing fparams.dat, U.cu:1730.)
+ *  - Getters that return a float or int in the reference write through an
+ *    out-pointer instead.
+ *  - Buffers passed in are owned by the caller; the handle owns everything it
+ *    allocates.  A handle is driven by one thread at a time and runs all its
+ *    GPU work on its own non-default stream.
+ *  - Plain pointers and sizes only; no CUDA or PyTorch types cross the ABI.
+ */
+#ifndef MSLICE_H
+#define MSLICE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ms_sim ms_sim;
+typedef int ms_status;
+
+enum {
+  MS_OK = 0,
+  MS_ERR_INVALID = 1,     /* bad argument (size, index, NaN parameter) */
+  MS_ERR_STATE = 2,       /* call order violated (e.g. stepping before initialising) */
+  MS_ERR_CUDA = 3,        /* CUDA runtime / cuFFT failure */
+  MS_ERR_IO = 4,          /* file missing or unreadable */
+  MS_ERR_NOMEM = 5,       /* device or host allocation failed */
+  MS_ERR_UNSUPPORTED = 6, /* combination not provided (e.g. fused path at this size) */
+  MS_ERR_NUMERIC = 7      /* no stable finite-difference step (U.cu:1823-1830) */
+};
+
+/* Options (ms_set_option). */
+enum {
+  MS_OPT_SLICE_PATH = 0,    /* 0 = fused hand-written FFT passes (default where the
+                               grid is a power of two 64..1024), 1 = plain path:
+                               cuFFT + one kernel per operation, the reference's
+                               launch sequence (U.cu:2101-2122) */
+  MS_OPT_ELEMENT_TABLE = 1, /* 0 = reference symbol table, unknown -> Z=1 (U.cu:1188-1243);
+                               1 = full periodic table Z = 1..103 */
+  MS_OPT_POTENTIAL = 2      /* 0 = conventional 3D-integrated potential, the live
+                               reference kernel binnedAtomPKernel3 (U.cu:582-653);
+                               1 = projected potential vzatom2 per slab (U.cu:119-152,
+                               xy scan of binnedAtomPKernel2 U.cu:513-578) */
+};
+
+/* ---- lifecycle ---- */
+/* Constructor U.cu:2551-2556 (creates the cuBLAS handle there; here a stream). */
+ms_status ms_create(int device, ms_sim** out);
+/* Destructor U.cu:2558-2561. */
+ms_status ms_destroy(ms_sim* sim);
+const char* ms_last_error(const ms_sim* sim);
+const char* ms_version(void);
+ms_status ms_set_option(ms_sim* sim, int option, int value);
+
+/* ---- structure ---- */
+/* LoadAtomFile U.cu:1293-1356 (.xyz: count, comment, "symbol x y z" rows; the
+ * bounding box is padded by 2 A on every side). */
+ms_status ms_import_atoms(ms_sim* sim, const char* path);
+/* New: atoms by atomic number (the reference's symbol table lacks Ti, Ga, ...). */
+ms_status ms_set_atoms(ms_sim* sim, const int* Z, const float* x, const float* y,
+                       const float* z, int n);
+/* UploadBinnedAtoms U.cu:1358-1536: bins of 50 x 50 in xy and 1 A in z, built
+ * on the device, bit-identical to the reference's CSR. */
+ms_status ms_upload_binned_atoms(ms_sim* sim);
+/* UploadBinnedAtomsTDS U.cu:1538-1716: positions displaced by N(0, sigma^2)
+ * per axis from a seeded counter-based generator (Philox4x32-10, counter =
+ * (atom, pass)) instead of the unseeded rand() of TDSRand U.cu:29-37. */
+ms_status ms_upload_binned_atoms_tds(ms_sim* sim, uint64_t seed, uint32_t pass, float sigma);
+/* GetParameterisation U.cu:1718-1747, with the table path given explicitly
+ * (the reference reads "fparams.dat" from the working directory). */
+ms_status ms_get_parameterisation(ms_sim* sim, const char* path);
+
+/* ---- microscope and set-up ---- */
+/* ApplyMicroscopeParameters U.cu:1749-1761: kV, defocus (A), two-fold
+ * astigmatism magnitude (A) and angle (rad), Cs (A), beta (mrad), delta (A),
+ * objective aperture (mrad). */
+ms_status ms_apply_microscope_parameters(ms_sim* sim, float kV, float df, float A2, float phi2,
+                                         float Cs, float beta, float delta, float aperture);
+/* SetCalculationVariables U.cu:1763-1875: pixel size (A), defocus, grid, the
+ * structure size, and the offset (A) of pixel (0,0) from the box corner. */
+ms_status ms_set_calculation_variables(ms_sim* sim, float ps, float df, int nx, int ny,
+                                       float sx, float sy, float sz, float xoff, float yoff);
+/* STEMSetCalculationVariables U.cu:2567-2670 (no offsets; FD step <= 0.06 A). */
+ms_status ms_stem_set_calculation_variables(ms_sim* sim, float ps, float df, int nx, int ny,
+                                            float sx, float sy, float sz);
+/* PreCalculateFrequencies U.cu:1877-1964. */
+ms_status ms_precalculate_frequencies(ms_sim* sim);
+
+/* ---- wavefunction initialisation ---- */
+/* InitialiseWavefunctions() U.cu:1966-2001 (conventional dz = 1 A). */
+ms_status ms_initialise_wavefunctions(ms_sim* sim);
+/* InitialiseWavefunctions(float dz) U.cu:2003-2038. */
+ms_status ms_initialise_wavefunctions_dz(ms_sim* sim, float dz);
+/* STEMInitialiseWavefunctions U.cu:2672-2724: probe at pixel (px, py). */
+ms_status ms_stem_initialise_wavefunctions(ms_sim* sim, int px, int py);
+/* New: override the automatic stable finite-difference step (U.cu:1815-1846). */
+ms_status ms_set_fd_dz(ms_sim* sim, float dz);
+
+/* ---- slice steps (iteration counts from 1, as the reference) ---- */
+/* MultisliceStep U.cu:2040-2083 (finite differences). */
+ms_status ms_multislice_step_fd(ms_sim* sim, int iteration);
+/* MultisliceStepConv U.cu:2085-2124. */
+ms_status ms_multislice_step_conventional(ms_sim* sim, int iteration);
+
+/* ---- queries (ManagedMultislice.cpp:89-117) ---- */
+ms_status ms_get_size_x(ms_sim* sim, float* out);
+ms_status ms_get_size_y(ms_sim* sim, float* out);
+ms_status ms_get_size_z(ms_sim* sim, float* out);
+/* GetSlices(bool conventional), ManagedMultislice.cpp:105-111. */
+ms_status ms_get_slices(ms_sim* sim, int conventional, int* out);
+ms_status ms_get_kmax(ms_sim* sim, float* out);
+
+/* ---- read-out ---- */
+/* GetExitWave U.cu:2231-2284: exit wave to the handle's host buffer, with the
+ * min/max |psi| (the reference finds them with cublasIsamin/Isamax). */
+ms_status ms_get_exit_wave(ms_sim* sim);
+/* GetSTEMExitWave U.cu:2180-2229: centred |FFT(psi)| kept as the exit wave. */
+ms_status ms_get_stem_exit_wave(ms_sim* sim);
+/* FreeExitWave U.cu:2286-2289. */
+ms_status ms_free_exit_wave(ms_sim* sim);
+/* GetEWValueAbs/Re/Im U.cu:2291-2304 and GetEWMin/Max ManagedMultislice.cpp:195-206. */
+ms_status ms_get_ew_value_abs(ms_sim* sim, int x, int y, float* out);
+ms_status ms_get_ew_value_re(ms_sim* sim, int x, int y, float* out);
+ms_status ms_get_ew_value_im(ms_sim* sim, int x, int y, float* out);
+ms_status ms_get_ew_min(ms_sim* sim, float* out);
+ms_status ms_get_ew_max(ms_sim* sim, float* out);
+
+/* AllocTDS U.cu:2726-2732 / AddTDSWaves U.cu:2734-2766 / GetTDSMin/Max/Val
+ * U.cu:2768-2791: accumulated centred |FFT(psi_exit)| (kept on the device). */
+ms_status ms_alloc_tds(ms_sim* sim);
+ms_status ms_add_tds_waves(ms_sim* sim);
+ms_status ms_get_tds_min(ms_sim* sim, float* out);
+ms_status ms_get_tds_max(ms_sim* sim, float* out);
+ms_status ms_get_tds_val(ms_sim* sim, int x, int y, float* out);
+
+/* AllocHostImage U.cu:2306-2309 / SimulateImage U.cu:2311-2343: the
+ * deterministic CTF image |IFFT(CTF * FFT(psi))|^2 (imagingKernel2
+ * U.cu:1044-1080).  The detector chain after it (U.cu:2345-2494: DQE/NTF,
+ * unseeded shot and readout noise) is not provided; `dose` is accepted and
+ * unused.  GetImValue (U.cu:2497-2512) returns the deterministic intensity. */
+ms_status ms_alloc_host_image(ms_sim* sim);
+ms_status ms_simulate_image(ms_sim* sim, float dose);
+ms_status ms_get_im_value(ms_sim* sim, int x, int y, float* out);
+ms_status ms_get_im_min(ms_sim* sim, float* out);
+ms_status ms_get_im_max(ms_sim* sim, float* out);
+/* GetImageContrast (ManagedMultislice.cpp:207-210; computed at U.cu:2453-2491):
+ * RMS contrast over rows [t, b) and columns [l, r) of the image. */
+ms_status ms_get_image_contrast(ms_sim* sim, int t, int l, int b, int r, float* out);
+
+/* ---- bulk read-out (new; replaces one managed call per pixel, MW.cs:314-321) ---- */
+ms_status ms_copy_exit_wave(ms_sim* sim, float* dst /* 2*nx*ny, interleaved re/im */);
+ms_status ms_copy_image(ms_sim* sim, float* dst /* nx*ny */);
+ms_status ms_copy_tds(ms_sim* sim, float* dst /* nx*ny */);
+ms_status ms_get_grid(ms_sim* sim, int* nx, int* ny);
+
+/* ---- whole-run entry points (new) ---- */
+/* Builds the potentials of slices 1..S into a device-resident stack. */
+ms_status ms_build_potential_stack(ms_sim* sim, int* nslices);
+/* Runs conventional slices 1..S from the initial wave (replayed as one
+ * captured CUDA graph); equivalent to ms_multislice_step_conventional(i)
+ * for i = 1..S. */
+ms_status ms_run_conventional(ms_sim* sim, int* nslices);
+/* Annular detector (new; no reference counterpart, north-star STEM signal):
+ * sum over inner <= theta < outer (mrad) of |FFT(psi)|^2 / N. */
+ms_status ms_annular_detector(ms_sim* sim, float inner_mrad, float outer_mrad, double* out);
+
+/* ---- inspection (parity tests and measurement) ---- */
+ms_status ms_get_binned_counts(ms_sim* sim, int* n_atoms, int* n_zbins);
+ms_status ms_copy_binned(ms_sim* sim, int* offsets, int* Z, float* x, float* y, float* z);
+/* kind: 0 conventional slice, 1 finite-difference plane, 2 projected slab (current
+ * conventional dz) */
+ms_status ms_copy_potential_slice(ms_sim* sim, int kind, int iteration, float* dst /* nx*ny */);
+/* 2D FFT of a host array through the engine's own FFT passes (sign -1
+ * forward, +1 inverse, unnormalised); grid must be fused-supported. */
+ms_status ms_fft2(ms_sim* sim, const float* in, float* out, int nx, int ny, int sign);
+/* Times `steps` fused (or plain) conventional steps over the resident
+ * potential stack with CUDA events on the handle's stream, repeated `reps`
+ * times; writes the total milliseconds and the per-launch average of the two
+ * fused passes (row pass, column pass; timed in separate loops). */
+ms_status ms_time_slices(ms_sim* sim, int steps, int reps, float* ms_total, float* ms_row_pass,
+                         float* ms_col_pass);
+/* Number of this library's kernels launched by the handle so far. */
+ms_status ms_get_launch_count(ms_sim* sim, long long* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MSLICE_H */

@@ -1,0 +1,262 @@
+"""Parity of the CUDA engine (through the C ABI) against the FP64 oracle.
+
+Bit-exact for the integer work (atom index); for the floating-point path the
+relative L2 error <= 1e-5 against FP64 for potentials,
+exit waves, images and detector signals."""
+import numpy as np
+import pytest
+
+from tests.conftest import FPARAMS
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5  # relative L2 error against the FP64 oracle
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.complex128) - b) / np.linalg.norm(b))
+
+
+@pytest.fixture(scope="module")
+def engine_cls():
+    from cudamultislice_b200 import ManagedMultisliceSimulation, build
+
+    build.build(verbose=False)
+    return ManagedMultisliceSimulation
+
+
+def make_pair(engine_cls, oracle_mod, atoms, n, ps, *, kV=200.0, df=-500.0, Cs=1e7, ap=20.0, beta=0.1,
+              delta=30.0, dz=1.9525, xoff=2.0, yoff=2.0, path=0, stem=False, A2=0.0, phi2=0.0):
+    Z, x, y, z = atoms
+    eng = engine_cls()
+    eng.SetSlicePath(path)
+    orc = oracle_mod.OracleSimulation()
+    for s in (eng, orc):
+        s.SetAtoms(Z, x, y, z)
+        s.UploadBinnedAtoms()
+        s.GetParameterisation(FPARAMS)
+        s.ApplyMicroscopeParameters(kV, df, A2, phi2, Cs, beta, delta, ap)
+        if stem:
+            s.STEMSetCalculationVariables(ps, df, n, n, s.GetSizeX(), s.GetSizeY(), s.GetSizeZ())
+        else:
+            s.SetCalculationVariables(ps, df, n, n, s.GetSizeX(), s.GetSizeY(), s.GetSizeZ(), xoff, yoff)
+        s.PreCalculateFrequencies()
+        if not stem:
+            s.InitialiseWavefunctions(dz)
+    return eng, orc
+
+
+def sto(nc=2, nz=4):
+    from cudamultislice_b200 import structures as S
+
+    return S.srtio3(nc, nc, nz)
+
+
+# ---------------------------------------------------------------- atom index
+@pytest.mark.parametrize("kind", ["random", "srtio3", "tds"])
+def test_atom_index_bit_exact(engine_cls, oracle_mod, kind):
+    from cudamultislice_b200 import structures as S
+
+    atoms = S.random_atoms(5000, size=(23.0, 17.0, 31.0), seed=11) if kind == "random" else S.srtio3(4, 4, 20)
+    eng = engine_cls()
+    orc = oracle_mod.OracleSimulation()
+    for s in (eng, orc):
+        s.SetAtoms(*atoms)
+    if kind == "tds":
+        eng.UploadBinnedAtomsTDS(0x5EED2026, 3, 0.076)
+        orc.UploadBinnedAtomsTDS(0x5EED2026, 3, 0.076)
+    else:
+        eng.UploadBinnedAtoms()
+        orc.UploadBinnedAtoms()
+    a, b = eng.Binned(), orc.Binned()
+    for u, v in zip(a, b):
+        assert u.dtype == v.dtype and np.array_equal(u, v)
+
+
+def test_atom_index_large(engine_cls, oracle_mod):
+    # many atoms per bin and a deep stack: ordering inside bins must be stable
+    from cudamultislice_b200 import structures as S
+
+    atoms = S.random_atoms(200000, size=(8.0, 8.0, 40.0), seed=12)
+    eng, orc = engine_cls(), oracle_mod.OracleSimulation()
+    for s in (eng, orc):
+        s.SetAtoms(*atoms)
+        s.UploadBinnedAtoms()
+    for u, v in zip(eng.Binned(), orc.Binned()):
+        assert np.array_equal(u, v)
+
+
+# ---------------------------------------------------------------- FFT
+@pytest.mark.parametrize("shape", [(64, 64), (128, 256), (512, 512), (1024, 1024), (256, 64), (1024, 512)])
+def test_fused_fft_against_numpy(engine_cls, shape):
+    rng = np.random.default_rng(7)
+    a = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+    eng = engine_cls()
+    for sign, ref in ((-1, np.fft.fft2(a.astype(np.complex128))),
+                      (+1, np.fft.ifft2(a.astype(np.complex128)) * a.size)):
+        out = eng.FFT2(a, sign)
+        assert rel_l2(out, ref) < 1e-6, (shape, sign, rel_l2(out, ref))
+
+
+# ---------------------------------------------------------------- potentials
+@pytest.mark.parametrize("kind", [0, 1, 2])
+def test_potential_slices(engine_cls, oracle_mod, kind):
+    eng, orc = make_pair(engine_cls, oracle_mod, sto(2, 4), 128, 0.1)
+    for it in (1, 3, 5):
+        v = eng.PotentialSlice(kind, it)
+        ref = {0: orc.PotentialConventional, 1: orc.PotentialFD,
+               2: lambda i: orc.PotentialProjected(i, 1.9525)}[kind](it)
+        assert np.abs(ref).max() > 0
+        e = np.linalg.norm(v - ref) / np.linalg.norm(ref)
+        assert e < TOL, (kind, it, e)
+        assert np.abs(v - ref).max() / np.abs(ref).max() < 5 * TOL
+
+
+# ---------------------------------------------------------------- TEM exit wave
+@pytest.mark.parametrize("path", [0, 1])
+def test_exit_wave_conventional(engine_cls, oracle_mod, path):
+    eng, orc = make_pair(engine_cls, oracle_mod, sto(2, 5), 128, 0.1, path=path)
+    S = eng.GetSlices(True)
+    assert S == orc.GetSlices(True)
+    for i in range(1, S + 1):
+        eng.MultisliceStepConventional(i)
+        orc.MultisliceStepConventional(i)
+    e = rel_l2(eng.ExitWave(), orc.Wave())
+    assert e < TOL, e
+
+
+def test_exit_wave_c1_srtio3_256(engine_cls, oracle_mod):
+    # SrTiO3 4x4x20 cells, 256^2 over 15.62 A, 1.9525 A slices, 200 kV
+    eng, orc = make_pair(engine_cls, oracle_mod, sto(4, 20), 256, 15.62 / 256)
+    nslices = eng.RunConventional()
+    psi = orc.run_conventional()
+    assert nslices == orc.GetSlices(True)
+    e = rel_l2(eng.ExitWave(), psi)
+    assert e < TOL, e
+    # CTF image (Cs = 1 mm, df = -50 nm, 20 mrad)
+    eng.SimulateImage(0.0)
+    img = orc.SimulateImage()
+    assert rel_l2(eng.Image(), img) < TOL
+
+
+def test_run_equals_step_loop(engine_cls, oracle_mod):
+    eng, _ = make_pair(engine_cls, oracle_mod, sto(2, 5), 256, 0.05)
+    S = eng.GetSlices(True)
+    for i in range(1, S + 1):
+        eng.MultisliceStepConventional(i)
+    w1 = eng.ExitWave()
+    eng.InitialiseWavefunctions(1.9525)
+    eng.RunConventional()
+    w2 = eng.ExitWave()
+    assert rel_l2(w2, w1.astype(np.complex128)) < 1e-6
+
+
+def test_fused_and_plain_agree(engine_cls, oracle_mod):
+    a, _ = make_pair(engine_cls, oracle_mod, sto(2, 5), 256, 0.05, path=0)
+    b, _ = make_pair(engine_cls, oracle_mod, sto(2, 5), 256, 0.05, path=1)
+    a.RunConventional()
+    b.RunConventional()
+    assert rel_l2(a.ExitWave(), b.ExitWave().astype(np.complex128)) < 2 * TOL
+
+
+@pytest.mark.parametrize("path", [0, 1])
+def test_ctf_image(engine_cls, oracle_mod, path):
+    eng, orc = make_pair(engine_cls, oracle_mod, sto(2, 3), 128, 0.1, path=path, A2=30.0, phi2=0.4)
+    S = eng.GetSlices(True)
+    for i in range(1, S + 1):
+        eng.MultisliceStepConventional(i)
+        orc.MultisliceStepConventional(i)
+    eng.AllocHostImage()
+    eng.SimulateImage(1000.0)
+    ref = orc.SimulateImage()
+    assert rel_l2(eng.Image(), ref) < TOL
+    assert abs(eng.GetImMax() - ref.max()) / ref.max() < TOL
+    assert eng.GetImValue(3, 5) == pytest.approx(ref[5, 3], rel=1e-4)
+    c = eng.GetImageContrast(0, 0, 64, 64)
+    assert c == pytest.approx(ref[:64, :64].std(), rel=1e-4)
+
+
+# ---------------------------------------------------------------- STEM
+@pytest.mark.parametrize("path", [0, 1])
+def test_stem_probe_cbed_and_haadf(engine_cls, oracle_mod, path):
+    eng, orc = make_pair(engine_cls, oracle_mod, sto(2, 3), 128, 0.1, kV=300.0, df=0.0, Cs=0.0, ap=25.0,
+                         stem=True, path=path)
+    eng.AllocTDS()
+    orc.AllocTDS()
+    for s in (eng, orc):
+        s.STEMInitialiseWavefunctions(40, 70)
+    S = eng.GetSlices(True)
+    for i in range(1, S + 1):
+        eng.MultisliceStepConventional(i)
+        orc.MultisliceStepConventional(i)
+    assert rel_l2(eng.ExitWave(), orc.Wave()) < TOL
+    eng.AddTDSWaves()
+    orc.AddTDSWaves()
+    assert rel_l2(eng.TDS(), orc.TDS()) < TOL
+    h_e, h_o = eng.AnnularDetector(70.0, 200.0), orc.AnnularDetector(70.0, 200.0)
+    assert h_o > 0 and abs(h_e - h_o) / h_o < 1e-4
+
+
+# ---------------------------------------------------------------- finite differences
+def test_finite_difference_steps(engine_cls, oracle_mod):
+    eng, orc = make_pair(engine_cls, oracle_mod, sto(2, 2), 128, 0.1, kV=200.0)
+    for s in (eng, orc):
+        s.InitialiseWavefunctions()
+        s.SetFDdz(0.05)
+    assert eng.GetSlices(False) == orc.GetSlices(False)
+    for i in range(1, 41):
+        eng.MultisliceStepFD(i)
+        orc.MultisliceStepFD(i)
+    assert rel_l2(eng.ExitWave(), orc.Wave()) < 5 * TOL
+
+
+def test_fd_stability_query(engine_cls, oracle_mod):
+    eng, orc = make_pair(engine_cls, oracle_mod, sto(2, 2), 128, 0.1)
+    sc = orc.Scalars()
+    if sc["nFD"] > 0:
+        assert eng.GetSlices(False) == int(sc["nFD"])
+
+
+# ---------------------------------------------------------------- errors
+def test_call_order_and_argument_errors(engine_cls, oracle_mod):
+    from cudamultislice_b200 import MultisliceError
+
+    eng = engine_cls()
+    with pytest.raises(MultisliceError) as e:
+        eng.MultisliceStepConventional(1)
+    assert e.value.code == 2
+    with pytest.raises(MultisliceError) as e:
+        eng.GetParameterisation("/nonexistent/fparams.dat")
+    assert e.value.code == 4
+    with pytest.raises(MultisliceError) as e:
+        eng.SetAtoms([0], [1.0], [1.0], [1.0])
+    assert e.value.code == 1
+    eng.SetAtoms(*sto(1, 1))
+    eng.ApplyMicroscopeParameters(200.0, 0, 0, 0, 0, 0, 0, 20)
+    with pytest.raises(MultisliceError) as e:
+        eng.SetCalculationVariables(0.1, 0, 0, 64, 1, 1, 1)
+    assert e.value.code == 1
+    with pytest.raises(MultisliceError) as e:
+        eng.GetEWValueAbs(0, 0)
+    assert e.value.code == 2
+
+
+def test_import_xyz_reference_table(engine_cls, oracle_mod, tmp_path):
+    from cudamultislice_b200 import structures as S
+
+    Z, x, y, z = sto(1, 2)
+    p = str(tmp_path / "sto.xyz")
+    S.write_xyz(p, Z, x, y, z)
+    eng = engine_cls()
+    eng.ImportAtoms(p)
+    eng.UploadBinnedAtoms()
+    orc = oracle_mod.OracleSimulation()
+    orc.ImportAtoms(p)
+    orc.UploadBinnedAtoms()
+    a, b = eng.Binned(), orc.Binned()
+    assert np.array_equal(a[1], b[1])  # Ti -> 1 as GetZNum (U.cu:1241)
+    assert 22 not in set(a[1].tolist())
+    eng.SetElementTable(True)
+    eng.ImportAtoms(p)
+    eng.UploadBinnedAtoms()
+    assert 22 in set(eng.Binned()[1].tolist())
