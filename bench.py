@@ -1,0 +1,356 @@
+"""Benchmark of the multislice hot path: slice-steps/s at 1024^2.
+
+Workload (the 1-GPU configuration of the metric): amorphous carbon slab
+50 x 50 x 200 A, Z = 6 atoms placed uniformly at random at 0.1 atoms/A^3
+(~50,000 atoms, minimum separation 1.2 A, seeded), 1024 x 1024 FP32-complex
+grid, 100 slices of 2 A, 300 kV, conventional (3D-integrated) potential.
+Synthetic seeded input stands in for a structure file.
+
+One bench step = one pass of the slice stack: 100 slice steps
+psi <- IFFT(P * FFT(exp(i sigma V) * psi)) over the device-resident potential
+stack (400 MB, larger than L2, so every step streams its V from HBM).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line (rank 0).  `value` is device time (CUDA events on the
+engine's stream) of K steps, max over ranks; `e2e` times the same metric
+through the C ABI with host buffers: atoms in, binning, potential build,
+the 100 slices, exit wave out.  Multi-GPU runs are independent replicas
+(weak scaling): a single specimen does not shard, frozen-phonon passes and
+probe positions do.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+GRID = 1024
+SLICE_DZ = 2.0
+KV = 300.0
+CS = 1.2e7
+SIZE = (50.0, 50.0, 200.0)
+METRIC = "slice-steps/s @1024^2 (conventional multislice, fused path)"
+UNIT = "slice-steps/s"
+BYTES_PER_PX_STEP = 20  # read+write psi (complex64) + read V (float)
+
+
+def workload():
+    from cudamultislice_b200 import structures as S
+
+    Z, x, y, z = S.amorphous_carbon(SIZE, density=0.1, min_sep=1.2)
+    return Z, x, y, z
+
+
+def configure(sim, atoms, fparams):
+    Z, x, y, z = atoms
+    sim.SetAtoms(Z, x, y, z)
+    sim.UploadBinnedAtoms()
+    sim.GetParameterisation(fparams)
+    sim.ApplyMicroscopeParameters(KV, 0.0, 0.0, 0.0, CS, 0.1, 30.0, 20.0)
+    # pixel 0 at the structure's corner: offset = the 2 A box padding
+    ps = SIZE[0] / GRID
+    sim.SetCalculationVariables(ps, 0.0, GRID, GRID, sim.GetSizeX(), sim.GetSizeY(), sim.GetSizeZ(), 2.0, 2.0)
+    sim.PreCalculateFrequencies()
+    sim.InitialiseWavefunctions(SLICE_DZ)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.t:
+            self.t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [q.strip() for q in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks() -> tuple[float, str]:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def allreduce_max(v: float, world: int) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def cpu_baseline(atoms, fparams, nslices: int, threads: int) -> dict:
+    """The FP64 OpenMP oracle on the host cores, on the first `nslices`
+    slices of the same workload (potential build + transmission +
+    propagation per slice); also returns its exit wave for the error check."""
+    from oracle import oracle
+
+    oracle.build()
+    oracle.set_threads(threads)
+    orc = oracle.OracleSimulation()
+    configure(orc, atoms, fparams)
+    t0 = time.perf_counter()
+    for i in range(1, nslices + 1):
+        orc.MultisliceStepConventional(i)
+    dt = time.perf_counter() - t0
+    return {"seconds": dt, "wave": orc.Wave(), "slices": nslices}
+
+
+def run_reference(args, world, rank):
+    """--impl reference: the reference path's CPU implementation (the FP64
+    OpenMP port in oracle/; the reference itself has no CPU path) on all host
+    threads, each step a bounded sample of the same workload."""
+    if rank != 0:
+        return
+    from cudamultislice_b200 import FPARAMS
+
+    atoms = workload()
+    threads = os.cpu_count() or 1
+    per_step = 2
+    if args.warmup > 0:
+        cpu_baseline(atoms, FPARAMS, 1, threads)
+    total = 0.0
+    for _ in range(args.steps):
+        total += cpu_baseline(atoms, FPARAMS, per_step, threads)["seconds"]
+    value = per_step * args.steps / total
+    sample = f"first {per_step} slices of the workload per step (potential build + transmission + propagation)"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128 (FP64)",
+        "data": "synthetic (seeded)", "config": config_dict(len(atoms[0])),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_dict(natoms: int) -> dict:
+    return {
+        "workload": f"amorphous carbon 50x50x200 A, 0.1 atoms/A^3 ({natoms} C, seeded), 1024x1024 grid, "
+                    "100 slices x 2 A, 300 kV, conventional potential (binnedAtomPKernel3 semantics)",
+        "grid": GRID, "slices_per_step": 100, "slice_dz_A": SLICE_DZ, "kV": KV, "atoms": natoms,
+        "parallelism": "replicas", "l2": "inputs larger than L2: 400 MB potential stack streamed per pass",
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-slices", type=int, default=2, help="slices in the bounded CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling mode: set-up plus the timed slice loop only (no e2e, plain or CPU legs)")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+
+    from cudamultislice_b200 import FPARAMS, ManagedMultisliceSimulation
+
+    atoms = workload()
+    sim = ManagedMultisliceSimulation(device=local)
+    configure(sim, atoms, FPARAMS)
+    nsl = sim.BuildPotentialStack()
+    assert nsl >= 100
+    steps_per = 100
+    for _ in range(max(args.warmup, 3)):
+        sim.TimeSlices(steps_per, 1, breakdown=False)
+
+    import torch
+
+    torch.cuda.set_device(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.25)
+    l0 = sim.LaunchCount()
+    total_ms, _, _ = sim.TimeSlices(steps_per, args.steps, breakdown=False)
+    launches = sim.LaunchCount() - l0
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    total_ms = allreduce_max(total_ms, world)
+    slice_steps = steps_per * args.steps * world
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"profile_mode": True, "value": slice_steps / (total_ms / 1000.0), "unit": UNIT,
+                              "gpu_launches": launches}), flush=True)
+        sim.close()
+        return
+    value = slice_steps / (total_ms / 1000.0)
+
+    # per-pass split of the same loop (events between passes) for the roofline
+    _, row_ms, col_ms = sim.TimeSlices(steps_per, 1, breakdown=True)
+    N = GRID * GRID
+    peak, peak_kind = measured_peaks()
+    step_ms = total_ms / (steps_per * args.steps)
+    row_bytes, col_bytes = 20 * N, 16 * N  # row pass: psi r/w + V; column pass: psi r/w
+    dom = ("row pass (k_pass_a: IFFT_row, x exp(i sigma V), FFT_row)", row_ms, row_bytes) if row_ms >= col_ms else \
+          ("column pass (k_pass_b: FFT_col, x P(k), IFFT_col)", col_ms, col_bytes)
+    achieved = dom[2] / (dom[1] / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                "launch_ms": dom[1], "row_pass_ms": row_ms, "col_pass_ms": col_ms,
+                "step_achieved_gbs": BYTES_PER_PX_STEP * N / (step_ms / 1000.0) / 1e9,
+                "step_frac": BYTES_PER_PX_STEP * N / (step_ms / 1000.0) / 1e9 / peak}
+    traffic_file = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(traffic_file):
+        with open(traffic_file) as f:
+            tr = json.load(f)
+        roofline["traffic"] = tr.get("row_pass" if row_ms >= col_ms else "col_pass")
+
+    # plain path (cuFFT + one kernel per operation) on the same GPU and stack
+    sim.SetSlicePath(1)
+    sim.TimeSlices(steps_per, 1, breakdown=False)
+    plain_ms, _, _ = sim.TimeSlices(steps_per, args.steps, breakdown=False)
+    plain_value = steps_per * args.steps / (plain_ms / 1000.0)
+    sim.SetSlicePath(0)
+
+    # end to end through the C ABI with host buffers
+    import numpy as np
+
+    Z, x, y, z = atoms
+    h2d = Z.nbytes + x.nbytes + y.nbytes + z.nbytes
+    e2e_times = []
+    for k in range(args.steps + 1):
+        t0 = time.perf_counter()
+        sim.SetAtoms(Z, x, y, z)
+        sim.UploadBinnedAtoms()
+        sim.InitialiseWavefunctions(SLICE_DZ)
+        ns = sim.RunConventional()
+        psi = sim.ExitWave()
+        dt = time.perf_counter() - t0
+        if k > 0:
+            e2e_times.append(dt)
+    e2e_s = allreduce_max(sum(e2e_times), world)
+    e2e_value = ns * len(e2e_times) * world / e2e_s
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64 (FP32 complex)", "data": "synthetic (seeded)",
+        "config": config_dict(len(Z)), "clocks": clk, "gpu_launches": launches,
+        "roofline": roofline,
+        "plain_path": {"value": plain_value, "unit": UNIT, "speedup_fused_vs_plain": value / world / plain_value},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(psi.nbytes),
+                "note": "host clock around the synchronous C-ABI calls: atoms in, binning, potential stack "
+                        "(100 slices), slice loop, exit wave out"},
+    }
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        cb = cpu_baseline(atoms, FPARAMS, args.cpu_slices, threads)
+        sim.InitialiseWavefunctions(SLICE_DZ)
+        for i in range(1, cb["slices"] + 1):
+            sim.MultisliceStepConventional(i)
+        psi_gpu = sim.ExitWave().astype(np.complex128)
+        err = float(np.linalg.norm(psi_gpu - cb["wave"]) / np.linalg.norm(cb["wave"]))
+        out["cpu_baseline"] = {
+            "value": cb["slices"] / cb["seconds"], "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"FP64 OpenMP oracle, first {cb['slices']} slices of the workload "
+                      "(potential build + transmission + propagation)"}
+        out["err_vs_fp64"] = {"value": err, "after_slices": cb["slices"],
+                              "definition": "||psi - psi64||_2 / ||psi64||_2 on the exit wave"}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    sim.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

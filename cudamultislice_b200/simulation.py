@@ -274,10 +274,16 @@ class ManagedMultisliceSimulation:
         self._chk(self._L.ms_fft2(self._h, _ptr(a), _ptr(out), nx, ny, int(sign)))
         return out
 
-    def TimeSlices(self, steps: int, reps: int = 1):
+    def TimeSlices(self, steps: int, reps: int = 1, breakdown: bool = True):
+        """Device time (ms) of reps x steps conventional steps over the
+        resident potential stack; with `breakdown`, also the average duration
+        of one row pass and one column pass (fused path)."""
         t, a, b = C.c_float(), C.c_float(), C.c_float()
-        self._chk(self._L.ms_time_slices(self._h, int(steps), int(reps), C.byref(t), C.byref(a), C.byref(b)))
-        return t.value, a.value, b.value
+        if breakdown:
+            self._chk(self._L.ms_time_slices(self._h, int(steps), int(reps), C.byref(t), C.byref(a), C.byref(b)))
+            return t.value, a.value, b.value
+        self._chk(self._L.ms_time_slices(self._h, int(steps), int(reps), C.byref(t), None, None))
+        return t.value, None, None
 
     def LaunchCount(self) -> int:
         out = C.c_longlong()

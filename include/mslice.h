@@ -194,8 +194,9 @@ ms_status ms_copy_potential_slice(ms_sim* sim, int kind, int iteration, float* d
 ms_status ms_fft2(ms_sim* sim, const float* in, float* out, int nx, int ny, int sign);
 /* Times `steps` fused (or plain) conventional steps over the resident
  * potential stack with CUDA events on the handle's stream, repeated `reps`
- * times; writes the total milliseconds and the per-launch average of the two
- * fused passes (row pass, column pass; timed in separate loops). */
+ * times; writes the total milliseconds and, when ms_row_pass and ms_col_pass
+ * are not NULL, the per-launch averages of the two fused passes measured in a
+ * second run of `steps` steps with an event between every pass. */
 ms_status ms_time_slices(ms_sim* sim, int steps, int reps, float* ms_total, float* ms_row_pass,
                          float* ms_col_pass);
 /* Number of this library's kernels launched by the handle so far. */

@@ -1,0 +1,1 @@
+// empty stand-in: the reference includes this Boost header but uses it only in commented-out code

@@ -1,0 +1,93 @@
+"""The FP64 oracle against golden vectors produced by the reference itself.
+
+tests/golden/ref_*.npz were generated by tests/golden/make_golden_ref.py,
+which runs the reference engine (GUI Simulation/UnmanagedGUISimulation.cu,
+compiled unchanged by oracle/ref_build.sh; string-named constant uploads
+routed to their symbols) on a B200.  The reference computes in FP32 with
+cuFFT, so its outputs carry FP32 rounding: integer work (the atom index) and
+the FP32 set-up scalars must match bit for bit, values within the FP32 error
+of a 1e-5-class computation."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from tests.conftest import FPARAMS, GOLDEN
+
+CASES = sorted(glob.glob(os.path.join(GOLDEN, "ref_*.npz")))
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.complex128) - b) / np.linalg.norm(b))
+
+
+def oracle_for(oracle_mod, g, tmp_path):
+    p = str(tmp_path / "s.xyz")
+    with open(p, "w") as f:
+        f.write(str(g["xyz"]))
+    o = oracle_mod.OracleSimulation()
+    o.ImportAtoms(p, False)
+    o.UploadBinnedAtoms()
+    o.GetParameterisation(FPARAMS)
+    o.ApplyMicroscopeParameters(*[float(v) for v in g["micro"]])
+    ps, df, xoff, yoff = [float(v) for v in g["calc"]]
+    nx, ny, stem = [int(v) for v in g["grid"]]
+    if stem:
+        o.STEMSetCalculationVariables(ps, df, nx, ny, o.GetSizeX(), o.GetSizeY(), o.GetSizeZ())
+    else:
+        o.SetCalculationVariables(ps, df, nx, ny, o.GetSizeX(), o.GetSizeY(), o.GetSizeZ(), xoff, yoff)
+    o.PreCalculateFrequencies()
+    if str(g["mode"]) == "fd":
+        o.InitialiseWavefunctions()
+    else:
+        o.InitialiseWavefunctions(float(g["dz"]))
+    if stem:
+        o.AllocTDS()
+        px, py = [int(v) for v in g["stem_pos"]]
+        o.STEMInitialiseWavefunctions(px, py)
+    return o
+
+
+@pytest.mark.skipif(not CASES, reason="golden vectors not generated")
+@pytest.mark.parametrize("path", CASES, ids=[os.path.basename(c)[:-4] for c in CASES])
+def test_oracle_matches_reference(oracle_mod, path, tmp_path):
+    g = np.load(path)
+    o = oracle_for(oracle_mod, g, tmp_path)
+    # bounding box and atom index: bit-exact
+    assert np.array_equal(o.Box(), g["box"])
+    off, Z, x, y, z = o.Binned()
+    assert np.array_equal(off, g["off"])
+    assert np.array_equal(Z, g["bZ"])
+    for a, b in ((x, g["bx"]), (y, g["by"]), (z, g["bz"])):
+        assert np.array_equal(a, b)
+    # FP32 set-up scalars: bit-exact
+    sc = o.Scalars()
+    ref = g["scalars"]
+    assert np.float32(sc["wavel"]) == ref[0]
+    assert np.float32(sc["sigma2"]) == ref[1]
+    assert np.float32(sc["kmax"]) == ref[4]
+    assert np.float32(sc["convdz"]) == ref[5]
+    if str(g["mode"]) == "fd":
+        assert np.float32(sc["dzFD"]) == ref[2] and int(sc["nFD"]) == int(ref[3])
+    # values
+    nsteps = int(g["nsteps"])
+    for i in range(1, nsteps + 1):
+        if str(g["mode"]) == "fd":
+            o.MultisliceStepFD(i)
+        else:
+            key = f"trans_{i}"
+            if key in g.files:
+                t = np.exp(1j * sc["sigma2"] * o.PotentialConventional(i))
+                assert rel_l2(g[key], t) < 2e-6, (i, rel_l2(g[key], t))
+            o.MultisliceStepConventional(i)
+    e = rel_l2(g["wave"], o.Wave())
+    tol = 1e-4 if str(g["mode"]) == "fd" else 2e-5
+    assert e < tol, e
+    if "tds" in g.files:
+        o.AddTDSWaves()
+        assert rel_l2(g["tds"], o.TDS()) < 2e-5
+    if "ew_minmax" in g.files:
+        a = np.abs(o.Wave())
+        assert abs(a.max() - g["ew_minmax"][1]) / a.max() < 1e-4
+        assert abs(a.min() - g["ew_minmax"][0]) / max(a.min(), 1e-3) < 1e-3
