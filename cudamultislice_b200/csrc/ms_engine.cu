@@ -18,6 +18,7 @@
 #include <fstream>
 #include <memory>
 #include <new>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -154,18 +155,40 @@ class Engine {
     if (!path) return fail(MS_ERR_INVALID, "null path");
     std::ifstream in(path);
     if (!in) return fail(MS_ERR_IO, std::string("cannot open structure file ") + path);
+    // LoadAtomFile reads the count, discards the rest of that line (its
+    // comment) and then reads "symbol x y z" records (U.cu:1309-1321).  A
+    // separate comment line, as in the common .xyz layout, would be read by the
+    // reference as an atom; here a line that is not an atom record is skipped.
     int n = 0;
     if (!(in >> n) || n <= 0) return fail(MS_ERR_IO, "structure file: bad atom count");
     std::string line;
     std::getline(in, line);
-    std::getline(in, line);  // comment line
-    std::vector<int> Z(n);
-    std::vector<float> x(n), y(n), z(n);
-    for (int i = 0; i < n; ++i) {
+    std::vector<int> Z;
+    std::vector<float> x, y, z;
+    Z.reserve(n);
+    x.reserve(n);
+    y.reserve(n);
+    z.reserve(n);
+    bool first = true;
+    while ((int)Z.size() < n && std::getline(in, line)) {
+      std::istringstream ls(line);
       std::string sym;
-      if (!(in >> sym >> x[i] >> y[i] >> z[i])) return fail(MS_ERR_IO, "structure file: truncated atom list");
-      Z[i] = znum(sym, full_table_);
+      float a, b, c;
+      if (!(ls >> sym >> a >> b >> c)) {
+        if (first && line.find_first_not_of(" \t\r") != std::string::npos) {
+          first = false;  // a comment line after the count
+          continue;
+        }
+        if (line.find_first_not_of(" \t\r") == std::string::npos) continue;
+        return fail(MS_ERR_IO, "structure file: malformed atom record");
+      }
+      first = false;
+      Z.push_back(znum(sym, full_table_));
+      x.push_back(a);
+      y.push_back(b);
+      z.push_back(c);
     }
+    if ((int)Z.size() < n) return fail(MS_ERR_IO, "structure file: truncated atom list");
     return set_atoms(Z.data(), x.data(), y.data(), z.data(), n);
   }
 
@@ -729,6 +752,92 @@ class Engine {
     return MS_OK;
   }
 
+  // ---- STEM raster: probes `batch` at a time through the fused passes ----
+  // Per probe: STEMInitialiseWavefunctions (U.cu:2672-2705, L1-normalised),
+  // conventional slices 1..S, and the annular detector read from the last
+  // column spectrum.  Linear in psi, so probes run unnormalised and each
+  // signal is divided by its L1 norm squared at the end.
+  int stem_raster(const int* px, const int* py, int n, float inner, float outer, int batch, double* signal) {
+    if (!have_freq_) return fail(MS_ERR_STATE, "frequencies not precalculated");
+    if (!px || !py || !signal) return fail(MS_ERR_INVALID, "null buffer");
+    if (n < 1) return fail(MS_ERR_INVALID, "need at least one probe position");
+    if (batch < 1 || batch > 1024) return fail(MS_ERR_INVALID, "batch must be 1..1024");
+    if (!(inner >= 0) || !(outer > inner)) return fail(MS_ERR_INVALID, "need 0 <= inner < outer");
+    if (!use_fused()) {
+      // plain path: one probe at a time through the reference sequence
+      for (int i = 0; i < n; ++i) {
+        if (int rc = stem_init_waves(px[i], py[i])) return rc;
+        int S = 0;
+        if (int rc = get_slices(true, &S)) return rc;
+        for (int it = 1; it <= S; ++it)
+          if (int rc = step_conventional(it)) return rc;
+        if (int rc = annular(inner, outer, signal + i)) return rc;
+      }
+      return MS_OK;
+    }
+    int S = 0;
+    if (int rc = build_stack(&S)) return rc;
+    if (int rc = ensure_prop_tables(convdz_)) return rc;
+    const long long N = (long long)nx_ * ny_;
+    const int B = std::min(batch, n);
+    const int nbr = pw_reduce_blocks(N);
+    MS_TRY(d_bwave_.resize((size_t)B * N));
+    MS_TRY(d_bpos_.resize(2 * (size_t)B));
+    MS_TRY(d_bsig_.resize(2 * (size_t)B));
+    MS_TRY(d_bpart_.resize((size_t)B * nbr));
+    std::vector<int> pos(2 * B);
+    std::vector<double> host(2 * B);
+    const Grid2 g{nx_, ny_};
+    const float apert = (float)((double)aperture_ * 0.001 / (double)wavel_);
+    const float kin = (inner * 0.001f) / wavel_, kout = (outer * 0.001f) / wavel_;
+    for (int start = 0; start < n; start += B) {
+      const int nb = std::min(B, n - start);
+      for (int b = 0; b < nb; ++b) {
+        pos[b] = px[start + b];
+        pos[B + b] = py[start + b];
+      }
+      MS_TRY(cudaMemcpyAsync(d_bpos_.p, pos.data(), sizeof(int) * 2 * B, cudaMemcpyHostToDevice, stream_));
+      MS_TRY(cudaMemsetAsync(d_bsig_.p, 0, sizeof(double) * B, stream_));
+      MS_TRY(pw_probe_batch(d_bwave_.p, N, nb, d_kx_.p, d_ky_.p, d_bpos_.p, d_bpos_.p + B, apert, ps_, df_, Cs_,
+                            wavel_, g, stream_, &launches));
+      PassBArgs bi = passb_args(d_bwave_.p, d_bwave_.p);
+      bi.batch_stride_wave = N;
+      MS_TRY(launch_pass_b(bi, B_INV_ONLY, nb, stream_));
+      PassAArgs ai = passa_args(d_bwave_.p, d_bwave_.p);
+      ai.batch_stride_wave = N;
+      MS_TRY(launch_pass_a(ai, A_INV, nb, stream_));
+      launches += 2;
+      MS_TRY(pw_sum_abs_batch(d_bwave_.p, N, N, nb, d_bpart_.p, d_bsig_.p + B, stream_, &launches));
+      for (int it = 1; it <= S; ++it) {
+        PassAArgs a = passa_args(d_bwave_.p, d_bwave_.p);
+        a.batch_stride_wave = N;
+        a.batch_stride_V = 0;
+        a.V = d_stack_.p + (size_t)(it - 1) * N;
+        MS_TRY(launch_pass_a(a, it == 1 ? (A_MULT_T | A_FWD) : (A_INV | A_MULT_T | A_FWD), nb, stream_));
+        PassBArgs b = passb_args(d_bwave_.p, d_bwave_.p);
+        b.batch_stride_wave = N;
+        if (it < S) {
+          MS_TRY(launch_pass_b(b, B_PROPAGATE, nb, stream_));
+        } else {
+          b.sig = d_bsig_.p;
+          b.kin2 = kin * kin;
+          b.kout2 = kout * kout;
+          b.scale = 1.0f / (float)N;
+          MS_TRY(launch_pass_b(b, B_DETECT, nb, stream_));
+        }
+        launches += 2;
+      }
+      MS_TRY(cudaMemcpyAsync(host.data(), d_bsig_.p, sizeof(double) * 2 * B, cudaMemcpyDeviceToHost, stream_));
+      MS_TRY(cudaStreamSynchronize(stream_));
+      for (int b = 0; b < nb; ++b) {
+        const double l1 = host[B + b];
+        if (!(l1 > 0)) return fail(MS_ERR_NUMERIC, "probe is empty (aperture smaller than one frequency pixel)");
+        signal[start + b] = host[b] / (l1 * l1);
+      }
+    }
+    return MS_OK;
+  }
+
   // ---- whole-run entry points ----
   int build_stack(int* nslices) {
     if (int rc = require_potential_inputs()) return rc;
@@ -1157,7 +1266,9 @@ class Engine {
   // waves
   DevBuf<float2> d_psi0_, d_psi_, d_psim_, d_t1_, d_t2_, d_grad_;
   DevBuf<float> d_V_, d_f_, d_tds_, d_stack_;
-  DevBuf<double> d_partial_;
+  DevBuf<double> d_partial_, d_bsig_, d_bpart_;
+  DevBuf<float2> d_bwave_;
+  DevBuf<int> d_bpos_;
   int domain_ = 0;  // 0 real space, 1 row-frequency state of the fused passes
   bool have_waves_ = false, stack_valid_ = false, have_tds_ = false, tds_host_valid_ = false;
   int nstack_ = 0;
@@ -1448,6 +1559,10 @@ ms_status ms_run_conventional(ms_sim* s, int* nslices) {
 ms_status ms_annular_detector(ms_sim* s, float inner, float outer, double* out) {
   if (ms_status r = out_check(s, out)) return r;
   return guarded(s, [&](ms::Engine& e) { return e.annular(inner, outer, out); });
+}
+ms_status ms_stem_raster(ms_sim* s, const int* px, const int* py, int n, float inner, float outer, int batch,
+                         double* signal) {
+  return guarded(s, [&](ms::Engine& e) { return e.stem_raster(px, py, n, inner, outer, batch, signal); });
 }
 ms_status ms_get_binned_counts(ms_sim* s, int* n, int* nz) {
   if (ms_status r = out_check(s, n)) return r;

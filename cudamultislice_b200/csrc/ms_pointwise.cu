@@ -111,6 +111,25 @@ __global__ void k_probe(float2* P, const float* kx, const float* ky, int px, int
   }
 }
 
+// k_probe for a batch: blockIdx.z selects the probe position.
+__global__ void k_probe_batch(float2* P, long long stride, const float* kx, const float* ky, const int* pxs,
+                              const int* pys, float apert, float ps, float df, float Cs, float wavel, Grid2 g) {
+  PW_INDEX
+  const int b = blockIdx.z;
+  const float kf = fsqrt_x(fadd_x(fmul_x(kx[x], kx[x]), fmul_x(ky[y], ky[y])));
+  float2 v = make_float2(0.f, 0.f);
+  if (kf < apert) {
+    const double kxd = kx[x], kyd = ky[y], k2 = kxd * kxd + kyd * kyd, lam = wavel;
+    const double chi = 3.14159265 * lam * k2 * ((double)Cs * lam * lam * k2 * 0.5 + (double)df);
+    const double phi = 2.0 * 3.14159265 * (kxd * pxs[b] * (double)ps + kyd * pys[b] * (double)ps);
+    const double ph = phi - chi, twopi = 6.283185307179586;
+    float sn, cs;
+    sincosf((float)(ph - twopi * rint(ph / twopi)), &sn, &cs);
+    v = make_float2(cs, sn);
+  }
+  P[b * stride + i] = v;
+}
+
 // makeComplex U.cu:322-336
 __global__ void k_real_to_complex(const float* in, float2* out, Grid2 g) {
   PW_INDEX
@@ -173,6 +192,25 @@ __global__ void __launch_bounds__(kRedThreads) k_sum_abs(const float2* a, long l
   }
   const double r = block_sum_d(acc);
   if (threadIdx.x == 0) partial[blockIdx.x] = r;
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_sum_abs_batch(const float2* a, long long n, long long stride,
+                                                               double* partial) {
+  const float2* ab = a + blockIdx.y * stride;
+  double acc = 0.0;
+  for (long long i = blockIdx.x * (long long)kRedThreads + threadIdx.x; i < n; i += (long long)gridDim.x * kRedThreads) {
+    const float2 v = ab[i];
+    acc += sqrt((double)v.x * v.x + (double)v.y * v.y);
+  }
+  const double r = block_sum_d(acc);
+  if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = r;
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_sum_partials_batch(const double* partial, int nb, double* out) {
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < nb; i += kRedThreads) acc += partial[blockIdx.x * nb + i];
+  const double r = block_sum_d(acc);
+  if (threadIdx.x == 0) out[blockIdx.x] = r;
 }
 
 __global__ void __launch_bounds__(kRedThreads) k_annular(const float2* F, const float* kx, const float* ky,
@@ -277,6 +315,25 @@ cudaError_t pw_sum_abs(const float2* a, long long n, double* partial, double* ou
   const int nb = pw_reduce_blocks(n);
   k_sum_abs<<<nb, kRedThreads, 0, s>>>(a, n, partial);
   k_sum_partials<<<1, kRedThreads, 0, s>>>(partial, nb, 1.0, out);
+  if (count) *count += 2;
+  return cudaGetLastError();
+}
+
+cudaError_t pw_probe_batch(float2* P, long long stride, int nb, const float* kx, const float* ky, const int* px,
+                           const int* py, float apert, float ps, float df, float Cs, float wavel, Grid2 g,
+                           cudaStream_t s, long long* count) {
+  dim3 grid = grid_of(g);
+  grid.z = nb;
+  k_probe_batch<<<grid, dim3(kBX, kBY), 0, s>>>(P, stride, kx, ky, px, py, apert, ps, df, Cs, wavel, g);
+  if (count) ++*count;
+  return cudaGetLastError();
+}
+
+cudaError_t pw_sum_abs_batch(const float2* a, long long n, long long stride, int nb, double* partial, double* out,
+                             cudaStream_t s, long long* count) {
+  const int blocks = pw_reduce_blocks(n);
+  k_sum_abs_batch<<<dim3(blocks, nb), kRedThreads, 0, s>>>(a, n, stride, partial);
+  k_sum_partials_batch<<<nb, kRedThreads, 0, s>>>(partial, blocks, out);
   if (count) *count += 2;
   return cudaGetLastError();
 }

@@ -40,6 +40,14 @@ cudaError_t pw_ctf(float2* F, const float* kx, const float* ky, double wavel, do
 int pw_reduce_blocks(long long n);
 cudaError_t pw_sum_abs(const float2* a, long long n, double* partial, double* out, cudaStream_t s,
                        long long* count);
+// Batched probes: probe b at pixel (px[b], py[b]) into P + b*stride (gridDim.z = b).
+cudaError_t pw_probe_batch(float2* P, long long stride, int nb, const float* kx, const float* ky, const int* px,
+                           const int* py, float apert, float ps, float df, float Cs, float wavel, Grid2 g,
+                           cudaStream_t s, long long* count);
+// Per-instance sum of |a| for nb instances of n points: out[b] (FP64).
+// `partial` holds nb * pw_reduce_blocks(n) doubles.
+cudaError_t pw_sum_abs_batch(const float2* a, long long n, long long stride, int nb, double* partial, double* out,
+                             cudaStream_t s, long long* count);
 // Annular detector sum over kin2 <= k^2 < kout2 of |F|^2 * scale (FP64).
 cudaError_t pw_annular(const float2* F, const float* kx, const float* ky, float kin2, float kout2, double scale,
                        Grid2 g, double* partial, double* out, cudaStream_t s, long long* count);

@@ -137,6 +137,25 @@ __global__ void __launch_bounds__(kWarpsB * 32) k_pass_b(PassBArgs a, float scal
       atomicAdd(a.acc + (long long)ys * nx + xs, m);
     }
     return;  // nothing to store back
+  } else if constexpr (MODE == B_DETECT) {
+    // |FFT2(psi_exit)|^2 = |P|^2 |FFT_col(Y)|^2: the last propagation only
+    // masks, so the detector reads the column spectrum before the inverse.
+    const float kx = a.kx[col];
+    const float kx2 = fmul_x(kx, kx);
+    float acc = 0.0f;
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int n = t + P * j;
+      const float ky = a.ky[n];
+      const float k2 = fadd_x(kx2, fmul_x(ky, ky));
+      const bool keep = fsqrt_x(k2) < a.kmax && k2 >= a.kin2 && k2 < a.kout2;
+      if (keep) acc += v[j].x * v[j].x + v[j].y * v[j].y;
+    }
+    double d = (double)acc;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d += __shfl_down_sync(0xffffffffu, d, o);
+    if (lane == 0 && d != 0.0) atomicAdd(a.sig + blockIdx.y, d * (double)scale);
+    return;
   }
 
   __syncthreads();  // every slot's FFT scratch use is finished
@@ -209,6 +228,7 @@ cudaError_t dispatch_b_mode(const PassBArgs& a, int mode, float scale, int batch
     case B_PROPAGATE: return run_b<NY, B_PROPAGATE>(a, scale, batch, s);
     case B_CTF: return run_b<NY, B_CTF>(a, scale, batch, s);
     case B_CBED: return run_b<NY, B_CBED>(a, scale, batch, s);
+    case B_DETECT: return run_b<NY, B_DETECT>(a, scale, batch, s);
     default: return cudaErrorInvalidValue;
   }
 }

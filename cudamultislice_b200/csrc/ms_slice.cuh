@@ -21,6 +21,7 @@ enum PassBMode : int {
   B_PROPAGATE = 2,   // FFT_col, x Px*Py (band-limited), IFFT_col
   B_CTF = 3,         // FFT_col, x CTF(k)/N (objective aperture), IFFT_col
   B_CBED = 4,        // FFT_col, accumulate |.| fftshifted into a float map
+  B_DETECT = 5,      // FFT_col, band limit of P, sum |.|^2 over an annulus per instance
 };
 
 struct PassAArgs {
@@ -53,6 +54,8 @@ struct PassBArgs {
   float kmax;
   CtfParams ctf;
   float scale;         // B_CTF: factor on the weight; B_CBED: factor on |.|
+  double* sig;         // B_DETECT: one FP64 sum per instance (blockIdx.y)
+  float kin2, kout2;   // B_DETECT: annulus kin^2 <= kx^2+ky^2 < kout^2 (FP32 decision)
   int nx, ny;
   long long batch_stride_wave;
 };

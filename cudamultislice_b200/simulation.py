@@ -252,6 +252,17 @@ class ManagedMultisliceSimulation:
         self._chk(self._L.ms_annular_detector(self._h, float(inner_mrad), float(outer_mrad), C.byref(out)))
         return out.value
 
+    def StemRaster(self, px, py, inner_mrad: float, outer_mrad: float, batch: int = 16) -> np.ndarray:
+        """Annular-detector signal for every probe position (pixels)."""
+        px = np.ascontiguousarray(px, np.int32).ravel()
+        py = np.ascontiguousarray(py, np.int32).ravel()
+        if px.size != py.size:
+            raise ValueError("px and py must have the same length")
+        out = np.zeros(px.size, np.float64)
+        self._chk(self._L.ms_stem_raster(self._h, _ptr(px), _ptr(py), px.size, float(inner_mrad),
+                                         float(outer_mrad), int(batch), _ptr(out)))
+        return out
+
     # ---- inspection ----
     def Binned(self):
         n, nz = C.c_int(), C.c_int()

@@ -127,9 +127,11 @@ def random_atoms(n: int, size=(10.0, 10.0, 10.0), Zs=(6, 8, 14, 38), seed: int =
     return Z, xyz[:, 0].astype(np.float32), xyz[:, 1].astype(np.float32), xyz[:, 2].astype(np.float32)
 
 
-def write_xyz(path: str, Z, x, y, z, symbols: dict[int, str] | None = None):
+def write_xyz(path: str, Z, x, y, z, symbols: dict[int, str] | None = None, comment_line: bool = True):
+    """Write an .xyz file.  comment_line=False writes the layout the reference
+    reader expects (count and comment on the first line)."""
     sym = symbols or {1: "H", 6: "C", 7: "N", 8: "O", 14: "Si", 22: "Ti", 31: "Ga", 38: "Sr"}
     with open(path, "w") as f:
-        f.write(f"{len(Z)}\ncomment\n")
+        f.write(f"{len(Z)}\ncomment\n" if comment_line else f"{len(Z)} comment\n")
         for zz, a, b, c in zip(Z, x, y, z):
             f.write(f"{sym[int(zz)]} {float(a):.6f} {float(b):.6f} {float(c):.6f}\n")

@@ -183,6 +183,15 @@ ms_status ms_run_conventional(ms_sim* sim, int* nslices);
  * sum over inner <= theta < outer (mrad) of |FFT(psi)|^2 / N. */
 ms_status ms_annular_detector(ms_sim* sim, float inner_mrad, float outer_mrad, double* out);
 
+/* STEM raster (new; the reference runs a single probe at the centre, with a
+ * "TODO: loop over all stem positions" at CUDA Simulation GUI/MainWindow.xaml.cs:366):
+ * for each probe position (px[i], py[i]) in pixels, the probe of
+ * STEMInitialiseWavefunctions (U.cu:2672-2705), conventional slices 1..S over
+ * the potential stack, and the annular-detector signal of ms_annular_detector,
+ * written to signal[i].  Probes run `batch` at a time in one set of launches. */
+ms_status ms_stem_raster(ms_sim* sim, const int* px, const int* py, int n, float inner_mrad,
+                         float outer_mrad, int batch, double* signal);
+
 /* ---- inspection (parity tests and measurement) ---- */
 ms_status ms_get_binned_counts(ms_sim* sim, int* n_atoms, int* n_zbins);
 ms_status ms_copy_binned(ms_sim* sim, int* offsets, int* Z, float* x, float* y, float* z);

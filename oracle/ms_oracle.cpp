@@ -376,7 +376,9 @@ extern "C" int or_set_atoms(or_sim* s, const int* Z, const float* x, const float
     return 0;
 }
 
-/* .xyz reader, U.cu:1293-1356: count, comment line, then "symbol x y z" rows. */
+/* .xyz reader, U.cu:1293-1356: the count, the rest of its line discarded
+ * (U.cu:1309-1310), then "symbol x y z" records.  A separate comment line
+ * (which the reference would misread as an atom) is skipped. */
 extern "C" int or_import_atoms(or_sim* s, const char* path, int full_table) {
     std::ifstream in(path);
     if (!in) return fail(s, "cannot open structure file");
@@ -384,14 +386,24 @@ extern "C" int or_import_atoms(or_sim* s, const char* path, int full_table) {
     std::string line;
     if (!(in >> n) || n <= 0) return fail(s, "bad atom count");
     std::getline(in, line);
-    std::getline(in, line); /* comment */
-    std::vector<int> Z(n);
-    std::vector<float> x(n), y(n), z(n);
-    for (int i = 0; i < n; ++i) {
+    std::vector<int> Z;
+    std::vector<float> x, y, z;
+    bool first = true;
+    while ((int)Z.size() < n && std::getline(in, line)) {
+        std::istringstream ls(line);
         std::string sym;
-        if (!(in >> sym >> x[i] >> y[i] >> z[i])) return fail(s, "truncated structure file");
-        Z[i] = or_znum(sym.c_str(), full_table);
+        float a, b, c;
+        const bool blank = line.find_first_not_of(" \t\r") == std::string::npos;
+        if (!(ls >> sym >> a >> b >> c)) {
+            if (blank) continue;
+            if (first) { first = false; continue; }
+            return fail(s, "malformed atom record");
+        }
+        first = false;
+        Z.push_back(or_znum(sym.c_str(), full_table));
+        x.push_back(a); y.push_back(b); z.push_back(c);
     }
+    if ((int)Z.size() < n) return fail(s, "truncated structure file");
     return or_set_atoms(s, Z.data(), x.data(), y.data(), z.data(), n);
 }
 

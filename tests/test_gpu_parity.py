@@ -263,3 +263,21 @@ def test_import_xyz_reference_table(engine_cls, oracle_mod, tmp_path):
     eng.ImportAtoms(p)
     eng.UploadBinnedAtoms()
     assert 22 in set(eng.Binned()[1].tolist())
+
+
+@pytest.mark.parametrize("path", [0, 1])
+def test_stem_raster_batched(engine_cls, oracle_mod, path):
+    eng, orc = make_pair(engine_cls, oracle_mod, sto(2, 3), 128, 0.1, kV=300.0, df=-50.0, Cs=1e4, ap=25.0,
+                         stem=True, path=path)
+    px = np.array([10, 64, 100, 3, 77, 120, 50], np.int32)
+    py = np.array([20, 64, 7, 99, 33, 110, 50], np.int32)
+    sig = eng.StemRaster(px, py, 10.0, 40.0, batch=4)  # two batches, the second partial
+    ref = []
+    for x, y in zip(px, py):
+        orc.STEMInitialiseWavefunctions(int(x), int(y))
+        for i in range(1, orc.GetSlices(True) + 1):
+            orc.MultisliceStepConventional(i)
+        ref.append(orc.AnnularDetector(10.0, 40.0))
+    ref = np.array(ref)
+    assert np.all(ref > 0)
+    assert np.max(np.abs(sig - ref) / ref) < 1e-4, (sig, ref)
