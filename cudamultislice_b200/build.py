@@ -18,7 +18,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmslice_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["ms_engine.cu", "ms_slice.cu", "ms_atoms.cu", "ms_pointwise.cu"]
+SOURCES = ["ms_engine.cu", "ms_slice.cu", "ms_atoms.cu", "ms_pointwise.cu", "ms_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", f"-I{INCLUDE}"]
 

@@ -1294,6 +1294,15 @@ struct ms_sim {
 
 namespace {
 thread_local std::string g_create_error;
+}  // namespace
+
+namespace ms {
+// Failures of calls made without a handle (ms_create, the no-allocation
+// index build) are reported by ms_last_error(NULL) on the calling thread.
+void set_handle_free_error(const std::string& m) { g_create_error = m; }
+}  // namespace ms
+
+namespace {
 
 template <class F>
 ms_status guarded(ms_sim* s, F&& f) {

@@ -67,6 +67,8 @@ enum {
 ms_status ms_create(int device, ms_sim** out);
 /* Destructor U.cu:2558-2561. */
 ms_status ms_destroy(ms_sim* sim);
+/* Message of the handle's last failure; with NULL, of the last failed call made
+ * without a handle (ms_create, ms_build_atom_index_noalloc) on this thread. */
 const char* ms_last_error(const ms_sim* sim);
 const char* ms_version(void);
 ms_status ms_set_option(ms_sim* sim, int option, int value);
@@ -210,6 +212,29 @@ ms_status ms_time_slices(ms_sim* sim, int steps, int reps, float* ms_total, floa
                          float* ms_col_pass);
 /* Number of this library's kernels launched by the handle so far. */
 ms_status ms_get_launch_count(ms_sim* sim, long long* out);
+
+/* ---- atom index without device allocation (no counterpart in the reference) ----
+ * For callers that cannot call cudaMalloc: an application whose memory manager
+ * owns every device allocation, work enqueued while a CUDA graph is captured, or
+ * a loop that cannot take cudaMalloc's implicit device synchronisation.  Builds
+ * the same bit-exact atom index as ms_upload_binned_atoms from atoms already on
+ * the device (d_Z, d_x, d_y, d_z: n entries each) into caller-owned device
+ * buffers: d_atoms (4*n floats, 16-byte aligned: x, y, z shifted by the box
+ * minimum, then Z as int bits, sorted z-bin -> y-bin -> x-bin, input order within
+ * a bin) and d_offsets (nz*2500 + 1 ints, offsets_capacity of them available).
+ * `box` is a host array {MaxX, MinX, MaxY, MinY, MaxZ, MinZ} (LoadAtomFile's
+ * padded box); nz = ceil(MaxZ - MinZ) one-angstrom z-bins is returned in *nz_out.
+ * Work is enqueued on `stream` (a cudaStream_t, NULL for the default stream) and
+ * the call returns without waiting.  Scratch is one fixed device array of about
+ * 3.1 MB inside the library, held by every GPU that loads it until exit; limits:
+ * n <= 131072 atoms and nz <= 209 z-bins, larger requests fail with
+ * MS_ERR_INVALID.  All calls share that array: calls whose GPU work overlaps
+ * race and corrupt each other's result.  The first call on a device looks up the
+ * array's device address, so make it before any stream capture.  Errors are
+ * reported by ms_last_error(NULL). */
+ms_status ms_build_atom_index_noalloc(const int* d_Z, const float* d_x, const float* d_y, const float* d_z,
+                                      int n, const float* box, float* d_atoms, int* d_offsets,
+                                      int offsets_capacity, int* nz_out, void* stream);
 
 #ifdef __cplusplus
 }
