@@ -79,14 +79,16 @@ def test_oracle_matches_reference(oracle_mod, path, tmp_path):
             key = f"trans_{i}"
             if key in g.files:
                 t = np.exp(1j * sc["sigma2"] * o.PotentialConventional(i))
-                assert rel_l2(g[key], t) < 2e-6, (i, rel_l2(g[key], t))
+                assert rel_l2(g[key], t) < 1e-7, (i, rel_l2(g[key], t))
             o.MultisliceStepConventional(i)
     e = rel_l2(g["wave"], o.Wave())
-    tol = 1e-4 if str(g["mode"]) == "fd" else 2e-5
+    # measured: TEM 2-3e-7, finite differences 5e-8, STEM probe 4e-6 (the probe's
+    # unnormalised inverse FFT and L1 sum run in FP32 in the reference)
+    tol = 1e-5 if "tds" in g.files else 2e-6
     assert e < tol, e
     if "tds" in g.files:
         o.AddTDSWaves()
-        assert rel_l2(g["tds"], o.TDS()) < 2e-5
+        assert rel_l2(g["tds"], o.TDS()) < 1e-5
     if "ew_minmax" in g.files:
         a = np.abs(o.Wave())
         assert abs(a.max() - g["ew_minmax"][1]) / a.max() < 1e-4

@@ -195,7 +195,7 @@ def test_stem_probe_cbed_and_haadf(engine_cls, oracle_mod, path):
     assert rel_l2(eng.TDS(), orc.TDS()) < TOL
     # a ring inside this grid's band limit (kmax ~ 2.5/A ~ 49 mrad at 300 kV)
     h_e, h_o = eng.AnnularDetector(10.0, 40.0), orc.AnnularDetector(10.0, 40.0)
-    assert h_o > 1e-3 and abs(h_e - h_o) / h_o < 1e-4
+    assert h_o > 1e-4 and abs(h_e - h_o) / h_o < 1e-4
     # a ring beyond the band limit collects nothing (FP32 rounding only)
     assert eng.AnnularDetector(70.0, 200.0) < 1e-12
 
