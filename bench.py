@@ -242,6 +242,7 @@ def main():
     configure(sim, atoms, FPARAMS)
     nsl = sim.BuildPotentialStack()
     assert nsl >= 100
+    fft_plan = sim.FFTPlan(1)
     steps_per = 100
     for _ in range(max(args.warmup, 3)):
         sim.TimeSlices(steps_per, 1, breakdown=False)
@@ -321,6 +322,7 @@ def main():
         "warmup": max(args.warmup, 3), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "c64 (FP32 complex)", "data": "synthetic (seeded)",
         "config": config_dict(len(Z)), "clocks": clk, "gpu_launches": launches,
+        "fft_plan": {"row_variant": fft_plan[0], "col_variant": fft_plan[1], "selected_by": "on-device autotuner"},
         "roofline": roofline,
         "plain_path": {"value": plain_value, "unit": UNIT, "speedup_fused_vs_plain": value / world / plain_value},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),

@@ -72,6 +72,7 @@ SIGNATURES = {
     "ms_copy_potential_slice": (_i, [_p, _i, _i, _p]),
     "ms_fft2": (_i, [_p, _p, _p, _i, _i, _i]),
     "ms_time_slices": (_i, [_p, _i, _i, _pf, _pf, _pf]),
+    "ms_get_fft_plan": (_i, [_p, _i, _pi, _pi]),
     "ms_get_launch_count": (_i, [_p, _pll]),
     "ms_build_atom_index_noalloc": (_i, [_p, _p, _p, _p, _i, _p, _p, _p, _i, _pi, _p]),
 }

@@ -145,6 +145,11 @@ class Engine {
         stack_valid_ = false;
         invalidate_graph();
         return MS_OK;
+      case MS_OPT_FFT_PLAN:
+        if (value < -1 || value >= plan_variants()) return fail(MS_ERR_INVALID, "FFT plan must be -1 (tuned) or a variant index");
+        forced_plan_ = value;
+        invalidate_graph();
+        return MS_OK;
       default:
         return fail(MS_ERR_INVALID, "unknown option");
     }
@@ -405,14 +410,17 @@ class Engine {
     if (cufftSetStream(plan_, stream_) != CUFFT_SUCCESS) return fail(MS_ERR_CUDA, "cufftSetStream failed");
     have_plan_ = true;
     fused_ok_ = fused_supported(nx, ny);
+    tuned_.clear();
     if (fused_ok_) {
-      std::vector<float2> tw(std::max(nx, ny));
-      MS_TRY(d_twx_.resize(nx));
-      MS_TRY(d_twy_.resize(ny));
-      make_twiddles(nx, tw.data());
-      MS_TRY(cudaMemcpy(d_twx_.p, tw.data(), sizeof(float2) * nx, cudaMemcpyHostToDevice));
-      make_twiddles(ny, tw.data());
-      MS_TRY(cudaMemcpy(d_twy_.p, tw.data(), sizeof(float2) * ny, cudaMemcpyHostToDevice));
+      std::vector<float2> tw(2 * (size_t)std::max(nx, ny));
+      for (int v = 0; v < plan_variants(); ++v) {
+        const int sx = make_twiddles(nx, v, tw.data());
+        MS_TRY(d_twx_[v].resize(std::max(sx, 1)));
+        MS_TRY(cudaMemcpy(d_twx_[v].p, tw.data(), sizeof(float2) * sx, cudaMemcpyHostToDevice));
+        const int sy = make_twiddles(ny, v, tw.data());
+        MS_TRY(d_twy_[v].resize(std::max(sy, 1)));
+        MS_TRY(cudaMemcpy(d_twy_[v].p, tw.data(), sizeof(float2) * sy, cudaMemcpyHostToDevice));
+      }
     }
     prop_dz_ = -1.0f;
     have_freq_ = true;
@@ -589,18 +597,18 @@ class Engine {
     if (!have_tds_) return fail(MS_ERR_STATE, "TDS buffer not allocated (ms_alloc_tds)");
     const Grid2 g{nx_, ny_};
     if (use_fused() && domain_ == 1) {
-      PassBArgs b = passb_args(d_psi_.p, d_psi_.p);
+      PassBArgs b = passb_args(d_psi_.p, d_psi_.p, 0);
       b.acc = d_tds_.p;
       b.scale = (float)nx_;  // FFT_rows(psi) = nx * X for the row-frequency state X
-      MS_TRY(launch_pass_b(b, B_CBED, 1, stream_));
+      MS_TRY(pass_b(b, B_CBED, 1));
       ++launches;
     } else if (use_fused()) {
-      PassAArgs a = passa_args(d_psi_.p, d_t1_.p);
-      MS_TRY(launch_pass_a(a, A_FWD, 1, stream_));
-      PassBArgs b = passb_args(d_t1_.p, d_t1_.p);
+      PassAArgs a = passa_args(d_psi_.p, d_t1_.p, 0);
+      MS_TRY(pass_a(a, A_FWD, 1));
+      PassBArgs b = passb_args(d_t1_.p, d_t1_.p, 0);
       b.acc = d_tds_.p;
       b.scale = 1.0f;
-      MS_TRY(launch_pass_b(b, B_CBED, 1, stream_));
+      MS_TRY(pass_b(b, B_CBED, 1));
       launches += 2;
     } else {
       MS_TRY_FFT(cufftExecC2C(plan_, d_psi_.p, d_t1_.p, CUFFT_FORWARD));
@@ -667,22 +675,22 @@ class Engine {
       float2* src = d_psi_.p;
       float scale = 1.0f / (float)N;
       if (domain_ == 0) {
-        PassAArgs a = passa_args(d_psi_.p, d_t1_.p);
-        MS_TRY(launch_pass_a(a, A_FWD, 1, stream_));
+        PassAArgs a = passa_args(d_psi_.p, d_t1_.p, 0);
+        MS_TRY(pass_a(a, A_FWD, 1));
         ++launches;
         src = d_t1_.p;
       } else {
         scale = (float)nx_ / (float)N;  // FFT_rows(psi) = nx * X
       }
-      b = passb_args(src, d_t2_.p);
+      b = passb_args(src, d_t2_.p, 0);
       b.ctf = CtfParams{(double)wavel, (double)Cs_, (double)df_, (double)A2_, (double)phi2_, 0.0, 0.0, beta,
                         (double)delta_, objap2};
       b.scale = scale;
-      MS_TRY(launch_pass_b(b, B_CTF, 1, stream_));
-      PassAArgs a = passa_args(d_t2_.p, nullptr);
+      MS_TRY(pass_b(b, B_CTF, 1));
+      PassAArgs a = passa_args(d_t2_.p, nullptr, 0);
       a.out_f = d_f_.p;
       a.scale = 1.0f;
-      MS_TRY(launch_pass_a(a, A_INV | A_INTENSITY, 1, stream_));
+      MS_TRY(pass_a(a, A_INV | A_INTENSITY, 1));
       launches += 2;
     } else {
       if (int rc = ensure_real()) return rc;
@@ -800,30 +808,30 @@ class Engine {
       MS_TRY(cudaMemsetAsync(d_bsig_.p, 0, sizeof(double) * B, stream_));
       MS_TRY(pw_probe_batch(d_bwave_.p, N, nb, d_kx_.p, d_ky_.p, d_bpos_.p, d_bpos_.p + B, apert, ps_, df_, Cs_,
                             wavel_, g, stream_, &launches));
-      PassBArgs bi = passb_args(d_bwave_.p, d_bwave_.p);
+      PassBArgs bi = passb_args(d_bwave_.p, d_bwave_.p, 0);
       bi.batch_stride_wave = N;
-      MS_TRY(launch_pass_b(bi, B_INV_ONLY, nb, stream_));
-      PassAArgs ai = passa_args(d_bwave_.p, d_bwave_.p);
+      MS_TRY(pass_b(bi, B_INV_ONLY, nb));
+      PassAArgs ai = passa_args(d_bwave_.p, d_bwave_.p, 0);
       ai.batch_stride_wave = N;
-      MS_TRY(launch_pass_a(ai, A_INV, nb, stream_));
+      MS_TRY(pass_a(ai, A_INV, nb));
       launches += 2;
       MS_TRY(pw_sum_abs_batch(d_bwave_.p, N, N, nb, d_bpart_.p, d_bsig_.p + B, stream_, &launches));
       for (int it = 1; it <= S; ++it) {
-        PassAArgs a = passa_args(d_bwave_.p, d_bwave_.p);
+        PassAArgs a = passa_args(d_bwave_.p, d_bwave_.p, 0);
         a.batch_stride_wave = N;
         a.batch_stride_V = 0;
         a.V = d_stack_.p + (size_t)(it - 1) * N;
-        MS_TRY(launch_pass_a(a, it == 1 ? (A_MULT_T | A_FWD) : (A_INV | A_MULT_T | A_FWD), nb, stream_));
-        PassBArgs b = passb_args(d_bwave_.p, d_bwave_.p);
+        MS_TRY(pass_a(a, it == 1 ? (A_MULT_T | A_FWD) : (A_INV | A_MULT_T | A_FWD), nb));
+        PassBArgs b = passb_args(d_bwave_.p, d_bwave_.p, 0);
         b.batch_stride_wave = N;
         if (it < S) {
-          MS_TRY(launch_pass_b(b, B_PROPAGATE, nb, stream_));
+          MS_TRY(pass_b(b, B_PROPAGATE, nb));
         } else {
           b.sig = d_bsig_.p;
           b.kin2 = kin * kin;
           b.kout2 = kout * kout;
           b.scale = 1.0f / (float)N;
-          MS_TRY(launch_pass_b(b, B_DETECT, nb, stream_));
+          MS_TRY(pass_b(b, B_DETECT, nb));
         }
         launches += 2;
       }
@@ -865,6 +873,7 @@ class Engine {
     if (int rc = build_stack(&S)) return rc;
     if (int rc = ensure_prop_tables(convdz_)) return rc;
     if (use_fused()) {
+      plan_for(1);  // tune outside the capture (tuning allocates and synchronises)
       if (!graph_exec_ || graph_S_ != S) {
         invalidate_graph();
         MS_TRY(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
@@ -924,11 +933,11 @@ class Engine {
       if (rc == MS_OK) {
         cudaEventRecord(ev[0], stream_);
         for (int k = 0; k < steps && rc == MS_OK; ++k) {
-          PassAArgs a = passa_args(k == 0 ? d_psi0_.p : d_psi_.p, d_psi_.p);
+          PassAArgs a = passa_args(k == 0 ? d_psi0_.p : d_psi_.p, d_psi_.p, 0);
           a.V = d_stack_.p + (size_t)(k % S) * N;
-          cudaError_t e1 = launch_pass_a(a, k == 0 ? (A_MULT_T | A_FWD) : (A_INV | A_MULT_T | A_FWD), 1, stream_);
+          cudaError_t e1 = pass_a(a, k == 0 ? (A_MULT_T | A_FWD) : (A_INV | A_MULT_T | A_FWD), 1);
           cudaEventRecord(ev[2 * k + 1], stream_);
-          cudaError_t e2 = launch_pass_b(passb_args(d_psi_.p, d_psi_.p), B_PROPAGATE, 1, stream_);
+          cudaError_t e2 = pass_b(passb_args(d_psi_.p, d_psi_.p, 0), B_PROPAGATE, 1);
           cudaEventRecord(ev[2 * k + 2], stream_);
           if (e1 != cudaSuccess || e2 != cudaSuccess) rc = cuda_fail(e1 != cudaSuccess ? e1 : e2, "timed pass launch");
         }
@@ -956,22 +965,23 @@ class Engine {
   int fft2_host(const float* in, float* out, int nx, int ny, int sign) {
     if (!fused_supported(nx, ny)) return fail(MS_ERR_UNSUPPORTED, "grid not supported by the fused FFT passes");
     const size_t N = (size_t)nx * ny;
+    const int v = forced_plan_ >= 0 ? forced_plan_ : 0;
     DevBuf<float2> buf, tw1, tw2;
     MS_TRY(buf.resize(N));
-    MS_TRY(tw1.resize(nx));
-    MS_TRY(tw2.resize(ny));
-    std::vector<float2> tw(std::max(nx, ny));
-    make_twiddles(nx, tw.data());
-    MS_TRY(cudaMemcpy(tw1.p, tw.data(), sizeof(float2) * nx, cudaMemcpyHostToDevice));
-    make_twiddles(ny, tw.data());
-    MS_TRY(cudaMemcpy(tw2.p, tw.data(), sizeof(float2) * ny, cudaMemcpyHostToDevice));
+    std::vector<float2> tw(2 * (size_t)std::max(nx, ny));
+    const int sx = make_twiddles(nx, v, tw.data());
+    MS_TRY(tw1.resize(std::max(sx, 1)));
+    MS_TRY(cudaMemcpy(tw1.p, tw.data(), sizeof(float2) * sx, cudaMemcpyHostToDevice));
+    const int sy = make_twiddles(ny, v, tw.data());
+    MS_TRY(tw2.resize(std::max(sy, 1)));
+    MS_TRY(cudaMemcpy(tw2.p, tw.data(), sizeof(float2) * sy, cudaMemcpyHostToDevice));
     MS_TRY(cudaMemcpy(buf.p, in, sizeof(float2) * N, cudaMemcpyHostToDevice));
     PassAArgs a{};
     a.in = buf.p; a.out = buf.p; a.tw = tw1.p; a.nx = nx; a.ny = ny; a.scale = 1.0f;
     PassBArgs b{};
     b.in = buf.p; b.out = buf.p; b.tw = tw2.p; b.nx = nx; b.ny = ny; b.scale = 1.0f;
-    MS_TRY(launch_pass_a(a, sign < 0 ? A_FWD : A_INV, 1, stream_));
-    MS_TRY(launch_pass_b(b, sign < 0 ? B_FWD_ONLY : B_INV_ONLY, 1, stream_));
+    MS_TRY(launch_pass_a(a, v, sign < 0 ? A_FWD : A_INV, 1, stream_));
+    MS_TRY(launch_pass_b(b, v, sign < 0 ? B_FWD_ONLY : B_INV_ONLY, 1, stream_));
     launches += 2;
     MS_TRY(cudaMemcpyAsync(out, buf.p, sizeof(float2) * N, cudaMemcpyDeviceToHost, stream_));
     MS_TRY(cudaStreamSynchronize(stream_));
@@ -979,6 +989,16 @@ class Engine {
   }
 
   // ---- inspection ----
+  int fft_plan(int batch, int* row, int* col) {
+    if (!have_freq_) return fail(MS_ERR_STATE, "frequencies not precalculated");
+    if (!use_fused()) return fail(MS_ERR_UNSUPPORTED, "grid not handled by the fused passes");
+    if (batch < 1) return fail(MS_ERR_INVALID, "batch must be >= 1");
+    const PlanChoice c = plan_for(batch);
+    *row = c.row;
+    *col = c.col;
+    return MS_OK;
+  }
+
   int binned_counts(int* n, int* nz) {
     if (!have_index_) return fail(MS_ERR_STATE, "atoms not binned");
     *n = natoms_;
@@ -1105,17 +1125,92 @@ class Engine {
     return MS_OK;
   }
 
-  PassAArgs passa_args(const float2* in, float2* out) {
+  // FFT plan variants of the row and column passes for a batch size: forced
+  // by MS_OPT_FFT_PLAN, else the autotuned choice (timed once per batch size).
+  struct PlanChoice {
+    int row = 0, col = 0;
+  };
+  PlanChoice plan_for(int batch) {
+    if (forced_plan_ >= 0) return PlanChoice{forced_plan_, forced_plan_};
+    const int key = batch <= 1 ? 1 : (batch < 8 ? 4 : 16);
+    for (auto& kv : tuned_)
+      if (kv.first == key) return kv.second;
+    PlanChoice c = autotune(key);
+    tuned_.push_back({key, c});
+    return c;
+  }
+
+  // Times every plan variant of the steady-state row pass and the propagating
+  // column pass on scratch waves (batch instances), on this device, and keeps
+  // the fastest.  Scratch is zero-filled so the transmission's sincos stays on
+  // its fast path.  On any launch failure the variant is skipped.
+  PlanChoice autotune(int batch) {
+    PlanChoice best;
+    const long long N = (long long)nx_ * ny_;
+    DevBuf<float2> w;
+    DevBuf<float> V;
+    if (w.resize((size_t)batch * N) != cudaSuccess || V.resize((size_t)N) != cudaSuccess) return best;
+    cudaMemsetAsync(w.p, 0, sizeof(float2) * batch * N, stream_);
+    cudaMemsetAsync(V.p, 0, sizeof(float) * N, stream_);
+    if (ensure_prop_tables(convdz_) != MS_OK) return best;
+    float best_a = INFINITY, best_b = INFINITY;
+    const int reps = 8;
+    for (int v = 0; v < plan_variants(); ++v) {
+      PassAArgs a = passa_args(w.p, w.p, v);
+      a.V = V.p;
+      a.batch_stride_wave = N;
+      a.batch_stride_V = 0;
+      PassBArgs b = passb_args(w.p, w.p, v);
+      b.batch_stride_wave = N;
+      bool ok = true;
+      for (int k = 0; k < 2 && ok; ++k)  // first launches load the kernels
+        ok = launch_pass_a(a, v, A_INV | A_MULT_T | A_FWD, batch, stream_) == cudaSuccess &&
+             launch_pass_b(b, v, B_PROPAGATE, batch, stream_) == cudaSuccess;
+      if (!ok || cudaStreamSynchronize(stream_) != cudaSuccess) {
+        cudaGetLastError();
+        continue;
+      }
+      float ta = 0, tb = 0;
+      cudaEventRecord(ev0_, stream_);
+      for (int k = 0; k < reps; ++k) launch_pass_a(a, v, A_INV | A_MULT_T | A_FWD, batch, stream_);
+      cudaEventRecord(ev1_, stream_);
+      cudaEventSynchronize(ev1_);
+      cudaEventElapsedTime(&ta, ev0_, ev1_);
+      cudaEventRecord(ev0_, stream_);
+      for (int k = 0; k < reps; ++k) launch_pass_b(b, v, B_PROPAGATE, batch, stream_);
+      cudaEventRecord(ev1_, stream_);
+      cudaEventSynchronize(ev1_);
+      cudaEventElapsedTime(&tb, ev0_, ev1_);
+      launches += 2LL * (reps + 2);
+      if (ta < best_a) { best_a = ta; best.row = v; }
+      if (tb < best_b) { best_b = tb; best.col = v; }
+    }
+    cudaStreamSynchronize(stream_);
+    return best;
+  }
+
+  PassAArgs passa_args(const float2* in, float2* out, int variant) {
     PassAArgs a{};
-    a.in = in; a.out = out; a.tw = d_twx_.p; a.nx = nx_; a.ny = ny_;
+    a.in = in; a.out = out; a.tw = d_twx_[variant].p; a.nx = nx_; a.ny = ny_;
     a.sigma = sigma2_; a.scale = 1.0f;
     return a;
   }
-  PassBArgs passb_args(const float2* in, float2* out) {
+  PassBArgs passb_args(const float2* in, float2* out, int variant) {
     PassBArgs b{};
-    b.in = in; b.out = out; b.tw = d_twy_.p; b.px = d_px_.p; b.py = d_py_.p;
+    b.in = in; b.out = out; b.tw = d_twy_[variant].p; b.px = d_px_.p; b.py = d_py_.p;
     b.kx = d_kx_.p; b.ky = d_ky_.p; b.kmax = kmax_; b.nx = nx_; b.ny = ny_; b.scale = 1.0f;
     return b;
+  }
+  // Row / column pass launchers with the plan tuned for `batch` instances.
+  cudaError_t pass_a(PassAArgs a, int flags, int batch = 1) {
+    const int v = plan_for(batch).row;
+    a.tw = d_twx_[v].p;
+    return launch_pass_a(a, v, flags, batch, stream_);
+  }
+  cudaError_t pass_b(PassBArgs b, int mode, int batch = 1) {
+    const int v = plan_for(batch).col;
+    b.tw = d_twy_[v].p;
+    return launch_pass_b(b, v, mode, batch, stream_);
   }
 
   // Enqueue one fused conventional step on the stream (no host sync, no
@@ -1124,11 +1219,11 @@ class Engine {
   int enqueue_fused_step(const float* V, bool first) {
     // iteration 1 starts from the initial wave (real space); later ones from
     // the current wave in whichever domain it is held
-    PassAArgs a = passa_args(first ? d_psi0_.p : d_psi_.p, d_psi_.p);
+    PassAArgs a = passa_args(first ? d_psi0_.p : d_psi_.p, d_psi_.p, 0);
     a.V = V;
     const int fl = (first || domain_ == 0) ? (A_MULT_T | A_FWD) : (A_INV | A_MULT_T | A_FWD);
-    MS_TRY(launch_pass_a(a, fl, 1, stream_));
-    MS_TRY(launch_pass_b(passb_args(d_psi_.p, d_psi_.p), B_PROPAGATE, 1, stream_));
+    MS_TRY(pass_a(a, fl, 1));
+    MS_TRY(pass_b(passb_args(d_psi_.p, d_psi_.p, 0), B_PROPAGATE, 1));
     domain_ = 1;
     return MS_OK;
   }
@@ -1157,8 +1252,8 @@ class Engine {
 
   int ensure_real() {
     if (domain_ == 0) return MS_OK;
-    PassAArgs a = passa_args(d_psi_.p, d_psi_.p);
-    MS_TRY(launch_pass_a(a, A_INV, 1, stream_));
+    PassAArgs a = passa_args(d_psi_.p, d_psi_.p, 0);
+    MS_TRY(pass_a(a, A_INV, 1));
     ++launches;
     domain_ = 0;
     return MS_OK;
@@ -1259,7 +1354,9 @@ class Engine {
   bool stem_ = false, have_calc_ = false, have_freq_ = false, fd_stable_ = false, fused_ok_ = false;
   std::vector<float> hkx_, hky_;
   DevBuf<float> d_kx_, d_ky_;
-  DevBuf<float2> d_twx_, d_twy_, d_px_, d_py_, d_P_;
+  DevBuf<float2> d_twx_[3], d_twy_[3], d_px_, d_py_, d_P_;
+  int forced_plan_ = -1;
+  std::vector<std::pair<int, PlanChoice>> tuned_;
   float prop_dz_ = -1.0f;
   cufftHandle plan_ = 0;
   bool have_plan_ = false;
@@ -1593,6 +1690,10 @@ ms_status ms_fft2(ms_sim* s, const float* in, float* out, int nx, int ny, int si
 ms_status ms_time_slices(ms_sim* s, int steps, int reps, float* total, float* row, float* col) {
   if (!total) return s && s->e ? s->e->fail(MS_ERR_INVALID, "null output") : MS_ERR_INVALID;
   return guarded(s, [&](ms::Engine& e) { return e.time_slices(steps, reps, total, row, col); });
+}
+ms_status ms_get_fft_plan(ms_sim* s, int batch, int* row, int* col) {
+  if (!row || !col) return s && s->e ? s->e->fail(MS_ERR_INVALID, "null output") : MS_ERR_INVALID;
+  return guarded(s, [&](ms::Engine& e) { return e.fft_plan(batch, row, col); });
 }
 ms_status ms_get_launch_count(ms_sim* s, long long* out) {
   if (ms_status r = out_check(s, out)) return r;

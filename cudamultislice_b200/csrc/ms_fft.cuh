@@ -1,19 +1,20 @@
 // ms_fft.cuh -- register/shared-memory Stockham FFT of one line (row or column).
 //
-// A line of N = E * P complex points is owned by P consecutive threads of one
-// warp (P <= 32); thread t holds element t + P*j in register j ("strided natural
-// layout"), which makes global loads and stores of a line fully coalesced.
-// The transform is two Stockham radix passes, N = E * P:
-//   pass 1: radix-E butterfly entirely in registers (butterfly i = t);
-//   exchange through the line's shared-memory slot (padded one point every E
-//   so that the stride-E writes hit 32 distinct banks);
-//   pass 2: E radix-P butterflies (E/P per thread) with twiddles W_N^{r*i}
-//   read from a per-size table laid out [r][i] (coalesced, L1-resident); its
-//   outputs land back in the strided natural layout, so the next pointwise
-//   operation (transmission, propagator) needs no reordering.
-// The in-register butterflies are radix-2 decimation-in-frequency networks
+// A line of N = E * P complex points is owned by P threads (P <= 32: part of
+// one warp; P = 64, 128, 256: whole warps of one CTA).  Thread t holds element
+// t + P*j in register j ("strided natural layout"), which makes global loads
+// and stores of a line fully coalesced.  The transform is a sequence of
+// Stockham radix passes N = R1 * R2 * ... (each radix divides E):
+//   pass 1: E/R1 radix-R1 butterflies on registers (no twiddles);
+//   middle passes: inputs read from the line's shared slot, twiddles
+//     W_{Ns R}^{r k} read from a per-pass [r][k] table (coalesced, L1-resident),
+//     outputs written back in Stockham order;
+//   last pass: outputs land in the strided natural layout, so the pointwise
+//     operation that follows (transmission, propagator) needs no reordering.
+// The slot is padded by one point every R1 points so the stride-R1 writes of
+// pass 1 hit distinct banks.  In-register butterflies are radix-2 DIF networks
 // with compile-time twiddle constants; trivial twiddles cost no multiply.
-// Forward = exp(-2 pi i jk/N) (cuFFT CUFFT_FORWARD), both directions unnormalised.
+// Forward = exp(-2 pi i jk/N) (cuFFT CUFFT_FORWARD); both directions unnormalised.
 #pragma once
 #include "ms_common.cuh"
 
@@ -87,60 +88,126 @@ MS_D void dft(float2 (&x)[R]) {
   if constexpr (R > 1) Dif<R, R / 2, INV>::run(x);
 }
 
-// Split of a line length into registers per thread (E) and threads per line (P).
-template <int N>
-struct Plan;
-template <> struct Plan<64>   { static constexpr int E = 8,  P = 8;  };
-template <> struct Plan<128>  { static constexpr int E = 16, P = 8;  };
-template <> struct Plan<256>  { static constexpr int E = 16, P = 16; };
-template <> struct Plan<512>  { static constexpr int E = 32, P = 16; };
-template <> struct Plan<1024> { static constexpr int E = 32, P = 32; };
+// A factorisation N = R1 * R2 * R3 * R4 (trailing radices 1 = absent) with E
+// points per thread; every radix divides E and is at most 32.
+template <int N_, int E_, int R1_, int R2_, int R3_ = 1, int R4_ = 1>
+struct Plan {
+  static constexpr int N = N_, E = E_, P = N_ / E_;
+  static constexpr int R1 = R1_, R2 = R2_, R3 = R3_, R4 = R4_;
+  static constexpr int NPASS = 1 + (R2_ > 1) + (R3_ > 1) + (R4_ > 1);
+  static_assert(R1_ * R2_ * R3_ * R4_ == N_, "radices must multiply to N");
+  static_assert(E_ % R1_ == 0 && E_ % R2_ == 0 && E_ % R3_ == 0 && E_ % R4_ == 0, "radix must divide E");
+  static_assert(R1_ <= 32 && R2_ <= 32 && R3_ <= 32 && R4_ <= 32, "radix above 32");
+  static_assert(P <= 32 || P % 32 == 0, "multi-warp lines need whole warps");
+  // Points in one line slot (one pad point every R1, slots 8 apart mod 16).
+  static constexpr int SLOT = ((N_ + N_ / R1_ + 15) / 16) * 16 + 8;
+  // Twiddle table: pass p >= 2 holds R_p * Ns_p entries [r][k].
+  // (absent passes, radix 1, take no entries; the sum never exceeds 2N)
+  static constexpr int TW2 = 0, TW3 = TW2 + R2_ * R1_, TW4 = TW3 + (R3_ > 1 ? R3_ * R1_ * R2_ : 0);
+  static constexpr int TWSIZE = TW4 + (R4_ > 1 ? R4_ * R1_ * R2_ * R3_ : 0);
+  static_assert(TWSIZE <= 2 * N_, "twiddle table larger than 2N");
+};
 
-// Shared-memory footprint of one line: N points plus one pad point every E,
-// rounded so that consecutive lines start 8 points (mod 16) apart, which keeps
-// two lines read by one 16-lane phase on disjoint banks.
-template <int N>
-MS_HD constexpr int line_stride() {
-  constexpr int E = Plan<N>::E;
-  constexpr int raw = N + N / E;
-  return ((raw + 15) / 16) * 16 + 8;
+template <class PL>
+MS_D int padi(int n) {
+  return n + n / PL::R1;
 }
-template <int N>
-MS_D int padi(int n) { return n + n / Plan<N>::E; }
+
+template <class PL>
+MS_D void line_sync() {
+  if constexpr (PL::P <= 32)
+    __syncwarp();
+  else
+    __syncthreads();
+}
+
+// Radix R of pass number IDX (0-based).
+template <class PL, int IDX>
+struct PassR {
+  static constexpr int R = IDX == 0 ? PL::R1 : IDX == 1 ? PL::R2 : IDX == 2 ? PL::R3 : PL::R4;
+  static constexpr int NS = IDX == 0 ? 1 : IDX == 1 ? PL::R1 : IDX == 2 ? PL::R1 * PL::R2 : PL::R1 * PL::R2 * PL::R3;
+  static constexpr int TW = IDX == 1 ? PL::TW2 : IDX == 2 ? PL::TW3 : PL::TW4;
+};
+
+template <class PL, int IDX, bool INV>
+MS_D void middle_or_last(float2 (&v)[PL::E], float2* __restrict__ sm, int t, const float2* __restrict__ tw) {
+  constexpr int N = PL::N, E = PL::E, P = PL::P;
+  constexpr int R = PassR<PL, IDX>::R, NS = PassR<PL, IDX>::NS, TWO = PassR<PL, IDX>::TW, LR = ilog2(R);
+  constexpr bool LAST = (IDX == PL::NPASS - 1);
+  if constexpr (LAST) {
+#pragma unroll
+    for (int b = 0; b < E / R; ++b) {
+      const int i = t + P * b;  // i < N/R = NS, so k = i
+      float2 x[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) x[r] = sm[padi<PL>(i + r * (N / R))];
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        float2 w = __ldg(tw + TWO + r * NS + i);
+        if (INV) w.y = -w.y;
+        x[r] = cmul(x[r], w);
+      }
+      dft<R, INV>(x);
+#pragma unroll
+      for (int q = 0; q < R; ++q) v[b + q * (E / R)] = x[brev(q, LR)];
+    }
+    line_sync<PL>();
+  } else {
+    // read every input of this thread's butterflies, then overwrite the slot
+#pragma unroll
+    for (int b = 0; b < E / R; ++b) {
+      const int i = t + P * b;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[b * R + r] = sm[padi<PL>(i + r * (N / R))];
+    }
+    line_sync<PL>();
+#pragma unroll
+    for (int b = 0; b < E / R; ++b) {
+      const int i = t + P * b;
+      const int k = i & (NS - 1);
+      float2 x[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) x[r] = v[b * R + r];
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        float2 w = __ldg(tw + TWO + r * NS + k);
+        if (INV) w.y = -w.y;
+        x[r] = cmul(x[r], w);
+      }
+      dft<R, INV>(x);
+      const int base = (i / NS) * NS * R + k;
+#pragma unroll
+      for (int q = 0; q < R; ++q) sm[padi<PL>(base + q * NS)] = x[brev(q, LR)];
+    }
+    line_sync<PL>();
+    middle_or_last<PL, IDX + 1, INV>(v, sm, t, tw);
+  }
+}
 
 // One N-point transform of the line held by threads t = 0..P-1 of a group.
-// `sm` is this line's shared slot (line_stride<N>() points), `tw` the
-// [r][i] twiddle table of size N (forward values; conjugated for INV).
-// Every thread of the warp must call this (it issues __syncwarp()).
-template <int N, bool INV>
-MS_D void line_fft(float2 (&v)[Plan<N>::E], float2* __restrict__ sm, int t,
-                   const float2* __restrict__ tw) {
-  constexpr int E = Plan<N>::E, P = Plan<N>::P, LE = ilog2(E), LP = ilog2(P);
-  static_assert(E * P == N && E % P == 0, "bad plan");
-  // pass 1: radix-E on registers (Ns = 1, no twiddles)
-  dft<E, INV>(v);
+// `sm` is this line's shared slot (PL::SLOT points), `tw` the plan's twiddle
+// table (forward values; conjugated for INV).  Every thread of the warp (or,
+// for P > 32, of the CTA) must call this: it synchronises.
+template <class PL, bool INV>
+MS_D void line_fft(float2 (&v)[PL::E], float2* __restrict__ sm, int t, const float2* __restrict__ tw) {
+  constexpr int E = PL::E, P = PL::P, R1 = PL::R1, L1 = ilog2(R1);
 #pragma unroll
-  for (int q = 0; q < E; ++q) sm[padi<N>(t * E + q)] = v[brev(q, LE)];
-  __syncwarp();
-  // pass 2: E radix-P butterflies, E/P per thread, then back to registers
+  for (int b = 0; b < E / R1; ++b) {
+    float2 x[R1];
 #pragma unroll
-  for (int b = 0; b < E / P; ++b) {
+    for (int r = 0; r < R1; ++r) x[r] = v[b + r * (E / R1)];
+    dft<R1, INV>(x);
     const int i = t + P * b;
-    float2 x[P];
 #pragma unroll
-    for (int r = 0; r < P; ++r) x[r] = sm[padi<N>(i + r * E)];
-#pragma unroll
-    for (int r = 1; r < P; ++r) {
-      float2 w = __ldg(tw + r * E + i);
-      if (INV) w.y = -w.y;
-      x[r] = cmul(x[r], w);
-    }
-    dft<P, INV>(x);
-#pragma unroll
-    for (int q = 0; q < P; ++q) v[b + q * (E / P)] = x[brev(q, LP)];
+    for (int q = 0; q < R1; ++q) sm[padi<PL>(i * R1 + q)] = x[brev(q, L1)];
   }
-  __syncwarp();
+  line_sync<PL>();
+  middle_or_last<PL, 1, INV>(v, sm, t, tw);
 }
+
+// Host-side twiddle table of a plan: pass p >= 2 entries W_{Ns R}^{r k},
+// r < R_p, k < Ns_p, laid out [r][k] after the previous pass's table.
+void make_plan_twiddles(int n, const int* radices, int npass, float2* out);
 
 }  // namespace fft
 }  // namespace ms

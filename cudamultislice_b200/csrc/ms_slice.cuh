@@ -10,6 +10,9 @@
 // wave once (8 MB at 1024^2: L2-resident on B200) and pass A streams V.
 #pragma once
 #include <cuda_runtime.h>
+
+#include <type_traits>
+
 #include "ms_common.cuh"
 
 namespace ms {
@@ -60,10 +63,14 @@ struct PassBArgs {
   long long batch_stride_wave;
 };
 
+// Line lengths 64..2048 (powers of two) in both directions.
 bool fused_supported(int nx, int ny);
-cudaError_t launch_pass_a(const PassAArgs& a, int flags, int batch, cudaStream_t s);
-cudaError_t launch_pass_b(const PassBArgs& a, int mode, int batch, cudaStream_t s);
-// forward twiddle table W_N^{r*i}, r < P, i < E, as [r][i]
-void make_twiddles(int n, float2* host_out);
+// Number of FFT plan variants per line length (autotuned by the engine).
+int plan_variants();
+// Twiddle table of plan `variant` for lines of n points into host_out
+// (at most 2n entries); returns its length.
+int make_twiddles(int n, int variant, float2* host_out);
+cudaError_t launch_pass_a(const PassAArgs& a, int variant, int flags, int batch, cudaStream_t s);
+cudaError_t launch_pass_b(const PassBArgs& a, int variant, int mode, int batch, cudaStream_t s);
 
 }  // namespace ms

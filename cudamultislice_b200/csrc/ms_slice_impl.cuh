@@ -1,0 +1,305 @@
+// ms_slice_impl.cuh -- templates of the fused slice passes, instantiated per
+// line length in ms_slice_n*.cu (see ms_slice.cuh for the scheme).
+#pragma once
+#include <cmath>
+
+#include "ms_ctf.cuh"
+#include "ms_fft.cuh"
+#include "ms_slice.cuh"
+
+namespace ms {
+
+// FFT plan variants per line length (chosen at run time by the autotuner):
+// variant 0 keeps the most points per thread (fewest exchanges), higher
+// variants spread a line over more threads (more warps in flight).
+template <int N, int V>
+struct PlanSel;
+template <> struct PlanSel<64, 0>   { using T = fft::Plan<64, 8, 8, 8>; };
+template <> struct PlanSel<64, 1>   { using T = fft::Plan<64, 4, 4, 4, 4>; };
+template <> struct PlanSel<64, 2>   { using T = fft::Plan<64, 4, 4, 4, 4>; };
+template <> struct PlanSel<128, 0>  { using T = fft::Plan<128, 16, 16, 8>; };
+template <> struct PlanSel<128, 1>  { using T = fft::Plan<128, 8, 8, 4, 4>; };
+template <> struct PlanSel<128, 2>  { using T = fft::Plan<128, 4, 4, 4, 4, 2>; };
+template <> struct PlanSel<256, 0>  { using T = fft::Plan<256, 16, 16, 16>; };
+template <> struct PlanSel<256, 1>  { using T = fft::Plan<256, 8, 8, 8, 4>; };
+template <> struct PlanSel<256, 2>  { using T = fft::Plan<256, 4, 4, 4, 4, 4>; };
+template <> struct PlanSel<512, 0>  { using T = fft::Plan<512, 32, 32, 16>; };
+template <> struct PlanSel<512, 1>  { using T = fft::Plan<512, 16, 16, 8, 4>; };
+template <> struct PlanSel<512, 2>  { using T = fft::Plan<512, 8, 8, 8, 8>; };
+template <> struct PlanSel<1024, 0> { using T = fft::Plan<1024, 32, 32, 32>; };
+template <> struct PlanSel<1024, 1> { using T = fft::Plan<1024, 16, 16, 16, 4>; };
+template <> struct PlanSel<1024, 2> { using T = fft::Plan<1024, 8, 8, 8, 8, 2>; };
+template <> struct PlanSel<2048, 0> { using T = fft::Plan<2048, 32, 32, 8, 8>; };
+template <> struct PlanSel<2048, 1> { using T = fft::Plan<2048, 16, 16, 16, 8>; };
+template <> struct PlanSel<2048, 2> { using T = fft::Plan<2048, 8, 8, 8, 8, 4>; };
+
+constexpr int kPlanVariants = 3;
+
+// Threads per CTA: rows, 256 (whole lines); columns, at least 4 columns per
+// CTA so the transposing tile access moves whole 32-byte sectors.
+template <class PL>
+__host__ __device__ constexpr int rows_per_cta() { return PL::P >= 256 ? 1 : 256 / PL::P; }
+template <class PL>
+__host__ __device__ constexpr int cols_per_cta() { return PL::P >= 64 ? 4 : 256 / PL::P; }
+// Column slots 2 points (mod 16) apart: the transposing tile load (8 columns x
+// 2 rows per 16-lane phase) is then free of bank conflicts.
+template <class PL>
+__host__ __device__ constexpr int col_slot() { return ((PL::N + PL::N / PL::R1 + 15) / 16) * 16 + 2; }
+
+template <class PL, int FLAGS>
+__global__ void __launch_bounds__(rows_per_cta<PL>() * PL::P) k_pass_a(PassAArgs a) {
+  constexpr int NX = PL::N, E = PL::E, P = PL::P, LS = PL::SLOT;
+  extern __shared__ float2 smem[];
+  const int g = threadIdx.x / P, t = threadIdx.x % P;
+  const int line = blockIdx.x * rows_per_cta<PL>() + g;
+  float2* sm = smem + g * LS;
+  const long long inst = blockIdx.y;
+  const long long row0 = inst * a.batch_stride_wave + (long long)line * NX;
+
+  float2 v[E];
+  const float2* in = a.in + row0;
+#pragma unroll
+  for (int j = 0; j < E; ++j) v[j] = in[t + P * j];
+
+  if constexpr ((FLAGS & A_INV) != 0) fft::line_fft<PL, true>(v, sm, t, a.tw);
+  if constexpr ((FLAGS & A_MULT_T) != 0) {
+    const float* V = a.V + inst * a.batch_stride_V + (long long)line * NX;
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      float s, c;
+      sincosf(fmul_x(a.sigma, V[t + P * j]), &s, &c);
+      v[j] = cmul(v[j], make_float2(c, s));
+    }
+  }
+  if constexpr ((FLAGS & A_FWD) != 0) fft::line_fft<PL, false>(v, sm, t, a.tw);
+
+  if constexpr ((FLAGS & A_INTENSITY) != 0) {
+    float* o = a.out_f + row0;
+#pragma unroll
+    for (int j = 0; j < E; ++j) o[t + P * j] = (v[j].x * v[j].x + v[j].y * v[j].y) * a.scale;
+  } else {
+    float2* o = a.out + row0;
+    if (a.scale != 1.0f) {
+#pragma unroll
+      for (int j = 0; j < E; ++j) v[j] = cscale(v[j], a.scale);
+    }
+#pragma unroll
+    for (int j = 0; j < E; ++j) o[t + P * j] = v[j];
+  }
+}
+
+template <class PL, int MODE>
+__global__ void __launch_bounds__(cols_per_cta<PL>() * PL::P) k_pass_b(PassBArgs a) {
+  constexpr int NY = PL::N, E = PL::E, P = PL::P, CB = cols_per_cta<PL>(), LS = col_slot<PL>();
+  constexpr int NT = CB * P;
+  extern __shared__ float2 smem[];
+  const int nx = a.nx;
+  const int c0 = blockIdx.x * CB;
+  const long long base = (long long)blockIdx.y * a.batch_stride_wave;
+  const float2* in = a.in + base;
+  const float scale = a.scale;
+
+  // transposing tile load: NY rows x CB columns -> one padded slot per column
+  for (int idx = threadIdx.x; idx < NY * CB; idx += NT) {
+    const int r = idx / CB, c = idx % CB;
+    smem[c * LS + fft::padi<PL>(r)] = in[(long long)r * nx + c0 + c];
+  }
+  __syncthreads();
+
+  const int lane = threadIdx.x & 31;
+  const int cl = threadIdx.x / P, t = threadIdx.x % P;
+  const int col = c0 + cl;
+  float2* sm = smem + cl * LS;
+  float2 v[E];
+#pragma unroll
+  for (int j = 0; j < E; ++j) v[j] = sm[fft::padi<PL>(t + P * j)];
+  fft::line_sync<PL>();
+
+  if constexpr (MODE == B_INV_ONLY) {
+    fft::line_fft<PL, true>(v, sm, t, a.tw);
+  } else {
+    fft::line_fft<PL, false>(v, sm, t, a.tw);
+  }
+
+  if constexpr (MODE == B_PROPAGATE) {
+    const float kx = a.kx[col];
+    const float kx2 = fmul_x(kx, kx);
+    const float2 pxv = a.px[col];
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int n = t + P * j;
+      const float ky = a.ky[n];
+      // CreatePropsKernel (U.cu:419): keep sqrtf(kx^2+ky^2) < kmax
+      const bool keep = fsqrt_x(fadd_x(kx2, fmul_x(ky, ky))) < a.kmax;
+      const float2 w = keep ? cmul(pxv, a.py[n]) : make_float2(0.f, 0.f);
+      v[j] = cmul(v[j], w);
+    }
+    fft::line_fft<PL, true>(v, sm, t, a.tw);
+  } else if constexpr (MODE == B_CTF) {
+    const float kx = a.kx[col];
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int n = t + P * j;
+      v[j] = cmul(v[j], ctf_weight(a.ctf.wavel, a.ctf.Cs, a.ctf.df, a.ctf.A2, a.ctf.phi2, a.ctf.A3, a.ctf.phi3,
+                                   a.ctf.beta, a.ctf.delta, a.ctf.objap2, kx, a.ky[n], scale));
+    }
+    fft::line_fft<PL, true>(v, sm, t, a.tw);
+  } else if constexpr (MODE == B_CBED) {
+    // AddTDSWaves (U.cu:2734-2766): |FFT(psi)| placed by CentreKernel's shift
+    const int xs = (col < nx / 2) ? col + nx / 2 : col - nx / 2;
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int n = t + P * j;
+      const int ys = (n < NY / 2) ? n + NY / 2 : n - NY / 2;
+      const float m = sqrtf(v[j].x * v[j].x + v[j].y * v[j].y) * scale;
+      atomicAdd(a.acc + (long long)ys * nx + xs, m);
+    }
+  } else if constexpr (MODE == B_DETECT) {
+    // |FFT2(psi_exit)|^2 = |P|^2 |FFT_col(Y)|^2: the last propagation only
+    // masks, so the detector reads the column spectrum before the inverse.
+    const float kx = a.kx[col];
+    const float kx2 = fmul_x(kx, kx);
+    float acc = 0.0f;
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int n = t + P * j;
+      const float ky = a.ky[n];
+      const float k2 = fadd_x(kx2, fmul_x(ky, ky));
+      const bool keep = fsqrt_x(k2) < a.kmax && k2 >= a.kin2 && k2 < a.kout2;
+      if (keep) acc += v[j].x * v[j].x + v[j].y * v[j].y;
+    }
+    double d = (double)acc;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d += __shfl_down_sync(0xffffffffu, d, o);
+    if (lane == 0 && d != 0.0) atomicAdd(a.sig + blockIdx.y, d * (double)scale);
+  }
+
+  if constexpr (MODE != B_CBED && MODE != B_DETECT) {
+    // line_fft ended with a line barrier; slots are free again
+#pragma unroll
+    for (int j = 0; j < E; ++j) sm[fft::padi<PL>(t + P * j)] = v[j];
+    __syncthreads();
+    float2* out = a.out + base;
+    for (int idx = threadIdx.x; idx < NY * CB; idx += NT) {
+      const int r = idx / CB, c = idx % CB;
+      out[(long long)r * nx + c0 + c] = smem[c * LS + fft::padi<PL>(r)];
+    }
+  }
+}
+
+inline bool attr_once(unsigned long long& mask) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (mask >> dev & 1ull) return false;
+  mask |= 1ull << dev;
+  return true;
+}
+
+template <class PL, int FLAGS>
+cudaError_t run_a(const PassAArgs& a, int batch, cudaStream_t s) {
+  constexpr int lines = rows_per_cta<PL>();
+  const size_t smem = (size_t)lines * PL::SLOT * sizeof(float2);
+  if (a.ny % lines) return cudaErrorInvalidValue;
+  static unsigned long long done = 0;
+  if (attr_once(done)) {
+    cudaError_t e = cudaFuncSetAttribute(k_pass_a<PL, FLAGS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  k_pass_a<PL, FLAGS><<<dim3(a.ny / lines, batch), lines * PL::P, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <class PL, int MODE>
+cudaError_t run_b(const PassBArgs& a, int batch, cudaStream_t s) {
+  constexpr int CB = cols_per_cta<PL>();
+  const size_t smem = (size_t)CB * col_slot<PL>() * sizeof(float2);
+  if (a.nx % CB) return cudaErrorInvalidValue;
+  static unsigned long long done = 0;
+  if (attr_once(done)) {
+    cudaError_t e = cudaFuncSetAttribute(k_pass_b<PL, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  k_pass_b<PL, MODE><<<dim3(a.nx / CB, batch), CB * PL::P, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <class PL>
+cudaError_t dispatch_a_plan(const PassAArgs& a, int flags, int batch, cudaStream_t s) {
+  switch (flags) {
+    case A_FWD: return run_a<PL, A_FWD>(a, batch, s);
+    case A_INV: return run_a<PL, A_INV>(a, batch, s);
+    case A_MULT_T | A_FWD: return run_a<PL, A_MULT_T | A_FWD>(a, batch, s);
+    case A_INV | A_MULT_T | A_FWD: return run_a<PL, A_INV | A_MULT_T | A_FWD>(a, batch, s);
+    case A_INV | A_INTENSITY: return run_a<PL, A_INV | A_INTENSITY>(a, batch, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <class PL>
+cudaError_t dispatch_b_plan(const PassBArgs& a, int mode, int batch, cudaStream_t s) {
+  switch (mode) {
+    case B_FWD_ONLY: return run_b<PL, B_FWD_ONLY>(a, batch, s);
+    case B_INV_ONLY: return run_b<PL, B_INV_ONLY>(a, batch, s);
+    case B_PROPAGATE: return run_b<PL, B_PROPAGATE>(a, batch, s);
+    case B_CTF: return run_b<PL, B_CTF>(a, batch, s);
+    case B_CBED: return run_b<PL, B_CBED>(a, batch, s);
+    case B_DETECT: return run_b<PL, B_DETECT>(a, batch, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <class PL>
+void fill_twiddles(float2* out) {
+  const long double twopi = 6.283185307179586476925286766559L;
+  const int R[4] = {PL::R1, PL::R2, PL::R3, PL::R4};
+  int ns = R[0], off = 0;
+  for (int p = 1; p < PL::NPASS; ++p) {
+    const int m = ns * R[p];
+    for (int r = 0; r < R[p]; ++r)
+      for (int k = 0; k < ns; ++k) {
+        const long double ang = twopi * (long double)(((long long)r * k) % m) / (long double)m;
+        out[off + r * ns + k] = make_float2((float)std::cos(ang), (float)(-std::sin(ang)));
+      }
+    off += m;
+    ns = m;
+  }
+}
+
+// Entry points of one line length (defined in ms_slice_n<N>.cu).
+template <int N>
+cudaError_t dispatch_a_n(const PassAArgs& a, int variant, int flags, int batch, cudaStream_t s);
+template <int N>
+cudaError_t dispatch_b_n(const PassBArgs& a, int variant, int mode, int batch, cudaStream_t s);
+template <int N>
+int twiddles_n(int variant, float2* out);
+
+#define MS_SLICE_INSTANTIATE(N)                                                                      \
+  template <>                                                                                        \
+  cudaError_t dispatch_a_n<N>(const PassAArgs& a, int variant, int flags, int batch, cudaStream_t s) { \
+    switch (variant) {                                                                               \
+      case 0: return dispatch_a_plan<PlanSel<N, 0>::T>(a, flags, batch, s);                          \
+      case 1: return dispatch_a_plan<PlanSel<N, 1>::T>(a, flags, batch, s);                          \
+      case 2: return dispatch_a_plan<PlanSel<N, 2>::T>(a, flags, batch, s);                          \
+      default: return cudaErrorInvalidValue;                                                         \
+    }                                                                                                \
+  }                                                                                                  \
+  template <>                                                                                        \
+  cudaError_t dispatch_b_n<N>(const PassBArgs& a, int variant, int mode, int batch, cudaStream_t s) {  \
+    switch (variant) {                                                                               \
+      case 0: return dispatch_b_plan<PlanSel<N, 0>::T>(a, mode, batch, s);                           \
+      case 1: return dispatch_b_plan<PlanSel<N, 1>::T>(a, mode, batch, s);                           \
+      case 2: return dispatch_b_plan<PlanSel<N, 2>::T>(a, mode, batch, s);                           \
+      default: return cudaErrorInvalidValue;                                                         \
+    }                                                                                                \
+  }                                                                                                  \
+  template <>                                                                                        \
+  int twiddles_n<N>(int variant, float2* out) {                                                      \
+    switch (variant) {                                                                               \
+      case 0: fill_twiddles<PlanSel<N, 0>::T>(out); return PlanSel<N, 0>::T::TWSIZE;                 \
+      case 1: fill_twiddles<PlanSel<N, 1>::T>(out); return PlanSel<N, 1>::T::TWSIZE;                 \
+      case 2: fill_twiddles<PlanSel<N, 2>::T>(out); return PlanSel<N, 2>::T::TWSIZE;                 \
+      default: return 0;                                                                             \
+    }                                                                                                \
+  }
+
+}  // namespace ms

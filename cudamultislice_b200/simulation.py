@@ -87,6 +87,10 @@ class ManagedMultisliceSimulation:
     def SetPotentialMode(self, projected: bool):
         self._chk(self._L.ms_set_option(self._h, 2, int(bool(projected))))
 
+    def SetFFTPlan(self, variant: int):
+        """-1: autotuned; 0..2: force a plan variant of the fused passes."""
+        self._chk(self._L.ms_set_option(self._h, 3, int(variant)))
+
     # ---- structure ----
     def ImportAtoms(self, filename: str):
         self._chk(self._L.ms_import_atoms(self._h, filename.encode()))
@@ -295,6 +299,12 @@ class ManagedMultisliceSimulation:
             return t.value, a.value, b.value
         self._chk(self._L.ms_time_slices(self._h, int(steps), int(reps), C.byref(t), None, None))
         return t.value, None, None
+
+    def FFTPlan(self, batch: int = 1):
+        """(row, column) FFT plan variants used for `batch` instances."""
+        r, c = C.c_int(), C.c_int()
+        self._chk(self._L.ms_get_fft_plan(self._h, int(batch), C.byref(r), C.byref(c)))
+        return r.value, c.value
 
     def LaunchCount(self) -> int:
         out = C.c_longlong()

@@ -56,10 +56,14 @@ enum {
                                launch sequence (U.cu:2101-2122) */
   MS_OPT_ELEMENT_TABLE = 1, /* 0 = reference symbol table, unknown -> Z=1 (U.cu:1188-1243);
                                1 = full periodic table Z = 1..103 */
-  MS_OPT_POTENTIAL = 2      /* 0 = conventional 3D-integrated potential, the live
+  MS_OPT_POTENTIAL = 2,     /* 0 = conventional 3D-integrated potential, the live
                                reference kernel binnedAtomPKernel3 (U.cu:582-653);
                                1 = projected potential vzatom2 per slab (U.cu:119-152,
                                xy scan of binnedAtomPKernel2 U.cu:513-578) */
+  MS_OPT_FFT_PLAN = 3       /* -1 = autotuned (default): every FFT plan variant of the
+                               fused passes is timed on the device once per grid and
+                               batch size and the fastest kept; 0..2 = force a variant
+                               (0: most points per thread ... 2: most threads per line) */
 };
 
 /* ---- lifecycle ---- */
@@ -210,6 +214,9 @@ ms_status ms_fft2(ms_sim* sim, const float* in, float* out, int nx, int ny, int 
  * second run of `steps` steps with an event between every pass. */
 ms_status ms_time_slices(ms_sim* sim, int steps, int reps, float* ms_total, float* ms_row_pass,
                          float* ms_col_pass);
+/* FFT plan variants (row pass, column pass) used for `batch` instances, tuning
+ * them first if needed (MS_OPT_FFT_PLAN). */
+ms_status ms_get_fft_plan(ms_sim* sim, int batch, int* row_variant, int* col_variant);
 /* Number of this library's kernels launched by the handle so far. */
 ms_status ms_get_launch_count(ms_sim* sim, long long* out);
 

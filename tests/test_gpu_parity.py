@@ -87,15 +87,27 @@ def test_atom_index_large(engine_cls, oracle_mod):
 
 
 # ---------------------------------------------------------------- FFT
-@pytest.mark.parametrize("shape", [(64, 64), (128, 256), (512, 512), (1024, 1024), (256, 64), (1024, 512)])
-def test_fused_fft_against_numpy(engine_cls, shape):
+@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("shape", [(64, 64), (128, 256), (512, 512), (1024, 1024), (256, 64), (1024, 512),
+                                   (2048, 2048), (64, 2048)])
+def test_fused_fft_against_numpy(engine_cls, shape, variant):
     rng = np.random.default_rng(7)
     a = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
     eng = engine_cls()
+    eng.SetFFTPlan(variant)
     for sign, ref in ((-1, np.fft.fft2(a.astype(np.complex128))),
                       (+1, np.fft.ifft2(a.astype(np.complex128)) * a.size)):
         out = eng.FFT2(a, sign)
-        assert rel_l2(out, ref) < 1e-6, (shape, sign, rel_l2(out, ref))
+        assert rel_l2(out, ref) < 1e-6, (shape, sign, variant, rel_l2(out, ref))
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2])
+def test_exit_wave_every_fft_plan(engine_cls, oracle_mod, variant):
+    eng, orc = make_pair(engine_cls, oracle_mod, sto(2, 4), 256, 0.05)
+    eng.SetFFTPlan(variant)
+    eng.RunConventional()
+    psi = orc.run_conventional()
+    assert rel_l2(eng.ExitWave(), psi) < TOL
 
 
 # ---------------------------------------------------------------- potentials
