@@ -164,6 +164,51 @@ def barrier(world: int):
         dist.barrier()
 
 
+def stem_leg(fparams, device: int, nprobes: int = 256, batch: int = 16) -> dict:
+    """STEM probes/s on the GaN [11-20] HAADF configuration: 10 x 6 x 40
+    orthohexagonal cells (19,200 atoms), 1024^2 grid, 1.5945 A slices, 300 kV,
+    25 mrad, Cs = 0, df = 0, annular detector 70-200 mrad; a subset of the
+    128 x 128 raster, probes batched through the fused passes.  A probe is one
+    position through all slices, including probe generation and detection."""
+    import numpy as np
+
+    from cudamultislice_b200 import ManagedMultisliceSimulation
+    from cudamultislice_b200 import structures as S
+
+    Z, x, y, z = S.gan_wurtzite_11_20(10, 6, 40)
+    sim = ManagedMultisliceSimulation(device=device)
+    sim.SetAtoms(Z, x, y, z)
+    sim.UploadBinnedAtoms()
+    sim.GetParameterisation(fparams)
+    sim.ApplyMicroscopeParameters(300.0, 0.0, 0.0, 0.0, 0.0, 0.1, 30.0, 25.0)
+    ps = float(sim.GetSizeX()) / GRID
+    sim.STEMSetCalculationVariables(ps, 0.0, GRID, GRID, sim.GetSizeX(), sim.GetSizeY(), sim.GetSizeZ())
+    sim.PreCalculateFrequencies()
+    sim.InitialiseWavefunctions(1.5945)
+    nsl = sim.BuildPotentialStack()
+    # probe positions: a 128 x 128 raster over the cell area, first `nprobes`
+    gx = np.linspace(0, GRID - 1, 128).astype(np.int32)
+    px, py = np.meshgrid(gx, gx)
+    px, py = px.ravel()[:nprobes], py.ravel()[:nprobes]
+    out = {}
+    for name, path, n in (("fused", 0, nprobes), ("plain", 1, max(nprobes // 16, 8))):
+        sim.SetSlicePath(path)
+        sim.StemRaster(px[:batch], py[:batch], 70.0, 200.0, batch=batch)  # warm-up / tuning
+        t0 = time.perf_counter()
+        sig = sim.StemRaster(px[:n], py[:n], 70.0, 200.0, batch=batch)
+        dt = time.perf_counter() - t0
+        out[name] = {"probes_per_s": n / dt, "probes": int(n), "slices": int(nsl)}
+        if name == "fused":
+            out["signal_mean"] = float(np.mean(sig))
+    sim.close()
+    return {"value": out["fused"]["probes_per_s"], "unit": "probes/s",
+            "plain_value": out["plain"]["probes_per_s"],
+            "speedup_fused_vs_plain": out["fused"]["probes_per_s"] / out["plain"]["probes_per_s"],
+            "config": f"GaN [11-20] 10x6x40 cells ({len(Z)} atoms), {GRID}^2, {nsl} slices of 1.5945 A, 300 kV, "
+                      f"25 mrad, HAADF 70-200 mrad, {nprobes} probes of the 128x128 raster, batch {batch}",
+            "timing": "host clock around ms_stem_raster (synchronous), potential stack resident"}
+
+
 def cpu_baseline(atoms, fparams, nslices: int, threads: int) -> dict:
     """The FP64 OpenMP oracle on the host cores, on the first `nslices`
     slices of the same workload (potential build + transmission +
@@ -330,6 +375,8 @@ def main():
                 "note": "host clock around the synchronous C-ABI calls: atoms in, binning, potential stack "
                         "(100 slices), slice loop, exit wave out"},
     }
+
+    out["stem"] = stem_leg(FPARAMS, local)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1

@@ -315,6 +315,128 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a) {
   if (inside) a.V[(long long)y * a.nx + x] = acc;
 }
 
+// exp2 on the MUFU (PTX ex2.approx.ftz.f32; relative error about 2^-22).
+__device__ __forceinline__ float ex2_fast(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// Conventional potential (binnedAtomPKernel3 semantics) with per-atom work
+// hoisted out of the pixel loop.  For each staged atom the 20 sub-plane offsets
+// dz_m^2 (rounded exactly as in the cut-off test) and the Gaussian factors
+// exp(-pi^2 dz_m^2 / d_i) are computed once per CTA; a pixel then needs
+// exp(-pi^2 rho^2 / d_i) once per atom and, per sub-plane inside the cut-off,
+// one rsqrt and three exp2 for the Lorentzian terms.  Inside r < 0.25 A (the
+// clamp) the full vatom is evaluated.  Cut-offs stay non-contracted FP32.
+constexpr int kConvChunk = 64;
+
+__global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
+  __shared__ float4 s_at[kConvChunk];
+  __shared__ float s_dz2[kConvChunk][20];
+  __shared__ float s_g[kConvChunk][3][20];
+  __shared__ float s_coef[103 * kCoefPerZ];
+  __shared__ int s_start[kMaxSeg];
+  __shared__ int s_pref[kMaxSeg + 1];
+  __shared__ int s_warp[33];
+
+  for (int i = threadIdx.x; i < 103 * kCoefPerZ; i += kPotThreads) s_coef[i] = a.coef[i];
+
+  const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
+  const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY;
+  const int x = x0 + tx, y = y0 + ty;
+  const bool inside = (x < a.nx) && (y < a.ny);
+  const float px = fadd_x(a.xoff, fmul_x((float)x, a.ps));
+  const float py = fadd_x(a.yoff, fmul_x((float)y, a.ps));
+  const float xlo = a.xoff + x0 * a.ps - 2.2361f, xhi = a.xoff + (x0 + kTX - 1) * a.ps + 2.2361f;
+  const float ylo = a.yoff + y0 * a.ps - 2.2361f, yhi = a.yoff + (y0 + kTY - 1) * a.ps + 2.2361f;
+  const int bxl = max((int)floorf(xlo / a.bw_x) - 1, 0);
+  const int bxh = min((int)floorf(xhi / a.bw_x) + 1, kBins - 1);
+  const int byl = max((int)floorf(ylo / a.bw_y) - 1, 0);
+  const int byh = min((int)floorf(yhi / a.bw_y) + 1, kBins - 1);
+  const int nyb = byh - byl + 1;
+
+  float acc = 0.0f;
+  if (bxl <= bxh && byl <= byh && a.kt <= a.kb) {
+    const int kstep = max(kMaxSeg / nyb, 1);
+    for (int kg = a.kt; kg <= a.kb; kg += kstep) {
+      const int kend = min(kg + kstep - 1, a.kb);
+      const int nseg = (kend - kg + 1) * nyb;
+      int len0 = 0, len1 = 0, st0 = 0, st1 = 0;
+      const int s0 = threadIdx.x, s1 = threadIdx.x + kPotThreads;
+      if (s0 < nseg) {
+        const int b = (kg + s0 / nyb) * kBins2 + (byl + s0 % nyb) * kBins;
+        st0 = a.off[b + bxl];
+        len0 = a.off[b + bxh + 1] - st0;
+      }
+      if (s1 < nseg) {
+        const int b = (kg + s1 / nyb) * kBins2 + (byl + s1 % nyb) * kBins;
+        st1 = a.off[b + bxl];
+        len1 = a.off[b + bxh + 1] - st1;
+      }
+      int total;
+      const int ex = block_exclusive_scan(len0 + len1, s_warp, &total);
+      if (s0 < nseg) { s_start[s0] = st0; s_pref[s0] = ex; }
+      if (s1 < nseg) { s_start[s1] = st1; s_pref[s1] = ex + len0; }
+      if (threadIdx.x == 0) s_pref[nseg] = total;
+      __syncthreads();
+
+      for (int base = 0; base < total; base += kConvChunk) {
+        const int cnt = min(kConvChunk, total - base);
+        if (threadIdx.x < cnt) {
+          const int gidx = base + threadIdx.x;
+          int lo = 0, hi = nseg - 1;
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (s_pref[mid] <= gidx) lo = mid; else hi = mid - 1;
+          }
+          s_at[threadIdx.x] = a.atoms[s_start[lo] + (gidx - s_pref[lo])];
+        }
+        __syncthreads();
+        // per (atom, sub-plane): dz^2 as the cut-off rounds it, Gaussian factors
+        for (int q = threadIdx.x; q < cnt * 20; q += kPotThreads) {
+          const int i = q / 20, m = q % 20;
+          const float4 at = s_at[i];
+          const float dz = fsub_x(a.zsub[m], at.z);
+          const float dz2 = fmul_x(dz, dz);
+          s_dz2[i][m] = dz2;
+          const float* c = s_coef + (__float_as_int(at.w) - 1) * kCoefPerZ;
+          s_g[i][0][m] = ex2_fast(-c[9] * dz2);
+          s_g[i][1][m] = ex2_fast(-c[10] * dz2);
+          s_g[i][2][m] = ex2_fast(-c[11] * dz2);
+        }
+        __syncthreads();
+        for (int i = 0; i < cnt; ++i) {
+          const float4 at = s_at[i];
+          const float dx = fsub_x(px, at.x), dy = fsub_x(py, at.y);
+          const float dxy = fadd_x(fmul_x(dx, dx), fmul_x(dy, dy));
+          if (!(dxy < 5.0f)) continue;
+          const float* c = s_coef + (__float_as_int(at.w) - 1) * kCoefPerZ;
+          const float g0 = c[6] * ex2_fast(-c[9] * dxy), g1 = c[7] * ex2_fast(-c[10] * dxy),
+                      g2 = c[8] * ex2_fast(-c[11] * dxy);
+#pragma unroll 4
+          for (int m = 0; m < 20; ++m) {
+            const float r2 = fadd_x(dxy, s_dz2[i][m]);
+            if (!(r2 < 5.0f)) continue;
+            float v;
+            if (r2 < 0.0625f) {
+              v = vatom_f(c, r2);  // inside the 0.25 A clamp
+            } else {
+              const float ri = rsqrtf(r2), r = r2 * ri;
+              const float L = c[0] * ex2_fast(-c[3] * r) + c[1] * ex2_fast(-c[4] * r) + c[2] * ex2_fast(-c[5] * r);
+              const float G = g0 * s_g[i][0][m] + g1 * s_g[i][1][m] + g2 * s_g[i][2][m];
+              v = L * ri + G;
+            }
+            acc += a.wsub * v;
+          }
+        }
+        __syncthreads();
+      }
+    }
+  }
+  if (inside) a.V[(long long)y * a.nx + x] = acc;
+}
+
 }  // namespace
 
 size_t bin_scratch_blocks(int nbins) { return (size_t)(nbins + kScanTile - 1) / kScanTile + 1; }
@@ -344,7 +466,7 @@ cudaError_t build_atom_index(const int* dZ, const float* dx, const float* dy, co
 cudaError_t launch_potential(const PotArgs& a, int kind, cudaStream_t s) {
   dim3 grid((a.nx + kTX - 1) / kTX, (a.ny + kTY - 1) / kTY);
   switch (kind) {
-    case POT_CONVENTIONAL: k_potential<POT_CONVENTIONAL><<<grid, kPotThreads, 0, s>>>(a); break;
+    case POT_CONVENTIONAL: k_potential_conv<<<grid, kPotThreads, 0, s>>>(a); break;
     case POT_FD: k_potential<POT_FD><<<grid, kPotThreads, 0, s>>>(a); break;
     case POT_PROJECTED: k_potential<POT_PROJECTED><<<grid, kPotThreads, 0, s>>>(a); break;
     default: return cudaErrorInvalidValue;

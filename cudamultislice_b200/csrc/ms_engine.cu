@@ -491,6 +491,7 @@ class Engine {
     if (it < 1) return fail(MS_ERR_INVALID, "iteration counts from 1");
     if (!fd_stable_) return fail(MS_ERR_NUMERIC, "no stable finite-difference step for these conditions");
     if (int rc = require_potential_inputs()) return rc;
+    if (use_fused()) return step_fd_fused(it);
     if (int rc = ensure_real()) return rc;
     const Grid2 g{nx_, ny_};
     const float nf = 1.0f / std::sqrt((float)(nx_ * ny_));
@@ -514,6 +515,62 @@ class Engine {
     // rotate psi- <- psi <- psi+ (U.cu:2081-2082) by swapping buffers
     std::swap(d_psim_.p, d_psi_.p);  // psim = old psi
     std::swap(d_psi_.p, d_t2_.p);    // psi = psi+
+    invalidate_graph();
+    return MS_OK;
+  }
+
+  // Finite-difference step on the fused passes.  Between steps the state is
+  // X (row-frequency form of psi_n, IFFT_row(X) = psi_n), the band-limited
+  // spectrum FFT2(psi_n) (column-major) and psi_{n-1} in real space.
+  // MultisliceStep (U.cu:2040-2083) becomes one row pass (IFFT_row, the
+  // three-level stencil without its Laplacian, FFT_row) and one column pass
+  // (FFT_col, + rc dz^2 4 pi^2 k^2 FFT2(psi_n), band limit, IFFT_col).
+  int step_fd_fused(int it) {
+    const Grid2 g{nx_, ny_};
+    const long long N = (long long)nx_ * ny_;
+    MS_TRY(d_fdX_.resize(N));
+    MS_TRY(d_fdQ_.resize(N));
+    MS_TRY(d_fdS_.resize(N));
+    if (!fd_state_) {
+      if (int rc = ensure_real()) return rc;
+      // X = FFT_row(psi_n), spectrum = FFT_col(X) stored column-major
+      MS_TRY(pass_a(passa_args(d_psi_.p, d_fdX_.p, 0), A_FWD, 1));
+      MS_TRY(pass_b(passb_args(d_fdX_.p, d_t1_.p, 0), B_FWD_ONLY, 1));
+      MS_TRY(pw_transpose(d_t1_.p, d_fdS_.p, g, stream_, &launches));
+      launches += 2;
+      fd_state_ = true;
+    }
+    // V at the plane, band-limited (U.cu:2053-2063), real part kept
+    if (int rc = potential_slice(POT_FD, it, d_f_.p)) return rc;
+    MS_TRY(pw_real_to_complex(d_f_.p, d_t1_.p, g, stream_, &launches));
+    MS_TRY(pass_a(passa_args(d_t1_.p, d_t1_.p, 0), A_FWD, 1));
+    PassBArgs bl = passb_args(d_t1_.p, d_t1_.p, 0);
+    bl.scale = 1.0f / (float)N;
+    MS_TRY(pass_b(bl, B_BANDLIMIT, 1));
+    PassAArgs vr = passa_args(d_t1_.p, nullptr, 0);
+    vr.out_f = d_f_.p;
+    MS_TRY(pass_a(vr, A_INV | A_REAL, 1));
+    launches += 3;
+    // coefficients of finiteDifferenceKernel (U.cu:1006-1012), pi = 3.14159
+    const double dz = dzFD_, lam = wavel_, aa = 2.0 * 3.14159 * dz / lam, den = 1.0 + aa * aa;
+    const double rcx = 1.0 / den, rcy = -aa / den;
+    PassAArgs a = passa_args(d_fdX_.p, d_fdQ_.p, 0);
+    a.in2 = d_psim_.p;
+    a.out2 = d_psi_.p;
+    a.V = d_f_.p;
+    a.fd_rc = make_float2((float)rcx, (float)rcy);
+    a.fd_ratio = make_float2((float)((1.0 - aa * aa) / den), (float)(-2.0 * aa / den));
+    a.fd_kv = (float)(dz * dz * 4.0 * 3.14159 * (double)sigma2_ / lam);
+    MS_TRY(pass_a(a, A_INV | A_FD | A_FWD, 1));
+    PassBArgs b = passb_args(d_fdQ_.p, d_fdX_.p, 0);
+    b.spec = d_fdS_.p;
+    const double cf = dz * dz * 4.0 * 3.14159 * 3.14159;
+    b.fd_c = make_float2((float)(rcx * cf), (float)(rcy * cf));
+    b.scale = 1.0f / (float)N;
+    MS_TRY(pass_b(b, B_FD, 1));
+    launches += 2;
+    std::swap(d_psim_.p, d_psi_.p);  // psi_n becomes psi_{n-1}
+    domain_ = 2;                      // current wave held as X
     invalidate_graph();
     return MS_OK;
   }
@@ -595,6 +652,8 @@ class Engine {
   int add_tds() {
     if (!have_waves_) return fail(MS_ERR_STATE, "wavefunctions not initialised");
     if (!have_tds_) return fail(MS_ERR_STATE, "TDS buffer not allocated (ms_alloc_tds)");
+    if (domain_ == 2)
+      if (int rc = ensure_real()) return rc;
     const Grid2 g{nx_, ny_};
     if (use_fused() && domain_ == 1) {
       PassBArgs b = passb_args(d_psi_.p, d_psi_.p, 0);
@@ -665,6 +724,8 @@ class Engine {
   int simulate_image() {
     if (!have_waves_) return fail(MS_ERR_STATE, "wavefunctions not initialised");
     if (!have_image_buf_) alloc_host_image();
+    if (domain_ == 2)
+      if (int rc = ensure_real()) return rc;
     const Grid2 g{nx_, ny_};
     const size_t N = (size_t)nx_ * ny_;
     const float wavel = wavel_, objap = aperture_;
@@ -1094,6 +1155,7 @@ class Engine {
     MS_TRY(pw_scale(d_psi_.p, nf, g, stream_, &launches));
     MS_TRY(cudaStreamSynchronize(stream_));
     domain_ = 0;
+    fd_state_ = false;
     have_waves_ = true;
     prop_dz_ = -1.0f;
     return MS_OK;
@@ -1217,6 +1279,7 @@ class Engine {
   // allocation or copy: safe inside stream capture once the propagator
   // tables exist).
   int enqueue_fused_step(const float* V, bool first) {
+    fd_state_ = false;
     // iteration 1 starts from the initial wave (real space); later ones from
     // the current wave in whichever domain it is held
     PassAArgs a = passa_args(first ? d_psi0_.p : d_psi_.p, d_psi_.p, 0);
@@ -1231,6 +1294,8 @@ class Engine {
   // transmission + propagation of one conventional slice with potential V.
   int transmit_propagate(const float* V, bool first) {
     if (int rc = ensure_prop_tables(convdz_)) return rc;
+    if (domain_ == 2)
+      if (int rc = ensure_real()) return rc;
     if (use_fused()) {
       if (int rc = enqueue_fused_step(V, first)) return rc;
       launches += 2;
@@ -1238,6 +1303,7 @@ class Engine {
     }
     // plain path: the reference's launch sequence (U.cu:2101-2122)
     if (int rc = ensure_real()) return rc;
+    fd_state_ = false;
     const Grid2 g{nx_, ny_};
     const float nf = 1.0f / std::sqrt((float)(nx_ * ny_));
     MS_TRY(pw_transmission(V, sigma2_, d_t2_.p, g, stream_, &launches));
@@ -1252,6 +1318,13 @@ class Engine {
 
   int ensure_real() {
     if (domain_ == 0) return MS_OK;
+    if (domain_ == 2) {
+      // fused finite differences: psi_n = IFFT_row(X), the FD state stays valid
+      MS_TRY(pass_a(passa_args(d_fdX_.p, d_psi_.p, 0), A_INV, 1));
+      ++launches;
+      domain_ = 0;
+      return MS_OK;
+    }
     PassAArgs a = passa_args(d_psi_.p, d_psi_.p, 0);
     MS_TRY(pass_a(a, A_INV, 1));
     ++launches;
@@ -1361,12 +1434,14 @@ class Engine {
   cufftHandle plan_ = 0;
   bool have_plan_ = false;
   // waves
-  DevBuf<float2> d_psi0_, d_psi_, d_psim_, d_t1_, d_t2_, d_grad_;
+  DevBuf<float2> d_psi0_, d_psi_, d_psim_, d_t1_, d_t2_, d_grad_, d_fdX_, d_fdQ_, d_fdS_;
+  bool fd_state_ = false;
   DevBuf<float> d_V_, d_f_, d_tds_, d_stack_;
   DevBuf<double> d_partial_, d_bsig_, d_bpart_;
   DevBuf<float2> d_bwave_;
   DevBuf<int> d_bpos_;
-  int domain_ = 0;  // 0 real space, 1 row-frequency state of the fused passes
+  int domain_ = 0;  // 0 real space, 1 row-frequency state of the fused passes,
+                    // 2 fused finite differences (d_psi_ stale, X in d_fdX_)
   bool have_waves_ = false, stack_valid_ = false, have_tds_ = false, tds_host_valid_ = false;
   int nstack_ = 0;
   cudaGraphExec_t graph_exec_ = nullptr;

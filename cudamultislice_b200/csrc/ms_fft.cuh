@@ -14,7 +14,9 @@
 // The slot is padded by one point every R1 points so the stride-R1 writes of
 // pass 1 hit distinct banks.  In-register butterflies are radix-2 DIF networks
 // with compile-time twiddle constants; trivial twiddles cost no multiply.
-// Forward = exp(-2 pi i jk/N) (cuFFT CUFFT_FORWARD); both directions unnormalised.
+// Forward = exp(-2 pi i jk/N) (cuFFT CUFFT_FORWARD); the inverse is computed as
+// conj(FFT(conj(x))) so that a kernel holds one copy of the transform code
+// (instruction-cache footprint); both directions unnormalised.
 #pragma once
 #include "ms_common.cuh"
 
@@ -129,11 +131,44 @@ struct PassR {
   static constexpr int TW = IDX == 1 ? PL::TW2 : IDX == 2 ? PL::TW3 : PL::TW4;
 };
 
-template <class PL, int IDX, bool INV>
-MS_D void middle_or_last(float2 (&v)[PL::E], float2* __restrict__ sm, int t, const float2* __restrict__ tw) {
+// Twiddles of pass IDX for this thread's butterflies, loaded ahead of the
+// barrier that precedes the pass so their latency overlaps the wait.  Plans
+// with more than 16 twiddles per thread load them at use instead.
+template <class PL, int IDX>
+struct TwiddleRegs {
+  static constexpr int R = PassR<PL, IDX>::R, NB = PL::E / R;
+  static constexpr bool PREFETCH = NB * (R - 1) <= 16;
+  float2 w[PREFETCH ? NB * (R - 1) : 1];
+  MS_D void load(const float2* __restrict__ tw, int t) {
+    if constexpr (PREFETCH) {
+      constexpr int NS = PassR<PL, IDX>::NS, TWO = PassR<PL, IDX>::TW;
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        const int k = (t + PL::P * b) & (NS - 1);
+#pragma unroll
+        for (int r = 1; r < R; ++r) w[b * (R - 1) + r - 1] = __ldg(tw + TWO + r * NS + k);
+      }
+    }
+  }
+  MS_D float2 get(const float2* __restrict__ tw, int b, int r, int k) const {
+    if constexpr (PREFETCH) {
+      return w[b * (R - 1) + r - 1];
+    } else {
+      return __ldg(tw + PassR<PL, IDX>::TW + r * PassR<PL, IDX>::NS + k);
+    }
+  }
+};
+
+// Stockham pass IDX >= 1: the previous pass has written the slot but not yet
+// synchronised.  Forward transform only; the inverse is conj(FFT(conj(x))).
+template <class PL, int IDX>
+MS_D void forward_pass(float2 (&v)[PL::E], float2* __restrict__ sm, int t, const float2* __restrict__ tw) {
   constexpr int N = PL::N, E = PL::E, P = PL::P;
-  constexpr int R = PassR<PL, IDX>::R, NS = PassR<PL, IDX>::NS, TWO = PassR<PL, IDX>::TW, LR = ilog2(R);
+  constexpr int R = PassR<PL, IDX>::R, NS = PassR<PL, IDX>::NS, LR = ilog2(R);
   constexpr bool LAST = (IDX == PL::NPASS - 1);
+  TwiddleRegs<PL, IDX> tr;
+  tr.load(tw, t);
+  line_sync<PL>();
   if constexpr (LAST) {
 #pragma unroll
     for (int b = 0; b < E / R; ++b) {
@@ -142,12 +177,8 @@ MS_D void middle_or_last(float2 (&v)[PL::E], float2* __restrict__ sm, int t, con
 #pragma unroll
       for (int r = 0; r < R; ++r) x[r] = sm[padi<PL>(i + r * (N / R))];
 #pragma unroll
-      for (int r = 1; r < R; ++r) {
-        float2 w = __ldg(tw + TWO + r * NS + i);
-        if (INV) w.y = -w.y;
-        x[r] = cmul(x[r], w);
-      }
-      dft<R, INV>(x);
+      for (int r = 1; r < R; ++r) x[r] = cmul(x[r], tr.get(tw, b, r, i));
+      dft<R, false>(x);
 #pragma unroll
       for (int q = 0; q < R; ++q) v[b + q * (E / R)] = x[brev(q, LR)];
     }
@@ -169,26 +200,21 @@ MS_D void middle_or_last(float2 (&v)[PL::E], float2* __restrict__ sm, int t, con
 #pragma unroll
       for (int r = 0; r < R; ++r) x[r] = v[b * R + r];
 #pragma unroll
-      for (int r = 1; r < R; ++r) {
-        float2 w = __ldg(tw + TWO + r * NS + k);
-        if (INV) w.y = -w.y;
-        x[r] = cmul(x[r], w);
-      }
-      dft<R, INV>(x);
+      for (int r = 1; r < R; ++r) x[r] = cmul(x[r], tr.get(tw, b, r, k));
+      dft<R, false>(x);
       const int base = (i / NS) * NS * R + k;
 #pragma unroll
       for (int q = 0; q < R; ++q) sm[padi<PL>(base + q * NS)] = x[brev(q, LR)];
     }
-    line_sync<PL>();
-    middle_or_last<PL, IDX + 1, INV>(v, sm, t, tw);
+    forward_pass<PL, IDX + 1>(v, sm, t, tw);
   }
 }
 
-// One N-point transform of the line held by threads t = 0..P-1 of a group.
-// `sm` is this line's shared slot (PL::SLOT points), `tw` the plan's twiddle
-// table (forward values; conjugated for INV).  Every thread of the warp (or,
-// for P > 32, of the CTA) must call this: it synchronises.
-template <class PL, bool INV>
+// Forward N-point transform of the line held by threads t = 0..P-1 of a
+// group.  `sm` is this line's shared slot (PL::SLOT points), `tw` the plan's
+// twiddle table.  Every thread of the warp (or, for P > 32, of the CTA) must
+// call this: it synchronises.  On return the slot may be reused.
+template <class PL>
 MS_D void line_fft(float2 (&v)[PL::E], float2* __restrict__ sm, int t, const float2* __restrict__ tw) {
   constexpr int E = PL::E, P = PL::P, R1 = PL::R1, L1 = ilog2(R1);
 #pragma unroll
@@ -196,13 +222,18 @@ MS_D void line_fft(float2 (&v)[PL::E], float2* __restrict__ sm, int t, const flo
     float2 x[R1];
 #pragma unroll
     for (int r = 0; r < R1; ++r) x[r] = v[b + r * (E / R1)];
-    dft<R1, INV>(x);
+    dft<R1, false>(x);
     const int i = t + P * b;
 #pragma unroll
     for (int q = 0; q < R1; ++q) sm[padi<PL>(i * R1 + q)] = x[brev(q, L1)];
   }
-  line_sync<PL>();
-  middle_or_last<PL, 1, INV>(v, sm, t, tw);
+  forward_pass<PL, 1>(v, sm, t, tw);
+}
+
+template <int E>
+MS_D void conj_all(float2 (&v)[E]) {
+#pragma unroll
+  for (int j = 0; j < E; ++j) v[j].y = -v[j].y;
 }
 
 // Host-side twiddle table of a plan: pass p >= 2 entries W_{Ns R}^{r k},

@@ -154,6 +154,11 @@ __global__ void k_centre(const float2* F, float2* out, Grid2 g) {
   out[i] = F[(long long)y2 * g.nx + x2];
 }
 
+__global__ void k_transpose(const float2* in, float2* out, Grid2 g) {
+  PW_INDEX
+  out[(long long)x * g.ny + y] = in[i];
+}
+
 __global__ void k_abs2(const float2* a, float* out, float scale, Grid2 g) {
   PW_INDEX
   const float2 v = a[i];
@@ -295,6 +300,9 @@ cudaError_t pw_centre_abs_acc(const float2* F, float* acc, float scale, Grid2 g,
 }
 cudaError_t pw_centre(const float2* F, float2* out, Grid2 g, cudaStream_t s, long long* count) {
   PW_LAUNCH(k_centre, F, out, g);
+}
+cudaError_t pw_transpose(const float2* in, float2* out, Grid2 g, cudaStream_t s, long long* count) {
+  PW_LAUNCH(k_transpose, in, out, g);
 }
 cudaError_t pw_abs2(const float2* a, float* out, float scale, Grid2 g, cudaStream_t s, long long* count) {
   PW_LAUNCH(k_abs2, a, out, scale, g);

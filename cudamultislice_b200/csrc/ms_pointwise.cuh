@@ -31,6 +31,8 @@ cudaError_t pw_real_to_complex(const float* in, float2* out, Grid2 g, cudaStream
 cudaError_t pw_centre_abs_acc(const float2* F, float* acc, float scale, Grid2 g, cudaStream_t s, long long* count);
 cudaError_t pw_centre(const float2* F, float2* out, Grid2 g, cudaStream_t s, long long* count);
 cudaError_t pw_abs2(const float2* a, float* out, float scale, Grid2 g, cudaStream_t s, long long* count);
+// out[x][y] = in[y][x] (one-time layout changes).
+cudaError_t pw_transpose(const float2* in, float2* out, Grid2 g, cudaStream_t s, long long* count);
 // CTF multiply for the plain path (same weight as the fused column pass).
 cudaError_t pw_ctf(float2* F, const float* kx, const float* ky, double wavel, double Cs, double df, double A2,
                    double phi2, double beta, double delta, float objap2, float scale, Grid2 g, cudaStream_t s,

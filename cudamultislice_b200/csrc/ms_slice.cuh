@@ -17,7 +17,14 @@
 
 namespace ms {
 
-enum PassAFlags : int { A_INV = 1, A_MULT_T = 2, A_FWD = 4, A_INTENSITY = 8 };
+enum PassAFlags : int {
+  A_INV = 1,        // IFFT_row of the input line
+  A_MULT_T = 2,     // x exp(i sigma V)
+  A_FWD = 4,        // FFT_row
+  A_INTENSITY = 8,  // store |.|^2 * scale as float
+  A_REAL = 16,      // store the real part * scale as float
+  A_FD = 32,        // finite-difference stencil (see PassAArgs.fd_*)
+};
 enum PassBMode : int {
   B_FWD_ONLY = 0,    // FFT_col
   B_INV_ONLY = 1,    // IFFT_col
@@ -25,6 +32,8 @@ enum PassBMode : int {
   B_CTF = 3,         // FFT_col, x CTF(k)/N (objective aperture), IFFT_col
   B_CBED = 4,        // FFT_col, accumulate |.| fftshifted into a float map
   B_DETECT = 5,      // FFT_col, band limit of P, sum |.|^2 over an annulus per instance
+  B_BANDLIMIT = 6,   // FFT_col, keep k <= kmax (x scale), IFFT_col
+  B_FD = 7,          // FFT_col = Q; spec <- BL Q + fd_c k^2 spec; IFFT_col(spec) * scale
 };
 
 struct PassAArgs {
@@ -34,6 +43,15 @@ struct PassAArgs {
   const float* V;     // potential slice [ny][nx] (A_MULT_T)
   float sigma;        // interaction constant
   float scale;        // applied to the result of the line (1 = none)
+  // A_FD: the input line is the row-frequency state of psi_n; the pass stores
+  // psi_n (real space) to out2 and FFT_row(q) to out, with
+  // q = fd_rc * (2 - fd_kv V) psi_n - fd_ratio * psi_{n-1} (psi_{n-1} from in2),
+  // the three-level update of finiteDifferenceKernel (U.cu:995-1023) without
+  // its Laplacian term, which the column pass adds in k-space.
+  const float2* in2;
+  float2* out2;
+  float2 fd_rc, fd_ratio;
+  float fd_kv;
   const float2* tw;   // twiddle table for nx
   int nx, ny;
   long long batch_stride_wave;  // elements between instances (blockIdx.y)
@@ -58,6 +76,9 @@ struct PassBArgs {
   CtfParams ctf;
   float scale;         // B_CTF: factor on the weight; B_CBED: factor on |.|
   double* sig;         // B_DETECT: one FP64 sum per instance (blockIdx.y)
+  float2* spec;        // B_FD: band-limited spectrum FFT2(psi_n) in, FFT2(psi_{n+1}) out,
+                       //       stored column-major [nx][ny] (coalesced in this pass)
+  float2 fd_c;         // B_FD: rc dz^2 4 pi^2 (pi = 3.14159, gradKernel U.cu:959)
   float kin2, kout2;   // B_DETECT: annulus kin^2 <= kx^2+ky^2 < kout^2 (FP32 decision)
   int nx, ny;
   long long batch_stride_wave;

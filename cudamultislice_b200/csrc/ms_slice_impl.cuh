@@ -46,9 +46,37 @@ __host__ __device__ constexpr int cols_per_cta() { return PL::P >= 64 ? 4 : 256 
 template <class PL>
 __host__ __device__ constexpr int col_slot() { return ((PL::N + PL::N / PL::R1 + 15) / 16) * 16 + 2; }
 
+// Pointwise work of the row pass between its inverse and forward transforms.
+template <class PL, int FLAGS>
+MS_D void row_mid(float2 (&v)[PL::E], const PassAArgs& a, long long inst, int line, long long row0, int t) {
+  constexpr int NX = PL::N, E = PL::E, P = PL::P;
+  if constexpr ((FLAGS & A_FD) != 0) {
+    const float* V = a.V + inst * a.batch_stride_V + (long long)line * NX;
+    const float2* pm = a.in2 + row0;
+    float2* pc = a.out2 + row0;
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int x = t + P * j;
+      pc[x] = v[j];
+      const float f = 2.0f - a.fd_kv * V[x];
+      v[j] = csub(cmul(a.fd_rc, cscale(v[j], f)), cmul(a.fd_ratio, pm[x]));
+    }
+  }
+  if constexpr ((FLAGS & A_MULT_T) != 0) {
+    const float* V = a.V + inst * a.batch_stride_V + (long long)line * NX;
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      float sn, cs;
+      sincos_red(fmul_x(a.sigma, V[t + P * j]), &sn, &cs);
+      v[j] = cmul(v[j], make_float2(cs, sn));
+    }
+  }
+}
+
 template <class PL, int FLAGS>
 __global__ void __launch_bounds__(rows_per_cta<PL>() * PL::P) k_pass_a(PassAArgs a) {
   constexpr int NX = PL::N, E = PL::E, P = PL::P, LS = PL::SLOT;
+  constexpr bool INVF = (FLAGS & A_INV) != 0, FWDF = (FLAGS & A_FWD) != 0;
   extern __shared__ float2 smem[];
   const int g = threadIdx.x / P, t = threadIdx.x % P;
   const int line = blockIdx.x * rows_per_cta<PL>() + g;
@@ -61,22 +89,29 @@ __global__ void __launch_bounds__(rows_per_cta<PL>() * PL::P) k_pass_a(PassAArgs
 #pragma unroll
   for (int j = 0; j < E; ++j) v[j] = in[t + P * j];
 
-  if constexpr ((FLAGS & A_INV) != 0) fft::line_fft<PL, true>(v, sm, t, a.tw);
-  if constexpr ((FLAGS & A_MULT_T) != 0) {
-    const float* V = a.V + inst * a.batch_stride_V + (long long)line * NX;
-#pragma unroll
-    for (int j = 0; j < E; ++j) {
-      float s, c;
-      sincosf(fmul_x(a.sigma, V[t + P * j]), &s, &c);
-      v[j] = cmul(v[j], make_float2(c, s));
+  if constexpr (!INVF) row_mid<PL, FLAGS>(v, a, inst, line, row0, t);
+  if constexpr (INVF || FWDF) {
+    // one copy of the transform code: iteration 0 is the inverse
+    // conj(FFT(conj(.))) followed by the pointwise work, iteration 1 the forward
+#pragma unroll 1
+    for (int it = INVF ? 0 : 1; it < (FWDF ? 2 : 1); ++it) {
+      if (it == 0) fft::conj_all(v);
+      fft::line_fft<PL>(v, sm, t, a.tw);
+      if (it == 0) {
+        fft::conj_all(v);
+        if constexpr (INVF) row_mid<PL, FLAGS>(v, a, inst, line, row0, t);
+      }
     }
   }
-  if constexpr ((FLAGS & A_FWD) != 0) fft::line_fft<PL, false>(v, sm, t, a.tw);
 
   if constexpr ((FLAGS & A_INTENSITY) != 0) {
     float* o = a.out_f + row0;
 #pragma unroll
     for (int j = 0; j < E; ++j) o[t + P * j] = (v[j].x * v[j].x + v[j].y * v[j].y) * a.scale;
+  } else if constexpr ((FLAGS & A_REAL) != 0) {
+    float* o = a.out_f + row0;
+#pragma unroll
+    for (int j = 0; j < E; ++j) o[t + P * j] = v[j].x * a.scale;
   } else {
     float2* o = a.out + row0;
     if (a.scale != 1.0f) {
@@ -88,10 +123,69 @@ __global__ void __launch_bounds__(rows_per_cta<PL>() * PL::P) k_pass_a(PassAArgs
   }
 }
 
+// Pointwise work of the column pass on the column spectrum (between the
+// forward and the inverse transform, or before the epilogue).
+template <class PL, int MODE>
+MS_D void col_mid(float2 (&v)[PL::E], const PassBArgs& a, int col, int t, long long base) {
+  constexpr int NY = PL::N, E = PL::E, P = PL::P;
+  const float scale = a.scale;
+  if constexpr (MODE == B_PROPAGATE) {
+    const float kx = a.kx[col];
+    const float kx2 = fmul_x(kx, kx);
+    const float2 pxv = a.px[col];
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int n = t + P * j;
+      const float ky = a.ky[n];
+      // CreatePropsKernel (U.cu:419): keep sqrtf(kx^2+ky^2) < kmax
+      const bool keep = fsqrt_x(fadd_x(kx2, fmul_x(ky, ky))) < a.kmax;
+      const float2 w = keep ? cmul(pxv, a.py[n]) : make_float2(0.f, 0.f);
+      v[j] = cmul(v[j], w);
+    }
+  } else if constexpr (MODE == B_CTF) {
+    const float kx = a.kx[col];
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int n = t + P * j;
+      v[j] = cmul(v[j], ctf_weight(a.ctf.wavel, a.ctf.Cs, a.ctf.df, a.ctf.A2, a.ctf.phi2, a.ctf.A3, a.ctf.phi3,
+                                   a.ctf.beta, a.ctf.delta, a.ctf.objap2, kx, a.ky[n], scale));
+    }
+  } else if constexpr (MODE == B_BANDLIMIT) {
+    // BandLimitKernel (U.cu:1025-1042): keep k <= kmax
+    const float kx = a.kx[col];
+    const float kx2 = fmul_x(kx, kx);
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const float ky = a.ky[t + P * j];
+      const bool keep = fsqrt_x(fadd_x(kx2, fmul_x(ky, ky))) <= a.kmax;
+      v[j] = keep ? cscale(v[j], scale) : make_float2(0.f, 0.f);
+    }
+  } else if constexpr (MODE == B_FD) {
+    // Psi_{n+1} = BL (FFT2(q) + c k^2 Psi_n)
+    const float kx = a.kx[col];
+    const float kx2 = fmul_x(kx, kx);
+    float2* sp = a.spec + base;
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int n = t + P * j;
+      const float ky = a.ky[n];
+      const float ky2 = fmul_x(ky, ky);
+      const bool keep = fsqrt_x(fadd_x(kx2, ky2)) <= a.kmax;
+      const long long o = (long long)col * NY + n;  // spectrum kept column-major
+      const float2 s0 = sp[o];
+      const float k2 = kx * kx + ky * ky;
+      const float2 nv = keep ? cadd(v[j], cscale(cmul(a.fd_c, s0), k2)) : make_float2(0.f, 0.f);
+      sp[o] = nv;
+      v[j] = cscale(nv, scale);
+    }
+  }
+}
+
 template <class PL, int MODE>
 __global__ void __launch_bounds__(cols_per_cta<PL>() * PL::P) k_pass_b(PassBArgs a) {
   constexpr int NY = PL::N, E = PL::E, P = PL::P, CB = cols_per_cta<PL>(), LS = col_slot<PL>();
   constexpr int NT = CB * P;
+  constexpr bool TWO = MODE == B_PROPAGATE || MODE == B_CTF || MODE == B_BANDLIMIT || MODE == B_FD;
   extern __shared__ float2 smem[];
   const int nx = a.nx;
   const int c0 = blockIdx.x * CB;
@@ -115,36 +209,25 @@ __global__ void __launch_bounds__(cols_per_cta<PL>() * PL::P) k_pass_b(PassBArgs
   for (int j = 0; j < E; ++j) v[j] = sm[fft::padi<PL>(t + P * j)];
   fft::line_sync<PL>();
 
-  if constexpr (MODE == B_INV_ONLY) {
-    fft::line_fft<PL, true>(v, sm, t, a.tw);
-  } else {
-    fft::line_fft<PL, false>(v, sm, t, a.tw);
+  // iteration 0: forward (or, for B_INV_ONLY, the conjugated inverse) and the
+  // pointwise work; iteration 1: the inverse as conj(FFT(conj(.)))
+#pragma unroll 1
+  for (int it = 0; it < (TWO ? 2 : 1); ++it) {
+    if (MODE == B_INV_ONLY) fft::conj_all(v);
+    fft::line_fft<PL>(v, sm, t, a.tw);
+    if (it == 0) {
+      if constexpr (MODE == B_INV_ONLY) {
+        fft::conj_all(v);
+      } else if constexpr (TWO) {
+        col_mid<PL, MODE>(v, a, col, t, base);
+        fft::conj_all(v);
+      }
+    } else {
+      fft::conj_all(v);
+    }
   }
 
-  if constexpr (MODE == B_PROPAGATE) {
-    const float kx = a.kx[col];
-    const float kx2 = fmul_x(kx, kx);
-    const float2 pxv = a.px[col];
-#pragma unroll
-    for (int j = 0; j < E; ++j) {
-      const int n = t + P * j;
-      const float ky = a.ky[n];
-      // CreatePropsKernel (U.cu:419): keep sqrtf(kx^2+ky^2) < kmax
-      const bool keep = fsqrt_x(fadd_x(kx2, fmul_x(ky, ky))) < a.kmax;
-      const float2 w = keep ? cmul(pxv, a.py[n]) : make_float2(0.f, 0.f);
-      v[j] = cmul(v[j], w);
-    }
-    fft::line_fft<PL, true>(v, sm, t, a.tw);
-  } else if constexpr (MODE == B_CTF) {
-    const float kx = a.kx[col];
-#pragma unroll
-    for (int j = 0; j < E; ++j) {
-      const int n = t + P * j;
-      v[j] = cmul(v[j], ctf_weight(a.ctf.wavel, a.ctf.Cs, a.ctf.df, a.ctf.A2, a.ctf.phi2, a.ctf.A3, a.ctf.phi3,
-                                   a.ctf.beta, a.ctf.delta, a.ctf.objap2, kx, a.ky[n], scale));
-    }
-    fft::line_fft<PL, true>(v, sm, t, a.tw);
-  } else if constexpr (MODE == B_CBED) {
+  if constexpr (MODE == B_CBED) {
     // AddTDSWaves (U.cu:2734-2766): |FFT(psi)| placed by CentreKernel's shift
     const int xs = (col < nx / 2) ? col + nx / 2 : col - nx / 2;
 #pragma unroll
@@ -172,9 +255,7 @@ __global__ void __launch_bounds__(cols_per_cta<PL>() * PL::P) k_pass_b(PassBArgs
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) d += __shfl_down_sync(0xffffffffu, d, o);
     if (lane == 0 && d != 0.0) atomicAdd(a.sig + blockIdx.y, d * (double)scale);
-  }
-
-  if constexpr (MODE != B_CBED && MODE != B_DETECT) {
+  } else {
     // line_fft ended with a line barrier; slots are free again
 #pragma unroll
     for (int j = 0; j < E; ++j) sm[fft::padi<PL>(t + P * j)] = v[j];
@@ -231,6 +312,8 @@ cudaError_t dispatch_a_plan(const PassAArgs& a, int flags, int batch, cudaStream
     case A_MULT_T | A_FWD: return run_a<PL, A_MULT_T | A_FWD>(a, batch, s);
     case A_INV | A_MULT_T | A_FWD: return run_a<PL, A_INV | A_MULT_T | A_FWD>(a, batch, s);
     case A_INV | A_INTENSITY: return run_a<PL, A_INV | A_INTENSITY>(a, batch, s);
+    case A_INV | A_REAL: return run_a<PL, A_INV | A_REAL>(a, batch, s);
+    case A_INV | A_FD | A_FWD: return run_a<PL, A_INV | A_FD | A_FWD>(a, batch, s);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -244,6 +327,8 @@ cudaError_t dispatch_b_plan(const PassBArgs& a, int mode, int batch, cudaStream_
     case B_CTF: return run_b<PL, B_CTF>(a, batch, s);
     case B_CBED: return run_b<PL, B_CBED>(a, batch, s);
     case B_DETECT: return run_b<PL, B_DETECT>(a, batch, s);
+    case B_BANDLIMIT: return run_b<PL, B_BANDLIMIT>(a, batch, s);
+    case B_FD: return run_b<PL, B_FD>(a, batch, s);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -302,8 +302,9 @@ struct or_sim {
     bool have_atoms = false;
     /* binned structure */
     int nzb = 0;
-    std::vector<int> off, bZ;
+    std::vector<int> off, bZ, perm; /* perm: sorted position -> input index */
     std::vector<float> bx, by, bz;
+    std::vector<double> valdx, valdy; /* value-only offsets by input index (tests) */
     bool have_bins = false;
     /* Kirkland table */
     std::vector<double> fp;
@@ -457,8 +458,10 @@ static void bin_positions(or_sim* s, const float* X, const float* Y, const float
     for (int b = 0; b < nb; ++b) s->off[b + 1] += s->off[b];
     std::vector<int> cur(s->off.begin(), s->off.end() - 1);
     s->bx.resize(n); s->by.resize(n); s->bz.resize(n); s->bZ.resize(n);
+    s->perm.resize(n);
     for (size_t i = 0; i < n; ++i) {
         int d = cur[key[i]]++;
+        s->perm[d] = (int)i;
         s->bx[d] = X[i] - s->MinX; /* stored shifted by the box minimum, U.cu:1479-1482 */
         s->by[d] = Y[i] - s->MinY;
         s->bz[d] = Zp[i] - s->MinZ;
@@ -731,7 +734,9 @@ extern "C" int or_potential_conventional(or_sim* s, int it, double* out) {
                         for (int l = s->off[b]; l < s->off[b + 1]; ++l) {
                             const float dxf = pxf - s->bx[l], dyf = pyf - s->by[l];
                             const float dxy = dxf * dxf + dyf * dyf;
-                            const double dxd = pxd - s->bx[l], dyd = pyd - s->by[l];
+                            double ox = 0, oy = 0;
+                            if (!s->valdx.empty()) { ox = s->valdx[s->perm[l]]; oy = s->valdy[s->perm[l]]; }
+                            const double dxd = pxd - (s->bx[l] + ox), dyd = pyd - (s->by[l] + oy);
                             const double dxyd = dxd * dxd + dyd * dyd;
                             for (int m = 0; m < 20; ++m) {
                                 const float dzf = z2f[m] - s->bz[l];
@@ -1014,5 +1019,210 @@ extern "C" int or_annular_detector(or_sim* s, float inner, float outer, double* 
             if (k2 >= kin2 && k2 < kout2) acc += I[(size_t)y * nx + x];
         }
     *out = acc;
+    return 0;
+}
+
+/* ======================================================================
+ * Differentiable focal series (no reference counterpart): FP64 forward and
+ * adjoint used to check the engine's gradient.
+ *   psi_n = A(t_n psi_{n-1}),  A = IFFT(P FFT(.))/N,  t_n = exp(i sigma V_n)
+ *   phi_d = B_d psi_S,  B_d = IFFT(CTF_d FFT(.)/sqrt N)/sqrt N,  I_d = |phi_d|^2
+ *   L = sum_d sum_px (I_d - T_d)^2
+ * Adjoint (g = dL/dpsi*):  g_S = sum_d B_d^H [2 (I_d - T_d) phi_d],
+ *   h = A^H g_n,  dL/dV_n = -2 sigma Im(conj(h) t_n psi_{n-1}),  g_{n-1} = conj(t_n) h.
+ * ==================================================================== */
+static void ctf_apply(const or_sim* s, double df, bool conjugate, std::vector<cd>& a) {
+    /* a <- IFFT(W FFT(a)/sqrt N)/sqrt N with W the CTF weight of or_simulate_image at defocus df */
+    const int nx = s->nx, ny = s->ny;
+    const double sN = std::sqrt((double)nx * ny);
+    fft2d(a.data(), nx, ny, -1);
+    const float wavel = s->wavel, objap = s->aperture;
+    const float objap2 = (((objap * 0.001f) / wavel) * ((objap * 0.001f) / wavel));
+    const double lam = wavel, Cs = s->Cs;
+    const double beta = (double)(s->beta / 1000), delta = s->delta;
+    const double Chi1 = 3.1415926 * lam, Chi2 = 0.5 * Cs * lam * lam, factor = beta * beta / (4 * lam * lam);
+    for (int y = 0; y < ny; ++y)
+        for (int x = 0; x < nx; ++x) {
+            const size_t i = (size_t)y * nx + x;
+            const float k2f = s->kx[x] * s->kx[x] + s->ky[y] * s->ky[y];
+            if (!(k2f < objap2)) { a[i] = 0; continue; }
+            const double kx = s->kx[x], ky = s->ky[y], k2 = kx * kx + ky * ky, k = std::sqrt(k2);
+            const double es = std::exp(-factor * std::pow(3.141593 * k * lam * 2 * df +
+                                                          2 * 3.141593 * lam * lam * lam * Cs * k2 * k, 2));
+            const double ed = std::exp(-0.25 * delta * delta * 3.141593 * 3.141593 * k2 * k2 * lam * lam);
+            const double phi = std::atan2(ky, kx);
+            const double chi = Chi1 * k2 * (Chi2 * k2 + df + (double)s->A2 * std::sin(2.0 * (phi - (double)s->phi2)));
+            cd w = std::polar(es * ed, -chi);
+            if (conjugate) w = std::conj(w);
+            a[i] = (a[i] / sN) * w;
+        }
+    fft2d(a.data(), nx, ny, +1);
+    for (auto& v : a) v /= sN;
+}
+
+static void propagate(const or_sim* s, const std::vector<cd>& P, bool conjugate, std::vector<cd>& a) {
+    fft2d(a.data(), s->nx, s->ny, -1);
+    for (size_t i = 0; i < a.size(); ++i) a[i] *= conjugate ? std::conj(P[i]) : P[i];
+    ifft_norm(a, s->nx, s->ny);
+}
+
+/* Forward of the focal series.  Vstack (S*N, may be NULL: the conventional
+ * potentials are computed) and optional images out (nd*N). */
+extern "C" int or_focal_forward(or_sim* s, const float* defoci, int nd, const double* targets,
+                                const double* Vstack, int S, double* loss, double* images) {
+    if (!s->have_waves) return fail(s, "waves not initialised");
+    const int nx = s->nx, ny = s->ny;
+    const size_t N = (size_t)nx * ny;
+    std::vector<cd> P, psi = s->psi0;
+    make_props(s, s->convdz, P);
+    std::vector<double> V(N);
+    for (int n = 1; n <= S; ++n) {
+        if (Vstack) std::copy(Vstack + (size_t)(n - 1) * N, Vstack + (size_t)n * N, V.begin());
+        else if (or_potential_conventional(s, n, V.data())) return -1;
+        for (size_t i = 0; i < N; ++i) psi[i] *= std::polar(1.0, (double)s->sigma2 * V[i]);
+        propagate(s, P, false, psi);
+    }
+    double L = 0;
+    for (int d = 0; d < nd; ++d) {
+        std::vector<cd> phi = psi;
+        ctf_apply(s, defoci[d], false, phi);
+        for (size_t i = 0; i < N; ++i) {
+            const double I = std::norm(phi[i]);
+            const double r = I - targets[(size_t)d * N + i];
+            L += r * r;
+            if (images) images[(size_t)d * N + i] = I;
+        }
+    }
+    *loss = L;
+    return 0;
+}
+
+/* dv/d(r^2) of vatom (U.cu:160-193) in FP64; zero inside the 0.25 A clamp. */
+static double dvatom_dr2(const double* fp, int Z, double r2) {
+    const double* f = fp + (Z - 1) * 12;
+    const double r = std::sqrt(r2);
+    if (r < 0.25) return 0.0;
+    const double pi = 3.141592654;
+    double d = 0;
+    for (int i = 0; i < 6; i += 2) {
+        const double b = 2.0 * pi * std::sqrt(f[i + 1]);
+        d += 150.4121417 * f[i] * std::exp(-b * r) * (-1.0 / (r * r) - b / r) / (2.0 * r);
+    }
+    for (int i = 6; i < 12; i += 2) {
+        const double g = pi * pi / f[i + 1];
+        d += 266.5157269 * f[i] * std::pow(f[i + 1], -1.5) * std::exp(-g * r2) * (-g);
+    }
+    return d;
+}
+
+/* FP64 loss and gradient: dLdV (S*N) and dLdxy (2*n_atoms, input order;
+ * derivative with the box held fixed), either may be NULL. */
+extern "C" int or_focal_grad(or_sim* s, const float* defoci, int nd, const double* targets, int S,
+                             double* loss, double* dLdV, double* dLdxy) {
+    if (!s->have_waves) return fail(s, "waves not initialised");
+    if (check_pot(s)) return -1;
+    const int nx = s->nx, ny = s->ny;
+    const size_t N = (size_t)nx * ny;
+    std::vector<cd> P;
+    make_props(s, s->convdz, P);
+    std::vector<std::vector<cd>> psis(S + 1);
+    std::vector<std::vector<double>> Vs(S + 1);
+    psis[0] = s->psi0;
+    for (int n = 1; n <= S; ++n) {
+        Vs[n].resize(N);
+        if (or_potential_conventional(s, n, Vs[n].data())) return -1;
+        std::vector<cd> a = psis[n - 1];
+        for (size_t i = 0; i < N; ++i) a[i] *= std::polar(1.0, (double)s->sigma2 * Vs[n][i]);
+        propagate(s, P, false, a);
+        psis[n] = a;
+    }
+    double L = 0;
+    std::vector<cd> g(N, cd(0, 0));
+    for (int d = 0; d < nd; ++d) {
+        std::vector<cd> phi = psis[S];
+        ctf_apply(s, defoci[d], false, phi);
+        for (size_t i = 0; i < N; ++i) {
+            const double I = std::norm(phi[i]);
+            const double r = I - targets[(size_t)d * N + i];
+            L += r * r;
+            phi[i] *= 2.0 * r;
+        }
+        ctf_apply(s, defoci[d], true, phi);
+        for (size_t i = 0; i < N; ++i) g[i] += phi[i];
+    }
+    *loss = L;
+    const double sig = s->sigma2;
+    std::vector<double> G(N);
+    if (dLdxy) std::fill(dLdxy, dLdxy + 2 * s->x.size(), 0.0);
+    const std::vector<int>& perm = s->perm;
+    for (int n = S; n >= 1; --n) {
+        std::vector<cd> h = g;
+        propagate(s, P, true, h);
+        for (size_t i = 0; i < N; ++i) {
+            const cd t = std::polar(1.0, sig * Vs[n][i]);
+            G[i] = -2.0 * sig * std::imag(std::conj(h[i]) * t * psis[n - 1][i]);
+            g[i] = std::conj(t) * h[i];
+        }
+        if (dLdV) std::copy(G.begin(), G.end(), dLdV + (size_t)(n - 1) * N);
+        if (dLdxy) {
+            /* chain rule through binnedAtomPKernel3's sum, same FP32 decisions */
+            const float z = s->MaxZ - s->MinZ - s->convdz * n;
+            const int K = (int)std::floor((s->MaxZ - s->MinZ - z) / (float)1);
+            const int kt = std::max(K - s->lbz, 0), kb = std::min(K + s->lbz, s->nzb - 1);
+            float z2f[20];
+            double z2d[20];
+            for (int m = 1; m <= 20; ++m) {
+                z2f[m - 1] = z - m * s->convdz / 20.0f;
+                z2d[m - 1] = (double)z - m * (double)s->convdz / 20.0;
+            }
+            const double wsub = (double)s->convdz / 20.0;
+            const int a0 = s->off[kt * kBins * kBins], a1 = s->off[(kb + 1) * kBins * kBins];
+#pragma omp parallel for schedule(dynamic, 8)
+            for (int l = a0; l < a1; ++l) {
+                double X = s->bx[l], Y = s->by[l];
+                if (!s->valdx.empty()) { X += s->valdx[perm[l]]; Y += s->valdy[perm[l]]; }
+                const int x0 = std::max(0, (int)std::floor((X - s->xoff - 2.3) / s->ps));
+                const int x1 = std::min(nx - 1, (int)std::ceil((X - s->xoff + 2.3) / s->ps));
+                const int y0 = std::max(0, (int)std::floor((Y - s->yoff - 2.3) / s->ps));
+                const int y1 = std::min(ny - 1, (int)std::ceil((Y - s->yoff + 2.3) / s->ps));
+                double gx = 0, gy = 0;
+                for (int y = y0; y <= y1; ++y)
+                    for (int x = x0; x <= x1; ++x) {
+                        const float pxf = s->xoff + x * s->ps, pyf = s->yoff + y * s->ps;
+                        const float dxf = pxf - s->bx[l], dyf = pyf - s->by[l];
+                        const float dxy = dxf * dxf + dyf * dyf;
+                        if (!(dxy < 5.0f)) continue;
+                        const double pxd = (double)s->xoff + x * (double)s->ps, pyd = (double)s->yoff + y * (double)s->ps;
+                        const double dxd = pxd - X, dyd = pyd - Y;
+                        double acc = 0;
+                        for (int m = 0; m < 20; ++m) {
+                            const float dzf = z2f[m] - s->bz[l];
+                            if (!(dxy + dzf * dzf < 5.0f)) continue;
+                            const double dzd = z2d[m] - s->bz[l];
+                            acc += wsub * dvatom_dr2(s->fp.data(), s->bZ[l], dxd * dxd + dyd * dyd + dzd * dzd);
+                        }
+                        const double Gp = G[(size_t)y * nx + x];
+                        gx += Gp * acc * (-2.0 * dxd);
+                        gy += Gp * acc * (-2.0 * dyd);
+                    }
+                dLdxy[2 * perm[l]] += gx;
+                dLdxy[2 * perm[l] + 1] += gy;
+            }
+        }
+    }
+    return 0;
+}
+
+/* Test hook: offset atom i's position by (dx, dy) in the potential VALUES
+ * only; every FP32 decision keeps the stored position.  Finite differences
+ * taken this way see no cut-off flips and measure the chain-rule gradient. */
+extern "C" int or_set_value_offset(or_sim* s, int i, double dx, double dy) {
+    if (!s->have_atoms || i < 0 || i >= (int)s->x.size()) return fail(s, "bad atom index");
+    if (s->valdx.empty()) {
+        s->valdx.assign(s->x.size(), 0.0);
+        s->valdy.assign(s->x.size(), 0.0);
+    }
+    s->valdx[i] = dx;
+    s->valdy[i] = dy;
     return 0;
 }

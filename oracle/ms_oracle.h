@@ -99,6 +99,17 @@ int or_annular_detector(or_sim*, float inner_mrad, float outer_mrad, double* out
 /* diffraction intensity |FFT(psi)/sqrt(N)|^2 (unshifted) */
 int or_diffraction(or_sim*, double* out);
 
+/* Differentiable focal series (no reference counterpart): loss
+ * sum_d sum_px (|B_d psi_S|^2 - T_d)^2 over conventional slices 1..S from the
+ * initial wave.  Vstack (S*N) replaces the computed potentials when not NULL. */
+int or_focal_forward(or_sim*, const float* defoci, int nd, const double* targets, const double* Vstack,
+                     int S, double* loss, double* images);
+/* FP64 adjoint: dLdV (S*N) and dLdxy (2 per atom, input order, box fixed). */
+int or_focal_grad(or_sim*, const float* defoci, int nd, const double* targets, int S, double* loss,
+                  double* dLdV, double* dLdxy);
+/* Test hook: value-only position offset of atom i (decisions unchanged). */
+int or_set_value_offset(or_sim*, int i, double dx, double dy);
+
 #ifdef __cplusplus
 }
 #endif

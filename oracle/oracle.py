@@ -87,6 +87,9 @@ def lib():
         "or_get_tds": (_i, [_p, _p]),
         "or_annular_detector": (_i, [_p, _f, _f, _p]),
         "or_diffraction": (_i, [_p, _p]),
+        "or_focal_forward": (_i, [_p, _p, _i, _p, _p, _i, _p, _p]),
+        "or_focal_grad": (_i, [_p, _p, _i, _p, _i, _p, _p, _p]),
+        "or_set_value_offset": (_i, [_p, _i, _d, _d]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -338,3 +341,31 @@ class OracleSimulation:
         for i in range(1, n + 1):
             self.MultisliceStepConventional(i)
         return self.Wave()
+
+    # ---- differentiable focal series ----
+    def FocalForward(self, defoci, targets, S: int, Vstack=None):
+        d = np.ascontiguousarray(defoci, np.float32)
+        T = np.ascontiguousarray(targets, np.float64)
+        imgs = np.zeros((d.size, self.ny, self.nx), np.float64)
+        loss = _d(0)
+        Vp = None
+        if Vstack is not None:
+            Vs = np.ascontiguousarray(Vstack, np.float64)
+            Vp = _ptr(Vs)
+        self._chk(self._L.or_focal_forward(self._h, _ptr(d), d.size, _ptr(T), Vp, int(S), C.byref(loss),
+                                           _ptr(imgs)))
+        return loss.value, imgs
+
+    def FocalGrad(self, defoci, targets, S: int, want_xy: bool = True):
+        d = np.ascontiguousarray(defoci, np.float32)
+        T = np.ascontiguousarray(targets, np.float64)
+        gV = np.zeros((S, self.ny, self.nx), np.float64)
+        n = self.Binned()[1].size
+        gxy = np.zeros((n, 2), np.float64) if want_xy else None
+        loss = _d(0)
+        self._chk(self._L.or_focal_grad(self._h, _ptr(d), d.size, _ptr(T), int(S), C.byref(loss), _ptr(gV),
+                                        _ptr(gxy) if want_xy else None))
+        return loss.value, gV, gxy
+
+    def SetValueOffset(self, i: int, dx: float, dy: float):
+        self._chk(self._L.or_set_value_offset(self._h, int(i), float(dx), float(dy)))

@@ -213,8 +213,9 @@ def test_stem_probe_cbed_and_haadf(engine_cls, oracle_mod, path):
 
 
 # ---------------------------------------------------------------- finite differences
-def test_finite_difference_steps(engine_cls, oracle_mod):
-    eng, orc = make_pair(engine_cls, oracle_mod, sto(2, 2), 128, 0.1, kV=200.0)
+@pytest.mark.parametrize("path", [0, 1])
+def test_finite_difference_steps(engine_cls, oracle_mod, path):
+    eng, orc = make_pair(engine_cls, oracle_mod, sto(2, 2), 128, 0.1, kV=200.0, path=path)
     for s in (eng, orc):
         s.InitialiseWavefunctions()
         s.SetFDdz(0.05)
@@ -293,3 +294,21 @@ def test_stem_raster_batched(engine_cls, oracle_mod, path):
     ref = np.array(ref)
     assert np.all(ref > 0)
     assert np.max(np.abs(sig - ref) / ref) < 1e-4, (sig, ref)
+
+
+def test_fd_readout_then_continue(engine_cls, oracle_mod):
+    # reading the wave mid-run must not disturb the fused finite-difference state
+    eng, orc = make_pair(engine_cls, oracle_mod, sto(2, 2), 128, 0.1, kV=200.0)
+    for s in (eng, orc):
+        s.InitialiseWavefunctions()
+        s.SetFDdz(0.05)
+    for i in range(1, 11):
+        eng.MultisliceStepFD(i)
+        orc.MultisliceStepFD(i)
+    assert rel_l2(eng.ExitWave(), orc.Wave()) < 5 * TOL
+    for i in range(11, 21):
+        eng.MultisliceStepFD(i)
+        orc.MultisliceStepFD(i)
+    assert rel_l2(eng.ExitWave(), orc.Wave()) < 5 * TOL
+    eng.SimulateImage(0.0)
+    assert rel_l2(eng.Image(), orc.SimulateImage()) < 5 * TOL
