@@ -209,6 +209,74 @@ def stem_leg(fparams, device: int, nprobes: int = 256, batch: int = 16) -> dict:
             "timing": "host clock around ms_stem_raster (synchronous), potential stack resident"}
 
 
+def adjoint_leg(fparams, device: int, reps: int = 3) -> dict:
+    """Differentiable focal series on the inverse-problem workload: SrTiO3
+    4 x 4 x 50 cells (4,000 atoms), 512^2 over the 15.62 A cell, 100 slices of
+    1.9525 A, 200 kV, Cs 1 mm, 20 mrad, 8 CTF images at defocus -80..+60 nm;
+    targets are the images of the same crystal with seeded position errors
+    (sigma 0.1 A in x, y, z); L2 loss.  Device time (CUDA events) of the
+    forward (potential build + 100 slices + 8 images + loss) against forward +
+    adjoint (dL/dV of every slice, dL/dxy of every atom, sqrt(S)-slice
+    checkpointing), potentials rebuilt on every call as in one optimisation
+    step; and the same pair with the potential stack resident (dL/dV only)."""
+    import numpy as np
+
+    from cudamultislice_b200 import ManagedMultisliceSimulation
+    from cudamultislice_b200 import structures as S
+
+    n, nslices = 512, 100
+    df = np.linspace(-800.0, 600.0, 8).astype(np.float32)
+    Z, x, y, z = S.srtio3(4, 4, 50)
+    rng = np.random.default_rng(2026)
+    pert = [(a + rng.normal(0.0, 0.1, a.size)).astype(np.float32) for a in (x, y, z)]
+    sim = ManagedMultisliceSimulation(device=device)
+
+    def setup(xx, yy, zz):
+        sim.SetAtoms(Z, xx, yy, zz)
+        sim.UploadBinnedAtoms()
+        sim.GetParameterisation(fparams)
+        sim.ApplyMicroscopeParameters(200.0, 0.0, 0.0, 0.0, 1.0e7, 0.1, 30.0, 20.0)
+        sim.SetCalculationVariables(3.905 * 4 / n, 0.0, n, n, sim.GetSizeX(), sim.GetSizeY(), sim.GetSizeZ(),
+                                    2.0, 2.0)
+        sim.PreCalculateFrequencies()
+        sim.InitialiseWavefunctions(1.9525)
+
+    setup(*pert)
+    _, T = sim.FocalSeries(df, np.zeros((8, n, n), np.float32), nslices, images=True)
+    setup(x, y, z)
+
+    def timed(fn, rebuild):
+        best = None
+        for k in range(reps + 1):
+            if rebuild:
+                sim.UploadBinnedAtoms()
+            fn()
+            if k > 0:
+                t = sim.LastDeviceMs()
+                best = t if best is None else min(best, t)
+        return best
+
+    fwd = timed(lambda: sim.FocalSeries(df, T, nslices), True)
+    grad = timed(lambda: sim.FocalSeriesGrad(df, T, nslices, want_v=True, want_xy=True), True)
+    fwd_res = timed(lambda: sim.FocalSeries(df, T, nslices), False)
+    grad_res = timed(lambda: sim.FocalSeriesGrad(df, T, nslices, want_v=True, want_xy=False), False)
+    sim.SetCheckpoint(1)
+    grad_res_k1 = timed(lambda: sim.FocalSeriesGrad(df, T, nslices, want_v=True, want_xy=False), False)
+    sim.SetCheckpoint(0)
+    loss = sim.FocalSeries(df, T, nslices)
+    sim.close()
+    return {
+        "config": f"SrTiO3 4x4x50 cells ({len(Z)} atoms), {n}^2, {nslices} slices of 1.9525 A, 200 kV, "
+                  "8 defoci -80..+60 nm, targets from seeded 0.1 A position errors",
+        "forward_ms": fwd, "grad_ms": grad, "grad_over_forward": grad / fwd,
+        "potentials_resident": {"forward_ms": fwd_res, "grad_dV_ms": grad_res, "grad_over_forward": grad_res / fwd_res,
+                                "grad_dV_ms_store_all": grad_res_k1,
+                                "store_all_over_forward": grad_res_k1 / fwd_res},
+        "checkpoint_stride": int(np.ceil(np.sqrt(nslices))), "loss": loss,
+        "timing": "device time (CUDA events on the engine stream), best of 3 after a warm-up call",
+    }
+
+
 def cpu_baseline(atoms, fparams, nslices: int, threads: int) -> dict:
     """The FP64 OpenMP oracle on the host cores, on the first `nslices`
     slices of the same workload (potential build + transmission +
@@ -274,10 +342,19 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="profiling mode: set-up plus the timed slice loop only (no e2e, plain or CPU legs)")
+    ap.add_argument("--leg", choices=["stem", "adjoint"],
+                    help="run one secondary leg alone and print its JSON (exploration)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.leg:
+        from cudamultislice_b200 import FPARAMS
+
+        leg = stem_leg(FPARAMS, local) if args.leg == "stem" else adjoint_leg(FPARAMS, local)
+        if rank == 0:
+            print(json.dumps({"leg": args.leg, **leg}), flush=True)
         return
 
     from cudamultislice_b200 import FPARAMS, ManagedMultisliceSimulation
@@ -377,6 +454,7 @@ def main():
     }
 
     out["stem"] = stem_leg(FPARAMS, local)
+    out["adjoint"] = adjoint_leg(FPARAMS, local)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1

@@ -1,4 +1,5 @@
 // ms_atoms.cu -- bit-exact atom binning and the potential-build kernels.
+#include <algorithm>
 #include <cmath>
 
 #include "ms_atoms.cuh"
@@ -437,7 +438,111 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
   if (inside) a.V[(long long)y * a.nx + x] = acc;
 }
 
+// Adjoint of k_potential_conv with respect to the atoms' x and y.  For slice
+// potential V(p) = sum_atoms sum_m wsub v(r^2), r^2 = (p - X)^2 + dz_m^2, and
+// the slice's dL/dV field G:
+//   dL/dX = sum_p G(p) wsub sum_m v'(r^2) (-2 (px - X)),  likewise for Y,
+// over exactly the (pixel, atom, sub-plane) triples the forward kept (the same
+// non-contracted FP32 cut-off tests on the same stored positions; the forward
+// visits every atom of the z-window within sqrt(5) A of a pixel).  Inside the
+// 0.25 A clamp v is constant and contributes nothing.  blockIdx.x picks the
+// atom of the window, blockIdx.y one of gridDim.y interleaved row sets of its
+// +-2.3 A pixel square (so that a window of few atoms still fills the GPU);
+// each CTA's sums (FP64 across threads) are added atomically to the atom's
+// entry in input order.
+//   v'(r^2) = sum_i c_i e^{-b_i r} (-b_i r - 1) / (2 r^3)
+//             - ln2 sum_k c9_k c6_k 2^{-c9_k r^2}     (c layout of vatom_f).
+__global__ void __launch_bounds__(kPotThreads) k_potential_conv_adjoint(PotArgs a, const float* __restrict__ G,
+                                                                        const int* __restrict__ perm, int a0,
+                                                                        double* __restrict__ dxy) {
+  __shared__ float s_dz2[20];
+  __shared__ float s_gz[3][20];
+  __shared__ double s_red[2][kPotThreads / 32];
+  constexpr float kLn2 = 0.6931471805599453f;
+  const int l = a0 + blockIdx.x;
+  const float4 at = a.atoms[l];
+  const float* c = a.coef + (__float_as_int(at.w) - 1) * kCoefPerZ;
+  if (threadIdx.x < 20) {
+    const int m = threadIdx.x;
+    const float dz = fsub_x(a.zsub[m], at.z);
+    const float dz2 = fmul_x(dz, dz);
+    s_dz2[m] = dz2;
+    s_gz[0][m] = ex2_fast(-c[9] * dz2);
+    s_gz[1][m] = ex2_fast(-c[10] * dz2);
+    s_gz[2][m] = ex2_fast(-c[11] * dz2);
+  }
+  __syncthreads();
+  const float b0 = c[3] * kLn2, b1 = c[4] * kLn2, b2 = c[5] * kLn2;
+  const float h0 = -kLn2 * c[9] * c[6], h1 = -kLn2 * c[10] * c[7], h2 = -kLn2 * c[11] * c[8];
+  const int xl = max((int)floorf((at.x - 2.3f - a.xoff) / a.ps), 0);
+  const int xh = min((int)ceilf((at.x + 2.3f - a.xoff) / a.ps), a.nx - 1);
+  const int yl = max((int)floorf((at.y - 2.3f - a.yoff) / a.ps), 0);
+  const int yh = min((int)ceilf((at.y + 2.3f - a.yoff) / a.ps), a.ny - 1);
+  const int wx = xh - xl + 1, wy = yh - yl + 1;
+  const int ns = gridDim.y, js = blockIdx.y;
+  float gx = 0.0f, gy = 0.0f;
+  if (wx > 0 && wy > js) {
+    const int npx = wx * ((wy - js + ns - 1) / ns);
+    for (int w = threadIdx.x; w < npx; w += kPotThreads) {
+      const int x = xl + w % wx, y = yl + js + (w / wx) * ns;
+      const float px = fadd_x(a.xoff, fmul_x((float)x, a.ps));
+      const float py = fadd_x(a.yoff, fmul_x((float)y, a.ps));
+      const float dx = fsub_x(px, at.x), dy = fsub_x(py, at.y);
+      const float dxy = fadd_x(fmul_x(dx, dx), fmul_x(dy, dy));
+      if (!(dxy < 5.0f)) continue;
+      const float gp = G[(long long)y * a.nx + x];
+      const float g0 = h0 * ex2_fast(-c[9] * dxy), g1 = h1 * ex2_fast(-c[10] * dxy), g2 = h2 * ex2_fast(-c[11] * dxy);
+      float D = 0.0f;
+#pragma unroll 4
+      for (int m = 0; m < 20; ++m) {
+        const float r2 = fadd_x(dxy, s_dz2[m]);
+        if (!(r2 < 5.0f) || r2 < 0.0625f) continue;
+        const float ri = rsqrtf(r2), r = r2 * ri;
+        const float L = c[0] * ex2_fast(-c[3] * r) * fmaf(-b0, r, -1.0f) +
+                        c[1] * ex2_fast(-c[4] * r) * fmaf(-b1, r, -1.0f) +
+                        c[2] * ex2_fast(-c[5] * r) * fmaf(-b2, r, -1.0f);
+        D += 0.5f * L * ri * ri * ri + g0 * s_gz[0][m] + g1 * s_gz[1][m] + g2 * s_gz[2][m];
+      }
+      gx += gp * D * dx;
+      gy += gp * D * dy;
+    }
+  }
+  double sx = gx, sy = gy;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    sx += __shfl_down_sync(0xffffffffu, sx, o);
+    sy += __shfl_down_sync(0xffffffffu, sy, o);
+  }
+  const int warp = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    s_red[0][warp] = sx;
+    s_red[1][warp] = sy;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tx = 0.0, ty = 0.0;
+    for (int k = 0; k < kPotThreads / 32; ++k) {
+      tx += s_red[0][k];
+      ty += s_red[1][k];
+    }
+    const double f = -2.0 * (double)a.wsub;
+    const int i = perm[l];
+    atomicAdd(dxy + 2 * i, f * tx);
+    atomicAdd(dxy + 2 * i + 1, f * ty);
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_potential_adjoint(const PotArgs& a, const float* G, const int* perm, int a0, int a1, double* dxy,
+                                     cudaStream_t s) {
+  if (a1 <= a0) return cudaSuccess;
+  // about 8 CTAs per SM (148 SMs) in all, at most 16 row sets per atom
+  const int na = a1 - a0;
+  const int ns = std::min(16, std::max(1, (8 * 148 + na - 1) / na));
+  k_potential_conv_adjoint<<<dim3(na, ns), kPotThreads, 0, s>>>(a, G, perm, a0, dxy);
+  return cudaGetLastError();
+}
 
 size_t bin_scratch_blocks(int nbins) { return (size_t)(nbins + kScanTile - 1) / kScanTile + 1; }
 

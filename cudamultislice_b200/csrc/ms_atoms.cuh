@@ -57,4 +57,10 @@ struct PotArgs {
 
 cudaError_t launch_potential(const PotArgs& a, int kind, cudaStream_t s);
 
+// Adjoint of the conventional potential of one slice with respect to atom x, y:
+// dxy[2 perm[l] + {0,1}] += dL/d{x,y} of sorted atoms l in [a0, a1) (the CSR
+// range of the slice's z-window), G = dL/dV of the slice [ny][nx].
+cudaError_t launch_potential_adjoint(const PotArgs& a, const float* G, const int* perm, int a0, int a1, double* dxy,
+                                     cudaStream_t s);
+
 }  // namespace ms

@@ -145,6 +145,10 @@ class Engine {
         stack_valid_ = false;
         invalidate_graph();
         return MS_OK;
+      case MS_OPT_CHECKPOINT:
+        if (value < 0) return fail(MS_ERR_INVALID, "checkpoint stride must be 0 (ceil(sqrt(S))) or >= 1");
+        ckpt_ = value;
+        return MS_OK;
       case MS_OPT_FFT_PLAN:
         if (value < -1 || value >= plan_variants()) return fail(MS_ERR_INVALID, "FFT plan must be -1 (tuned) or a variant index");
         forced_plan_ = value;
@@ -265,6 +269,7 @@ class Engine {
     natoms_ = n;
     nzb_ = nz;
     have_index_ = true;
+    hzoff_.clear();
     stack_valid_ = false;
     invalidate_graph();
     return MS_OK;
@@ -310,7 +315,7 @@ class Engine {
       if (!ok) return fail(MS_ERR_IO, "parameterisation row with b < 0 or d <= 0");
     }
     MS_TRY(d_coef_.resize(coef.size()));
-    MS_TRY(cudaMemcpy(d_coef_.p, coef.data(), sizeof(float) * coef.size(), cudaMemcpyHostToDevice));
+    MS_TRY(copy_sync(d_coef_.p, coef.data(), sizeof(float) * coef.size(), cudaMemcpyHostToDevice));
     have_fp_ = true;
     stack_valid_ = false;
     invalidate_graph();
@@ -389,8 +394,8 @@ class Engine {
     const size_t N = (size_t)nx * ny;
     MS_TRY(d_kx_.resize(nx));
     MS_TRY(d_ky_.resize(ny));
-    MS_TRY(cudaMemcpy(d_kx_.p, hkx_.data(), sizeof(float) * nx, cudaMemcpyHostToDevice));
-    MS_TRY(cudaMemcpy(d_ky_.p, hky_.data(), sizeof(float) * ny, cudaMemcpyHostToDevice));
+    MS_TRY(copy_sync(d_kx_.p, hkx_.data(), sizeof(float) * nx, cudaMemcpyHostToDevice));
+    MS_TRY(copy_sync(d_ky_.p, hky_.data(), sizeof(float) * ny, cudaMemcpyHostToDevice));
     // wave buffers
     MS_TRY(d_psi0_.resize(N));
     MS_TRY(d_psi_.resize(N));
@@ -416,10 +421,10 @@ class Engine {
       for (int v = 0; v < plan_variants(); ++v) {
         const int sx = make_twiddles(nx, v, tw.data());
         MS_TRY(d_twx_[v].resize(std::max(sx, 1)));
-        MS_TRY(cudaMemcpy(d_twx_[v].p, tw.data(), sizeof(float2) * sx, cudaMemcpyHostToDevice));
+        MS_TRY(copy_sync(d_twx_[v].p, tw.data(), sizeof(float2) * sx, cudaMemcpyHostToDevice));
         const int sy = make_twiddles(ny, v, tw.data());
         MS_TRY(d_twy_[v].resize(std::max(sy, 1)));
-        MS_TRY(cudaMemcpy(d_twy_[v].p, tw.data(), sizeof(float2) * sy, cudaMemcpyHostToDevice));
+        MS_TRY(copy_sync(d_twy_[v].p, tw.data(), sizeof(float2) * sy, cudaMemcpyHostToDevice));
       }
     }
     prop_dz_ = -1.0f;
@@ -533,11 +538,15 @@ class Engine {
     MS_TRY(d_fdS_.resize(N));
     if (!fd_state_) {
       if (int rc = ensure_real()) return rc;
-      // X = FFT_row(psi_n), spectrum = FFT_col(X) stored column-major
-      MS_TRY(pass_a(passa_args(d_psi_.p, d_fdX_.p, 0), A_FWD, 1));
-      MS_TRY(pass_b(passb_args(d_fdX_.p, d_t1_.p, 0), B_FWD_ONLY, 1));
+      // spectrum FFT2(psi_n) = FFT_col(FFT_row(psi_n)) stored column-major,
+      // X = FFT_row(psi_n) / nx (so that IFFT_row(X) = psi_n)
+      MS_TRY(pass_a(passa_args(d_psi_.p, d_t2_.p, 0), A_FWD, 1));
+      MS_TRY(pass_b(passb_args(d_t2_.p, d_t1_.p, 0), B_FWD_ONLY, 1));
       MS_TRY(pw_transpose(d_t1_.p, d_fdS_.p, g, stream_, &launches));
-      launches += 2;
+      PassAArgs x0 = passa_args(d_psi_.p, d_fdX_.p, 0);
+      x0.scale = 1.0f / (float)nx_;
+      MS_TRY(pass_a(x0, A_FWD, 1));
+      launches += 3;
       fd_state_ = true;
     }
     // V at the plane, band-limited (U.cu:2053-2063), real part kept
@@ -1032,11 +1041,11 @@ class Engine {
     std::vector<float2> tw(2 * (size_t)std::max(nx, ny));
     const int sx = make_twiddles(nx, v, tw.data());
     MS_TRY(tw1.resize(std::max(sx, 1)));
-    MS_TRY(cudaMemcpy(tw1.p, tw.data(), sizeof(float2) * sx, cudaMemcpyHostToDevice));
+    MS_TRY(copy_sync(tw1.p, tw.data(), sizeof(float2) * sx, cudaMemcpyHostToDevice));
     const int sy = make_twiddles(ny, v, tw.data());
     MS_TRY(tw2.resize(std::max(sy, 1)));
-    MS_TRY(cudaMemcpy(tw2.p, tw.data(), sizeof(float2) * sy, cudaMemcpyHostToDevice));
-    MS_TRY(cudaMemcpy(buf.p, in, sizeof(float2) * N, cudaMemcpyHostToDevice));
+    MS_TRY(copy_sync(tw2.p, tw.data(), sizeof(float2) * sy, cudaMemcpyHostToDevice));
+    MS_TRY(copy_sync(buf.p, in, sizeof(float2) * N, cudaMemcpyHostToDevice));
     PassAArgs a{};
     a.in = buf.p; a.out = buf.p; a.tw = tw1.p; a.nx = nx; a.ny = ny; a.scale = 1.0f;
     PassBArgs b{};
@@ -1046,6 +1055,181 @@ class Engine {
     launches += 2;
     MS_TRY(cudaMemcpyAsync(out, buf.p, sizeof(float2) * N, cudaMemcpyDeviceToHost, stream_));
     MS_TRY(cudaStreamSynchronize(stream_));
+    return MS_OK;
+  }
+
+  // ---- differentiable focal series (no reference counterpart) ----
+  // L = sum_d sum_p (I_d - T_d)^2 with I_d = |B_d psi_S|^2, psi_S the wave
+  // after conventional slices 1..S of the potential stack from the initial
+  // wave and B_d the coherent transfer of SimulateImage (U.cu:2311-2343) at
+  // defocus d.  The adjoint runs the slices backwards with the conjugated
+  // propagator and transmission:
+  //   g_S = sum_d B_d^H [2 (I_d - T_d) B_d psi_S],   h = A^H g_n,
+  //   dL/dV_n = -2 sigma Im(conj(h) t_n psi_{n-1}),  g_{n-1} = conj(t_n) h,
+  // and through the potential build to the atoms' x, y.  The waves psi_{n-1}
+  // are recomputed segment by segment from checkpoints every K slices
+  // (K = ceil(sqrt(S)) unless MS_OPT_CHECKPOINT sets it; K >= S keeps one
+  // segment, K = 1 stores every wave in the forward sweep).
+  // All waves are held in the fused passes' row-frequency form X with
+  // IFFT_row(X) = field; the adjoint state g uses the same form.
+  int focal(const float* defoci, int nd, const float* targets, int S, double* loss, float* images, float* dLdV,
+            double* dLdxy, bool grad) {
+    if (!have_waves_) return fail(MS_ERR_STATE, "wavefunctions not initialised");
+    if (!defoci || !targets || !loss || nd < 1) return fail(MS_ERR_INVALID, "need defoci, targets, loss and nd >= 1");
+    for (int d = 0; d < nd; ++d)
+      if (!std::isfinite(defoci[d])) return fail(MS_ERR_INVALID, "non-finite defocus");
+    if (!use_fused()) return fail(MS_ERR_UNSUPPORTED, "the focal series runs on the fused passes (grid 64..2048, powers of two)");
+    if (stem_) return fail(MS_ERR_UNSUPPORTED, "the focal series needs TEM calculation variables");
+    if (int rc = require_potential_inputs()) return rc;
+    int Sall = 0;
+    if (int rc = get_slices(true, &Sall)) return rc;
+    if (S < 1 || S > Sall) return fail(MS_ERR_INVALID, "slice count must be 1..ms_get_slices(conventional)");
+    if (dLdxy && pot_mode_ != 0)
+      return fail(MS_ERR_UNSUPPORTED, "atom gradients need the conventional potential (MS_OPT_POTENTIAL 0)");
+    if (int rc = ensure_prop_tables(convdz_)) return rc;
+    plan_for(1);
+    const size_t N = (size_t)nx_ * ny_;
+    const int K = grad ? (ckpt_ > 0 ? std::min(ckpt_, S) : (int)std::ceil(std::sqrt((double)S))) : S;
+    const int nck = (S + K - 1) / K;
+    MS_TRY(d_T_.resize(N * nd));
+    MS_TRY(d_Phi_.resize(N));
+    MS_TRY(d_loss_.resize(1));
+    if (images) MS_TRY(d_img_.resize(N * nd));
+    if (grad) {
+      MS_TRY(d_G_.resize(N));
+      MS_TRY(d_U_.resize(N));
+      MS_TRY(d_ck_.resize(N * std::max(nck - 1, 1)));
+      MS_TRY(d_seg_.resize(N * K));
+      MS_TRY(d_dV_.resize(dLdV ? N * S : N));
+      if (dLdxy) {
+        MS_TRY(d_dxy_.resize(2 * (size_t)natoms_));
+        if (int rc = zbin_starts()) return rc;
+      }
+    }
+    invalidate_graph();  // the sweep below leaves d_psi_ at psi_S
+    MS_TRY(cudaMemcpyAsync(d_T_.p, targets, sizeof(float) * N * nd, cudaMemcpyHostToDevice, stream_));
+    MS_TRY(cudaMemsetAsync(d_loss_.p, 0, sizeof(double), stream_));
+    if (grad && dLdxy) MS_TRY(cudaMemsetAsync(d_dxy_.p, 0, sizeof(double) * 2 * natoms_, stream_));
+    // timed from here: the potential stack (when the atoms changed), the sweeps
+    MS_TRY(cudaEventRecord(ev0_, stream_));
+    if (int rc = build_stack(&Sall)) return rc;
+    // forward sweep; checkpoint c (c = 1..nck-1) holds X_{cK}; the waves of
+    // the last segment (psi_{clast} .. psi_{S-1}) are kept as they pass
+    const int clast = ((S - 1) / K) * K;
+    for (int n = 1; n <= S; ++n) {
+      if (grad && n > 1 && (n - 1) % K == 0)
+        MS_TRY(cudaMemcpyAsync(d_ck_.p + (size_t)((n - 1) / K - 1) * N, d_psi_.p, sizeof(float2) * N,
+                               cudaMemcpyDeviceToDevice, stream_));
+      if (grad && n - 1 >= clast) {
+        PassAArgs a = passa_args(n == 1 ? d_psi0_.p : d_psi_.p, d_psi_.p, 0);
+        a.V = d_stack_.p + (size_t)(n - 1) * N;
+        a.out2 = d_seg_.p + (size_t)(n - 1 - clast) * N;
+        MS_TRY(pass_a(a, n == 1 ? (A_SAVE | A_MULT_T | A_FWD) : (A_INV | A_SAVE | A_MULT_T | A_FWD), 1));
+        MS_TRY(pass_b(passb_args(d_psi_.p, d_psi_.p, 0), B_PROPAGATE, 1));
+        domain_ = 1;
+      } else if (int rc = enqueue_fused_step(d_stack_.p + (size_t)(n - 1) * N, n == 1)) {
+        return rc;
+      }
+      launches += 2;
+    }
+    // images, loss and the adjoint seed
+    const float wavel = wavel_, objap = aperture_;
+    const float objap2 = (((objap * 0.001f) / wavel) * ((objap * 0.001f) / wavel));
+    for (int d = 0; d < nd; ++d) {
+      PassBArgs b = passb_args(d_psi_.p, d_Phi_.p, 0);
+      b.ctf = CtfParams{(double)wavel, (double)Cs_, (double)defoci[d], (double)A2_, (double)phi2_, 0.0, 0.0,
+                        (double)(beta_ / 1000), (double)delta_, objap2};
+      b.scale = (float)nx_ / (float)N;  // FFT_rows(psi) = nx X
+      MS_TRY(pass_b(b, B_CTF, 1));
+      PassAArgs a = passa_args(d_Phi_.p, grad ? d_U_.p : nullptr, 0);
+      a.T = d_T_.p + (size_t)d * N;
+      a.loss = d_loss_.p;
+      a.out_f = images ? d_img_.p + (size_t)d * N : nullptr;
+      MS_TRY(pass_a(a, grad ? (A_INV | A_RESID | A_FWD) : (A_INV | A_RESID), 1));
+      launches += 2;
+      if (grad) {
+        b.in = d_U_.p;
+        b.out = d_G_.p;
+        b.scale = 1.0f / (float)N;
+        b.accumulate = d > 0;
+        MS_TRY(pass_b(b, B_CTF_ADJ, 1));
+        ++launches;
+      }
+    }
+    if (grad) {
+      for (int c = clast; c >= 0; c -= K) {
+        const int e = std::min(c + K, S);
+        // psi_c .. psi_{e-1} (real space) into segment slots 0 .. e-1-c
+        // (the last segment's are there from the forward sweep)
+        const float2* src = c == 0 ? d_psi0_.p : d_ck_.p + (size_t)(c / K - 1) * N;
+        const float2* cur = src;
+        for (int n = c + 1; n <= e - 1 && c != clast; ++n) {
+          PassAArgs a = passa_args(cur, d_t1_.p, 0);
+          a.V = d_stack_.p + (size_t)(n - 1) * N;
+          a.out2 = d_seg_.p + (size_t)(n - 1 - c) * N;
+          const bool real_in = (n == 1);
+          MS_TRY(pass_a(a, real_in ? (A_SAVE | A_MULT_T | A_FWD) : (A_INV | A_SAVE | A_MULT_T | A_FWD), 1));
+          MS_TRY(pass_b(passb_args(d_t1_.p, d_t1_.p, 0), B_PROPAGATE, 1));
+          launches += 2;
+          cur = d_t1_.p;
+        }
+        float2* last = d_seg_.p + (size_t)(e - 1 - c) * N;
+        if (c == clast) {
+          // saved by the forward sweep
+        } else if (e - 1 == 0) {
+          MS_TRY(cudaMemcpyAsync(last, d_psi0_.p, sizeof(float2) * N, cudaMemcpyDeviceToDevice, stream_));
+        } else {
+          MS_TRY(pass_a(passa_args(cur, last, 0), A_INV, 1));
+          ++launches;
+        }
+        // adjoint steps e .. c+1
+        for (int n = e; n >= c + 1; --n) {
+          PassBArgs b = passb_args(d_G_.p, d_G_.p, 0);
+          b.scale = (float)nx_;
+          MS_TRY(pass_b(b, B_PROPAGATE_ADJ, 1));
+          PassAArgs a = passa_args(d_G_.p, d_G_.p, 0);
+          a.V = d_stack_.p + (size_t)(n - 1) * N;
+          a.in2 = d_seg_.p + (size_t)(n - 1 - c) * N;
+          float* dV = dLdV ? d_dV_.p + (size_t)(n - 1) * N : d_dV_.p;
+          a.out_f = dV;
+          a.scale = 1.0f / (float)nx_;
+          MS_TRY(pass_a(a, A_INV | A_ADJ | A_FWD, 1));
+          launches += 2;
+          if (dLdxy) {
+            const PotArgs pa = pot_args(POT_CONVENTIONAL, n, nullptr);
+            const int a0 = hzoff_[pa.kt], a1 = hzoff_[pa.kb + 1];
+            MS_TRY(launch_potential_adjoint(pa, dV, d_idx_.p, a0, a1, d_dxy_.p, stream_));
+            ++launches;
+          }
+        }
+      }
+    }
+    MS_TRY(cudaEventRecord(ev1_, stream_));
+    MS_TRY(cudaMemcpyAsync(loss, d_loss_.p, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    if (images)
+      MS_TRY(cudaMemcpyAsync(images, d_img_.p, sizeof(float) * N * nd, cudaMemcpyDeviceToHost, stream_));
+    if (grad && dLdV)
+      MS_TRY(cudaMemcpyAsync(dLdV, d_dV_.p, sizeof(float) * N * S, cudaMemcpyDeviceToHost, stream_));
+    if (grad && dLdxy)
+      MS_TRY(cudaMemcpyAsync(dLdxy, d_dxy_.p, sizeof(double) * 2 * natoms_, cudaMemcpyDeviceToHost, stream_));
+    MS_TRY(cudaStreamSynchronize(stream_));
+    MS_TRY(cudaEventElapsedTime(&last_device_ms_, ev0_, ev1_));
+    domain_ = 1;
+    return MS_OK;
+  }
+
+  // First sorted atom of every 1-A z-bin (CSR offsets at bin k * 2500), k = 0..nz.
+  int zbin_starts() {
+    if ((int)hzoff_.size() == nzb_ + 1) return MS_OK;
+    hzoff_.assign(nzb_ + 1, 0);
+    MS_TRY(cudaMemcpy2DAsync(hzoff_.data(), sizeof(int), d_off_.p, sizeof(int) * kBins2, sizeof(int), nzb_ + 1,
+                             cudaMemcpyDeviceToHost, stream_));
+    MS_TRY(cudaStreamSynchronize(stream_));
+    return MS_OK;
+  }
+
+  int last_device_ms(float* out) {
+    *out = last_device_ms_;
     return MS_OK;
   }
 
@@ -1070,8 +1254,8 @@ class Engine {
   int copy_binned(int* off, int* Z, float* x, float* y, float* z) {
     if (!have_index_) return fail(MS_ERR_STATE, "atoms not binned");
     std::vector<float4> at(natoms_);
-    MS_TRY(cudaMemcpy(at.data(), d_atoms_.p, sizeof(float4) * natoms_, cudaMemcpyDeviceToHost));
-    MS_TRY(cudaMemcpy(off, d_off_.p, sizeof(int) * ((size_t)nzb_ * kBins2 + 1), cudaMemcpyDeviceToHost));
+    MS_TRY(copy_sync(at.data(), d_atoms_.p, sizeof(float4) * natoms_, cudaMemcpyDeviceToHost));
+    MS_TRY(copy_sync(off, d_off_.p, sizeof(int) * ((size_t)nzb_ * kBins2 + 1), cudaMemcpyDeviceToHost));
     for (int i = 0; i < natoms_; ++i) {
       x[i] = at[i].x;
       y[i] = at[i].y;
@@ -1107,6 +1291,14 @@ class Engine {
   float im_min() const { return im_min_; }
   float im_max() const { return im_max_; }
   bool have_image() const { return have_image_; }
+
+  // Copies through the handle's stream and waits.  A plain cudaMemcpy runs on
+  // the legacy default stream, which the handle's non-blocking stream does not
+  // wait for, and from pageable memory it may return before the DMA lands.
+  cudaError_t copy_sync(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, stream_);
+    return e == cudaSuccess ? cudaStreamSynchronize(stream_) : e;
+  }
 
   int fail(int code, const std::string& m) {
     err = m;
@@ -1178,8 +1370,8 @@ class Engine {
     }
     MS_TRY(d_px_.resize(nx_));
     MS_TRY(d_py_.resize(ny_));
-    MS_TRY(cudaMemcpy(d_px_.p, px.data(), sizeof(float2) * nx_, cudaMemcpyHostToDevice));
-    MS_TRY(cudaMemcpy(d_py_.p, py.data(), sizeof(float2) * ny_, cudaMemcpyHostToDevice));
+    MS_TRY(copy_sync(d_px_.p, px.data(), sizeof(float2) * nx_, cudaMemcpyHostToDevice));
+    MS_TRY(copy_sync(d_py_.p, py.data(), sizeof(float2) * ny_, cudaMemcpyHostToDevice));
     prop_dz_ = dz;
     // plain path: full propagator array, as CreatePropsKernel
     MS_TRY(d_P_.resize((size_t)nx_ * ny_));
@@ -1334,6 +1526,13 @@ class Engine {
 
   // Potential of one slice into out (ny x nx floats).
   int potential_slice(int kind, int it, float* out) {
+    const PotArgs a = pot_args(kind, it, out);
+    MS_TRY(launch_potential(a, kind, stream_));
+    ++launches;
+    return MS_OK;
+  }
+
+  PotArgs pot_args(int kind, int it, float* out) {
     PotArgs a{};
     a.atoms = d_atoms_.p;
     a.off = d_off_.p;
@@ -1378,9 +1577,7 @@ class Engine {
       a.kt = std::max((int)std::floor((it - 1) * convdz_) - 1, 0);
       a.kb = std::min((int)std::floor(it * convdz_) + 1, nzb_ - 1);
     }
-    MS_TRY(launch_potential(a, kind, stream_));
-    ++launches;
-    return MS_OK;
+    return a;
   }
 
   static void tds_displace(const float* x, const float* y, const float* z, int n, uint64_t seed, uint32_t pass,
@@ -1428,7 +1625,12 @@ class Engine {
   std::vector<float> hkx_, hky_;
   DevBuf<float> d_kx_, d_ky_;
   DevBuf<float2> d_twx_[3], d_twy_[3], d_px_, d_py_, d_P_;
-  int forced_plan_ = -1;
+  int forced_plan_ = -1, ckpt_ = 0;
+  float last_device_ms_ = 0.0f;
+  std::vector<int> hzoff_;  // first sorted atom per z-bin (focal-series atom gradient)
+  DevBuf<float2> d_ck_, d_seg_, d_G_, d_U_, d_Phi_;
+  DevBuf<float> d_T_, d_dV_, d_img_;
+  DevBuf<double> d_loss_, d_dxy_;
   std::vector<std::pair<int, PlanChoice>> tuned_;
   float prop_dz_ = -1.0f;
   cufftHandle plan_ = 0;
@@ -1769,6 +1971,22 @@ ms_status ms_time_slices(ms_sim* s, int steps, int reps, float* total, float* ro
 ms_status ms_get_fft_plan(ms_sim* s, int batch, int* row, int* col) {
   if (!row || !col) return s && s->e ? s->e->fail(MS_ERR_INVALID, "null output") : MS_ERR_INVALID;
   return guarded(s, [&](ms::Engine& e) { return e.fft_plan(batch, row, col); });
+}
+ms_status ms_focal_series(ms_sim* s, const float* defoci, int nd, const float* targets, int nslices, double* loss,
+                          float* images) {
+  return guarded(s, [&](ms::Engine& e) {
+    return e.focal(defoci, nd, targets, nslices, loss, images, nullptr, nullptr, false);
+  });
+}
+ms_status ms_focal_series_grad(ms_sim* s, const float* defoci, int nd, const float* targets, int nslices,
+                               double* loss, float* dLdV, double* dLdxy) {
+  return guarded(s, [&](ms::Engine& e) {
+    return e.focal(defoci, nd, targets, nslices, loss, nullptr, dLdV, dLdxy, true);
+  });
+}
+ms_status ms_get_last_device_ms(ms_sim* s, float* out) {
+  if (ms_status r = out_check(s, out)) return r;
+  return guarded(s, [&](ms::Engine& e) { return e.last_device_ms(out); });
 }
 ms_status ms_get_launch_count(ms_sim* s, long long* out) {
   if (ms_status r = out_check(s, out)) return r;

@@ -24,6 +24,11 @@ enum PassAFlags : int {
   A_INTENSITY = 8,  // store |.|^2 * scale as float
   A_REAL = 16,      // store the real part * scale as float
   A_FD = 32,        // finite-difference stencil (see PassAArgs.fd_*)
+  A_SAVE = 64,      // store the real-space line (before x t) to out2
+  A_RESID = 128,    // focal-series residual: I = |.|^2, r = I - T, loss += r^2,
+                    // line <- 2 r line (I to out_f when not null)
+  A_ADJ = 256,      // adjoint of x t: dV = -2 sigma Im(conj(h) t psi) to out_f
+                    // (psi from in2), line <- conj(t) line
 };
 enum PassBMode : int {
   B_FWD_ONLY = 0,    // FFT_col
@@ -34,6 +39,8 @@ enum PassBMode : int {
   B_DETECT = 5,      // FFT_col, band limit of P, sum |.|^2 over an annulus per instance
   B_BANDLIMIT = 6,   // FFT_col, keep k <= kmax (x scale), IFFT_col
   B_FD = 7,          // FFT_col = Q; spec <- BL Q + fd_c k^2 spec; IFFT_col(spec) * scale
+  B_PROPAGATE_ADJ = 8,  // FFT_col, x conj(Px*Py) * scale (band-limited), IFFT_col
+  B_CTF_ADJ = 9,        // FFT_col, x conj(CTF(k)) * scale, IFFT_col; out += when accumulate
 };
 
 struct PassAArgs {
@@ -52,6 +59,8 @@ struct PassAArgs {
   float2* out2;
   float2 fd_rc, fd_ratio;
   float fd_kv;
+  const float* T;     // A_RESID: target intensity [ny][nx] (instance stride batch_stride_V)
+  double* loss;       // A_RESID: FP64 sum of r^2 (atomic)
   const float2* tw;   // twiddle table for nx
   int nx, ny;
   long long batch_stride_wave;  // elements between instances (blockIdx.y)
@@ -80,6 +89,7 @@ struct PassBArgs {
                        //       stored column-major [nx][ny] (coalesced in this pass)
   float2 fd_c;         // B_FD: rc dz^2 4 pi^2 (pi = 3.14159, gradKernel U.cu:959)
   float kin2, kout2;   // B_DETECT: annulus kin^2 <= kx^2+ky^2 < kout^2 (FP32 decision)
+  int accumulate;      // B_CTF_ADJ: add to out instead of storing
   int nx, ny;
   long long batch_stride_wave;
 };

@@ -62,6 +62,11 @@ MS_D void row_mid(float2 (&v)[PL::E], const PassAArgs& a, long long inst, int li
       v[j] = csub(cmul(a.fd_rc, cscale(v[j], f)), cmul(a.fd_ratio, pm[x]));
     }
   }
+  if constexpr ((FLAGS & A_SAVE) != 0) {
+    float2* o = a.out2 + row0;
+#pragma unroll
+    for (int j = 0; j < E; ++j) o[t + P * j] = v[j];
+  }
   if constexpr ((FLAGS & A_MULT_T) != 0) {
     const float* V = a.V + inst * a.batch_stride_V + (long long)line * NX;
 #pragma unroll
@@ -69,6 +74,41 @@ MS_D void row_mid(float2 (&v)[PL::E], const PassAArgs& a, long long inst, int li
       float sn, cs;
       sincos_red(fmul_x(a.sigma, V[t + P * j]), &sn, &cs);
       v[j] = cmul(v[j], make_float2(cs, sn));
+    }
+  }
+  if constexpr ((FLAGS & A_RESID) != 0) {
+    const long long r0 = inst * a.batch_stride_V + (long long)line * NX;
+    const float* T = a.T + r0;
+    float* img = a.out_f ? a.out_f + r0 : nullptr;
+    double part = 0.0;
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int x = t + P * j;
+      const float I = v[j].x * v[j].x + v[j].y * v[j].y;
+      if (img) img[x] = I;
+      const float r = I - T[x];
+      part += (double)r * (double)r;
+      v[j] = cscale(v[j], 2.0f * r);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(a.loss, part);
+  }
+  if constexpr ((FLAGS & A_ADJ) != 0) {
+    const long long r0 = inst * a.batch_stride_V + (long long)line * NX;
+    const float* V = a.V + r0;
+    const float2* pp = a.in2 + row0;
+    float* dV = a.out_f + r0;
+    const float m2s = -2.0f * a.sigma;
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int x = t + P * j;
+      float sn, cs;
+      sincos_red(fmul_x(a.sigma, V[x]), &sn, &cs);
+      const float2 tt = make_float2(cs, sn);
+      const float2 q = cmul(tt, pp[x]);
+      dV[x] = m2s * (v[j].x * q.y - v[j].y * q.x);
+      v[j] = cmul(cconj(tt), v[j]);
     }
   }
 }
@@ -112,6 +152,8 @@ __global__ void __launch_bounds__(rows_per_cta<PL>() * PL::P) k_pass_a(PassAArgs
     float* o = a.out_f + row0;
 #pragma unroll
     for (int j = 0; j < E; ++j) o[t + P * j] = v[j].x * a.scale;
+  } else if constexpr ((FLAGS & A_RESID) != 0 && !FWDF) {
+    // residual only: the loss (and the image) are the results
   } else {
     float2* o = a.out + row0;
     if (a.scale != 1.0f) {
@@ -142,13 +184,26 @@ MS_D void col_mid(float2 (&v)[PL::E], const PassBArgs& a, int col, int t, long l
       const float2 w = keep ? cmul(pxv, a.py[n]) : make_float2(0.f, 0.f);
       v[j] = cmul(v[j], w);
     }
-  } else if constexpr (MODE == B_CTF) {
+  } else if constexpr (MODE == B_PROPAGATE_ADJ) {
+    const float kx = a.kx[col];
+    const float kx2 = fmul_x(kx, kx);
+    const float2 pxv = a.px[col];
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int n = t + P * j;
+      const float ky = a.ky[n];
+      const bool keep = fsqrt_x(fadd_x(kx2, fmul_x(ky, ky))) < a.kmax;
+      const float2 w = keep ? cscale(cconj(cmul(pxv, a.py[n])), scale) : make_float2(0.f, 0.f);
+      v[j] = cmul(v[j], w);
+    }
+  } else if constexpr (MODE == B_CTF || MODE == B_CTF_ADJ) {
     const float kx = a.kx[col];
 #pragma unroll
     for (int j = 0; j < E; ++j) {
       const int n = t + P * j;
-      v[j] = cmul(v[j], ctf_weight(a.ctf.wavel, a.ctf.Cs, a.ctf.df, a.ctf.A2, a.ctf.phi2, a.ctf.A3, a.ctf.phi3,
-                                   a.ctf.beta, a.ctf.delta, a.ctf.objap2, kx, a.ky[n], scale));
+      const float2 w = ctf_weight(a.ctf.wavel, a.ctf.Cs, a.ctf.df, a.ctf.A2, a.ctf.phi2, a.ctf.A3, a.ctf.phi3,
+                                  a.ctf.beta, a.ctf.delta, a.ctf.objap2, kx, a.ky[n], scale);
+      v[j] = cmul(v[j], MODE == B_CTF ? w : cconj(w));
     }
   } else if constexpr (MODE == B_BANDLIMIT) {
     // BandLimitKernel (U.cu:1025-1042): keep k <= kmax
@@ -185,7 +240,8 @@ template <class PL, int MODE>
 __global__ void __launch_bounds__(cols_per_cta<PL>() * PL::P) k_pass_b(PassBArgs a) {
   constexpr int NY = PL::N, E = PL::E, P = PL::P, CB = cols_per_cta<PL>(), LS = col_slot<PL>();
   constexpr int NT = CB * P;
-  constexpr bool TWO = MODE == B_PROPAGATE || MODE == B_CTF || MODE == B_BANDLIMIT || MODE == B_FD;
+  constexpr bool TWO = MODE == B_PROPAGATE || MODE == B_CTF || MODE == B_BANDLIMIT || MODE == B_FD ||
+                      MODE == B_PROPAGATE_ADJ || MODE == B_CTF_ADJ;
   extern __shared__ float2 smem[];
   const int nx = a.nx;
   const int c0 = blockIdx.x * CB;
@@ -261,9 +317,17 @@ __global__ void __launch_bounds__(cols_per_cta<PL>() * PL::P) k_pass_b(PassBArgs
     for (int j = 0; j < E; ++j) sm[fft::padi<PL>(t + P * j)] = v[j];
     __syncthreads();
     float2* out = a.out + base;
-    for (int idx = threadIdx.x; idx < NY * CB; idx += NT) {
-      const int r = idx / CB, c = idx % CB;
-      out[(long long)r * nx + c0 + c] = smem[c * LS + fft::padi<PL>(r)];
+    if (MODE == B_CTF_ADJ && a.accumulate) {
+      for (int idx = threadIdx.x; idx < NY * CB; idx += NT) {
+        const int r = idx / CB, c = idx % CB;
+        float2* o = out + (long long)r * nx + c0 + c;
+        *o = cadd(*o, smem[c * LS + fft::padi<PL>(r)]);
+      }
+    } else {
+      for (int idx = threadIdx.x; idx < NY * CB; idx += NT) {
+        const int r = idx / CB, c = idx % CB;
+        out[(long long)r * nx + c0 + c] = smem[c * LS + fft::padi<PL>(r)];
+      }
     }
   }
 }
@@ -314,6 +378,11 @@ cudaError_t dispatch_a_plan(const PassAArgs& a, int flags, int batch, cudaStream
     case A_INV | A_INTENSITY: return run_a<PL, A_INV | A_INTENSITY>(a, batch, s);
     case A_INV | A_REAL: return run_a<PL, A_INV | A_REAL>(a, batch, s);
     case A_INV | A_FD | A_FWD: return run_a<PL, A_INV | A_FD | A_FWD>(a, batch, s);
+    case A_SAVE | A_MULT_T | A_FWD: return run_a<PL, A_SAVE | A_MULT_T | A_FWD>(a, batch, s);
+    case A_INV | A_SAVE | A_MULT_T | A_FWD: return run_a<PL, A_INV | A_SAVE | A_MULT_T | A_FWD>(a, batch, s);
+    case A_INV | A_RESID: return run_a<PL, A_INV | A_RESID>(a, batch, s);
+    case A_INV | A_RESID | A_FWD: return run_a<PL, A_INV | A_RESID | A_FWD>(a, batch, s);
+    case A_INV | A_ADJ | A_FWD: return run_a<PL, A_INV | A_ADJ | A_FWD>(a, batch, s);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -329,6 +398,8 @@ cudaError_t dispatch_b_plan(const PassBArgs& a, int mode, int batch, cudaStream_
     case B_DETECT: return run_b<PL, B_DETECT>(a, batch, s);
     case B_BANDLIMIT: return run_b<PL, B_BANDLIMIT>(a, batch, s);
     case B_FD: return run_b<PL, B_FD>(a, batch, s);
+    case B_PROPAGATE_ADJ: return run_b<PL, B_PROPAGATE_ADJ>(a, batch, s);
+    case B_CTF_ADJ: return run_b<PL, B_CTF_ADJ>(a, batch, s);
     default: return cudaErrorInvalidValue;
   }
 }

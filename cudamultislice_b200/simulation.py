@@ -91,6 +91,10 @@ class ManagedMultisliceSimulation:
         """-1: autotuned; 0..2: force a plan variant of the fused passes."""
         self._chk(self._L.ms_set_option(self._h, 3, int(variant)))
 
+    def SetCheckpoint(self, stride: int):
+        """Focal-series gradient: slices between stored waves (0: ceil(sqrt(S)))."""
+        self._chk(self._L.ms_set_option(self._h, 4, int(stride)))
+
     # ---- structure ----
     def ImportAtoms(self, filename: str):
         self._chk(self._L.ms_import_atoms(self._h, filename.encode()))
@@ -266,6 +270,43 @@ class ManagedMultisliceSimulation:
         self._chk(self._L.ms_stem_raster(self._h, _ptr(px), _ptr(py), px.size, float(inner_mrad),
                                          float(outer_mrad), int(batch), _ptr(out)))
         return out
+
+    # ---- differentiable focal series ----
+    def FocalSeries(self, defoci, targets, nslices: int, images: bool = False):
+        """Loss sum_d sum_px (I_d - T_d)^2 of the CTF images at `defoci` (A) of
+        the wave after conventional slices 1..nslices; with `images`, also the
+        simulated images (nd, ny, nx)."""
+        d = np.ascontiguousarray(defoci, np.float32).ravel()
+        T = np.ascontiguousarray(targets, np.float32)
+        if T.size != d.size * self.nx * self.ny:
+            raise ValueError("targets must hold nd * ny * nx values")
+        loss = C.c_double()
+        imgs = np.zeros((d.size, self.ny, self.nx), np.float32) if images else None
+        self._chk(self._L.ms_focal_series(self._h, _ptr(d), d.size, _ptr(T), int(nslices), C.byref(loss),
+                                          _ptr(imgs) if images else None))
+        return (loss.value, imgs) if images else loss.value
+
+    def FocalSeriesGrad(self, defoci, targets, nslices: int, want_v: bool = True, want_xy: bool = True):
+        """Loss, dL/dV (nslices, ny, nx) and dL/dxy (n_atoms, 2; input order)."""
+        d = np.ascontiguousarray(defoci, np.float32).ravel()
+        T = np.ascontiguousarray(targets, np.float32)
+        if T.size != d.size * self.nx * self.ny:
+            raise ValueError("targets must hold nd * ny * nx values")
+        loss = C.c_double()
+        gV = np.zeros((int(nslices), self.ny, self.nx), np.float32) if want_v else None
+        gxy = None
+        if want_xy:
+            n, nz = C.c_int(), C.c_int()
+            self._chk(self._L.ms_get_binned_counts(self._h, C.byref(n), C.byref(nz)))
+            gxy = np.zeros((n.value, 2), np.float64)
+        self._chk(self._L.ms_focal_series_grad(self._h, _ptr(d), d.size, _ptr(T), int(nslices), C.byref(loss),
+                                               _ptr(gV) if want_v else None, _ptr(gxy) if want_xy else None))
+        return loss.value, gV, gxy
+
+    def LastDeviceMs(self) -> float:
+        out = C.c_float()
+        self._chk(self._L.ms_get_last_device_ms(self._h, C.byref(out)))
+        return out.value
 
     # ---- inspection ----
     def Binned(self):

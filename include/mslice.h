@@ -60,10 +60,13 @@ enum {
                                reference kernel binnedAtomPKernel3 (U.cu:582-653);
                                1 = projected potential vzatom2 per slab (U.cu:119-152,
                                xy scan of binnedAtomPKernel2 U.cu:513-578) */
-  MS_OPT_FFT_PLAN = 3       /* -1 = autotuned (default): every FFT plan variant of the
+  MS_OPT_FFT_PLAN = 3,      /* -1 = autotuned (default): every FFT plan variant of the
                                fused passes is timed on the device once per grid and
                                batch size and the fastest kept; 0..2 = force a variant
                                (0: most points per thread ... 2: most threads per line) */
+  MS_OPT_CHECKPOINT = 4     /* focal-series gradient: slices between stored waves;
+                               0 = ceil(sqrt(S)) (default), 1 = store every wave,
+                               >= S = one segment recomputed from the initial wave */
 };
 
 /* ---- lifecycle ---- */
@@ -198,7 +201,29 @@ ms_status ms_annular_detector(ms_sim* sim, float inner_mrad, float outer_mrad, d
 ms_status ms_stem_raster(ms_sim* sim, const int* px, const int* py, int n, float inner_mrad,
                          float outer_mrad, int batch, double* signal);
 
+/* ---- differentiable focal series (new; no reference counterpart) ----
+ * Loss L = sum_d sum_px (I_d(px) - T_d(px))^2, with I_d the CTF image of
+ * ms_simulate_image (imagingKernel2, U.cu:1044-1080, at the microscope
+ * parameters of ms_apply_microscope_parameters except the defocus, which is
+ * defoci[d] in A) of the exit wave after conventional slices 1..nslices from
+ * the initial wave (ms_initialise_wavefunctions_dz).  targets: nd*nx*ny floats,
+ * image d at offset d*nx*ny, row-major [y][x].  The wave is left at slice
+ * nslices in the handle.  images (nd*nx*ny floats) may be NULL. */
+ms_status ms_focal_series(ms_sim* sim, const float* defoci, int nd, const float* targets, int nslices,
+                          double* loss, float* images);
+/* Forward and adjoint of the same loss: dLdV = dL/dV for slices 1..nslices
+ * (nslices*nx*ny floats, slice n-1 at offset (n-1)*nx*ny; V in the units of
+ * ms_copy_potential_slice), dLdxy = dL/dx, dL/dy per atom in the order given to
+ * ms_set_atoms / ms_import_atoms (2 doubles per atom, A^-1; the bounding box is
+ * held fixed; needs the conventional potential).  Either may be NULL.  Waves
+ * are recomputed from checkpoints every MS_OPT_CHECKPOINT slices. */
+ms_status ms_focal_series_grad(ms_sim* sim, const float* defoci, int nd, const float* targets, int nslices,
+                               double* loss, float* dLdV, double* dLdxy);
+
 /* ---- inspection (parity tests and measurement) ---- */
+/* Device milliseconds (CUDA events on the handle's stream) of the last
+ * focal-series call, from after the target upload to before the read-back. */
+ms_status ms_get_last_device_ms(ms_sim* sim, float* out);
 ms_status ms_get_binned_counts(ms_sim* sim, int* n_atoms, int* n_zbins);
 ms_status ms_copy_binned(ms_sim* sim, int* offsets, int* Z, float* x, float* y, float* z);
 /* kind: 0 conventional slice, 1 finite-difference plane, 2 projected slab (current
