@@ -1233,6 +1233,46 @@ class Engine {
     return MS_OK;
   }
 
+  // Device time of one fused pass (pass 0: row pass with `op` = PassAFlags;
+  // pass 1: column pass with `op` = PassBMode) of plan `variant` over `batch`
+  // scratch instances, averaged over `reps` back-to-back launches.
+  int time_pass(int pass, int op, int variant, int batch, int reps, float* us) {
+    if (!have_freq_ || !use_fused()) return fail(MS_ERR_STATE, "fused grid not set up (ms_precalculate_frequencies)");
+    if (pass < 0 || pass > 1 || variant < 0 || variant >= plan_variants() || batch < 1 || batch > 256 || reps < 1)
+      return fail(MS_ERR_INVALID, "bad pass, variant, batch or reps");
+    if (pass == 0 && (op & (A_FD | A_RESID | A_ADJ | A_SAVE | A_INTENSITY | A_REAL)) != 0)
+      return fail(MS_ERR_INVALID, "row-pass timing covers A_INV, A_MULT_T and A_FWD");
+    if (pass == 1 && (op == B_CBED || op == B_DETECT || op == B_FD || op == B_CTF_ADJ))
+      return fail(MS_ERR_INVALID, "column-pass timing covers the wave-to-wave modes");
+    if (int rc = ensure_prop_tables(convdz_)) return rc;
+    const long long N = (long long)nx_ * ny_;
+    DevBuf<float2> w;
+    DevBuf<float> V;
+    MS_TRY(w.resize((size_t)batch * N));
+    MS_TRY(V.resize((size_t)N));
+    MS_TRY(cudaMemsetAsync(w.p, 0, sizeof(float2) * batch * N, stream_));
+    MS_TRY(cudaMemsetAsync(V.p, 0, sizeof(float) * N, stream_));
+    PassAArgs a = passa_args(w.p, w.p, variant);
+    a.V = V.p;
+    a.batch_stride_wave = N;
+    PassBArgs b = passb_args(w.p, w.p, variant);
+    b.batch_stride_wave = N;
+    b.ctf = CtfParams{(double)wavel_, (double)Cs_, (double)df_, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1e30f};
+    auto launch = [&]() {
+      return pass == 0 ? launch_pass_a(a, variant, op, batch, stream_) : launch_pass_b(b, variant, op, batch, stream_);
+    };
+    for (int k = 0; k < 2; ++k) MS_TRY(launch());
+    MS_TRY(cudaEventRecord(ev0_, stream_));
+    for (int k = 0; k < reps; ++k) MS_TRY(launch());
+    MS_TRY(cudaEventRecord(ev1_, stream_));
+    MS_TRY(cudaEventSynchronize(ev1_));
+    float ms = 0.0f;
+    MS_TRY(cudaEventElapsedTime(&ms, ev0_, ev1_));
+    launches += reps + 2;
+    *us = 1000.0f * ms / (float)reps;
+    return MS_OK;
+  }
+
   // ---- inspection ----
   int fft_plan(int batch, int* row, int* col) {
     if (!have_freq_) return fail(MS_ERR_STATE, "frequencies not precalculated");
@@ -1983,6 +2023,10 @@ ms_status ms_focal_series_grad(ms_sim* s, const float* defoci, int nd, const flo
   return guarded(s, [&](ms::Engine& e) {
     return e.focal(defoci, nd, targets, nslices, loss, nullptr, dLdV, dLdxy, true);
   });
+}
+ms_status ms_time_pass(ms_sim* s, int pass, int op, int variant, int batch, int reps, float* us) {
+  if (ms_status r = out_check(s, us)) return r;
+  return guarded(s, [&](ms::Engine& e) { return e.time_pass(pass, op, variant, batch, reps, us); });
 }
 ms_status ms_get_last_device_ms(ms_sim* s, float* out) {
   if (ms_status r = out_check(s, out)) return r;

@@ -115,12 +115,16 @@ MS_D int padi(int n) {
   return n + n / PL::R1;
 }
 
+// Barrier of the P threads that own one line: the warp's lanes for P <= 32,
+// else named barrier 1 + (line index in the CTA) over P threads, so that the
+// lines of a CTA do not wait for one another (lines are contiguous groups of
+// P threads; at most 4 lines of P > 32 per CTA).
 template <class PL>
 MS_D void line_sync() {
   if constexpr (PL::P <= 32)
     __syncwarp();
   else
-    __syncthreads();
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + (int)threadIdx.x / PL::P), "n"(PL::P) : "memory");
 }
 
 // Radix R of pass number IDX (0-based).

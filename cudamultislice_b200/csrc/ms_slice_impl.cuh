@@ -46,20 +46,60 @@ __host__ __device__ constexpr int cols_per_cta() { return PL::P >= 64 ? 4 : 256 
 template <class PL>
 __host__ __device__ constexpr int col_slot() { return ((PL::N + PL::N / PL::R1 + 15) / 16) * 16 + 2; }
 
+// Programmatic dependent launch: the passes are launched with programmatic
+// stream serialisation, so a pass may start while the previous kernel of the
+// stream drains.  Every pass signals its dependents at entry and waits for its
+// predecessor's completion (and memory) before its first global access.
+MS_D void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+MS_D void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// Per-point operands of the row pass's pointwise work, loaded with the line
+// so that their latency overlaps the inverse transform: V (transmission,
+// stencil, adjoint), T (residual), and the second wave (stencil, adjoint)
+// where registers allow.
+template <class PL, int FLAGS>
+struct RowOperands {
+  static constexpr int E = PL::E, P = PL::P, NX = PL::N;
+  static constexpr bool HAS_V = (FLAGS & (A_MULT_T | A_FD | A_ADJ)) != 0;
+  static constexpr bool HAS_T = (FLAGS & A_RESID) != 0;
+  static constexpr bool HAS_W = (FLAGS & (A_FD | A_ADJ)) != 0 && E <= 16;
+  float V[HAS_V ? E : 1];
+  float T[HAS_T ? E : 1];
+  float2 W[HAS_W ? E : 1];
+  MS_D void load(const PassAArgs& a, long long inst, int line, long long row0, int t) {
+    const long long r0 = inst * a.batch_stride_V + (long long)line * NX;
+    if constexpr (HAS_V) {
+#pragma unroll
+      for (int j = 0; j < E; ++j) V[j] = a.V[r0 + t + P * j];
+    }
+    if constexpr (HAS_T) {
+#pragma unroll
+      for (int j = 0; j < E; ++j) T[j] = a.T[r0 + t + P * j];
+    }
+    if constexpr (HAS_W) {
+#pragma unroll
+      for (int j = 0; j < E; ++j) W[j] = a.in2[row0 + t + P * j];
+    }
+  }
+  MS_D float2 w(const PassAArgs& a, long long row0, int j, int t) const {
+    if constexpr (HAS_W) return W[j];
+    else return a.in2[row0 + t + P * j];
+  }
+};
+
 // Pointwise work of the row pass between its inverse and forward transforms.
 template <class PL, int FLAGS>
-MS_D void row_mid(float2 (&v)[PL::E], const PassAArgs& a, long long inst, int line, long long row0, int t) {
+MS_D void row_mid(float2 (&v)[PL::E], const PassAArgs& a, const RowOperands<PL, FLAGS>& op, long long inst,
+                  int line, long long row0, int t) {
   constexpr int NX = PL::N, E = PL::E, P = PL::P;
   if constexpr ((FLAGS & A_FD) != 0) {
-    const float* V = a.V + inst * a.batch_stride_V + (long long)line * NX;
-    const float2* pm = a.in2 + row0;
     float2* pc = a.out2 + row0;
 #pragma unroll
     for (int j = 0; j < E; ++j) {
       const int x = t + P * j;
       pc[x] = v[j];
-      const float f = 2.0f - a.fd_kv * V[x];
-      v[j] = csub(cmul(a.fd_rc, cscale(v[j], f)), cmul(a.fd_ratio, pm[x]));
+      const float f = 2.0f - a.fd_kv * op.V[j];
+      v[j] = csub(cmul(a.fd_rc, cscale(v[j], f)), cmul(a.fd_ratio, op.w(a, row0, j, t)));
     }
   }
   if constexpr ((FLAGS & A_SAVE) != 0) {
@@ -68,17 +108,15 @@ MS_D void row_mid(float2 (&v)[PL::E], const PassAArgs& a, long long inst, int li
     for (int j = 0; j < E; ++j) o[t + P * j] = v[j];
   }
   if constexpr ((FLAGS & A_MULT_T) != 0) {
-    const float* V = a.V + inst * a.batch_stride_V + (long long)line * NX;
 #pragma unroll
     for (int j = 0; j < E; ++j) {
       float sn, cs;
-      sincos_red(fmul_x(a.sigma, V[t + P * j]), &sn, &cs);
+      sincos_red(fmul_x(a.sigma, op.V[j]), &sn, &cs);
       v[j] = cmul(v[j], make_float2(cs, sn));
     }
   }
   if constexpr ((FLAGS & A_RESID) != 0) {
     const long long r0 = inst * a.batch_stride_V + (long long)line * NX;
-    const float* T = a.T + r0;
     float* img = a.out_f ? a.out_f + r0 : nullptr;
     double part = 0.0;
 #pragma unroll
@@ -86,7 +124,7 @@ MS_D void row_mid(float2 (&v)[PL::E], const PassAArgs& a, long long inst, int li
       const int x = t + P * j;
       const float I = v[j].x * v[j].x + v[j].y * v[j].y;
       if (img) img[x] = I;
-      const float r = I - T[x];
+      const float r = I - op.T[j];
       part += (double)r * (double)r;
       v[j] = cscale(v[j], 2.0f * r);
     }
@@ -96,17 +134,15 @@ MS_D void row_mid(float2 (&v)[PL::E], const PassAArgs& a, long long inst, int li
   }
   if constexpr ((FLAGS & A_ADJ) != 0) {
     const long long r0 = inst * a.batch_stride_V + (long long)line * NX;
-    const float* V = a.V + r0;
-    const float2* pp = a.in2 + row0;
     float* dV = a.out_f + r0;
     const float m2s = -2.0f * a.sigma;
 #pragma unroll
     for (int j = 0; j < E; ++j) {
       const int x = t + P * j;
       float sn, cs;
-      sincos_red(fmul_x(a.sigma, V[x]), &sn, &cs);
+      sincos_red(fmul_x(a.sigma, op.V[j]), &sn, &cs);
       const float2 tt = make_float2(cs, sn);
-      const float2 q = cmul(tt, pp[x]);
+      const float2 q = cmul(tt, op.w(a, row0, j, t));
       dV[x] = m2s * (v[j].x * q.y - v[j].y * q.x);
       v[j] = cmul(cconj(tt), v[j]);
     }
@@ -124,12 +160,16 @@ __global__ void __launch_bounds__(rows_per_cta<PL>() * PL::P) k_pass_a(PassAArgs
   const long long inst = blockIdx.y;
   const long long row0 = inst * a.batch_stride_wave + (long long)line * NX;
 
+  pdl_launch_dependents();
+  pdl_wait();
   float2 v[E];
   const float2* in = a.in + row0;
 #pragma unroll
   for (int j = 0; j < E; ++j) v[j] = in[t + P * j];
+  RowOperands<PL, FLAGS> op;
+  op.load(a, inst, line, row0, t);
 
-  if constexpr (!INVF) row_mid<PL, FLAGS>(v, a, inst, line, row0, t);
+  if constexpr (!INVF) row_mid<PL, FLAGS>(v, a, op, inst, line, row0, t);
   if constexpr (INVF || FWDF) {
     // one copy of the transform code: iteration 0 is the inverse
     // conj(FFT(conj(.))) followed by the pointwise work, iteration 1 the forward
@@ -139,7 +179,7 @@ __global__ void __launch_bounds__(rows_per_cta<PL>() * PL::P) k_pass_a(PassAArgs
       fft::line_fft<PL>(v, sm, t, a.tw);
       if (it == 0) {
         fft::conj_all(v);
-        if constexpr (INVF) row_mid<PL, FLAGS>(v, a, inst, line, row0, t);
+        if constexpr (INVF) row_mid<PL, FLAGS>(v, a, op, inst, line, row0, t);
       }
     }
   }
@@ -249,11 +289,20 @@ __global__ void __launch_bounds__(cols_per_cta<PL>() * PL::P) k_pass_b(PassBArgs
   const float2* in = a.in + base;
   const float scale = a.scale;
 
-  // transposing tile load: NY rows x CB columns -> one padded slot per column
-  for (int idx = threadIdx.x; idx < NY * CB; idx += NT) {
+  // transposing tile load: NY rows x CB columns -> one padded slot per column,
+  // E asynchronous 8-byte copies per thread, all in flight together
+  pdl_launch_dependents();
+  pdl_wait();
+#pragma unroll
+  for (int k = 0; k < E; ++k) {
+    const int idx = threadIdx.x + k * NT;
     const int r = idx / CB, c = idx % CB;
-    smem[c * LS + fft::padi<PL>(r)] = in[(long long)r * nx + c0 + c];
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem + c * LS + fft::padi<PL>(r));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(in + (long long)r * nx + c0 + c)
+                 : "memory");
   }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
   __syncthreads();
 
   const int lane = threadIdx.x & 31;
@@ -340,6 +389,22 @@ inline bool attr_once(unsigned long long& mask) {
   return true;
 }
 
+// Launch with programmatic stream serialisation (see pdl_wait).
+template <class K, class Args>
+cudaError_t launch_pdl(K kernel, dim3 grid, int threads, size_t smem, cudaStream_t s, const Args& args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args);
+}
+
 template <class PL, int FLAGS>
 cudaError_t run_a(const PassAArgs& a, int batch, cudaStream_t s) {
   constexpr int lines = rows_per_cta<PL>();
@@ -350,8 +415,7 @@ cudaError_t run_a(const PassAArgs& a, int batch, cudaStream_t s) {
     cudaError_t e = cudaFuncSetAttribute(k_pass_a<PL, FLAGS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  k_pass_a<PL, FLAGS><<<dim3(a.ny / lines, batch), lines * PL::P, smem, s>>>(a);
-  return cudaGetLastError();
+  return launch_pdl(k_pass_a<PL, FLAGS>, dim3(a.ny / lines, batch), lines * PL::P, smem, s, a);
 }
 
 template <class PL, int MODE>
@@ -364,8 +428,7 @@ cudaError_t run_b(const PassBArgs& a, int batch, cudaStream_t s) {
     cudaError_t e = cudaFuncSetAttribute(k_pass_b<PL, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  k_pass_b<PL, MODE><<<dim3(a.nx / CB, batch), CB * PL::P, smem, s>>>(a);
-  return cudaGetLastError();
+  return launch_pdl(k_pass_b<PL, MODE>, dim3(a.nx / CB, batch), CB * PL::P, smem, s, a);
 }
 
 template <class PL>

@@ -303,6 +303,13 @@ class ManagedMultisliceSimulation:
                                                _ptr(gV) if want_v else None, _ptr(gxy) if want_xy else None))
         return loss.value, gV, gxy
 
+    def TimePass(self, pass_: int, op: int, variant: int, batch: int = 1, reps: int = 20) -> float:
+        """Microseconds per launch of one fused pass (see ms_time_pass)."""
+        out = C.c_float()
+        self._chk(self._L.ms_time_pass(self._h, int(pass_), int(op), int(variant), int(batch), int(reps),
+                                       C.byref(out)))
+        return out.value
+
     def LastDeviceMs(self) -> float:
         out = C.c_float()
         self._chk(self._L.ms_get_last_device_ms(self._h, C.byref(out)))

@@ -221,6 +221,13 @@ ms_status ms_focal_series_grad(ms_sim* sim, const float* defoci, int nd, const f
                                double* loss, float* dLdV, double* dLdxy);
 
 /* ---- inspection (parity tests and measurement) ---- */
+/* Microseconds per launch of one fused pass on scratch waves (CUDA events,
+ * `reps` back-to-back launches after two warm-up launches): pass 0 = row pass
+ * with op = a combination of 1 (inverse row FFT), 2 (x exp(i sigma V)),
+ * 4 (forward row FFT); pass 1 = column pass with op = 0 (forward column FFT),
+ * 1 (inverse), 2 (propagate), 3 (CTF), 6 (band limit), 8 (adjoint propagate);
+ * FFT plan `variant`, `batch` instances. */
+ms_status ms_time_pass(ms_sim* sim, int pass, int op, int variant, int batch, int reps, float* us);
 /* Device milliseconds (CUDA events on the handle's stream) of the last
  * focal-series call, from after the target upload to before the read-back. */
 ms_status ms_get_last_device_ms(ms_sim* sim, float* out);
