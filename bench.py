@@ -277,6 +277,49 @@ def adjoint_leg(fparams, device: int, reps: int = 3) -> dict:
     }
 
 
+def tds_leg(fparams, device: int, nconf: int = 16, batch: int = 16) -> dict:
+    """Frozen-phonon series on the batched-TDS workload: Si [110], 8 x 6 x 50
+    orthogonal 4-atom cells (9,600 atoms), 512^2 square pixels over 32.6 A, 1.92 A slices,
+    200 kV, u_rms 0.076 A (seeded Philox), sum of centred |FFT(psi)| and the
+    mean CTF image; `nconf` of the 64 configurations timed (device time),
+    `batch` configurations per launch on the fused path, one at a time on the
+    plain path.  Reports configurations/s and slice-steps/s (potential build
+    included: every configuration has its own potentials)."""
+    from cudamultislice_b200 import ManagedMultisliceSimulation
+    from cudamultislice_b200 import structures as S
+
+    n = 512
+    Z, x, y, z = S.silicon_110(8, 6, 50)
+    sim = ManagedMultisliceSimulation(device=device)
+    sim.SetAtoms(Z, x, y, z)
+    sim.UploadBinnedAtoms()
+    sim.GetParameterisation(fparams)
+    sim.ApplyMicroscopeParameters(200.0, 0.0, 0.0, 0.0, 1.0e7, 0.1, 30.0, 20.0)
+    ps = 6 * 5.431 / n
+    sim.SetCalculationVariables(ps, 0.0, n, n, sim.GetSizeX(), sim.GetSizeY(), sim.GetSizeZ(), 2.0, 2.0)
+    sim.PreCalculateFrequencies()
+    sim.InitialiseWavefunctions(1.92)
+    nsl = sim.GetSlices(True)
+    out = {}
+    for name, path, nc, b in (("fused", 0, nconf, batch), ("plain", 1, max(nconf // 4, 2), 1)):
+        sim.SetSlicePath(path)
+        sim.FrozenPhonon(0x5EED2026, 0, min(b, nc), 0.076, batch=b)  # warm-up / tuning
+        sim.FrozenPhonon(0x5EED2026, 0, nc, 0.076, batch=b)
+        ms = sim.LastDeviceMs()
+        out[name] = {"configs_per_s": nc / (ms / 1000.0), "slice_steps_per_s": nc * nsl / (ms / 1000.0),
+                     "configs": nc, "batch": b, "ms": ms}
+    sim.SetSlicePath(0)
+    sim.close()
+    return {"value": out["fused"]["configs_per_s"], "unit": "configs/s",
+            "slice_steps_per_s": out["fused"]["slice_steps_per_s"],
+            "plain_value": out["plain"]["configs_per_s"],
+            "speedup_fused_vs_plain": out["fused"]["configs_per_s"] / out["plain"]["configs_per_s"],
+            "config": f"Si [110] 8x6x50 cells ({len(Z)} atoms), {n}^2, {nsl} slices of 1.92 A, 200 kV, "
+                      f"u_rms 0.076 A, {nconf} of 64 configurations, batch {batch}",
+            "timing": "device time (CUDA events) of ms_frozen_phonon, potential build of every configuration "
+                      "included", "detail": out}
+
+
 def cpu_baseline(atoms, fparams, nslices: int, threads: int) -> dict:
     """The FP64 OpenMP oracle on the host cores, on the first `nslices`
     slices of the same workload (potential build + transmission +
@@ -342,7 +385,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="profiling mode: set-up plus the timed slice loop only (no e2e, plain or CPU legs)")
-    ap.add_argument("--leg", choices=["stem", "adjoint"],
+    ap.add_argument("--leg", choices=["stem", "adjoint", "tds"],
                     help="run one secondary leg alone and print its JSON (exploration)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
@@ -352,7 +395,7 @@ def main():
     if args.leg:
         from cudamultislice_b200 import FPARAMS
 
-        leg = stem_leg(FPARAMS, local) if args.leg == "stem" else adjoint_leg(FPARAMS, local)
+        leg = {"stem": stem_leg, "adjoint": adjoint_leg, "tds": tds_leg}[args.leg](FPARAMS, local)
         if rank == 0:
             print(json.dumps({"leg": args.leg, **leg}), flush=True)
         return
@@ -455,6 +498,7 @@ def main():
 
     out["stem"] = stem_leg(FPARAMS, local)
     out["adjoint"] = adjoint_leg(FPARAMS, local)
+    out["tds"] = tds_leg(FPARAMS, local)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1

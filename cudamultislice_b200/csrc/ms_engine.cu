@@ -916,6 +916,113 @@ class Engine {
     return MS_OK;
   }
 
+  // ---- frozen-phonon series (the GUI's pass loop, MainWindow.xaml.cs:353-402) ----
+  // Configurations first_pass .. first_pass + nconf - 1, each displaced as
+  // ms_upload_binned_atoms_tds(seed, pass, sigma), through conventional slices
+  // 1..S from the initial wave.  diff = sum over configurations of
+  // |centre(FFT(psi_exit))| (AddTDSWaves, U.cu:2734-2766), image = mean of the
+  // deterministic CTF images (SimulateImage).  Fused path: `batch`
+  // configurations share every pass launch (instance = blockIdx.y, each with its
+  // own potential stack); plain path: one configuration at a time through the
+  // reference's launch sequence.  The handle's atom index is left at the last
+  // configuration.
+  int frozen_phonon(uint64_t seed, uint32_t first_pass, int nconf, float sigma, int batch, float* diff, float* image) {
+    if (!have_waves_) return fail(MS_ERR_STATE, "wavefunctions not initialised");
+    if (stem_) return fail(MS_ERR_UNSUPPORTED, "the frozen-phonon series runs in TEM mode");
+    if (nconf < 1 || batch < 1 || batch > 256) return fail(MS_ERR_INVALID, "need nconf >= 1 and batch 1..256");
+    if (!(sigma >= 0) || !std::isfinite(sigma)) return fail(MS_ERR_INVALID, "bad thermal displacement sigma");
+    if (int rc = require_potential_inputs()) return rc;
+    int S = 0;
+    if (int rc = get_slices(true, &S)) return rc;
+    if (S < 1) return fail(MS_ERR_INVALID, "structure has no slices");
+    if (int rc = ensure_prop_tables(convdz_)) return rc;
+    const long long N = (long long)nx_ * ny_;
+    const Grid2 g{nx_, ny_};
+    const float wavel = wavel_, objap = aperture_;
+    const float objap2 = (((objap * 0.001f) / wavel) * ((objap * 0.001f) / wavel));
+    const CtfParams ctf{(double)wavel, (double)Cs_, (double)df_, (double)A2_, (double)phi2_, 0.0, 0.0,
+                        (double)(beta_ / 1000), (double)delta_, objap2};
+    const int kind = pot_mode_ == 1 ? POT_PROJECTED : POT_CONVENTIONAL;
+    const bool fused = use_fused();
+    const int B = fused ? std::min(batch, nconf) : 1;
+    MS_TRY(d_fpdiff_.resize(N));
+    MS_TRY(d_fpsum_.resize(N));
+    MS_TRY(d_fpimg_.resize((size_t)B * N));
+    MS_TRY(cudaMemsetAsync(d_fpdiff_.p, 0, sizeof(float) * N, stream_));
+    MS_TRY(cudaMemsetAsync(d_fpsum_.p, 0, sizeof(float) * N, stream_));
+    if (fused) {
+      MS_TRY(d_fpstack_.resize((size_t)B * S * N));
+      MS_TRY(d_bwave_.resize((size_t)B * N));
+      plan_for(B);
+    }
+    invalidate_graph();
+    MS_TRY(cudaEventRecord(ev0_, stream_));
+    for (int start = 0; start < nconf; start += B) {
+      const int nb = std::min(B, nconf - start);
+      if (!fused) {
+        if (int rc = upload_binned(true, seed, first_pass + (uint32_t)start, sigma)) return rc;
+        for (int it = 1; it <= S; ++it)
+          if (int rc = step_conventional(it)) return rc;
+        MS_TRY_FFT(cufftExecC2C(plan_, d_psi_.p, d_t1_.p, CUFFT_FORWARD));
+        if (diff) MS_TRY(pw_centre_abs_acc(d_t1_.p, d_fpdiff_.p, 1.0f, g, stream_, &launches));
+        if (image) {
+          MS_TRY(pw_ctf(d_t1_.p, d_kx_.p, d_ky_.p, wavel, Cs_, df_, A2_, phi2_, (double)(beta_ / 1000), delta_,
+                        objap2, 1.0f / (float)N, g, stream_, &launches));
+          MS_TRY_FFT(cufftExecC2C(plan_, d_t1_.p, d_t2_.p, CUFFT_INVERSE));
+          MS_TRY(pw_abs2(d_t2_.p, d_fpimg_.p, 1.0f, g, stream_, &launches));
+          MS_TRY(pw_add_batch(d_fpimg_.p, N, 1, d_fpsum_.p, 1.0f / (float)nconf, g, stream_, &launches));
+        }
+        continue;
+      }
+      // potential stacks of the nb configurations: [config][slice][ny][nx]
+      for (int k = 0; k < nb; ++k) {
+        if (int rc = upload_binned(true, seed, first_pass + (uint32_t)(start + k), sigma)) return rc;
+        for (int it = 1; it <= S; ++it)
+          if (int rc = potential_slice(kind, it, d_fpstack_.p + ((size_t)k * S + (it - 1)) * N)) return rc;
+        MS_TRY(cudaMemcpyAsync(d_bwave_.p + (size_t)k * N, d_psi0_.p, sizeof(float2) * N, cudaMemcpyDeviceToDevice,
+                               stream_));
+      }
+      for (int it = 1; it <= S; ++it) {
+        PassAArgs a = passa_args(d_bwave_.p, d_bwave_.p, 0);
+        a.batch_stride_wave = N;
+        a.batch_stride_V = (long long)S * N;
+        a.V = d_fpstack_.p + (size_t)(it - 1) * N;
+        MS_TRY(pass_a(a, it == 1 ? (A_MULT_T | A_FWD) : (A_INV | A_MULT_T | A_FWD), nb));
+        PassBArgs b = passb_args(d_bwave_.p, d_bwave_.p, 0);
+        b.batch_stride_wave = N;
+        MS_TRY(pass_b(b, B_PROPAGATE, nb));
+        launches += 2;
+      }
+      if (diff) {
+        PassBArgs b = passb_args(d_bwave_.p, d_bwave_.p, 0);
+        b.batch_stride_wave = N;
+        b.acc = d_fpdiff_.p;
+        b.scale = (float)nx_;  // FFT2(psi) = nx FFT_col(X)
+        MS_TRY(pass_b(b, B_CBED, nb));
+        ++launches;
+      }
+      if (image) {
+        PassBArgs b = passb_args(d_bwave_.p, d_bwave_.p, 0);
+        b.batch_stride_wave = N;
+        b.ctf = ctf;
+        b.scale = (float)nx_ / (float)N;
+        MS_TRY(pass_b(b, B_CTF, nb));
+        PassAArgs a = passa_args(d_bwave_.p, nullptr, 0);
+        a.batch_stride_wave = N;
+        a.out_f = d_fpimg_.p;
+        MS_TRY(pass_a(a, A_INV | A_INTENSITY, nb));
+        MS_TRY(pw_add_batch(d_fpimg_.p, N, nb, d_fpsum_.p, 1.0f / (float)nconf, g, stream_, &launches));
+        launches += 2;
+      }
+    }
+    MS_TRY(cudaEventRecord(ev1_, stream_));
+    if (diff) MS_TRY(cudaMemcpyAsync(diff, d_fpdiff_.p, sizeof(float) * N, cudaMemcpyDeviceToHost, stream_));
+    if (image) MS_TRY(cudaMemcpyAsync(image, d_fpsum_.p, sizeof(float) * N, cudaMemcpyDeviceToHost, stream_));
+    MS_TRY(cudaStreamSynchronize(stream_));
+    MS_TRY(cudaEventElapsedTime(&last_device_ms_, ev0_, ev1_));
+    return MS_OK;
+  }
+
   // ---- whole-run entry points ----
   int build_stack(int* nslices) {
     if (int rc = require_potential_inputs()) return rc;
@@ -1669,7 +1776,7 @@ class Engine {
   float last_device_ms_ = 0.0f;
   std::vector<int> hzoff_;  // first sorted atom per z-bin (focal-series atom gradient)
   DevBuf<float2> d_ck_, d_seg_, d_G_, d_U_, d_Phi_;
-  DevBuf<float> d_T_, d_dV_, d_img_;
+  DevBuf<float> d_T_, d_dV_, d_img_, d_fpstack_, d_fpdiff_, d_fpsum_, d_fpimg_;
   DevBuf<double> d_loss_, d_dxy_;
   std::vector<std::pair<int, PlanChoice>> tuned_;
   float prop_dz_ = -1.0f;
@@ -2027,6 +2134,12 @@ ms_status ms_focal_series_grad(ms_sim* s, const float* defoci, int nd, const flo
 ms_status ms_time_pass(ms_sim* s, int pass, int op, int variant, int batch, int reps, float* us) {
   if (ms_status r = out_check(s, us)) return r;
   return guarded(s, [&](ms::Engine& e) { return e.time_pass(pass, op, variant, batch, reps, us); });
+}
+ms_status ms_frozen_phonon(ms_sim* s, uint64_t seed, uint32_t first_pass, int nconfigs, float sigma, int batch,
+                           float* diffraction, float* image) {
+  return guarded(s, [&](ms::Engine& e) {
+    return e.frozen_phonon(seed, first_pass, nconfigs, sigma, batch, diffraction, image);
+  });
 }
 ms_status ms_get_last_device_ms(ms_sim* s, float* out) {
   if (ms_status r = out_check(s, out)) return r;

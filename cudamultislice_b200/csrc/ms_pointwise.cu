@@ -165,6 +165,14 @@ __global__ void k_abs2(const float2* a, float* out, float scale, Grid2 g) {
   out[i] = (v.x * v.x + v.y * v.y) * scale;
 }
 
+// acc += scale * sum_b in[b * stride + i] (batched images into one sum)
+__global__ void k_add_batch(const float* in, long long stride, int nb, float* acc, float scale, Grid2 g) {
+  PW_INDEX
+  float s = 0.0f;
+  for (int b = 0; b < nb; ++b) s += in[(long long)b * stride + i];
+  acc[i] += scale * s;
+}
+
 __global__ void k_ctf(float2* F, const float* kx, const float* ky, double wavel, double Cs, double df, double A2,
                       double phi2, double beta, double delta, float objap2, float scale, Grid2 g) {
   PW_INDEX
@@ -306,6 +314,10 @@ cudaError_t pw_transpose(const float2* in, float2* out, Grid2 g, cudaStream_t s,
 }
 cudaError_t pw_abs2(const float2* a, float* out, float scale, Grid2 g, cudaStream_t s, long long* count) {
   PW_LAUNCH(k_abs2, a, out, scale, g);
+}
+cudaError_t pw_add_batch(const float* in, long long stride, int nb, float* acc, float scale, Grid2 g, cudaStream_t s,
+                         long long* count) {
+  PW_LAUNCH(k_add_batch, in, stride, nb, acc, scale, g);
 }
 cudaError_t pw_ctf(float2* F, const float* kx, const float* ky, double wavel, double Cs, double df, double A2,
                    double phi2, double beta, double delta, float objap2, float scale, Grid2 g, cudaStream_t s,

@@ -31,6 +31,9 @@ cudaError_t pw_real_to_complex(const float* in, float2* out, Grid2 g, cudaStream
 cudaError_t pw_centre_abs_acc(const float2* F, float* acc, float scale, Grid2 g, cudaStream_t s, long long* count);
 cudaError_t pw_centre(const float2* F, float2* out, Grid2 g, cudaStream_t s, long long* count);
 cudaError_t pw_abs2(const float2* a, float* out, float scale, Grid2 g, cudaStream_t s, long long* count);
+// acc += scale * sum over nb instances (stride apart) of in.
+cudaError_t pw_add_batch(const float* in, long long stride, int nb, float* acc, float scale, Grid2 g, cudaStream_t s,
+                         long long* count);
 // out[x][y] = in[y][x] (one-time layout changes).
 cudaError_t pw_transpose(const float2* in, float2* out, Grid2 g, cudaStream_t s, long long* count);
 // CTF multiply for the plain path (same weight as the fused column pass).

@@ -36,15 +36,19 @@ template <> struct PlanSel<2048, 2> { using T = fft::Plan<2048, 8, 8, 8, 8, 4>; 
 constexpr int kPlanVariants = 3;
 
 // Threads per CTA: rows, 256 (whole lines); columns, at least 4 columns per
-// CTA so the transposing tile access moves whole 32-byte sectors.
+// CTA so the transposing tile access moves whole 32-byte sectors (256 threads
+// for lines of at most 32 threads; wider tiles measured slower).
 template <class PL>
 __host__ __device__ constexpr int rows_per_cta() { return PL::P >= 256 ? 1 : 256 / PL::P; }
 template <class PL>
 __host__ __device__ constexpr int cols_per_cta() { return PL::P >= 64 ? 4 : 256 / PL::P; }
-// Column slots 2 points (mod 16) apart: the transposing tile load (8 columns x
-// 2 rows per 16-lane phase) is then free of bank conflicts.
+// Column slots 16/CB points (mod 16) apart for CB <= 16 columns per CTA (1 for
+// more): a 16-lane phase of the transposing tile access covers 16/CB rows of
+// CB columns, whose 8-byte points then fall in distinct bank pairs.
 template <class PL>
-__host__ __device__ constexpr int col_slot() { return ((PL::N + PL::N / PL::R1 + 15) / 16) * 16 + 2; }
+__host__ __device__ constexpr int col_slot() {
+  return ((PL::N + PL::N / PL::R1 + 15) / 16) * 16 + (cols_per_cta<PL>() <= 16 ? 16 / cols_per_cta<PL>() : 1);
+}
 
 // Programmatic dependent launch: the passes are launched with programmatic
 // stream serialisation, so a pass may start while the previous kernel of the

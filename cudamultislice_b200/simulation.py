@@ -271,6 +271,17 @@ class ManagedMultisliceSimulation:
                                          float(outer_mrad), int(batch), _ptr(out)))
         return out
 
+    # ---- frozen phonons ----
+    def FrozenPhonon(self, seed: int, first_pass: int, nconfigs: int, sigma: float, batch: int = 16,
+                     diffraction: bool = True, image: bool = True):
+        """Sum of centred |FFT(psi_exit)| and mean CTF image over thermal configurations."""
+        d = np.zeros((self.ny, self.nx), np.float32) if diffraction else None
+        im = np.zeros((self.ny, self.nx), np.float32) if image else None
+        self._chk(self._L.ms_frozen_phonon(self._h, int(seed), int(first_pass), int(nconfigs), float(sigma),
+                                           int(batch), _ptr(d) if diffraction else None,
+                                           _ptr(im) if image else None))
+        return d, im
+
     # ---- differentiable focal series ----
     def FocalSeries(self, defoci, targets, nslices: int, images: bool = False):
         """Loss sum_d sum_px (I_d - T_d)^2 of the CTF images at `defoci` (A) of

@@ -201,6 +201,19 @@ ms_status ms_annular_detector(ms_sim* sim, float inner_mrad, float outer_mrad, d
 ms_status ms_stem_raster(ms_sim* sim, const int* px, const int* py, int n, float inner_mrad,
                          float outer_mrad, int batch, double* signal);
 
+/* Frozen-phonon series (new; the reference's GUI loops UploadBinnedAtomsTDS,
+ * the slices and AddTDSWaves over passes, CUDA Simulation GUI/MainWindow.xaml.cs:353-402):
+ * configurations pass = first_pass .. first_pass + nconfigs - 1, each displaced as
+ * ms_upload_binned_atoms_tds(seed, pass, sigma), run through conventional slices
+ * 1..S from the initial wave (ms_initialise_wavefunctions_dz), `batch`
+ * configurations at a time sharing every launch of the fused passes.
+ * diffraction (nx*ny floats, may be NULL) = sum over configurations of
+ * |centre(FFT(psi_exit))| as AddTDSWaves (U.cu:2734-2766); image (nx*ny floats,
+ * may be NULL) = mean over configurations of the ms_simulate_image CTF image.
+ * The handle's atom index is left at the last configuration. */
+ms_status ms_frozen_phonon(ms_sim* sim, uint64_t seed, uint32_t first_pass, int nconfigs, float sigma, int batch,
+                           float* diffraction, float* image);
+
 /* ---- differentiable focal series (new; no reference counterpart) ----
  * Loss L = sum_d sum_px (I_d(px) - T_d(px))^2, with I_d the CTF image of
  * ms_simulate_image (imagingKernel2, U.cu:1044-1080, at the microscope

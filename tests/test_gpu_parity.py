@@ -312,3 +312,24 @@ def test_fd_readout_then_continue(engine_cls, oracle_mod):
     assert rel_l2(eng.ExitWave(), orc.Wave()) < 5 * TOL
     eng.SimulateImage(0.0)
     assert rel_l2(eng.Image(), orc.SimulateImage()) < 5 * TOL
+
+
+# ---------------------------------------------------------------- frozen phonons
+@pytest.mark.parametrize("path", [0, 1])
+def test_frozen_phonon_series(engine_cls, oracle_mod, path):
+    """Batched thermal configurations (fused: 2 per launch, 3 in all) against the
+    oracle's pass loop: UploadBinnedAtomsTDS, the slices, AddTDSWaves, SimulateImage."""
+    eng, orc = make_pair(engine_cls, oracle_mod, sto(2, 2), 128, 0.1, path=path)
+    seed, sigma, first, nconf = 0x5EED2026, 0.076, 5, 3
+    d, im = eng.FrozenPhonon(seed, first, nconf, sigma, batch=2)
+    S = orc.GetSlices(True)
+    orc.AllocTDS()
+    imgs = []
+    for p in range(first, first + nconf):
+        orc.UploadBinnedAtomsTDS(seed, p, sigma)
+        for i in range(1, S + 1):
+            orc.MultisliceStepConventional(i)
+        orc.AddTDSWaves()
+        imgs.append(orc.SimulateImage())
+    assert rel_l2(d, orc.TDS()) < TOL
+    assert rel_l2(im, np.mean(imgs, axis=0)) < TOL
