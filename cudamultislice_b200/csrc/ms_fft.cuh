@@ -101,8 +101,11 @@ struct Plan {
   static_assert(E_ % R1_ == 0 && E_ % R2_ == 0 && E_ % R3_ == 0 && E_ % R4_ == 0, "radix must divide E");
   static_assert(R1_ <= 32 && R2_ <= 32 && R3_ <= 32 && R4_ <= 32, "radix above 32");
   static_assert(P <= 32 || P % 32 == 0, "multi-warp lines need whole warps");
-  // Points in one line slot (one pad point every R1, slots 8 apart mod 16).
-  static constexpr int SLOT = ((N_ + N_ / R1_ + 15) / 16) * 16 + 8;
+  // Shared-memory map of a line's points (see padi): an XOR swizzle for first
+  // radices 4 and 8 on lines of at least 16 threads, else one pad point every R1.
+  static constexpr bool XOR_MAP = (R1_ == 4 || R1_ == 8) && P >= 16;
+  // Points in one line slot (slots 8 apart mod 16).
+  static constexpr int SLOT = XOR_MAP ? N_ + 8 : ((N_ + N_ / R1_ + 15) / 16) * 16 + 8;
   // Twiddle table: pass p >= 2 holds R_p * Ns_p entries [r][k].
   // (absent passes, radix 1, take no entries; the sum never exceeds 2N)
   static constexpr int TW2 = 0, TW3 = TW2 + R2_ * R1_, TW4 = TW3 + (R3_ > 1 ? R3_ * R1_ * R2_ : 0);
@@ -110,9 +113,24 @@ struct Plan {
   static_assert(TWSIZE <= 2 * N_, "twiddle table larger than 2N");
 };
 
+// Slot position of point n.  A 64-bit access of 16 lanes is one wavefront when
+// its points fall in 16 distinct (point mod 16) classes.  Lines read 16
+// consecutive, 16-aligned points per half-warp in every pass; the writes of the
+// first pass are R1 apart and those of a middle pass with NS < 16 come in
+// groups of NS.  Padding one point every R1 serves the strided writes but
+// wraps the consecutive reads when R1 < 16; the XOR map n ^ f(n >> 4) permutes
+// each aligned block of 16 (reads stay conflict-free) with f chosen so that the
+// R1-strided and NS-grouped writes of the plan also land in distinct classes
+// (checked exhaustively on the host for every plan).
 template <class PL>
 MS_D int padi(int n) {
-  return n + n / PL::R1;
+  if constexpr (PL::XOR_MAP) {
+    const int r = n >> 4;
+    const int f = PL::R1 == 8 ? ((r ^ ((r & 4) << 1)) & 15) : (((r & 3) * 5) & 15);
+    return n ^ f;
+  } else {
+    return n + n / PL::R1;
+  }
 }
 
 // Barrier of the P threads that own one line: the warp's lanes for P <= 32,

@@ -47,7 +47,8 @@ __host__ __device__ constexpr int cols_per_cta() { return PL::P >= 64 ? 4 : 256 
 // CB columns, whose 8-byte points then fall in distinct bank pairs.
 template <class PL>
 __host__ __device__ constexpr int col_slot() {
-  return ((PL::N + PL::N / PL::R1 + 15) / 16) * 16 + (cols_per_cta<PL>() <= 16 ? 16 / cols_per_cta<PL>() : 1);
+  return (PL::XOR_MAP ? PL::N : ((PL::N + PL::N / PL::R1 + 15) / 16) * 16) +
+         (cols_per_cta<PL>() <= 16 ? 16 / cols_per_cta<PL>() : 1);
 }
 
 // Programmatic dependent launch: the passes are launched with programmatic
