@@ -35,6 +35,7 @@ SIGNATURES = {
     "ms_set_fd_dz": (_i, [_p, _f]),
     "ms_multislice_step_fd": (_i, [_p, _i]),
     "ms_multislice_step_conventional": (_i, [_p, _i]),
+    "ms_multislice_step_rs": (_i, [_p, _i]),
     "ms_get_size_x": (_i, [_p, _pf]),
     "ms_get_size_y": (_i, [_p, _pf]),
     "ms_get_size_z": (_i, [_p, _pf]),

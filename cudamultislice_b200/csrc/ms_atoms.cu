@@ -224,7 +224,7 @@ __device__ __forceinline__ float vzatom2_f(const float* __restrict__ c, float r2
 
 template <int KIND>
 __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a) {
-  constexpr int NSUB = (KIND == POT_CONVENTIONAL) ? 20 : 1;
+  constexpr int NSUB = (KIND == POT_CONVENTIONAL) ? 20 : (KIND == POT_RS) ? 10 : 1;
   __shared__ float4 s_at[kChunk];
   __shared__ float s_coef[103 * kCoefPerZ];
   __shared__ int s_start[kMaxSeg];
@@ -574,6 +574,7 @@ cudaError_t launch_potential(const PotArgs& a, int kind, cudaStream_t s) {
     case POT_CONVENTIONAL: k_potential_conv<<<grid, kPotThreads, 0, s>>>(a); break;
     case POT_FD: k_potential<POT_FD><<<grid, kPotThreads, 0, s>>>(a); break;
     case POT_PROJECTED: k_potential<POT_PROJECTED><<<grid, kPotThreads, 0, s>>>(a); break;
+    case POT_RS: k_potential<POT_RS><<<grid, kPotThreads, 0, s>>>(a); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

@@ -35,7 +35,7 @@ cudaError_t build_atom_index(const int* dZ, const float* dx, const float* dy, co
 // host in FP64: 12 floats for vatom, then 12 for vzatom2 (see engine).
 constexpr int kCoefPerZ = 24;
 
-enum PotKind : int { POT_CONVENTIONAL = 0, POT_FD = 1, POT_PROJECTED = 2 };
+enum PotKind : int { POT_CONVENTIONAL = 0, POT_FD = 1, POT_PROJECTED = 2, POT_RS = 3 };
 
 struct PotArgs {
   const float4* atoms;

@@ -524,6 +524,33 @@ class Engine {
     return MS_OK;
   }
 
+  // MultisliceStepRS (U.cu:2126-2178) as written: the RS potential of the
+  // plane (not exponentiated), ten series terms w <- w + i pre_m (L w + V w)
+  // restarting from w = 1 (ping-pong buffers), then PsiMinus = w * Psi for
+  // iterations after the first and Psi = w.  The reference does not expose
+  // this step through its managed wrapper.
+  int step_rs(int it) {
+    if (!have_waves_) return fail(MS_ERR_STATE, "wavefunctions not initialised");
+    if (it < 1) return fail(MS_ERR_INVALID, "iteration counts from 1");
+    if (int rc = require_potential_inputs()) return rc;
+    if (int rc = ensure_real()) return rc;
+    fd_state_ = false;
+    const Grid2 g{nx_, ny_};
+    if (int rc = potential_slice(POT_RS, it, d_f_.p)) return rc;
+    const float pre0 = wavel_ * 1.0f / (4.0f * 3.1415927f);
+    const float ips2 = 1.0f / (ps_ * ps_);
+    float2* bufs[2] = {d_t1_.p, d_t2_.p};
+    for (int m = 1; m <= 10; ++m)
+      MS_TRY(pw_rs_term(bufs[m % 2], bufs[(m + 1) % 2], d_f_.p, (1.0f / (float)m) * pre0, ips2, m, g, stream_,
+                        &launches));
+    float2* w = bufs[11 % 2];
+    if (it > 1) MS_TRY(pw_cmul(w, d_psi_.p, d_psim_.p, 1.0f, g, stream_, &launches));
+    MS_TRY(cudaMemcpyAsync(d_psi_.p, w, sizeof(float2) * nx_ * ny_, cudaMemcpyDeviceToDevice, stream_));
+    domain_ = 0;
+    invalidate_graph();
+    return MS_OK;
+  }
+
   // Finite-difference step on the fused passes.  Between steps the state is
   // X (row-frequency form of psi_n, IFFT_row(X) = psi_n), the band-limited
   // spectrum FFT2(psi_n) (column-major) and psi_{n-1} in real space.
@@ -1417,7 +1444,7 @@ class Engine {
   int copy_potential(int kind, int it, float* dst) {
     if (int rc = require_potential_inputs()) return rc;
     if (it < 1) return fail(MS_ERR_INVALID, "iteration counts from 1");
-    if (kind < 0 || kind > 2) return fail(MS_ERR_INVALID, "unknown potential kind");
+    if (kind < 0 || kind > 3) return fail(MS_ERR_INVALID, "unknown potential kind");
     if (int rc = potential_slice(kind, it, d_f_.p)) return rc;
     MS_TRY(cudaMemcpyAsync(dst, d_f_.p, sizeof(float) * nx_ * ny_, cudaMemcpyDeviceToHost, stream_));
     MS_TRY(cudaStreamSynchronize(stream_));
@@ -1703,6 +1730,17 @@ class Engine {
       a.nsub = 20;
       for (int m = 1; m <= 20; ++m) a.zsub[m - 1] = z - m * convdz_ / 20.0f;
       a.wsub = convdz_ / 20.0f;
+    } else if (kind == POT_RS) {
+      // binnedAtomPKernelRS U.cu:655-727 at z = top - dz*it, dz = 1 (int) (U.cu:2129-2137)
+      const float z = box_.MaxZ - box_.MinZ - (float)(1 * it);
+      const int K = (int)std::floor((box_.MaxZ - box_.MinZ - z) / (float)1);
+      a.kt = std::max(K - lbz_, 0);
+      a.kb = std::min(K + lbz_, nzb_ - 1);
+      a.xoff = xoff_;
+      a.yoff = yoff_;
+      a.nsub = 10;
+      for (int m = 1; m <= 10; ++m) a.zsub[m - 1] = z - (float)(m * 1) / 10.0f;
+      a.wsub = 1 / 10.0f;
     } else if (kind == POT_FD) {
       // binnedAtomPKernelFD U.cu:883-946 at z = top - dzFD*it, no offsets
       const float z = box_.MaxZ - box_.MinZ - dzFD_ * it;
@@ -1935,6 +1973,9 @@ ms_status ms_set_fd_dz(ms_sim* s, float dz) {
 }
 ms_status ms_multislice_step_fd(ms_sim* s, int it) {
   return guarded(s, [&](ms::Engine& e) { return e.step_fd(it); });
+}
+ms_status ms_multislice_step_rs(ms_sim* s, int it) {
+  return guarded(s, [&](ms::Engine& e) { return e.step_rs(it); });
 }
 ms_status ms_multislice_step_conventional(ms_sim* s, int it) {
   return guarded(s, [&](ms::Engine& e) { return e.step_conventional(it); });

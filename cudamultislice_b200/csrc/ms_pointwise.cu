@@ -165,6 +165,33 @@ __global__ void k_abs2(const float2* a, float* out, float scale, Grid2 g) {
   out[i] = (v.x * v.x + v.y * v.y) * scale;
 }
 
+// One term of MultisliceStepRS's series (RSMS U.cu:849-877 over
+// DifferentialXKernel + DifferentialYKernel U.cu:797-847, as written):
+//   m = 1:  out = 1 + i pre V
+//   m > 1:  out = w + i pre (L w + V w),
+//   L w = inv_ps2 (4/3 (w[+1] + w[-1] - w) - 1/12 (w[+2] + w[-2] - w)) per direction,
+// neighbours beyond an edge read at index 0 of the line ((i>0)*(i-1) indices).
+__global__ void k_rs_term(const float2* w, float2* out, const float* V, float pre, float inv_ps2, int m, Grid2 g) {
+  PW_INDEX
+  if (m == 1) {
+    out[i] = make_float2(1.0f, pre * V[i]);
+    return;
+  }
+  const int p1 = (x > 0) * (x - 1), p2 = (x > 1) * (x - 2);
+  const int n1 = (x < g.nx - 1) * (x + 1), n2 = (x < g.nx - 2) * (x + 2);
+  const int q1 = (y > 0) * (y - 1), q2 = (y > 1) * (y - 2);
+  const int o1 = (y < g.ny - 1) * (y + 1), o2 = (y < g.ny - 2) * (y + 2);
+  const long long row = (long long)y * g.nx;
+  const float2 c = w[i];
+  const float2 dx1 = csub(cadd(w[row + n1], w[row + p1]), c), dx2 = csub(cadd(w[row + n2], w[row + p2]), c);
+  const float2 dy1 = csub(cadd(w[(long long)o1 * g.nx + x], w[(long long)q1 * g.nx + x]), c);
+  const float2 dy2 = csub(cadd(w[(long long)o2 * g.nx + x], w[(long long)q2 * g.nx + x]), c);
+  const float lx = inv_ps2 * (4.0f * dx1.x / 3.0f - dx2.x / 12.0f) + inv_ps2 * (4.0f * dy1.x / 3.0f - dy2.x / 12.0f);
+  const float ly = inv_ps2 * (4.0f * dx1.y / 3.0f - dx2.y / 12.0f) + inv_ps2 * (4.0f * dy1.y / 3.0f - dy2.y / 12.0f);
+  const float v = V[i];
+  out[i] = make_float2(c.x - pre * (ly + v * c.y), c.y + pre * (lx + v * c.x));
+}
+
 // acc += scale * sum_b in[b * stride + i] (batched images into one sum)
 __global__ void k_add_batch(const float* in, long long stride, int nb, float* acc, float scale, Grid2 g) {
   PW_INDEX
@@ -318,6 +345,10 @@ cudaError_t pw_abs2(const float2* a, float* out, float scale, Grid2 g, cudaStrea
 cudaError_t pw_add_batch(const float* in, long long stride, int nb, float* acc, float scale, Grid2 g, cudaStream_t s,
                          long long* count) {
   PW_LAUNCH(k_add_batch, in, stride, nb, acc, scale, g);
+}
+cudaError_t pw_rs_term(const float2* w, float2* out, const float* V, float pre, float inv_ps2, int m, Grid2 g,
+                       cudaStream_t s, long long* count) {
+  PW_LAUNCH(k_rs_term, w, out, V, pre, inv_ps2, m, g);
 }
 cudaError_t pw_ctf(float2* F, const float* kx, const float* ky, double wavel, double Cs, double df, double A2,
                    double phi2, double beta, double delta, float objap2, float scale, Grid2 g, cudaStream_t s,

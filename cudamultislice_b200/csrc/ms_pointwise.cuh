@@ -31,6 +31,9 @@ cudaError_t pw_real_to_complex(const float* in, float2* out, Grid2 g, cudaStream
 cudaError_t pw_centre_abs_acc(const float2* F, float* acc, float scale, Grid2 g, cudaStream_t s, long long* count);
 cudaError_t pw_centre(const float2* F, float2* out, Grid2 g, cudaStream_t s, long long* count);
 cudaError_t pw_abs2(const float2* a, float* out, float scale, Grid2 g, cudaStream_t s, long long* count);
+// Term m of the real-space (RS) series, as written in the reference (see .cu).
+cudaError_t pw_rs_term(const float2* w, float2* out, const float* V, float pre, float inv_ps2, int m, Grid2 g,
+                       cudaStream_t s, long long* count);
 // acc += scale * sum over nb instances (stride apart) of in.
 cudaError_t pw_add_batch(const float* in, long long stride, int nb, float* acc, float scale, Grid2 g, cudaStream_t s,
                          long long* count);

@@ -153,6 +153,10 @@ class ManagedMultisliceSimulation:
     def MultisliceStepConventional(self, iteration: int):
         self._chk(self._L.ms_multislice_step_conventional(self._h, int(iteration)))
 
+    def MultisliceStepRS(self, iteration: int):
+        """MultisliceStepRS as written (not exposed by the reference's wrapper)."""
+        self._chk(self._L.ms_multislice_step_rs(self._h, int(iteration)))
+
     # ---- queries ----
     def GetSizeX(self) -> float:
         return self._f(self._L.ms_get_size_x)

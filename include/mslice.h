@@ -129,6 +129,14 @@ ms_status ms_set_fd_dz(ms_sim* sim, float dz);
 ms_status ms_multislice_step_fd(ms_sim* sim, int iteration);
 /* MultisliceStepConv U.cu:2085-2124. */
 ms_status ms_multislice_step_conventional(ms_sim* sim, int iteration);
+/* MultisliceStepRS (U.cu:2126-2178; not exposed by the reference's managed
+ * wrapper), as written: the real-space series of ten terms over the
+ * un-exponentiated RS potential (binnedAtomPKernelRS U.cu:655-727, dz = 1,
+ * ten sub-planes), with the reference's 5-point stencil (centre coefficient 1,
+ * edge neighbours read at index 0), restarting from 1 every step; afterwards
+ * the wave is the series result and, from the second iteration on, the
+ * previous-level wave is that result times the previous wave. */
+ms_status ms_multislice_step_rs(ms_sim* sim, int iteration);
 
 /* ---- queries (ManagedMultislice.cpp:89-117) ---- */
 ms_status ms_get_size_x(ms_sim* sim, float* out);
@@ -247,7 +255,7 @@ ms_status ms_get_last_device_ms(ms_sim* sim, float* out);
 ms_status ms_get_binned_counts(ms_sim* sim, int* n_atoms, int* n_zbins);
 ms_status ms_copy_binned(ms_sim* sim, int* offsets, int* Z, float* x, float* y, float* z);
 /* kind: 0 conventional slice, 1 finite-difference plane, 2 projected slab (current
- * conventional dz) */
+ * conventional dz), 3 RS plane (ms_multislice_step_rs) */
 ms_status ms_copy_potential_slice(ms_sim* sim, int kind, int iteration, float* dst /* nx*ny */);
 /* 2D FFT of a host array through the engine's own FFT passes (sign -1
  * forward, +1 inverse, unnormalised); grid must be fused-supported. */

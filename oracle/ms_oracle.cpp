@@ -702,10 +702,29 @@ static int check_pot(or_sim* s) {
  * Slice `it` integrates 20 sub-planes z2 = z - m*convdz/20 (m = 1..20) below
  * z = (MaxZ-MinZ) - convdz*it over atoms whose 1-A z-bin lies within +-3 of
  * floor((MaxZ-MinZ) - z), with the r^2 < 5 cutoff per sub-plane. */
+/* Sub-plane integrated potential below plane z (FP32 shifted frame): the sum
+ * over atoms of the z-bin window K -+ lbz, K = floor((top - z) / 1), and over
+ * sub-planes z - m * dz / nsub (m = 1..nsub, FP32 as written) with
+ * r^2 < 5 A^2 (FP32), of (dz / nsub) * vatom(r^2).  nsub = 20:
+ * binnedAtomPKernel3 (U.cu:582-653); nsub = 10, dz = 1: binnedAtomPKernelRS
+ * (U.cu:655-727). */
+static int sub_plane_potential(or_sim* s, float z, float dz, int nsub, double* out);
+
 extern "C" int or_potential_conventional(or_sim* s, int it, double* out) {
     if (check_pot(s)) return -1;
-    const int nx = s->nx, ny = s->ny, nz = s->nzb;
     const float z = s->MaxZ - s->MinZ - s->convdz * it; /* U.cu:2097, FP32 */
+    return sub_plane_potential(s, z, s->convdz, 20, out);
+}
+
+/* binnedAtomPKernelRS at MultisliceStepRS's plane z = top - 1 * it (U.cu:2137). */
+extern "C" int or_potential_rs(or_sim* s, int it, double* out) {
+    if (check_pot(s)) return -1;
+    const float z = s->MaxZ - s->MinZ - (float)(1 * it);
+    return sub_plane_potential(s, z, 1.0f, 10, out);
+}
+
+static int sub_plane_potential(or_sim* s, float z, float dz, int nsub, double* out) {
+    const int nx = s->nx, ny = s->ny, nz = s->nzb;
     const int K = (int)std::floor((s->MaxZ - s->MinZ - z) / (float)1);
     int kt = K - s->lbz, kb = K + s->lbz;
     if (kt < 0) kt = 0;
@@ -714,11 +733,11 @@ extern "C" int or_potential_conventional(or_sim* s, int it, double* out) {
     const int rx = (int)std::ceil(2.2361 / w_x) + 1, ry = (int)std::ceil(2.2361 / w_y) + 1;
     float z2f[20];
     double z2d[20];
-    for (int m = 1; m <= 20; ++m) {
-        z2f[m - 1] = z - m * s->convdz / 20.0f;
-        z2d[m - 1] = (double)z - m * (double)s->convdz / 20.0;
+    for (int m = 1; m <= nsub; ++m) {
+        z2f[m - 1] = z - m * dz / (float)nsub;
+        z2d[m - 1] = (double)z - m * (double)dz / (double)nsub;
     }
-    const double wsub = (double)s->convdz / 20.0;
+    const double wsub = (double)dz / (double)nsub;
 #pragma omp parallel for schedule(dynamic, 4)
     for (int y = 0; y < ny; ++y) {
         for (int x = 0; x < nx; ++x) {
@@ -738,7 +757,7 @@ extern "C" int or_potential_conventional(or_sim* s, int it, double* out) {
                             if (!s->valdx.empty()) { ox = s->valdx[s->perm[l]]; oy = s->valdy[s->perm[l]]; }
                             const double dxd = pxd - (s->bx[l] + ox), dyd = pyd - (s->by[l] + oy);
                             const double dxyd = dxd * dxd + dyd * dyd;
-                            for (int m = 0; m < 20; ++m) {
+                            for (int m = 0; m < nsub; ++m) {
                                 const float dzf = z2f[m] - s->bz[l];
                                 const float r2f = dxy + dzf * dzf;
                                 if (r2f < 5.0f) {
@@ -849,6 +868,57 @@ static void tp_step(or_sim* s, const std::vector<double>& V, const std::vector<c
 
 /* MultisliceStepConv U.cu:2085-2124.  Iteration 1 starts from the initial wave
  * (plane wave or probe), later iterations from the current wave. */
+/* MultisliceStepRS (U.cu:2126-2178) as written.  Ten terms, m = 1..10, of
+ *   w <- w + i pre_m (L w + V w),  pre_m = (1/m) lambda dz / (4 * 3.1415927), dz = 1,
+ * where the first term restarts from w = 1 (RSMS U.cu:849-877) and L is the
+ * sum of DifferentialXKernel and DifferentialYKernel (U.cu:797-847):
+ *   (1/ps^2) (4/3 (w[+1] + w[-1] - w[0]) - 1/12 (w[+2] + w[-2] - w[0]))
+ * per direction, with neighbours beyond an edge read at index 0 of that
+ * line (the kernels' (i>0)*(i-1) style indices), and V the un-exponentiated
+ * RS potential.  Afterwards Psi = w; from the second iteration on
+ * PsiMinus = w * Psi_previous (the multiplication is kept, the final copy
+ * overwrites Psi with w). */
+extern "C" int or_step_rs(or_sim* s, int it) {
+    if (!s->have_waves) return fail(s, "waves not initialised");
+    const int nx = s->nx, ny = s->ny;
+    const size_t N = (size_t)nx * ny;
+    std::vector<double> V(N);
+    if (or_potential_rs(s, it, V.data())) return -1;
+    const double pre0 = (double)s->wavel * 1.0 / (4.0 * 3.1415927);
+    const double ips2 = 1.0 / ((double)s->ps * (double)s->ps);
+    std::vector<cd> w(N, cd(1.0, 0.0)), nw(N);
+    for (int m = 1; m <= 10; ++m) {
+        const double pre = pre0 / m;
+        if (m == 1) {
+            for (size_t i = 0; i < N; ++i) w[i] = cd(1.0, pre * V[i]);
+            continue;
+        }
+#pragma omp parallel for schedule(static)
+        for (int y = 0; y < ny; ++y)
+            for (int x = 0; x < nx; ++x) {
+                const size_t i = (size_t)y * nx + x;
+                const int p1 = (x > 0) * (x - 1), p2 = (x > 1) * (x - 2);
+                const int n1 = (x < nx - 1) * (x + 1), n2 = (x < nx - 2) * (x + 2);
+                const int q1 = (y > 0) * (y - 1), q2 = (y > 1) * (y - 2);
+                const int o1 = (y < ny - 1) * (y + 1), o2 = (y < ny - 2) * (y + 2);
+                const size_t row = (size_t)y * nx;
+                const cd c = w[i];
+                const cd dx1 = w[row + n1] + w[row + p1] - c, dx2 = w[row + n2] + w[row + p2] - c;
+                const cd dy1 = w[(size_t)o1 * nx + x] + w[(size_t)q1 * nx + x] - c;
+                const cd dy2 = w[(size_t)o2 * nx + x] + w[(size_t)q2 * nx + x] - c;
+                const cd lap = ips2 * (4.0 * dx1 / 3.0 - dx2 / 12.0) + ips2 * (4.0 * dy1 / 3.0 - dy2 / 12.0);
+                nw[i] = c + cd(0.0, pre) * (lap + V[i] * c);
+            }
+        w.swap(nw);
+    }
+    if (it > 1) {
+        s->psi_minus.resize(N);
+        for (size_t i = 0; i < N; ++i) s->psi_minus[i] = w[i] * s->psi[i];
+    }
+    s->psi = w;
+    return 0;
+}
+
 extern "C" int or_step_conventional(or_sim* s, int it) {
     if (!s->have_waves) return fail(s, "waves not initialised");
     std::vector<double> V((size_t)s->nx * s->ny);

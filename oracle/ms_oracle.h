@@ -83,10 +83,12 @@ int or_set_fd_dz(or_sim*, float dz);          /* override the automatic stable F
 int or_potential_conventional(or_sim*, int iteration, double* out);  /* binnedAtomPKernel3 U.cu:582-653 */
 int or_potential_fd(or_sim*, int iteration, double* out);            /* binnedAtomPKernelFD U.cu:883-946 */
 int or_potential_projected(or_sim*, int iteration, float dz, double* out); /* vzatom2 slab mode */
+int or_potential_rs(or_sim*, int iteration, double* out);            /* binnedAtomPKernelRS U.cu:655-727 */
 
 int or_step_conventional(or_sim*, int iteration);                    /* U.cu:2085-2124 */
 int or_step_projected(or_sim*, int iteration);                       /* same step, projected V */
 int or_step_fd(or_sim*, int iteration);                              /* U.cu:2040-2083 */
+int or_step_rs(or_sim*, int iteration);                              /* U.cu:2126-2178, as written */
 int or_get_wave(or_sim*, double* out /* 2N */);
 int or_set_wave(or_sim*, const double* in /* 2N */);
 

@@ -79,6 +79,8 @@ def lib():
         "or_step_conventional": (_i, [_p, _i]),
         "or_step_projected": (_i, [_p, _i]),
         "or_step_fd": (_i, [_p, _i]),
+        "or_potential_rs": (_i, [_p, _i, _p]),
+        "or_step_rs": (_i, [_p, _i]),
         "or_get_wave": (_i, [_p, _p]),
         "or_set_wave": (_i, [_p, _p]),
         "or_simulate_image": (_i, [_p, _p]),
@@ -299,6 +301,14 @@ class OracleSimulation:
 
     def MultisliceStepFD(self, it: int):
         self._chk(self._L.or_step_fd(self._h, it))
+
+    def MultisliceStepRS(self, it: int):
+        self._chk(self._L.or_step_rs(self._h, it))
+
+    def PotentialRS(self, it: int) -> np.ndarray:
+        out = np.zeros((self.ny, self.nx), np.float64)
+        self._chk(self._L.or_potential_rs(self._h, it, _ptr(out)))
+        return out
 
     # ---- read-out ----
     def Wave(self) -> np.ndarray:

@@ -333,3 +333,17 @@ def test_frozen_phonon_series(engine_cls, oracle_mod, path):
         imgs.append(orc.SimulateImage())
     assert rel_l2(d, orc.TDS()) < TOL
     assert rel_l2(im, np.mean(imgs, axis=0)) < TOL
+
+
+# ---------------------------------------------------------------- RS path
+def test_rs_potential_and_steps(engine_cls, oracle_mod):
+    """MultisliceStepRS as written (ten-term real-space series, 5-point stencil
+    with the reference's centre coefficient and edge indices) vs the oracle."""
+    eng, orc = make_pair(engine_cls, oracle_mod, sto(2, 2), 128, 0.1)
+    for it in (2, 4):
+        v = eng.PotentialSlice(3, it)
+        assert rel_l2(v, orc.PotentialRS(it)) < TOL
+    for it in range(1, 6):
+        eng.MultisliceStepRS(it)
+        orc.MultisliceStepRS(it)
+    assert rel_l2(eng.ExitWave(), orc.Wave()) < TOL
