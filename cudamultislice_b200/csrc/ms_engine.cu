@@ -863,12 +863,11 @@ class Engine {
   // column spectrum.  Linear in psi, so probes run unnormalised and each
   // signal is divided by its L1 norm squared at the end.
   int stem_raster(const int* px, const int* py, int n, float inner, float outer, int batch, double* signal) {
-    if (!have_freq_) return fail(MS_ERR_STATE, "frequencies not precalculated");
     if (!px || !py || !signal) return fail(MS_ERR_INVALID, "null buffer");
-    if (n < 1) return fail(MS_ERR_INVALID, "need at least one probe position");
-    if (batch < 1 || batch > 1024) return fail(MS_ERR_INVALID, "batch must be 1..1024");
-    if (!(inner >= 0) || !(outer > inner)) return fail(MS_ERR_INVALID, "need 0 <= inner < outer");
     if (!use_fused()) {
+      if (!have_freq_) return fail(MS_ERR_STATE, "frequencies not precalculated");
+      if (n < 1) return fail(MS_ERR_INVALID, "need at least one probe position");
+      if (!(inner >= 0) || !(outer > inner)) return fail(MS_ERR_INVALID, "need 0 <= inner < outer");
       // plain path: one probe at a time through the reference sequence
       for (int i = 0; i < n; ++i) {
         if (int rc = stem_init_waves(px[i], py[i])) return rc;
@@ -880,68 +879,103 @@ class Engine {
       }
       return MS_OK;
     }
-    int S = 0;
-    if (int rc = build_stack(&S)) return rc;
+    if (int rc = raster_prepare(px, py, n, inner, outer, batch)) return rc;
+    if (int rc = raster_enqueue(stream_)) return rc;
+    return raster_finish(signal);
+  }
+
+  // Probe raster in three phases so that several handles can be captured into
+  // one CUDA graph: prepare (stack, tables, tuning, buffers, positions: may
+  // allocate and synchronise), enqueue (kernels and async device work only, on
+  // `st`), finish (signals to the host).
+  // Per probe: STEMInitialiseWavefunctions (U.cu:2672-2705, L1-normalised),
+  // conventional slices 1..S, and the annular detector read from the last
+  // column spectrum.  Linear in psi, so probes run unnormalised and each
+  // signal is divided by its L1 norm squared at the end.
+  int raster_prepare(const int* px, const int* py, int n, float inner, float outer, int batch) {
+    if (!have_freq_) return fail(MS_ERR_STATE, "frequencies not precalculated");
+    if (!use_fused()) return fail(MS_ERR_UNSUPPORTED, "the enqueued raster runs on the fused passes");
+    if (!px || !py) return fail(MS_ERR_INVALID, "null buffer");
+    if (n < 1) return fail(MS_ERR_INVALID, "need at least one probe position");
+    if (batch < 1 || batch > 1024) return fail(MS_ERR_INVALID, "batch must be 1..1024");
+    if (!(inner >= 0) || !(outer > inner)) return fail(MS_ERR_INVALID, "need 0 <= inner < outer");
+    if (int rc = build_stack(&rs_S_)) return rc;
     if (int rc = ensure_prop_tables(convdz_)) return rc;
     const long long N = (long long)nx_ * ny_;
-    const int B = std::min(batch, n);
-    const int nbr = pw_reduce_blocks(N);
-    MS_TRY(d_bwave_.resize((size_t)B * N));
-    MS_TRY(d_bpos_.resize(2 * (size_t)B));
-    MS_TRY(d_bsig_.resize(2 * (size_t)B));
-    MS_TRY(d_bpart_.resize((size_t)B * nbr));
-    std::vector<int> pos(2 * B);
-    std::vector<double> host(2 * B);
+    rs_n_ = n;
+    rs_B_ = std::min(batch, n);
+    plan_for(rs_B_);
+    MS_TRY(d_bwave_.resize((size_t)rs_B_ * N));
+    MS_TRY(d_bpos_.resize(2 * (size_t)n));
+    MS_TRY(d_bsig_.resize(2 * (size_t)n));
+    MS_TRY(d_bpart_.resize((size_t)rs_B_ * pw_reduce_blocks(N)));
+    std::vector<int> pos(2 * (size_t)n);
+    std::copy(px, px + n, pos.begin());
+    std::copy(py, py + n, pos.begin() + n);
+    MS_TRY(copy_sync(d_bpos_.p, pos.data(), sizeof(int) * 2 * n, cudaMemcpyHostToDevice));
+    const float kin = (inner * 0.001f) / wavel_, kout = (outer * 0.001f) / wavel_;
+    rs_kin2_ = kin * kin;
+    rs_kout2_ = kout * kout;
+    return MS_OK;
+  }
+
+  int raster_enqueue(cudaStream_t st) {
+    const long long N = (long long)nx_ * ny_;
+    const int B = rs_B_, n = rs_n_, S = rs_S_;
     const Grid2 g{nx_, ny_};
     const float apert = (float)((double)aperture_ * 0.001 / (double)wavel_);
-    const float kin = (inner * 0.001f) / wavel_, kout = (outer * 0.001f) / wavel_;
+    const int vr = plan_for(B).row, vc = plan_for(B).col;
+    MS_TRY(cudaMemsetAsync(d_bsig_.p, 0, sizeof(double) * 2 * n, st));
     for (int start = 0; start < n; start += B) {
       const int nb = std::min(B, n - start);
-      for (int b = 0; b < nb; ++b) {
-        pos[b] = px[start + b];
-        pos[B + b] = py[start + b];
-      }
-      MS_TRY(cudaMemcpyAsync(d_bpos_.p, pos.data(), sizeof(int) * 2 * B, cudaMemcpyHostToDevice, stream_));
-      MS_TRY(cudaMemsetAsync(d_bsig_.p, 0, sizeof(double) * B, stream_));
-      MS_TRY(pw_probe_batch(d_bwave_.p, N, nb, d_kx_.p, d_ky_.p, d_bpos_.p, d_bpos_.p + B, apert, ps_, df_, Cs_,
-                            wavel_, g, stream_, &launches));
-      PassBArgs bi = passb_args(d_bwave_.p, d_bwave_.p, 0);
+      MS_TRY(pw_probe_batch(d_bwave_.p, N, nb, d_kx_.p, d_ky_.p, d_bpos_.p + start, d_bpos_.p + n + start, apert,
+                            ps_, df_, Cs_, wavel_, g, st, &launches));
+      PassBArgs bi = passb_args(d_bwave_.p, d_bwave_.p, vc);
       bi.batch_stride_wave = N;
-      MS_TRY(pass_b(bi, B_INV_ONLY, nb));
-      PassAArgs ai = passa_args(d_bwave_.p, d_bwave_.p, 0);
+      MS_TRY(launch_pass_b(bi, vc, B_INV_ONLY, nb, st));
+      PassAArgs ai = passa_args(d_bwave_.p, d_bwave_.p, vr);
       ai.batch_stride_wave = N;
-      MS_TRY(pass_a(ai, A_INV, nb));
+      MS_TRY(launch_pass_a(ai, vr, A_INV, nb, st));
       launches += 2;
-      MS_TRY(pw_sum_abs_batch(d_bwave_.p, N, N, nb, d_bpart_.p, d_bsig_.p + B, stream_, &launches));
+      MS_TRY(pw_sum_abs_batch(d_bwave_.p, N, N, nb, d_bpart_.p, d_bsig_.p + n + start, st, &launches));
       for (int it = 1; it <= S; ++it) {
-        PassAArgs a = passa_args(d_bwave_.p, d_bwave_.p, 0);
+        PassAArgs a = passa_args(d_bwave_.p, d_bwave_.p, vr);
         a.batch_stride_wave = N;
         a.batch_stride_V = 0;
         a.V = d_stack_.p + (size_t)(it - 1) * N;
-        MS_TRY(pass_a(a, it == 1 ? (A_MULT_T | A_FWD) : (A_INV | A_MULT_T | A_FWD), nb));
-        PassBArgs b = passb_args(d_bwave_.p, d_bwave_.p, 0);
+        MS_TRY(launch_pass_a(a, vr, it == 1 ? (A_MULT_T | A_FWD) : (A_INV | A_MULT_T | A_FWD), nb, st));
+        PassBArgs b = passb_args(d_bwave_.p, d_bwave_.p, vc);
         b.batch_stride_wave = N;
         if (it < S) {
-          MS_TRY(pass_b(b, B_PROPAGATE, nb));
+          MS_TRY(launch_pass_b(b, vc, B_PROPAGATE, nb, st));
         } else {
-          b.sig = d_bsig_.p;
-          b.kin2 = kin * kin;
-          b.kout2 = kout * kout;
+          b.sig = d_bsig_.p + start;
+          b.kin2 = rs_kin2_;
+          b.kout2 = rs_kout2_;
           b.scale = 1.0f / (float)N;
-          MS_TRY(pass_b(b, B_DETECT, nb));
+          MS_TRY(launch_pass_b(b, vc, B_DETECT, nb, st));
         }
         launches += 2;
-      }
-      MS_TRY(cudaMemcpyAsync(host.data(), d_bsig_.p, sizeof(double) * 2 * B, cudaMemcpyDeviceToHost, stream_));
-      MS_TRY(cudaStreamSynchronize(stream_));
-      for (int b = 0; b < nb; ++b) {
-        const double l1 = host[B + b];
-        if (!(l1 > 0)) return fail(MS_ERR_NUMERIC, "probe is empty (aperture smaller than one frequency pixel)");
-        signal[start + b] = host[b] / (l1 * l1);
       }
     }
     return MS_OK;
   }
+
+  int raster_finish(double* signal) {
+    const int n = rs_n_;
+    std::vector<double> host(2 * (size_t)n);
+    MS_TRY(copy_sync(host.data(), d_bsig_.p, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; ++i) {
+      const double l1 = host[n + i];
+      if (!(l1 > 0)) return fail(MS_ERR_NUMERIC, "probe is empty (aperture smaller than one frequency pixel)");
+      signal[i] = host[i] / (l1 * l1);
+    }
+    return MS_OK;
+  }
+
+  cudaStream_t stream() const { return stream_; }
+  bool fused() const { return use_fused(); }
+  void set_last_device_ms(float ms) { last_device_ms_ = ms; }
 
   // ---- frozen-phonon series (the GUI's pass loop, MainWindow.xaml.cs:353-402) ----
   // Configurations first_pass .. first_pass + nconf - 1, each displaced as
@@ -1812,6 +1846,8 @@ class Engine {
   DevBuf<float2> d_twx_[3], d_twy_[3], d_px_, d_py_, d_P_;
   int forced_plan_ = -1, ckpt_ = 0;
   float last_device_ms_ = 0.0f;
+  int rs_n_ = 0, rs_B_ = 1, rs_S_ = 0;  // prepared probe raster
+  float rs_kin2_ = 0, rs_kout2_ = 0;
   std::vector<int> hzoff_;  // first sorted atom per z-bin (focal-series atom gradient)
   DevBuf<float2> d_ck_, d_seg_, d_G_, d_U_, d_Phi_;
   DevBuf<float> d_T_, d_dV_, d_img_, d_fpstack_, d_fpdiff_, d_fpsum_, d_fpimg_;
@@ -2186,6 +2222,81 @@ ms_status ms_get_last_device_ms(ms_sim* s, float* out) {
   if (ms_status r = out_check(s, out)) return r;
   return guarded(s, [&](ms::Engine& e) { return e.last_device_ms(out); });
 }
+// Several handles' probe rasters (different specimens and grid sizes, one
+// device) captured into one CUDA graph: one branch per handle on its own
+// stream, forked from and joined into the first handle's stream, launched once.
+ms_status ms_stem_raster_concurrent(ms_sim* const* sims, int nsims, const int* const* px, const int* const* py,
+                                    const int* n, float inner_mrad, float outer_mrad, int batch,
+                                    double* const* signal) {
+  if (!sims || nsims < 1 || !px || !py || !n || !signal) return MS_ERR_INVALID;
+  for (int k = 0; k < nsims; ++k)
+    if (!sims[k] || !sims[k]->e) return MS_ERR_INVALID;
+  return guarded(sims[0], [&](ms::Engine& e0) -> int {
+    for (int k = 0; k < nsims; ++k) {
+      ms::Engine& e = *sims[k]->e;
+      if (e.device() != e0.device()) return e0.fail(MS_ERR_INVALID, "all handles must use the same device");
+      if (!e.fused()) return e0.fail(MS_ERR_UNSUPPORTED, "every handle must run the fused passes");
+      if (!signal[k]) return e0.fail(MS_ERR_INVALID, "null signal buffer");
+      if (int rc = e.raster_prepare(px[k], py[k], n[k], inner_mrad, outer_mrad, batch))
+        return e0.fail(rc, "handle " + std::to_string(k) + ": " + e.err);
+    }
+    cudaStream_t st0 = e0.stream();
+    std::vector<cudaEvent_t> ev(nsims + 2, nullptr);
+    for (auto& x : ev)
+      if (cudaEventCreate(&x) != cudaSuccess) {
+        for (auto& y : ev)
+          if (y) cudaEventDestroy(y);
+        return e0.fail(MS_ERR_CUDA, "cudaEventCreate failed");
+      }
+    auto cleanup = [&]() {
+      for (auto& y : ev) cudaEventDestroy(y);
+    };
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t ce = cudaStreamBeginCapture(st0, cudaStreamCaptureModeThreadLocal);
+    int rc = MS_OK;
+    if (ce == cudaSuccess) {
+      ce = cudaEventRecord(ev[0], st0);
+      for (int k = 1; k < nsims && ce == cudaSuccess; ++k) ce = cudaStreamWaitEvent(sims[k]->e->stream(), ev[0], 0);
+      for (int k = 0; k < nsims && ce == cudaSuccess && rc == MS_OK; ++k) {
+        ms::Engine& e = *sims[k]->e;
+        rc = e.raster_enqueue(e.stream());
+        if (rc != MS_OK) rc = e0.fail(rc, "handle " + std::to_string(k) + ": " + e.err);
+      }
+      for (int k = 1; k < nsims && ce == cudaSuccess; ++k) {
+        ce = cudaEventRecord(ev[k], sims[k]->e->stream());
+        if (ce == cudaSuccess) ce = cudaStreamWaitEvent(st0, ev[k], 0);
+      }
+      const cudaError_t ee = cudaStreamEndCapture(st0, &graph);
+      if (ce == cudaSuccess) ce = ee;
+    }
+    if (ce == cudaSuccess && rc == MS_OK) ce = cudaGraphInstantiate(&exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    // ev[0]: fork, ev[1..nsims-1]: joins, ev[nsims], ev[nsims+1]: timing
+    if (ce == cudaSuccess && rc == MS_OK) {
+      ce = cudaEventRecord(ev[nsims], st0);
+      if (ce == cudaSuccess) ce = cudaGraphLaunch(exec, st0);
+      if (ce == cudaSuccess) ce = cudaEventRecord(ev[nsims + 1], st0);
+    }
+    if (exec) {
+      if (ce == cudaSuccess) ce = cudaStreamSynchronize(st0);
+      cudaGraphExecDestroy(exec);
+    }
+    if (ce == cudaSuccess && rc == MS_OK) {
+      float ms = 0.0f;
+      if (cudaEventElapsedTime(&ms, ev[nsims], ev[nsims + 1]) == cudaSuccess) e0.set_last_device_ms(ms);
+    }
+    cleanup();
+    if (rc != MS_OK) return rc;
+    if (ce != cudaSuccess) return e0.fail(MS_ERR_CUDA, std::string("concurrent raster graph: ") + cudaGetErrorString(ce));
+    for (int k = 0; k < nsims; ++k) {
+      ms::Engine& e = *sims[k]->e;
+      if (int r2 = e.raster_finish(signal[k])) return e0.fail(r2, "handle " + std::to_string(k) + ": " + e.err);
+    }
+    return (int)MS_OK;
+  });
+}
+
 ms_status ms_get_launch_count(ms_sim* s, long long* out) {
   if (ms_status r = out_check(s, out)) return r;
   return guarded(s, [&](ms::Engine& e) {

@@ -373,3 +373,21 @@ class ManagedMultisliceSimulation:
         out = C.c_longlong()
         self._chk(self._L.ms_get_launch_count(self._h, C.byref(out)))
         return out.value
+
+
+def stem_raster_concurrent(sims, positions, inner_mrad: float, outer_mrad: float, batch: int = 16):
+    """Probe rasters of several handles (different specimens and grid sizes) in
+    one CUDA-graph launch; positions[k] = (px, py) for sims[k].  Returns the
+    signals per handle and the device milliseconds of the launch."""
+    k = len(sims)
+    pxs = [np.ascontiguousarray(p[0], np.int32).ravel() for p in positions]
+    pys = [np.ascontiguousarray(p[1], np.int32).ravel() for p in positions]
+    outs = [np.zeros(a.size, np.float64) for a in pxs]
+    hs = (C.c_void_p * k)(*[s._h for s in sims])
+    PX = (C.c_void_p * k)(*[a.ctypes.data for a in pxs])
+    PY = (C.c_void_p * k)(*[a.ctypes.data for a in pys])
+    NN = (C.c_int * k)(*[a.size for a in pxs])
+    OUT = (C.c_void_p * k)(*[o.ctypes.data for o in outs])
+    sims[0]._chk(sims[0]._L.ms_stem_raster_concurrent(hs, k, PX, PY, NN, float(inner_mrad), float(outer_mrad),
+                                                      int(batch), OUT))
+    return outs, sims[0].LastDeviceMs()

@@ -241,6 +241,18 @@ ms_status ms_focal_series(ms_sim* sim, const float* defoci, int nd, const float*
 ms_status ms_focal_series_grad(ms_sim* sim, const float* defoci, int nd, const float* targets, int nslices,
                                double* loss, float* dLdV, double* dLdxy);
 
+/* Several specimens' probe rasters in one CUDA-graph launch (north-star
+ * batching of mixed grid sizes; no reference counterpart): handle k (its own
+ * specimen, grid and potentials; all handles on one device, fused path) runs
+ * the raster of ms_stem_raster over its n[k] positions px[k], py[k] into
+ * signal[k].  The handles' work is captured as concurrent branches of one graph
+ * (one stream each, forked from and joined into sims[0]'s stream) and launched
+ * once; ms_get_last_device_ms(sims[0]) then gives its device time.  Errors are
+ * reported on sims[0]. */
+ms_status ms_stem_raster_concurrent(ms_sim* const* sims, int nsims, const int* const* px, const int* const* py,
+                                    const int* n, float inner_mrad, float outer_mrad, int batch,
+                                    double* const* signal);
+
 /* ---- inspection (parity tests and measurement) ---- */
 /* Microseconds per launch of one fused pass on scratch waves (CUDA events,
  * `reps` back-to-back launches after two warm-up launches): pass 0 = row pass

@@ -347,3 +347,27 @@ def test_rs_potential_and_steps(engine_cls, oracle_mod):
         eng.MultisliceStepRS(it)
         orc.MultisliceStepRS(it)
     assert rel_l2(eng.ExitWave(), orc.Wave()) < TOL
+
+
+# ---------------------------------------------------------------- mixed grids in one graph
+def test_stem_raster_concurrent_mixed_grids(engine_cls, oracle_mod):
+    """Two specimens on 128^2 and 256^2 grids, rastered as concurrent branches of
+    one CUDA graph, give each handle's own raster (and the oracle's signal)."""
+    from cudamultislice_b200 import stem_raster_concurrent
+
+    a, orc_a = make_pair(engine_cls, oracle_mod, sto(2, 3), 128, 0.1, kV=300.0, df=-50.0, Cs=1e4, ap=25.0,
+                         stem=True)
+    b, _ = make_pair(engine_cls, oracle_mod, sto(3, 2), 256, 0.06, kV=300.0, df=0.0, Cs=0.0, ap=25.0, stem=True)
+    pa = (np.array([10, 64, 100, 3, 77], np.int32), np.array([20, 64, 7, 99, 33], np.int32))
+    pb = (np.array([0, 128, 200, 17, 90, 250, 31], np.int32), np.array([5, 128, 60, 240, 90, 1, 140], np.int32))
+    (sa, sb), ms = stem_raster_concurrent([a, b], [pa, pb], 10.0, 40.0, batch=3)
+    ra = a.StemRaster(*pa, 10.0, 40.0, batch=3)
+    rb = b.StemRaster(*pb, 10.0, 40.0, batch=3)
+    assert ms > 0
+    np.testing.assert_allclose(sa, ra, rtol=1e-12)
+    np.testing.assert_allclose(sb, rb, rtol=1e-12)
+    orc_a.STEMInitialiseWavefunctions(int(pa[0][1]), int(pa[1][1]))
+    for i in range(1, orc_a.GetSlices(True) + 1):
+        orc_a.MultisliceStepConventional(i)
+    ref = orc_a.AnnularDetector(10.0, 40.0)
+    assert abs(sa[1] - ref) / ref < 1e-4
