@@ -810,6 +810,58 @@ class Engine {
     return MS_OK;
   }
 
+  // CTF images of the current exit wave at n (defocus, Cs) pairs (the batch
+  // Cs/df sweep the reference's GUI leaves as a stub, BP.cs:131-134): the
+  // wave is transformed once and re-imaged per pair with SimulateImage's
+  // transfer (imagingKernel2, U.cu:1044-1080); Cs = NULL keeps the microscope's.
+  int image_series(const float* df, const float* cs, int n, float* images) {
+    if (!have_waves_) return fail(MS_ERR_STATE, "wavefunctions not initialised");
+    if (!df || !images || n < 1) return fail(MS_ERR_INVALID, "need defoci, an output buffer and n >= 1");
+    for (int i = 0; i < n; ++i)
+      if (!std::isfinite(df[i]) || (cs && !std::isfinite(cs[i]))) return fail(MS_ERR_INVALID, "non-finite defocus or Cs");
+    if (domain_ == 2)
+      if (int rc = ensure_real()) return rc;
+    const Grid2 g{nx_, ny_};
+    const size_t N = (size_t)nx_ * ny_;
+    const float wavel = wavel_, objap = aperture_;
+    const float objap2 = (((objap * 0.001f) / wavel) * ((objap * 0.001f) / wavel));
+    const double beta = (double)(beta_ / 1000);
+    MS_TRY(d_img_.resize(N * n));
+    if (use_fused()) {
+      const float2* src = d_psi_.p;
+      float scale = (float)nx_ / (float)N;  // FFT_rows(psi) = nx X
+      if (domain_ == 0) {
+        MS_TRY(pass_a(passa_args(d_psi_.p, d_t1_.p, 0), A_FWD, 1));
+        ++launches;
+        src = d_t1_.p;
+        scale = 1.0f / (float)N;
+      }
+      for (int i = 0; i < n; ++i) {
+        PassBArgs b = passb_args(src, d_t2_.p, 0);
+        b.ctf = CtfParams{(double)wavel, cs ? (double)cs[i] : (double)Cs_, (double)df[i], (double)A2_, (double)phi2_,
+                          0.0, 0.0, beta, (double)delta_, objap2};
+        b.scale = scale;
+        MS_TRY(pass_b(b, B_CTF, 1));
+        PassAArgs a = passa_args(d_t2_.p, nullptr, 0);
+        a.out_f = d_img_.p + (size_t)i * N;
+        MS_TRY(pass_a(a, A_INV | A_INTENSITY, 1));
+        launches += 2;
+      }
+    } else {
+      MS_TRY_FFT(cufftExecC2C(plan_, d_psi_.p, d_t1_.p, CUFFT_FORWARD));
+      for (int i = 0; i < n; ++i) {
+        MS_TRY(cudaMemcpyAsync(d_t2_.p, d_t1_.p, sizeof(float2) * N, cudaMemcpyDeviceToDevice, stream_));
+        MS_TRY(pw_ctf(d_t2_.p, d_kx_.p, d_ky_.p, wavel, cs ? cs[i] : Cs_, df[i], A2_, phi2_, beta, delta_, objap2,
+                      1.0f / (float)N, g, stream_, &launches));
+        MS_TRY_FFT(cufftExecC2C(plan_, d_t2_.p, d_t2_.p, CUFFT_INVERSE));
+        MS_TRY(pw_abs2(d_t2_.p, d_img_.p + (size_t)i * N, 1.0f, g, stream_, &launches));
+      }
+    }
+    MS_TRY(cudaMemcpyAsync(images, d_img_.p, sizeof(float) * N * n, cudaMemcpyDeviceToHost, stream_));
+    MS_TRY(cudaStreamSynchronize(stream_));
+    return MS_OK;
+  }
+
   int im_value(int x, int y, float* out) {
     if (!have_image_) return fail(MS_ERR_STATE, "image not simulated (ms_simulate_image)");
     if (x < 0 || y < 0 || x >= nx_ || y >= ny_) return fail(MS_ERR_INVALID, "pixel index out of range");
@@ -2211,6 +2263,9 @@ ms_status ms_focal_series_grad(ms_sim* s, const float* defoci, int nd, const flo
 ms_status ms_time_pass(ms_sim* s, int pass, int op, int variant, int batch, int reps, float* us) {
   if (ms_status r = out_check(s, us)) return r;
   return guarded(s, [&](ms::Engine& e) { return e.time_pass(pass, op, variant, batch, reps, us); });
+}
+ms_status ms_simulate_image_series(ms_sim* s, const float* defoci, const float* cs, int n, float* images) {
+  return guarded(s, [&](ms::Engine& e) { return e.image_series(defoci, cs, n, images); });
 }
 ms_status ms_frozen_phonon(ms_sim* s, uint64_t seed, uint32_t first_pass, int nconfigs, float sigma, int batch,
                            float* diffraction, float* image) {

@@ -275,6 +275,17 @@ class ManagedMultisliceSimulation:
                                          float(outer_mrad), int(batch), _ptr(out)))
         return out
 
+    def SimulateImageSeries(self, defoci, cs=None) -> np.ndarray:
+        """CTF images of the current exit wave at each defocus (and Cs), (n, ny, nx)."""
+        d = np.ascontiguousarray(defoci, np.float32).ravel()
+        c = None if cs is None else np.ascontiguousarray(cs, np.float32).ravel()
+        if c is not None and c.size != d.size:
+            raise ValueError("defoci and cs must have the same length")
+        out = np.zeros((d.size, self.ny, self.nx), np.float32)
+        self._chk(self._L.ms_simulate_image_series(self._h, _ptr(d), None if c is None else _ptr(c), d.size,
+                                                   _ptr(out)))
+        return out
+
     # ---- frozen phonons ----
     def FrozenPhonon(self, seed: int, first_pass: int, nconfigs: int, sigma: float, batch: int = 16,
                      diffraction: bool = True, image: bool = True):

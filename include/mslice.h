@@ -209,6 +209,13 @@ ms_status ms_annular_detector(ms_sim* sim, float inner_mrad, float outer_mrad, d
 ms_status ms_stem_raster(ms_sim* sim, const int* px, const int* py, int n, float inner_mrad,
                          float outer_mrad, int batch, double* signal);
 
+/* Batch Cs/defocus sweep of the current exit wave (new; the reference's GUI
+ * leaves it as a stub, CUDA Simulation GUI/BatchProcessing.xaml.cs:131-134): image i
+ * of images (n * nx * ny floats) is the ms_simulate_image CTF image at defocus
+ * defoci[i] (A) and spherical aberration cs[i] (A; cs = NULL keeps the value
+ * of ms_apply_microscope_parameters).  The slices are not re-run. */
+ms_status ms_simulate_image_series(ms_sim* sim, const float* defoci, const float* cs, int n, float* images);
+
 /* Frozen-phonon series (new; the reference's GUI loops UploadBinnedAtomsTDS,
  * the slices and AddTDSWaves over passes, CUDA Simulation GUI/MainWindow.xaml.cs:353-402):
  * configurations pass = first_pass .. first_pass + nconfigs - 1, each displaced as

@@ -371,3 +371,23 @@ def test_stem_raster_concurrent_mixed_grids(engine_cls, oracle_mod):
         orc_a.MultisliceStepConventional(i)
     ref = orc_a.AnnularDetector(10.0, 40.0)
     assert abs(sa[1] - ref) / ref < 1e-4
+
+
+# ---------------------------------------------------------------- Cs / defocus sweep
+@pytest.mark.parametrize("path", [0, 1])
+def test_image_series_sweep(engine_cls, oracle_mod, path):
+    """Re-imaging one exit wave at several (defocus, Cs) pairs equals
+    SimulateImage after ApplyMicroscopeParameters with each pair."""
+    eng, orc = make_pair(engine_cls, oracle_mod, sto(2, 4), 128, 0.1, path=path)
+    eng.RunConventional()
+    psi = orc.run_conventional()
+    df = np.array([-800.0, -100.0, 0.0, 450.0], np.float32)
+    cs = np.array([1e7, 5e6, 0.0, 1.2e7], np.float32)
+    imgs = eng.SimulateImageSeries(df, cs)
+    for i in range(df.size):
+        orc.ApplyMicroscopeParameters(200.0, float(df[i]), 0.0, 0.0, float(cs[i]), 0.1, 30.0, 20.0)
+        assert rel_l2(imgs[i], orc.SimulateImage()) < TOL, i
+    # without Cs: the microscope's value
+    imgs2 = eng.SimulateImageSeries(df[:1])
+    orc.ApplyMicroscopeParameters(200.0, float(df[0]), 0.0, 0.0, 1e7, 0.1, 30.0, 20.0)
+    assert rel_l2(imgs2[0], orc.SimulateImage()) < TOL
