@@ -756,8 +756,11 @@ class Engine {
     return MS_OK;
   }
 
-  // SimulateImage U.cu:2311-2343 (deterministic part).
-  int simulate_image() {
+  // SimulateImage U.cu:2311-2343: the CTF image, and with a detector model
+  // (ms_set_detector) the noisy chain of U.cu:2345-2437.
+  int simulate_image(float dose = 0.0f) {
+    if (det_n_ > 0 && !(dose >= 0 && std::isfinite(dose))) return fail(MS_ERR_INVALID, "bad dose per pixel");
+    image_noisy_ = false;
     if (!have_waves_) return fail(MS_ERR_STATE, "wavefunctions not initialised");
     if (!have_image_buf_) alloc_host_image();
     if (domain_ == 2)
@@ -796,6 +799,9 @@ class Engine {
                     stream_, &launches));
       MS_TRY_FFT(cufftExecC2C(plan_, d_t1_.p, d_t2_.p, CUFFT_INVERSE));
       MS_TRY(pw_abs2(d_t2_.p, d_f_.p, 1.0f, g, stream_, &launches));
+    }
+    if (det_n_ > 0) {
+      if (int rc = detector_chain(dose)) return rc;
     }
     MS_TRY(cudaMemcpyAsync(image_.data(), d_f_.p, sizeof(float) * N, cudaMemcpyDeviceToHost, stream_));
     MS_TRY(cudaStreamSynchronize(stream_));
@@ -865,7 +871,69 @@ class Engine {
   int im_value(int x, int y, float* out) {
     if (!have_image_) return fail(MS_ERR_STATE, "image not simulated (ms_simulate_image)");
     if (x < 0 || y < 0 || x >= nx_ || y >= ny_) return fail(MS_ERR_INVALID, "pixel index out of range");
-    *out = image_[(size_t)y * nx_ + x];
+    const size_t p = (size_t)y * nx_ + x;
+    if (det_n_ > 0 && image_noisy_) {
+      // GetImValue (U.cu:2497-2512): readout noise offset + sigma z on the
+      // detector image; z seeded per (pixel, image), so a read repeats
+      const uint32_t ctr[4] = {(uint32_t)p, det_serial_ - 1, 0x4EADu, 0u};
+      const uint32_t key[2] = {(uint32_t)det_seed_, (uint32_t)(det_seed_ >> 32)};
+      uint32_t r[4];
+      philox4x32_10(ctr, key, r);
+      *out = (float)(det_ro_off_ + clipped_normal(r[0], r[1]) * det_ro_sig_ + image_[p]);
+      return MS_OK;
+    }
+    *out = image_[p];
+    return MS_OK;
+  }
+
+  // Detector model of the noisy image chain: radial DQE and NTF tables
+  // (entries per binned frequency pixel), camera counts per electron, readout
+  // noise, seed.  n = 0 removes it.
+  int set_detector(const float* dqe, const float* ntf, int n, int binning, float conversion, float ro_off, float ro_sig,
+                   uint64_t seed) {
+    if (n == 0) {
+      det_n_ = 0;
+      return MS_OK;
+    }
+    if (n < 1 || n > (1 << 20) || !dqe || !ntf || binning < 1) return fail(MS_ERR_INVALID, "need tables of n >= 1 entries and binning >= 1");
+    if (!std::isfinite(conversion) || !std::isfinite(ro_off) || !std::isfinite(ro_sig)) return fail(MS_ERR_INVALID, "non-finite detector constant");
+    for (int i = 0; i < n; ++i)
+      if (!(dqe[i] >= 0) || !std::isfinite(ntf[i])) return fail(MS_ERR_INVALID, "bad DQE/NTF table entry");
+    MS_TRY(d_dqe_.resize(n));
+    MS_TRY(d_ntf_.resize(n));
+    MS_TRY(copy_sync(d_dqe_.p, dqe, sizeof(float) * n, cudaMemcpyHostToDevice));
+    MS_TRY(copy_sync(d_ntf_.p, ntf, sizeof(float) * n, cudaMemcpyHostToDevice));
+    det_n_ = n;
+    det_bin_ = binning;
+    det_conv_ = conversion;
+    det_ro_off_ = ro_off;
+    det_ro_sig_ = ro_sig;
+    det_seed_ = seed;
+    det_serial_ = 0;
+    return MS_OK;
+  }
+
+  // The noisy chain of SimulateImage (U.cu:2345-2437) on the CTF intensity I
+  // in d_f_ (FFTs by cuFFT, normalisations folded into the filters):
+  //   a = |IFFT(sqrt(DQE) FFT(I)) / N|, counts = round(dose a + sqrt(dose a) z),
+  //   image = |IFFT(NTF FFT(counts)) conversion^2 / N|.
+  int detector_chain(float dose) {
+    const Grid2 g{nx_, ny_};
+    const float invN = 1.0f / ((float)nx_ * (float)ny_);
+    if (!have_plan_) return fail(MS_ERR_STATE, "FFT plan not created");
+    MS_TRY(pw_real_to_complex(d_f_.p, d_t1_.p, g, stream_, &launches));
+    MS_TRY_FFT(cufftExecC2C(plan_, d_t1_.p, d_t2_.p, CUFFT_FORWARD));
+    MS_TRY(pw_detector_filter(d_t2_.p, d_dqe_.p, det_n_, det_bin_, true, invN, g, stream_, &launches));
+    MS_TRY_FFT(cufftExecC2C(plan_, d_t2_.p, d_t1_.p, CUFFT_INVERSE));
+    MS_TRY(pw_shot_noise(d_t1_.p, d_f_.p, dose, det_seed_, det_serial_, g, stream_, &launches));
+    MS_TRY(pw_real_to_complex(d_f_.p, d_t1_.p, g, stream_, &launches));
+    MS_TRY_FFT(cufftExecC2C(plan_, d_t1_.p, d_t2_.p, CUFFT_FORWARD));
+    MS_TRY(pw_detector_filter(d_t2_.p, d_ntf_.p, det_n_, det_bin_, false, det_conv_ * det_conv_ * invN, g, stream_,
+                              &launches));
+    MS_TRY_FFT(cufftExecC2C(plan_, d_t2_.p, d_t1_.p, CUFFT_INVERSE));
+    MS_TRY(pw_abs(d_t1_.p, d_f_.p, g, stream_, &launches));
+    ++det_serial_;
+    image_noisy_ = true;
     return MS_OK;
   }
 
@@ -1898,6 +1966,13 @@ class Engine {
   DevBuf<float2> d_twx_[3], d_twy_[3], d_px_, d_py_, d_P_;
   int forced_plan_ = -1, ckpt_ = 0;
   float last_device_ms_ = 0.0f;
+  // detector model of the noisy image chain
+  DevBuf<float> d_dqe_, d_ntf_;
+  int det_n_ = 0, det_bin_ = 4;
+  float det_conv_ = 8.0f, det_ro_off_ = 4.0f, det_ro_sig_ = 1.33f;
+  uint64_t det_seed_ = 0;
+  uint32_t det_serial_ = 0;
+  bool image_noisy_ = false;
   int rs_n_ = 0, rs_B_ = 1, rs_S_ = 0;  // prepared probe raster
   float rs_kin2_ = 0, rs_kout2_ = 0;
   std::vector<int> hzoff_;  // first sorted atom per z-bin (focal-series atom gradient)
@@ -2164,7 +2239,7 @@ ms_status ms_alloc_host_image(ms_sim* s) {
 }
 ms_status ms_simulate_image(ms_sim* s, float dose) {
   (void)dose;
-  return guarded(s, [&](ms::Engine& e) { return e.simulate_image(); });
+  return guarded(s, [&](ms::Engine& e) { return e.simulate_image(dose); });
 }
 ms_status ms_get_im_value(ms_sim* s, int x, int y, float* out) {
   if (ms_status r = out_check(s, out)) return r;
@@ -2263,6 +2338,12 @@ ms_status ms_focal_series_grad(ms_sim* s, const float* defoci, int nd, const flo
 ms_status ms_time_pass(ms_sim* s, int pass, int op, int variant, int batch, int reps, float* us) {
   if (ms_status r = out_check(s, us)) return r;
   return guarded(s, [&](ms::Engine& e) { return e.time_pass(pass, op, variant, batch, reps, us); });
+}
+ms_status ms_set_detector(ms_sim* s, const float* dqe, const float* ntf, int n, int binning, float conversion,
+                          float readout_offset, float readout_sigma, uint64_t seed) {
+  return guarded(s, [&](ms::Engine& e) {
+    return e.set_detector(dqe, ntf, n, binning, conversion, readout_offset, readout_sigma, seed);
+  });
 }
 ms_status ms_simulate_image_series(ms_sim* s, const float* defoci, const float* cs, int n, float* images) {
   return guarded(s, [&](ms::Engine& e) { return e.image_series(defoci, cs, n, images); });

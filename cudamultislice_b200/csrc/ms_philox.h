@@ -1,12 +1,19 @@
 // ms_philox.h -- Philox4x32-10 counter-based generator (J. Salmon, M. Moraes,
 // R. Dror, D. Shaw, "Parallel random numbers: as easy as 1, 2, 3", SC'11),
-// used for reproducible thermal (frozen-phonon) displacements.
+// used for reproducible thermal (frozen-phonon) displacements and detector noise.
 #pragma once
+#include <math.h>
 #include <stdint.h>
+
+#ifdef __CUDACC__
+#define MS_PHILOX_HD __host__ __device__ inline
+#else
+#define MS_PHILOX_HD inline
+#endif
 
 namespace ms {
 
-inline void philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+MS_PHILOX_HD void philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
   const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;  // round multipliers
   const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;  // Weyl key increments
   uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3], k0 = key[0], k1 = key[1];
@@ -27,6 +34,17 @@ inline void philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t
   out[1] = c1;
   out[2] = c2;
   out[3] = c3;
+}
+
+// Standard normal from two 32-bit words by the Box-Muller form of the
+// reference's noise (U.cu:2389-2397): u = r * 2^-32 in [0, 1),
+// z = sqrt(-2 log(FLT_MIN + u1)) sin(6.2831852 u2) in FP64, clipped to [-3, 3].
+MS_PHILOX_HD double clipped_normal(uint32_t r1, uint32_t r2) {
+  const double u1 = (double)r1 * 2.3283064365386963e-10, u2 = (double)r2 * 2.3283064365386963e-10;
+  double z = sqrt(-2.0 * log(1.17549435e-38 + u1)) * sin((double)(2.0f * 3.1415926f) * u2);
+  if (z <= -3.0) z = -3.0;
+  if (z >= 3.0) z = 3.0;
+  return z;
 }
 
 }  // namespace ms

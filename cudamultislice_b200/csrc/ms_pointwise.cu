@@ -4,6 +4,7 @@
 #include <cmath>
 
 #include "ms_ctf.cuh"
+#include "ms_philox.h"
 #include "ms_pointwise.cuh"
 
 namespace ms {
@@ -192,6 +193,41 @@ __global__ void k_rs_term(const float2* w, float2* out, const float* V, float pr
   out[i] = make_float2(c.x - pre * (ly + v * c.y), c.y + pre * (lx + v * c.x));
 }
 
+// Detector transfer of the noisy image chain (DQEFunc/DQEKernel/NTFKernel,
+// U.cu:1120-1186): the table entry at floor(sqrtf(dx^2 + dy^2) / binning), dx,
+// dy the frequency-index distances to the nearest corner, 0.0001 beyond the
+// table; the square root of it for the DQE stage.  `scale` carries the FFT
+// normalisations of both transforms around the filter.
+__global__ void k_detector_filter(float2* F, const float* tab, int n, int binning, int use_sqrt, float scale, Grid2 g) {
+  PW_INDEX
+  const int xd = x - (x < g.nx / 2 ? 0 : g.nx), yd = y - (y < g.ny / 2 ? 0 : g.ny);
+  const float rad = sqrtf((float)(xd * xd + yd * yd)) / binning;
+  const int r2 = (int)floorf(rad);
+  float v = r2 <= n - 1 ? tab[r2] : 0.0001f;
+  if (use_sqrt) v = sqrtf(v);
+  F[i] = cscale(cscale(F[i], v), scale);
+}
+
+// Shot noise of the chain (U.cu:2383-2409): counts = round(dose a + sqrt(|dose a|) z)
+// with a = |F| and z the clipped normal of Philox4x32-10 at counter
+// (pixel, serial, 0x5407, 0) under key (seed lo, seed hi).
+__global__ void k_shot_noise(const float2* F, float* counts, float dose, uint32_t k0, uint32_t k1, uint32_t serial,
+                             Grid2 g) {
+  PW_INDEX
+  const float a = sqrtf(F[i].x * F[i].x + F[i].y * F[i].y);
+  const uint32_t ctr[4] = {(uint32_t)i, serial, 0x5407u, 0u}, key[2] = {k0, k1};
+  uint32_t r[4];
+  philox4x32_10(ctr, key, r);
+  const double z = clipped_normal(r[0], r[1]);
+  const float na = dose * a;
+  counts[i] = (float)round((double)na + (double)sqrtf(fabsf(na)) * z);
+}
+
+__global__ void k_abs(const float2* a, float* out, Grid2 g) {
+  PW_INDEX
+  out[i] = sqrtf(a[i].x * a[i].x + a[i].y * a[i].y);
+}
+
 // acc += scale * sum_b in[b * stride + i] (batched images into one sum)
 __global__ void k_add_batch(const float* in, long long stride, int nb, float* acc, float scale, Grid2 g) {
   PW_INDEX
@@ -345,6 +381,17 @@ cudaError_t pw_abs2(const float2* a, float* out, float scale, Grid2 g, cudaStrea
 cudaError_t pw_add_batch(const float* in, long long stride, int nb, float* acc, float scale, Grid2 g, cudaStream_t s,
                          long long* count) {
   PW_LAUNCH(k_add_batch, in, stride, nb, acc, scale, g);
+}
+cudaError_t pw_detector_filter(float2* F, const float* tab, int n, int binning, bool use_sqrt, float scale, Grid2 g,
+                               cudaStream_t s, long long* count) {
+  PW_LAUNCH(k_detector_filter, F, tab, n, binning, use_sqrt ? 1 : 0, scale, g);
+}
+cudaError_t pw_shot_noise(const float2* F, float* counts, float dose, uint64_t seed, uint32_t serial, Grid2 g,
+                          cudaStream_t s, long long* count) {
+  PW_LAUNCH(k_shot_noise, F, counts, dose, (uint32_t)seed, (uint32_t)(seed >> 32), serial, g);
+}
+cudaError_t pw_abs(const float2* a, float* out, Grid2 g, cudaStream_t s, long long* count) {
+  PW_LAUNCH(k_abs, a, out, g);
 }
 cudaError_t pw_rs_term(const float2* w, float2* out, const float* V, float pre, float inv_ps2, int m, Grid2 g,
                        cudaStream_t s, long long* count) {

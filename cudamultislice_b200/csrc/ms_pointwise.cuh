@@ -2,6 +2,7 @@
 // operation) slice path, finite differences, probe generation, read-out.
 #pragma once
 #include <cuda_runtime.h>
+#include <stdint.h>
 #include "ms_common.cuh"
 
 namespace ms {
@@ -31,6 +32,12 @@ cudaError_t pw_real_to_complex(const float* in, float2* out, Grid2 g, cudaStream
 cudaError_t pw_centre_abs_acc(const float2* F, float* acc, float scale, Grid2 g, cudaStream_t s, long long* count);
 cudaError_t pw_centre(const float2* F, float2* out, Grid2 g, cudaStream_t s, long long* count);
 cudaError_t pw_abs2(const float2* a, float* out, float scale, Grid2 g, cudaStream_t s, long long* count);
+// Noisy image chain (see .cu): radial detector transfer, seeded shot noise, |.|.
+cudaError_t pw_detector_filter(float2* F, const float* tab, int n, int binning, bool use_sqrt, float scale, Grid2 g,
+                               cudaStream_t s, long long* count);
+cudaError_t pw_shot_noise(const float2* F, float* counts, float dose, uint64_t seed, uint32_t serial, Grid2 g,
+                          cudaStream_t s, long long* count);
+cudaError_t pw_abs(const float2* a, float* out, Grid2 g, cudaStream_t s, long long* count);
 // Term m of the real-space (RS) series, as written in the reference (see .cu).
 cudaError_t pw_rs_term(const float2* w, float2* out, const float* V, float pre, float inv_ps2, int m, Grid2 g,
                        cudaStream_t s, long long* count);

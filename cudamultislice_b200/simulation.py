@@ -275,6 +275,21 @@ class ManagedMultisliceSimulation:
                                          float(outer_mrad), int(batch), _ptr(out)))
         return out
 
+    def SetDetector(self, dqe, ntf, binning: int = 4, conversion: float = 8.0, readout_offset: float = 4.0,
+                    readout_sigma: float = 1.33, seed: int = 0x5EED2026):
+        """Detector model of SimulateImage's noisy chain (radial DQE/NTF tables);
+        dqe=None removes it.  The defaults are the reference's constants."""
+        if dqe is None:
+            self._chk(self._L.ms_set_detector(self._h, None, None, 0, int(binning), float(conversion),
+                                              float(readout_offset), float(readout_sigma), int(seed)))
+            return
+        d = np.ascontiguousarray(dqe, np.float32).ravel()
+        t = np.ascontiguousarray(ntf, np.float32).ravel()
+        if d.size != t.size:
+            raise ValueError("DQE and NTF tables must have the same length")
+        self._chk(self._L.ms_set_detector(self._h, _ptr(d), _ptr(t), d.size, int(binning), float(conversion),
+                                          float(readout_offset), float(readout_sigma), int(seed)))
+
     def SimulateImageSeries(self, defoci, cs=None) -> np.ndarray:
         """CTF images of the current exit wave at each defocus (and Cs), (n, ny, nx)."""
         d = np.ascontiguousarray(defoci, np.float32).ravel()

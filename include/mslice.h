@@ -169,14 +169,27 @@ ms_status ms_get_tds_min(ms_sim* sim, float* out);
 ms_status ms_get_tds_max(ms_sim* sim, float* out);
 ms_status ms_get_tds_val(ms_sim* sim, int x, int y, float* out);
 
-/* AllocHostImage U.cu:2306-2309 / SimulateImage U.cu:2311-2343: the
- * deterministic CTF image |IFFT(CTF * FFT(psi))|^2 (imagingKernel2
- * U.cu:1044-1080).  The detector chain after it (U.cu:2345-2494: DQE/NTF,
- * unseeded shot and readout noise) is not provided; `dose` is accepted and
- * unused.  GetImValue (U.cu:2497-2512) returns the deterministic intensity. */
+/* AllocHostImage U.cu:2306-2309 / SimulateImage U.cu:2311-2343: the CTF image
+ * |IFFT(CTF * FFT(psi))|^2 (imagingKernel2 U.cu:1044-1080).  Without a detector
+ * model (the default) that deterministic image is the result and `dose` is
+ * unused.  With one (ms_set_detector) the detector chain of U.cu:2345-2437
+ * follows: the DQE transfer (sqrt(DQE) on the image spectrum), |.|, shot noise
+ * counts = round(dose a + sqrt(dose a) z) with `dose` electrons per pixel, the
+ * NTF transfer times conversion^2, |.|; GetImValue (U.cu:2497-2512) then adds
+ * readout noise offset + sigma z.  The reference draws z from unseeded rand();
+ * here z is seeded Philox4x32-10 (per pixel and per simulated image), clipped
+ * to +-3 as the reference does. */
 ms_status ms_alloc_host_image(ms_sim* sim);
 ms_status ms_simulate_image(ms_sim* sim, float dose);
 ms_status ms_get_im_value(ms_sim* sim, int x, int y, float* out);
+/* Detector model for ms_simulate_image (new; the reference compiles fixed K2
+ * camera tables in, MTF.h): dqe[n], ntf[n] radial tables indexed by
+ * floor(|frequency-pixel distance to the nearest corner| / binning), 0.0001
+ * beyond the table (DQEFunc U.cu:1120-1132; the reference uses n = 725,
+ * binning 4, conversion 8 counts per electron, readout noise 4 + 1.33 z);
+ * seed for the shot and readout noise.  n = 0 removes the model. */
+ms_status ms_set_detector(ms_sim* sim, const float* dqe, const float* ntf, int n, int binning, float conversion,
+                          float readout_offset, float readout_sigma, uint64_t seed);
 ms_status ms_get_im_min(ms_sim* sim, float* out);
 ms_status ms_get_im_max(ms_sim* sim, float* out);
 /* GetImageContrast (ManagedMultislice.cpp:207-210; computed at U.cu:2453-2491):

@@ -1296,3 +1296,60 @@ extern "C" int or_set_value_offset(or_sim* s, int i, double dx, double dy) {
     s->valdy[i] = dy;
     return 0;
 }
+
+/* ======================================================================
+ * Detector chain of SimulateImage (U.cu:2345-2437) on an FP64 CTF intensity
+ * I (N doubles): F = FFT(I)/sqrt N * sqrt(DQE(r)), a = |IFFT(F)/sqrt N|,
+ * counts = round(dose a + sqrt(|dose a|) z), G = FFT(counts)/sqrt N * NTF(r),
+ * out = |IFFT(G)/sqrt N| * conversion^2.  r: the table index
+ * floor(sqrtf(dx^2 + dy^2) / binning) in FP32 (DQEFunc U.cu:1120-1132),
+ * 0.0001 beyond the table; z: the clipped normal of Philox4x32-10 at counter
+ * (pixel, serial, 0x5407, 0), key (seed lo, seed hi), Box-Muller as the
+ * reference (U.cu:2389-2397) with u = r * 2^-32.
+ * ==================================================================== */
+extern "C" double or_clipped_normal(uint32_t r1, uint32_t r2) {
+    const double u1 = (double)r1 * 2.3283064365386963e-10, u2 = (double)r2 * 2.3283064365386963e-10;
+    double z = std::sqrt(-2.0 * std::log(1.17549435e-38 + u1)) * std::sin((double)(2.0f * 3.1415926f) * u2);
+    if (z <= -3.0) z = -3.0;
+    if (z >= 3.0) z = 3.0;
+    return z;
+}
+
+static double detector_table(int x, int y, int nx, int ny, const float* tab, int n, int binning) {
+    const int xd = x - (x < nx / 2 ? 0 : nx), yd = y - (y < ny / 2 ? 0 : ny);
+    const float rad = std::sqrt((float)(xd * xd + yd * yd)) / binning;
+    const int r2 = (int)std::floor(rad);
+    return r2 <= n - 1 ? (double)tab[r2] : (double)0.0001f;
+}
+
+extern "C" int or_detector_chain(or_sim* s, const double* I, float dose, uint32_t serial, const float* dqe,
+                                 const float* ntf, int n, int binning, float conversion, uint64_t seed, double* out) {
+    const int nx = s->nx, ny = s->ny;
+    const size_t N = (size_t)nx * ny;
+    const double isN = 1.0 / std::sqrt((double)N);
+    std::vector<cd> a(N);
+    for (size_t i = 0; i < N; ++i) a[i] = cd(I[i], 0.0);
+    fft2d(a.data(), nx, ny, -1);
+    for (int y = 0; y < ny; ++y)
+        for (int x = 0; x < nx; ++x)
+            a[(size_t)y * nx + x] *= isN * std::sqrt(detector_table(x, y, nx, ny, dqe, n, binning));
+    fft2d(a.data(), nx, ny, +1);
+    const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    for (size_t i = 0; i < N; ++i) {
+        const double amp = std::abs(a[i] * isN);
+        const uint32_t ctr[4] = {(uint32_t)i, serial, 0x5407u, 0u};
+        uint32_t r[4];
+        or_philox4x32_10(ctr, key, r);
+        const double z = or_clipped_normal(r[0], r[1]);
+        const double na = (double)dose * amp;
+        a[i] = cd(std::round(na + std::sqrt(std::fabs(na)) * z), 0.0);
+    }
+    fft2d(a.data(), nx, ny, -1);
+    for (int y = 0; y < ny; ++y)
+        for (int x = 0; x < nx; ++x)
+            a[(size_t)y * nx + x] *= isN * detector_table(x, y, nx, ny, ntf, n, binning);
+    fft2d(a.data(), nx, ny, +1);
+    const double c2 = (double)conversion * (double)conversion;
+    for (size_t i = 0; i < N; ++i) out[i] = std::abs(a[i]) * isN * c2;
+    return 0;
+}

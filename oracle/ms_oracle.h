@@ -109,6 +109,11 @@ int or_focal_forward(or_sim*, const float* defoci, int nd, const double* targets
 /* FP64 adjoint: dLdV (S*N) and dLdxy (2 per atom, input order, box fixed). */
 int or_focal_grad(or_sim*, const float* defoci, int nd, const double* targets, int S, double* loss,
                   double* dLdV, double* dLdxy);
+/* Detector chain of SimulateImage (U.cu:2345-2437) on an FP64 CTF intensity I. */
+int or_detector_chain(or_sim*, const double* I, float dose, uint32_t serial, const float* dqe, const float* ntf,
+                      int n, int binning, float conversion, uint64_t seed, double* out);
+/* The clipped standard normal of the noise (Box-Muller as U.cu:2389-2397). */
+double or_clipped_normal(uint32_t r1, uint32_t r2);
 /* Test hook: value-only position offset of atom i (decisions unchanged). */
 int or_set_value_offset(or_sim*, int i, double dx, double dy);
 

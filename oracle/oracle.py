@@ -92,6 +92,8 @@ def lib():
         "or_focal_forward": (_i, [_p, _p, _i, _p, _p, _i, _p, _p]),
         "or_focal_grad": (_i, [_p, _p, _i, _p, _i, _p, _p, _p]),
         "or_set_value_offset": (_i, [_p, _i, _d, _d]),
+        "or_detector_chain": (_i, [_p, _p, _f, C.c_uint32, _p, _p, _i, _i, _f, C.c_uint64, _p]),
+        "or_clipped_normal": (_d, [C.c_uint32, C.c_uint32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -377,5 +379,18 @@ class OracleSimulation:
                                         _ptr(gxy) if want_xy else None))
         return loss.value, gV, gxy
 
+    def DetectorChain(self, I, dose: float, serial: int, dqe, ntf, binning: int, conversion: float, seed: int):
+        I = np.ascontiguousarray(I, np.float64)
+        d = np.ascontiguousarray(dqe, np.float32)
+        t = np.ascontiguousarray(ntf, np.float32)
+        out = np.zeros_like(I)
+        self._chk(self._L.or_detector_chain(self._h, _ptr(I), float(dose), int(serial), _ptr(d), _ptr(t), d.size,
+                                            int(binning), float(conversion), int(seed), _ptr(out)))
+        return out
+
     def SetValueOffset(self, i: int, dx: float, dy: float):
         self._chk(self._L.or_set_value_offset(self._h, int(i), float(dx), float(dy)))
+
+
+def clipped_normal(r1: int, r2: int) -> float:
+    return lib().or_clipped_normal(int(r1), int(r2))

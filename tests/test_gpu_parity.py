@@ -391,3 +391,37 @@ def test_image_series_sweep(engine_cls, oracle_mod, path):
     imgs2 = eng.SimulateImageSeries(df[:1])
     orc.ApplyMicroscopeParameters(200.0, float(df[0]), 0.0, 0.0, 1e7, 0.1, 30.0, 20.0)
     assert rel_l2(imgs2[0], orc.SimulateImage()) < TOL
+
+
+# ---------------------------------------------------------------- detector noise chain
+def test_detector_noise_chain(engine_cls, oracle_mod):
+    """SimulateImage's detector chain (DQE, seeded shot noise, NTF, conversion)
+    and GetImValue's readout noise vs the oracle fed the same Philox draws.
+    Integer rounding of the counts may flip by one count where FP32 and FP64
+    land on opposite sides of a half; at 5000 electrons per pixel that stays
+    below 1e-4 of the image norm."""
+    eng, orc = make_pair(engine_cls, oracle_mod, sto(2, 4), 128, 0.1)
+    eng.RunConventional()
+    orc.run_conventional()
+    r = np.arange(64)
+    dqe = (0.7 * np.exp(-r / 30.0) + 0.05).astype(np.float32)
+    ntf = (0.9 * np.exp(-r / 40.0) + 0.1).astype(np.float32)
+    seed, dose = 0x1234ABCD5678, 5000.0
+    eng.SetDetector(dqe, ntf, binning=2, conversion=8.0, seed=seed)
+    I = orc.SimulateImage()
+    for serial in (0, 1):
+        eng.SimulateImage(dose)
+        img = eng.Image()
+        ref = orc.DetectorChain(I, dose, serial, dqe, ntf, 2, 8.0, seed)
+        assert rel_l2(img, ref) < 1e-4, (serial, rel_l2(img, ref))
+        if serial == 0:
+            first = img
+    assert rel_l2(img, first) > 1e-3  # the next image draws new noise
+    x, y = 17, 40
+    w = oracle_mod.philox([y * 128 + x, 1, 0x4EAD, 0], [seed & 0xFFFFFFFF, seed >> 32])
+    z = oracle_mod.clipped_normal(int(w[0]), int(w[1]))
+    v = eng.GetImValue(x, y)
+    assert abs(v - (4.0 + 1.33 * z + img[y, x])) <= 1e-5 * abs(v)
+    eng.SetDetector(None, None)
+    eng.SimulateImage(dose)
+    assert rel_l2(eng.Image(), I) < TOL
