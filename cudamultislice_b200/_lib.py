@@ -81,6 +81,8 @@ SIGNATURES = {
     "ms_frozen_phonon": (_i, [_p, C.c_uint64, C.c_uint32, _i, _f, _i, _p, _p]),
     "ms_simulate_image_series": (_i, [_p, _p, _p, _i, _p]),
     "ms_set_detector": (_i, [_p, _p, _p, _i, _i, _f, _f, _f, C.c_uint64]),
+    "ms_write_tiff": (_i, [_p, _i, _s]),
+    "ms_write_tiff_f32": (_i, [_s, _p, _i, _i]),
     "ms_stem_raster_concurrent": (_i, [_p, _i, _p, _p, _p, _f, _f, _i, _p]),
     "ms_get_launch_count": (_i, [_p, _pll]),
     "ms_build_atom_index_noalloc": (_i, [_p, _p, _p, _p, _i, _p, _p, _p, _i, _pi, _p]),

@@ -18,7 +18,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmslice_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["ms_engine.cu", "ms_slice.cu", "ms_atoms.cu", "ms_pointwise.cu", "ms_noalloc.cu",
+SOURCES = ["ms_engine.cu", "ms_slice.cu", "ms_atoms.cu", "ms_pointwise.cu", "ms_noalloc.cu", "ms_tiff.cu",
            "ms_slice_n64.cu", "ms_slice_n128.cu", "ms_slice_n256.cu", "ms_slice_n512.cu", "ms_slice_n1024.cu",
            "ms_slice_n2048.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

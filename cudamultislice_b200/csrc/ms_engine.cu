@@ -25,6 +25,7 @@
 #include "../../include/mslice.h"
 #include "ms_atoms.cuh"
 #include "ms_philox.h"
+#include "ms_tiff.h"
 #include "ms_pointwise.cuh"
 #include "ms_slice.cuh"
 
@@ -813,6 +814,37 @@ class Engine {
     im_min_ = mn;
     im_max_ = mx;
     have_image_ = true;
+    return MS_OK;
+  }
+
+  // Float32 TIFF of a read-out (the GUI's exports, MainWindow.xaml.cs:684-890):
+  // 0 image as GetImValue reads it (readout noise included with a detector
+  // model), 1 / 2 exit-wave real / imaginary part (GetEWValueRe/Im, after
+  // ms_get_exit_wave), 3 TDS/CBED accumulation (GetTDSVal), 4 exit-wave amplitude.
+  int write_tiff(int what, const char* path) {
+    if (!path) return fail(MS_ERR_INVALID, "null path");
+    const size_t N = (size_t)nx_ * ny_;
+    std::vector<float> buf(N);
+    if (what == 0) {
+      if (!have_image_) return fail(MS_ERR_STATE, "image not simulated (ms_simulate_image)");
+      for (int y = 0; y < ny_; ++y)
+        for (int x = 0; x < nx_; ++x)
+          if (int rc = im_value(x, y, &buf[(size_t)y * nx_ + x])) return rc;
+    } else if (what == 1 || what == 2 || what == 4) {
+      if (!have_ew_) return fail(MS_ERR_STATE, "exit wave not read out (ms_get_exit_wave)");
+      for (size_t i = 0; i < N; ++i) {
+        const float2 v = ew_[i];
+        buf[i] = what == 1 ? v.x : what == 2 ? v.y : std::sqrt(v.x * v.x + v.y * v.y);
+      }
+    } else if (what == 3) {
+      if (int rc = tds_host()) return rc;
+      std::copy(htds_.begin(), htds_.end(), buf.begin());
+    } else {
+      return fail(MS_ERR_INVALID, "unknown read-out for TIFF output");
+    }
+    const int rc = write_tiff_f32(path, buf.data(), nx_, ny_);
+    if (rc == 1) return fail(MS_ERR_INVALID, "bad TIFF arguments");
+    if (rc != 0) return fail(MS_ERR_IO, std::string("cannot write ") + path);
     return MS_OK;
   }
 
@@ -2338,6 +2370,21 @@ ms_status ms_focal_series_grad(ms_sim* s, const float* defoci, int nd, const flo
 ms_status ms_time_pass(ms_sim* s, int pass, int op, int variant, int batch, int reps, float* us) {
   if (ms_status r = out_check(s, us)) return r;
   return guarded(s, [&](ms::Engine& e) { return e.time_pass(pass, op, variant, batch, reps, us); });
+}
+ms_status ms_write_tiff(ms_sim* s, int what, const char* path) {
+  return guarded(s, [&](ms::Engine& e) { return e.write_tiff(what, path); });
+}
+ms_status ms_write_tiff_f32(const char* path, const float* data, int nx, int ny) {
+  const int rc = ms::write_tiff_f32(path, data, nx, ny);
+  if (rc == 1) {
+    ms::set_handle_free_error("ms_write_tiff_f32: bad arguments");
+    return MS_ERR_INVALID;
+  }
+  if (rc != 0) {
+    ms::set_handle_free_error(std::string("ms_write_tiff_f32: cannot write ") + path);
+    return MS_ERR_IO;
+  }
+  return MS_OK;
 }
 ms_status ms_set_detector(ms_sim* s, const float* dqe, const float* ntf, int n, int binning, float conversion,
                           float readout_offset, float readout_sigma, uint64_t seed) {

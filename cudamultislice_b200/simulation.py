@@ -290,6 +290,10 @@ class ManagedMultisliceSimulation:
         self._chk(self._L.ms_set_detector(self._h, _ptr(d), _ptr(t), d.size, int(binning), float(conversion),
                                           float(readout_offset), float(readout_sigma), int(seed)))
 
+    def WriteTIFF(self, what: int, path: str):
+        """Float32 TIFF: 0 image, 1 / 2 exit-wave real / imaginary, 3 TDS/CBED, 4 amplitude."""
+        self._chk(self._L.ms_write_tiff(self._h, int(what), path.encode()))
+
     def SimulateImageSeries(self, defoci, cs=None) -> np.ndarray:
         """CTF images of the current exit wave at each defocus (and Cs), (n, ny, nx)."""
         d = np.ascontiguousarray(defoci, np.float32).ravel()
@@ -417,3 +421,14 @@ def stem_raster_concurrent(sims, positions, inner_mrad: float, outer_mrad: float
     sims[0]._chk(sims[0]._L.ms_stem_raster_concurrent(hs, k, PX, PY, NN, float(inner_mrad), float(outer_mrad),
                                                       int(batch), OUT))
     return outs, sims[0].LastDeviceMs()
+
+
+def write_tiff(path: str, data) -> None:
+    """Float32 TIFF of a 2D array (the library's writer, no GPU needed)."""
+    a = np.ascontiguousarray(data, np.float32)
+    if a.ndim != 2:
+        raise ValueError("need a 2D array")
+    L = lib()
+    rc = L.ms_write_tiff_f32(path.encode(), a.ctypes.data_as(C.c_void_p), a.shape[1], a.shape[0])
+    if rc != 0:
+        raise MultisliceError(rc, (L.ms_last_error(None) or b"").decode())

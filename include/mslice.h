@@ -222,6 +222,17 @@ ms_status ms_annular_detector(ms_sim* sim, float inner_mrad, float outer_mrad, d
 ms_status ms_stem_raster(ms_sim* sim, const int* px, const int* py, int n, float inner_mrad,
                          float outer_mrad, int batch, double* signal);
 
+/* Float32 TIFF output (new; replaces the GUI's LibTiff.NET export,
+ * CUDA Simulation GUI/MainWindow.xaml.cs:684-890, with the same fields: one
+ * uncompressed strip of 32-bit IEEE floats, MinIsBlack, top-left, little-endian).
+ * what: 0 the simulated image as ms_get_im_value reads it, 1 / 2 the exit wave's
+ * real / imaginary part and 4 its amplitude (after ms_get_exit_wave), 3 the TDS /
+ * CBED accumulation (ms_add_tds_waves). */
+ms_status ms_write_tiff(ms_sim* sim, int what, const char* path);
+/* The same TIFF of any nx * ny float array (row 0 at the top); errors are
+ * reported by ms_last_error(NULL). */
+ms_status ms_write_tiff_f32(const char* path, const float* data, int nx, int ny);
+
 /* Batch Cs/defocus sweep of the current exit wave (new; the reference's GUI
  * leaves it as a stub, CUDA Simulation GUI/BatchProcessing.xaml.cs:131-134): image i
  * of images (n * nx * ny floats) is the ms_simulate_image CTF image at defocus

@@ -425,3 +425,18 @@ def test_detector_noise_chain(engine_cls, oracle_mod):
     eng.SetDetector(None, None)
     eng.SimulateImage(dose)
     assert rel_l2(eng.Image(), I) < TOL
+
+
+def test_tiff_readouts(engine_cls, oracle_mod, tmp_path):
+    from tests.test_tiff import read_tiff_f32
+
+    eng, _ = make_pair(engine_cls, oracle_mod, sto(2, 2), 128, 0.1)
+    eng.RunConventional()
+    psi = eng.ExitWave()
+    eng.GetExitWave()  # the GUI's order: GetExitWave, then the per-pixel read-outs
+    eng.SimulateImage(0.0)
+    for what, ref in ((1, psi.real), (2, psi.imag), (4, np.abs(psi)), (0, eng.Image())):
+        p = str(tmp_path / f"r{what}.tiff")
+        eng.WriteTIFF(what, p)
+        _, d = read_tiff_f32(p)
+        assert np.allclose(d, ref, rtol=1e-6, atol=1e-7), what
