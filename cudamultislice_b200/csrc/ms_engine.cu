@@ -1054,6 +1054,14 @@ class Engine {
     if (int rc = build_stack(&rs_S_)) return rc;
     if (int rc = ensure_prop_tables(convdz_)) return rc;
     const long long N = (long long)nx_ * ny_;
+    // every probe of a batch meets the same slices: their transmissions are
+    // formed once (same sincos as the on-the-fly row pass) and read per probe
+    if (!tstack_valid_ || tstack_S_ != rs_S_) {
+      MS_TRY(d_tstack_.resize((size_t)rs_S_ * N));
+      MS_TRY(pw_transmission_stack(d_stack_.p, sigma2_, d_tstack_.p, (long long)rs_S_ * N, stream_, &launches));
+      tstack_valid_ = true;
+      tstack_S_ = rs_S_;
+    }
     rs_n_ = n;
     rs_B_ = std::min(batch, n);
     plan_for(rs_B_);
@@ -1094,8 +1102,8 @@ class Engine {
         PassAArgs a = passa_args(d_bwave_.p, d_bwave_.p, vr);
         a.batch_stride_wave = N;
         a.batch_stride_V = 0;
-        a.V = d_stack_.p + (size_t)(it - 1) * N;
-        MS_TRY(launch_pass_a(a, vr, it == 1 ? (A_MULT_T | A_FWD) : (A_INV | A_MULT_T | A_FWD), nb, st));
+        a.tr = d_tstack_.p + (size_t)(it - 1) * N;
+        MS_TRY(launch_pass_a(a, vr, it == 1 ? (A_MULT_TC | A_FWD) : (A_INV | A_MULT_TC | A_FWD), nb, st));
         PassBArgs b = passb_args(d_bwave_.p, d_bwave_.p, vc);
         b.batch_stride_wave = N;
         if (it < S) {
@@ -1251,6 +1259,7 @@ class Engine {
       MS_TRY(cudaStreamSynchronize(stream_));
       nstack_ = S;
       stack_valid_ = true;
+      tstack_valid_ = false;
       invalidate_graph();
     }
     if (nslices) *nslices = S;
@@ -2019,6 +2028,9 @@ class Engine {
   DevBuf<float2> d_psi0_, d_psi_, d_psim_, d_t1_, d_t2_, d_grad_, d_fdX_, d_fdQ_, d_fdS_;
   bool fd_state_ = false;
   DevBuf<float> d_V_, d_f_, d_tds_, d_stack_;
+  DevBuf<float2> d_tstack_;  // transmissions of the stack (probe rasters)
+  bool tstack_valid_ = false;
+  int tstack_S_ = 0;
   DevBuf<double> d_partial_, d_bsig_, d_bpart_;
   DevBuf<float2> d_bwave_;
   DevBuf<int> d_bpos_;

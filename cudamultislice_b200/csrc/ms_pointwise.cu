@@ -228,6 +228,16 @@ __global__ void k_abs(const float2* a, float* out, Grid2 g) {
   out[i] = sqrtf(a[i].x * a[i].x + a[i].y * a[i].y);
 }
 
+// Transmission exp(i sigma V) of n values with the fused row pass's sincos
+// (identical values to the on-the-fly transmission).
+__global__ void k_transmission_stack(const float* V, float sigma, float2* t, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float sn, cs;
+  sincos_red(fmul_x(sigma, V[i]), &sn, &cs);
+  t[i] = make_float2(cs, sn);
+}
+
 // acc += scale * sum_b in[b * stride + i] (batched images into one sum)
 __global__ void k_add_batch(const float* in, long long stride, int nb, float* acc, float scale, Grid2 g) {
   PW_INDEX
@@ -392,6 +402,12 @@ cudaError_t pw_shot_noise(const float2* F, float* counts, float dose, uint64_t s
 }
 cudaError_t pw_abs(const float2* a, float* out, Grid2 g, cudaStream_t s, long long* count) {
   PW_LAUNCH(k_abs, a, out, g);
+}
+cudaError_t pw_transmission_stack(const float* V, float sigma, float2* t, long long n, cudaStream_t s,
+                                  long long* count) {
+  k_transmission_stack<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(V, sigma, t, n);
+  if (count) ++*count;
+  return cudaGetLastError();
 }
 cudaError_t pw_rs_term(const float2* w, float2* out, const float* V, float pre, float inv_ps2, int m, Grid2 g,
                        cudaStream_t s, long long* count) {

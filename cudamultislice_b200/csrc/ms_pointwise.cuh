@@ -38,6 +38,9 @@ cudaError_t pw_detector_filter(float2* F, const float* tab, int n, int binning, 
 cudaError_t pw_shot_noise(const float2* F, float* counts, float dose, uint64_t seed, uint32_t serial, Grid2 g,
                           cudaStream_t s, long long* count);
 cudaError_t pw_abs(const float2* a, float* out, Grid2 g, cudaStream_t s, long long* count);
+// t = exp(i sigma V) over n values, with the fused row pass's sincos.
+cudaError_t pw_transmission_stack(const float* V, float sigma, float2* t, long long n, cudaStream_t s,
+                                  long long* count);
 // Term m of the real-space (RS) series, as written in the reference (see .cu).
 cudaError_t pw_rs_term(const float2* w, float2* out, const float* V, float pre, float inv_ps2, int m, Grid2 g,
                        cudaStream_t s, long long* count);

@@ -29,6 +29,7 @@ enum PassAFlags : int {
                     // line <- 2 r line (I to out_f when not null)
   A_ADJ = 256,      // adjoint of x t: dV = -2 sigma Im(conj(h) t psi) to out_f
                     // (psi from in2), line <- conj(t) line
+  A_MULT_TC = 512,  // x t from a precomputed transmission slice (PassAArgs.tr)
 };
 enum PassBMode : int {
   B_FWD_ONLY = 0,    // FFT_col
@@ -59,6 +60,7 @@ struct PassAArgs {
   float2* out2;
   float2 fd_rc, fd_ratio;
   float fd_kv;
+  const float2* tr;   // A_MULT_TC: transmission exp(i sigma V) [ny][nx] (instance stride batch_stride_V)
   const float* T;     // A_RESID: target intensity [ny][nx] (instance stride batch_stride_V)
   double* loss;       // A_RESID: FP64 sum of r^2 (atomic)
   const float2* tw;   // twiddle table for nx

@@ -68,7 +68,9 @@ struct RowOperands {
   static constexpr bool HAS_V = (FLAGS & (A_MULT_T | A_FD | A_ADJ)) != 0;
   static constexpr bool HAS_T = (FLAGS & A_RESID) != 0;
   static constexpr bool HAS_W = (FLAGS & (A_FD | A_ADJ)) != 0 && E <= 16;
+  static constexpr bool HAS_TC = (FLAGS & A_MULT_TC) != 0;
   float V[HAS_V ? E : 1];
+  float2 TC[HAS_TC ? E : 1];
   float T[HAS_T ? E : 1];
   float2 W[HAS_W ? E : 1];
   MS_D void load(const PassAArgs& a, long long inst, int line, long long row0, int t) {
@@ -80,6 +82,10 @@ struct RowOperands {
     if constexpr (HAS_T) {
 #pragma unroll
       for (int j = 0; j < E; ++j) T[j] = a.T[r0 + t + P * j];
+    }
+    if constexpr (HAS_TC) {
+#pragma unroll
+      for (int j = 0; j < E; ++j) TC[j] = a.tr[r0 + t + P * j];
     }
     if constexpr (HAS_W) {
 #pragma unroll
@@ -119,6 +125,10 @@ MS_D void row_mid(float2 (&v)[PL::E], const PassAArgs& a, const RowOperands<PL, 
       sincos_red(fmul_x(a.sigma, op.V[j]), &sn, &cs);
       v[j] = cmul(v[j], make_float2(cs, sn));
     }
+  }
+  if constexpr ((FLAGS & A_MULT_TC) != 0) {
+#pragma unroll
+    for (int j = 0; j < E; ++j) v[j] = cmul(v[j], op.TC[j]);
   }
   if constexpr ((FLAGS & A_RESID) != 0) {
     const long long r0 = inst * a.batch_stride_V + (long long)line * NX;
@@ -212,8 +222,19 @@ __global__ void __launch_bounds__(rows_per_cta<PL>() * PL::P) k_pass_a(PassAArgs
 
 // Pointwise work of the column pass on the column spectrum (between the
 // forward and the inverse transform, or before the epilogue).
+// Column modes whose pointwise work reads the row frequencies ky, and the
+// propagator's row factors py: staged in shared memory per CTA.
+template <int MODE>
+__host__ __device__ constexpr bool col_uses_ky() {
+  return MODE == B_PROPAGATE || MODE == B_PROPAGATE_ADJ || MODE == B_CTF || MODE == B_CTF_ADJ ||
+         MODE == B_BANDLIMIT || MODE == B_FD || MODE == B_DETECT;
+}
+template <int MODE>
+__host__ __device__ constexpr bool col_uses_py() { return MODE == B_PROPAGATE || MODE == B_PROPAGATE_ADJ; }
+
 template <class PL, int MODE>
-MS_D void col_mid(float2 (&v)[PL::E], const PassBArgs& a, int col, int t, long long base) {
+MS_D void col_mid(float2 (&v)[PL::E], const PassBArgs& a, const float* __restrict__ sky,
+                  const float2* __restrict__ spy, int col, int t, long long base) {
   constexpr int NY = PL::N, E = PL::E, P = PL::P;
   const float scale = a.scale;
   if constexpr (MODE == B_PROPAGATE) {
@@ -223,10 +244,10 @@ MS_D void col_mid(float2 (&v)[PL::E], const PassBArgs& a, int col, int t, long l
 #pragma unroll
     for (int j = 0; j < E; ++j) {
       const int n = t + P * j;
-      const float ky = a.ky[n];
+      const float ky = sky[n];
       // CreatePropsKernel (U.cu:419): keep sqrtf(kx^2+ky^2) < kmax
       const bool keep = fsqrt_x(fadd_x(kx2, fmul_x(ky, ky))) < a.kmax;
-      const float2 w = keep ? cmul(pxv, a.py[n]) : make_float2(0.f, 0.f);
+      const float2 w = keep ? cmul(pxv, spy[n]) : make_float2(0.f, 0.f);
       v[j] = cmul(v[j], w);
     }
   } else if constexpr (MODE == B_PROPAGATE_ADJ) {
@@ -236,9 +257,9 @@ MS_D void col_mid(float2 (&v)[PL::E], const PassBArgs& a, int col, int t, long l
 #pragma unroll
     for (int j = 0; j < E; ++j) {
       const int n = t + P * j;
-      const float ky = a.ky[n];
+      const float ky = sky[n];
       const bool keep = fsqrt_x(fadd_x(kx2, fmul_x(ky, ky))) < a.kmax;
-      const float2 w = keep ? cscale(cconj(cmul(pxv, a.py[n])), scale) : make_float2(0.f, 0.f);
+      const float2 w = keep ? cscale(cconj(cmul(pxv, spy[n])), scale) : make_float2(0.f, 0.f);
       v[j] = cmul(v[j], w);
     }
   } else if constexpr (MODE == B_CTF || MODE == B_CTF_ADJ) {
@@ -247,7 +268,7 @@ MS_D void col_mid(float2 (&v)[PL::E], const PassBArgs& a, int col, int t, long l
     for (int j = 0; j < E; ++j) {
       const int n = t + P * j;
       const float2 w = ctf_weight(a.ctf.wavel, a.ctf.Cs, a.ctf.df, a.ctf.A2, a.ctf.phi2, a.ctf.A3, a.ctf.phi3,
-                                  a.ctf.beta, a.ctf.delta, a.ctf.objap2, kx, a.ky[n], scale);
+                                  a.ctf.beta, a.ctf.delta, a.ctf.objap2, kx, sky[n], scale);
       v[j] = cmul(v[j], MODE == B_CTF ? w : cconj(w));
     }
   } else if constexpr (MODE == B_BANDLIMIT) {
@@ -256,7 +277,7 @@ MS_D void col_mid(float2 (&v)[PL::E], const PassBArgs& a, int col, int t, long l
     const float kx2 = fmul_x(kx, kx);
 #pragma unroll
     for (int j = 0; j < E; ++j) {
-      const float ky = a.ky[t + P * j];
+      const float ky = sky[t + P * j];
       const bool keep = fsqrt_x(fadd_x(kx2, fmul_x(ky, ky))) <= a.kmax;
       v[j] = keep ? cscale(v[j], scale) : make_float2(0.f, 0.f);
     }
@@ -268,7 +289,7 @@ MS_D void col_mid(float2 (&v)[PL::E], const PassBArgs& a, int col, int t, long l
 #pragma unroll
     for (int j = 0; j < E; ++j) {
       const int n = t + P * j;
-      const float ky = a.ky[n];
+      const float ky = sky[n];
       const float ky2 = fmul_x(ky, ky);
       const bool keep = fsqrt_x(fadd_x(kx2, ky2)) <= a.kmax;
       const long long o = (long long)col * NY + n;  // spectrum kept column-major
@@ -294,9 +315,19 @@ __global__ void __launch_bounds__(cols_per_cta<PL>() * PL::P) k_pass_b(PassBArgs
   const float2* in = a.in + base;
   const float scale = a.scale;
 
+  // constant frequency tables for the pointwise work (written before any pass
+  // runs, so they may be read before the predecessor completes)
+  float* sky = reinterpret_cast<float*>(smem + CB * LS);
+  float2* spy = smem + CB * LS + (col_uses_ky<MODE>() ? (NY + 1) / 2 : 0);
+  pdl_launch_dependents();
+  if constexpr (col_uses_ky<MODE>()) {
+    for (int i = threadIdx.x; i < NY; i += NT) sky[i] = a.ky[i];
+  }
+  if constexpr (col_uses_py<MODE>()) {
+    for (int i = threadIdx.x; i < NY; i += NT) spy[i] = a.py[i];
+  }
   // transposing tile load: NY rows x CB columns -> one padded slot per column,
   // E asynchronous 8-byte copies per thread, all in flight together
-  pdl_launch_dependents();
   pdl_wait();
 #pragma unroll
   for (int k = 0; k < E; ++k) {
@@ -329,7 +360,7 @@ __global__ void __launch_bounds__(cols_per_cta<PL>() * PL::P) k_pass_b(PassBArgs
       if constexpr (MODE == B_INV_ONLY) {
         fft::conj_all(v);
       } else if constexpr (TWO) {
-        col_mid<PL, MODE>(v, a, col, t, base);
+        col_mid<PL, MODE>(v, a, sky, spy, col, t, base);
         fft::conj_all(v);
       }
     } else {
@@ -356,7 +387,7 @@ __global__ void __launch_bounds__(cols_per_cta<PL>() * PL::P) k_pass_b(PassBArgs
 #pragma unroll
     for (int j = 0; j < E; ++j) {
       const int n = t + P * j;
-      const float ky = a.ky[n];
+      const float ky = sky[n];
       const float k2 = fadd_x(kx2, fmul_x(ky, ky));
       const bool keep = fsqrt_x(k2) < a.kmax && k2 >= a.kin2 && k2 < a.kout2;
       if (keep) acc += v[j].x * v[j].x + v[j].y * v[j].y;
@@ -426,7 +457,9 @@ cudaError_t run_a(const PassAArgs& a, int batch, cudaStream_t s) {
 template <class PL, int MODE>
 cudaError_t run_b(const PassBArgs& a, int batch, cudaStream_t s) {
   constexpr int CB = cols_per_cta<PL>();
-  const size_t smem = (size_t)CB * col_slot<PL>() * sizeof(float2);
+  const size_t smem = (size_t)CB * col_slot<PL>() * sizeof(float2) +
+                      (col_uses_ky<MODE>() ? (size_t)(PL::N + 1) / 2 * sizeof(float2) : 0) +
+                      (col_uses_py<MODE>() ? (size_t)PL::N * sizeof(float2) : 0);
   if (a.nx % CB) return cudaErrorInvalidValue;
   static unsigned long long done = 0;
   if (attr_once(done)) {
@@ -451,6 +484,8 @@ cudaError_t dispatch_a_plan(const PassAArgs& a, int flags, int batch, cudaStream
     case A_INV | A_RESID: return run_a<PL, A_INV | A_RESID>(a, batch, s);
     case A_INV | A_RESID | A_FWD: return run_a<PL, A_INV | A_RESID | A_FWD>(a, batch, s);
     case A_INV | A_ADJ | A_FWD: return run_a<PL, A_INV | A_ADJ | A_FWD>(a, batch, s);
+    case A_MULT_TC | A_FWD: return run_a<PL, A_MULT_TC | A_FWD>(a, batch, s);
+    case A_INV | A_MULT_TC | A_FWD: return run_a<PL, A_INV | A_MULT_TC | A_FWD>(a, batch, s);
     default: return cudaErrorInvalidValue;
   }
 }
