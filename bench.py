@@ -164,7 +164,7 @@ def barrier(world: int):
         dist.barrier()
 
 
-def stem_leg(fparams, device: int, nprobes: int = 256, batch: int = 16) -> dict:
+def stem_leg(fparams, device: int, nprobes: int = 256, batch: int = 0) -> dict:
     """STEM probes/s on the GaN [11-20] HAADF configuration: 10 x 6 x 40
     orthohexagonal cells (19,200 atoms), 1024^2 grid, 1.5945 A slices, 300 kV,
     25 mrad, Cs = 0, df = 0, annular detector 70-200 mrad; a subset of the
@@ -193,7 +193,7 @@ def stem_leg(fparams, device: int, nprobes: int = 256, batch: int = 16) -> dict:
     out = {}
     for name, path, n in (("fused", 0, nprobes), ("plain", 1, max(nprobes // 16, 8))):
         sim.SetSlicePath(path)
-        sim.StemRaster(px[:batch], py[:batch], 70.0, 200.0, batch=batch)  # warm-up / tuning
+        sim.StemRaster(px[:64], py[:64], 70.0, 200.0, batch=batch)  # warm-up / tuning
         t0 = time.perf_counter()
         sig = sim.StemRaster(px[:n], py[:n], 70.0, 200.0, batch=batch)
         dt = time.perf_counter() - t0
@@ -205,11 +205,12 @@ def stem_leg(fparams, device: int, nprobes: int = 256, batch: int = 16) -> dict:
             "plain_value": out["plain"]["probes_per_s"],
             "speedup_fused_vs_plain": out["fused"]["probes_per_s"] / out["plain"]["probes_per_s"],
             "config": f"GaN [11-20] 10x6x40 cells ({len(Z)} atoms), {GRID}^2, {nsl} slices of 1.5945 A, 300 kV, "
-                      f"25 mrad, HAADF 70-200 mrad, {nprobes} probes of the 128x128 raster, batch {batch}",
+                      f"25 mrad, HAADF 70-200 mrad, {nprobes} probes of the 128x128 raster, "
+                      f"batch {'automatic (64)' if batch <= 0 else batch}",
             "timing": "host clock around ms_stem_raster (synchronous), potential stack resident"}
 
 
-def mixed_leg(fparams, device: int, n1024: int = 256, n512: int = 256, batch: int = 16) -> dict:
+def mixed_leg(fparams, device: int, n1024: int = 256, n512: int = 256, batch: int = 64) -> dict:
     """The mixed-grid STEM configuration: GaN [11-20] 10 x 6 x 40 cells on
     1024^2 together with the same crystal cropped to 5 x 3 x 40 cells on 512^2
     (1.5945 A slices, 300 kV, 25 mrad, HAADF 70-200 mrad), `n1024` probes of
@@ -238,20 +239,26 @@ def mixed_leg(fparams, device: int, n1024: int = 256, n512: int = 256, batch: in
         px, py = np.meshgrid(g, g)
         pos.append((px.ravel()[:npr], py.ravel()[:npr]))
         sims.append(sim)
-    stem_raster_concurrent(sims, [(p[0][:batch], p[1][:batch]) for p in pos], 70.0, 200.0, batch)  # warm-up
-    _, ms_conc = stem_raster_concurrent(sims, pos, 70.0, 200.0, batch)
-    ms_seq = 0.0
-    for sim, p in zip(sims, pos):
-        _, ms1 = stem_raster_concurrent([sim], [p], 70.0, 200.0, batch)
-        ms_seq += ms1
+    nprobes = n1024 + n512
+    res = {}
+    for b in (16, batch):
+        stem_raster_concurrent(sims, [(p[0][:b], p[1][:b]) for p in pos], 70.0, 200.0, b)  # warm-up
+        _, ms_conc = stem_raster_concurrent(sims, pos, 70.0, 200.0, b)
+        ms_seq = 0.0
+        for sim, p in zip(sims, pos):
+            _, ms1 = stem_raster_concurrent([sim], [p], 70.0, 200.0, b)
+            ms_seq += ms1
+        res[b] = (nprobes / (ms_conc / 1000.0), nprobes / (ms_seq / 1000.0))
     for sim in sims:
         sim.close()
-    nprobes = n1024 + n512
-    return {"value": nprobes / (ms_conc / 1000.0), "unit": "probes/s", "sequential_value": nprobes / (ms_seq / 1000.0),
-            "speedup_concurrent_vs_sequential": ms_seq / ms_conc,
+    best = max(max(v) for v in res.values())
+    return {"value": best, "unit": "probes/s",
+            "by_batch": {str(b): {"concurrent": c, "sequential": q, "concurrent_over_sequential": c / q}
+                         for b, (c, q) in res.items()},
             "config": f"GaN [11-20]: 10x6x40 cells on 1024^2 ({n1024} probes) + 5x3x40 cells on 512^2 "
-                      f"({n512} probes), 1.5945 A slices, 300 kV, 25 mrad, HAADF 70-200 mrad, batch {batch}",
-            "timing": "device time of one CUDA-graph launch holding both rasters as concurrent branches"}
+                      f"({n512} probes), 1.5945 A slices, 300 kV, 25 mrad, HAADF 70-200 mrad",
+            "timing": "device time of one CUDA-graph launch: both rasters as concurrent branches, or one after "
+                      "the other; value = the faster arrangement"}
 
 
 def adjoint_leg(fparams, device: int, reps: int = 3) -> dict:

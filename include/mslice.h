@@ -218,7 +218,8 @@ ms_status ms_annular_detector(ms_sim* sim, float inner_mrad, float outer_mrad, d
  * for each probe position (px[i], py[i]) in pixels, the probe of
  * STEMInitialiseWavefunctions (U.cu:2672-2705), conventional slices 1..S over
  * the potential stack, and the annular-detector signal of ms_annular_detector,
- * written to signal[i].  Probes run `batch` at a time in one set of launches. */
+ * written to signal[i].  Probes run `batch` at a time in one set of launches
+ * (batch <= 0: automatic, 64 or what a quarter of the free memory holds). */
 ms_status ms_stem_raster(ms_sim* sim, const int* px, const int* py, int n, float inner_mrad,
                          float outer_mrad, int batch, double* signal);
 
