@@ -202,6 +202,7 @@ def stem_leg(fparams, device: int, nprobes: int = 256, batch: int = 0) -> dict:
             out["signal_mean"] = float(np.mean(sig))
     sim.close()
     return {"value": out["fused"]["probes_per_s"], "unit": "probes/s",
+            "slice_steps_per_s": out["fused"]["probes_per_s"] * nsl,
             "plain_value": out["plain"]["probes_per_s"],
             "speedup_fused_vs_plain": out["fused"]["probes_per_s"] / out["plain"]["probes_per_s"],
             "config": f"GaN [11-20] 10x6x40 cells ({len(Z)} atoms), {GRID}^2, {nsl} slices of 1.5945 A, 300 kV, "
@@ -259,6 +260,32 @@ def mixed_leg(fparams, device: int, n1024: int = 256, n512: int = 256, batch: in
                       f"({n512} probes), 1.5945 A slices, 300 kV, 25 mrad, HAADF 70-200 mrad",
             "timing": "device time of one CUDA-graph launch: both rasters as concurrent branches, or one after "
                       "the other; value = the faster arrangement"}
+
+
+def focal_profile_leg(fparams, device: int) -> dict:
+    """A reduced inverse-problem case for kernel captures: SrTiO3 4 x 4 x 10
+    cells on 512^2, 200 kV, one focal-series gradient (8 defoci, 20 slices,
+    dL/dxy) -- one potential build per slice and one potential adjoint per slice."""
+    import numpy as np
+
+    from cudamultislice_b200 import ManagedMultisliceSimulation
+    from cudamultislice_b200 import structures as S
+
+    n = 512
+    Z, x, y, z = S.srtio3(4, 4, 10)
+    sim = ManagedMultisliceSimulation(device=device)
+    sim.SetAtoms(Z, x, y, z)
+    sim.UploadBinnedAtoms()
+    sim.GetParameterisation(fparams)
+    sim.ApplyMicroscopeParameters(200.0, 0.0, 0.0, 0.0, 1.0e7, 0.1, 30.0, 20.0)
+    sim.SetCalculationVariables(3.905 * 4 / n, 0.0, n, n, sim.GetSizeX(), sim.GetSizeY(), sim.GetSizeZ(), 2.0, 2.0)
+    sim.PreCalculateFrequencies()
+    sim.InitialiseWavefunctions(1.9525)
+    df = np.linspace(-800.0, 600.0, 8).astype(np.float32)
+    L, _, gxy = sim.FocalSeriesGrad(df, np.ones((8, n, n), np.float32), 20, want_v=False)
+    ms = sim.LastDeviceMs()
+    sim.close()
+    return {"loss": L, "grad_abs_sum": float(np.abs(gxy).sum()), "device_ms": ms}
 
 
 def adjoint_leg(fparams, device: int, reps: int = 3) -> dict:
@@ -437,7 +464,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="profiling mode: set-up plus the timed slice loop only (no e2e, plain or CPU legs)")
-    ap.add_argument("--leg", choices=["stem", "adjoint", "tds", "mixed"],
+    ap.add_argument("--leg", choices=["stem", "adjoint", "tds", "mixed", "focal_profile"],
                     help="run one secondary leg alone and print its JSON (exploration)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
@@ -447,7 +474,8 @@ def main():
     if args.leg:
         from cudamultislice_b200 import FPARAMS
 
-        leg = {"stem": stem_leg, "adjoint": adjoint_leg, "tds": tds_leg, "mixed": mixed_leg}[args.leg](FPARAMS, local)
+        leg = {"stem": stem_leg, "adjoint": adjoint_leg, "tds": tds_leg, "mixed": mixed_leg,
+               "focal_profile": focal_profile_leg}[args.leg](FPARAMS, local)
         if rank == 0:
             print(json.dumps({"leg": args.leg, **leg}), flush=True)
         return
