@@ -440,3 +440,30 @@ def test_tiff_readouts(engine_cls, oracle_mod, tmp_path):
         eng.WriteTIFF(what, p)
         _, d = read_tiff_f32(p)
         assert np.allclose(d, ref, rtol=1e-6, atol=1e-7), what
+
+
+# ---------------------------------------------------------------- non-square grids
+@pytest.mark.parametrize("path", [0, 1])
+@pytest.mark.parametrize("shape", [(256, 128), (128, 512)])
+def test_non_square_grid(engine_cls, oracle_mod, shape, path):
+    """nx != ny: the row and column passes use different line lengths (and plans)."""
+    nx, ny = shape
+    Z, x, y, z = sto(3, 2)
+    eng = engine_cls()
+    eng.SetSlicePath(path)
+    orc = oracle_mod.OracleSimulation()
+    for s in (eng, orc):
+        s.SetAtoms(Z, x, y, z)
+        s.UploadBinnedAtoms()
+        s.GetParameterisation(FPARAMS)
+        s.ApplyMicroscopeParameters(200.0, -300.0, 0.0, 0.0, 1e7, 0.1, 30.0, 20.0)
+        s.SetCalculationVariables(0.08, -300.0, nx, ny, s.GetSizeX(), s.GetSizeY(), s.GetSizeZ(), 2.0, 2.0)
+        s.PreCalculateFrequencies()
+        s.InitialiseWavefunctions(1.9525)
+    n = orc.GetSlices(True)
+    for i in range(1, n + 1):
+        eng.MultisliceStepConventional(i)
+        orc.MultisliceStepConventional(i)
+    assert rel_l2(eng.ExitWave(), orc.Wave()) < TOL
+    eng.SimulateImage(0.0)
+    assert rel_l2(eng.Image(), orc.SimulateImage()) < TOL
