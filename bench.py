@@ -576,10 +576,11 @@ def main():
                         "(100 slices), slice loop, exit wave out"},
     }
 
-    out["stem"] = stem_leg(FPARAMS, local)
-    out["adjoint"] = adjoint_leg(FPARAMS, local)
-    out["tds"] = tds_leg(FPARAMS, local)
-    out["stem_mixed"] = mixed_leg(FPARAMS, local)
+    if rank == 0:  # secondary legs: one GPU, after the collective timing
+        out["stem"] = stem_leg(FPARAMS, local)
+        out["adjoint"] = adjoint_leg(FPARAMS, local)
+        out["tds"] = tds_leg(FPARAMS, local)
+        out["stem_mixed"] = mixed_leg(FPARAMS, local)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1

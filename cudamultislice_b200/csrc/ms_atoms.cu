@@ -336,6 +336,8 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
   __shared__ float4 s_at[kConvChunk];
   __shared__ float s_dz2[kConvChunk][20];
   __shared__ float s_g[kConvChunk][3][20];
+  __shared__ int s_mlo[kConvChunk], s_mhi[kConvChunk];
+  __shared__ float s_dzmin[kConvChunk];
   __shared__ float s_coef[103 * kCoefPerZ];
   __shared__ int s_start[kMaxSeg];
   __shared__ int s_pref[kMaxSeg + 1];
@@ -391,7 +393,25 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
             const int mid = (lo + hi + 1) >> 1;
             if (s_pref[mid] <= gidx) lo = mid; else hi = mid - 1;
           }
-          s_at[threadIdx.x] = a.atoms[s_start[lo] + (gidx - s_pref[lo])];
+          const float4 at = a.atoms[s_start[lo] + (gidx - s_pref[lo])];
+          s_at[threadIdx.x] = at;
+          // sub-planes that can pass the cut-off for some pixel (dz_m^2 < 5: an
+          // interval of m, since the non-contracted dz and dz^2 are monotone in
+          // the plane height) and the smallest dz_m^2 (the clamp test below)
+          int mlo = 20, mhi = -1;
+          float dmin = 1e30f;
+          for (int m = 0; m < 20; ++m) {
+            const float dz = fsub_x(a.zsub[m], at.z);
+            const float dz2 = fmul_x(dz, dz);
+            if (dz2 < 5.0f) {
+              mlo = min(mlo, m);
+              mhi = m;
+            }
+            dmin = fminf(dmin, dz2);
+          }
+          s_mlo[threadIdx.x] = mlo;
+          s_mhi[threadIdx.x] = mhi;
+          s_dzmin[threadIdx.x] = dmin;
         }
         __syncthreads();
         // per (atom, sub-plane): dz^2 as the cut-off rounds it, Gaussian factors
@@ -415,20 +435,34 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
           const float* c = s_coef + (__float_as_int(at.w) - 1) * kCoefPerZ;
           const float g0 = c[6] * ex2_fast(-c[9] * dxy), g1 = c[7] * ex2_fast(-c[10] * dxy),
                       g2 = c[8] * ex2_fast(-c[11] * dxy);
+          const int mlo = s_mlo[i], mhi = s_mhi[i];
+          if (!(fadd_x(dxy, s_dzmin[i]) < 0.0625f)) {
+            // no sub-plane reaches the 0.25 A clamp for this pixel
 #pragma unroll 4
-          for (int m = 0; m < 20; ++m) {
-            const float r2 = fadd_x(dxy, s_dz2[i][m]);
-            if (!(r2 < 5.0f)) continue;
-            float v;
-            if (r2 < 0.0625f) {
-              v = vatom_f(c, r2);  // inside the 0.25 A clamp
-            } else {
+            for (int m = mlo; m <= mhi; ++m) {
+              const float r2 = fadd_x(dxy, s_dz2[i][m]);
+              if (!(r2 < 5.0f)) continue;
               const float ri = rsqrtf(r2), r = r2 * ri;
               const float L = c[0] * ex2_fast(-c[3] * r) + c[1] * ex2_fast(-c[4] * r) + c[2] * ex2_fast(-c[5] * r);
               const float G = g0 * s_g[i][0][m] + g1 * s_g[i][1][m] + g2 * s_g[i][2][m];
-              v = L * ri + G;
+              acc += a.wsub * (L * ri + G);
             }
-            acc += a.wsub * v;
+          } else {
+            for (int m = mlo; m <= mhi; ++m) {
+              const float r2 = fadd_x(dxy, s_dz2[i][m]);
+              if (!(r2 < 5.0f)) continue;
+              float v;
+              if (r2 < 0.0625f) {
+                v = vatom_f(c, r2);  // inside the 0.25 A clamp
+              } else {
+                const float ri = rsqrtf(r2), r = r2 * ri;
+                const float L =
+                    c[0] * ex2_fast(-c[3] * r) + c[1] * ex2_fast(-c[4] * r) + c[2] * ex2_fast(-c[5] * r);
+                const float G = g0 * s_g[i][0][m] + g1 * s_g[i][1][m] + g2 * s_g[i][2][m];
+                v = L * ri + G;
+              }
+              acc += a.wsub * v;
+            }
           }
         }
         __syncthreads();
