@@ -323,6 +323,39 @@ __device__ __forceinline__ float ex2_fast(float x) {
   return y;
 }
 
+// Packed FP32x2 arithmetic of sm_100 (PTX add/mul/fma.rn.f32x2: two
+// independent, correctly rounded FP32 operations in one instruction) on pairs
+// held in 64-bit registers (low half = first value).
+typedef unsigned long long f2p;
+__device__ __forceinline__ f2p pk2(float lo, float hi) {
+  f2p r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void up2(f2p v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2p add2(f2p a, f2p b) {
+  f2p d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f2p mul2(f2p a, f2p b) {
+  f2p d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f2p fma2(f2p a, f2p b, f2p c) {
+  f2p d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ f2p ex2_pair(f2p a) {
+  float lo, hi;
+  up2(a, lo, hi);
+  return pk2(ex2_fast(lo), ex2_fast(hi));
+}
+
 // Conventional potential (binnedAtomPKernel3 semantics) with per-atom work
 // hoisted out of the pixel loop.  For each staged atom the 20 sub-plane offsets
 // dz_m^2 (rounded exactly as in the cut-off test) and the Gaussian factors
@@ -334,8 +367,8 @@ constexpr int kConvChunk = 64;
 
 __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
   __shared__ float4 s_at[kConvChunk];
-  __shared__ float s_dz2[kConvChunk][20];
-  __shared__ float s_g[kConvChunk][3][20];
+  __shared__ __align__(8) float s_dz2[kConvChunk][20];
+  __shared__ __align__(8) float s_g[kConvChunk][3][20];
   __shared__ int s_mlo[kConvChunk], s_mhi[kConvChunk];
   __shared__ float s_dzmin[kConvChunk];
   __shared__ float s_coef[103 * kCoefPerZ];
@@ -437,16 +470,36 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
                       g2 = c[8] * ex2_fast(-c[11] * dxy);
           const int mlo = s_mlo[i], mhi = s_mhi[i];
           if (!(fadd_x(dxy, s_dzmin[i]) < 0.0625f)) {
-            // no sub-plane reaches the 0.25 A clamp for this pixel
-#pragma unroll 4
-            for (int m = mlo; m <= mhi; ++m) {
-              const float r2 = fadd_x(dxy, s_dz2[i][m]);
-              if (!(r2 < 5.0f)) continue;
-              const float ri = rsqrtf(r2), r = r2 * ri;
-              const float L = c[0] * ex2_fast(-c[3] * r) + c[1] * ex2_fast(-c[4] * r) + c[2] * ex2_fast(-c[5] * r);
-              const float G = g0 * s_g[i][0][m] + g1 * s_g[i][1][m] + g2 * s_g[i][2][m];
-              acc += a.wsub * (L * ri + G);
+            // No sub-plane reaches the 0.25 A clamp for this pixel: sub-planes in
+            // pairs (m, m+1) on the packed FP32x2 pipe.  add.rn.f32x2 rounds each
+            // lane as fadd_x does, so the r^2 < 5 decisions are unchanged; sub-
+            // planes outside [mlo, mhi] have dz^2 >= 5 and fail the test.
+            const f2p d2 = pk2(dxy, dxy);
+            const f2p c0 = pk2(c[0], c[0]), c1 = pk2(c[1], c[1]), c2 = pk2(c[2], c[2]);
+            const f2p n3 = pk2(-c[3], -c[3]), n4 = pk2(-c[4], -c[4]), n5 = pk2(-c[5], -c[5]);
+            const f2p q0 = pk2(g0, g0), q1 = pk2(g1, g1), q2 = pk2(g2, g2);
+            f2p acc2 = pk2(0.0f, 0.0f);
+            for (int m = mlo & ~1; m <= mhi; m += 2) {
+              const f2p r2 = add2(d2, *reinterpret_cast<const f2p*>(&s_dz2[i][m]));
+              float ra, rb;
+              up2(r2, ra, rb);
+              const bool ka = ra < 5.0f, kb = rb < 5.0f;
+              if (!(ka || kb)) continue;
+              const f2p ri = pk2(rsqrtf(ra), rsqrtf(rb));
+              const f2p r = mul2(r2, ri);
+              f2p L = mul2(c0, ex2_pair(mul2(n3, r)));
+              L = fma2(c1, ex2_pair(mul2(n4, r)), L);
+              L = fma2(c2, ex2_pair(mul2(n5, r)), L);
+              f2p G = mul2(q0, *reinterpret_cast<const f2p*>(&s_g[i][0][m]));
+              G = fma2(q1, *reinterpret_cast<const f2p*>(&s_g[i][1][m]), G);
+              G = fma2(q2, *reinterpret_cast<const f2p*>(&s_g[i][2][m]), G);
+              float va, vb;
+              up2(fma2(L, ri, G), va, vb);
+              acc2 = fma2(pk2(ka ? a.wsub : 0.0f, kb ? a.wsub : 0.0f), pk2(va, vb), acc2);
             }
+            float ea, eb;
+            up2(acc2, ea, eb);
+            acc += ea + eb;
           } else {
             for (int m = mlo; m <= mhi; ++m) {
               const float r2 = fadd_x(dxy, s_dz2[i][m]);
