@@ -2015,7 +2015,7 @@ class Engine {
   bool stem_ = false, have_calc_ = false, have_freq_ = false, fd_stable_ = false, fused_ok_ = false;
   std::vector<float> hkx_, hky_;
   DevBuf<float> d_kx_, d_ky_;
-  DevBuf<float2> d_twx_[3], d_twy_[3], d_px_, d_py_, d_P_;
+  DevBuf<float2> d_twx_[6], d_twy_[6], d_px_, d_py_, d_P_;
   int forced_plan_ = -1, ckpt_ = 0;
   float last_device_ms_ = 0.0f;
   // detector model of the noisy image chain

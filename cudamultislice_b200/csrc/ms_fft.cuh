@@ -66,14 +66,34 @@ MS_D float2 twc(float2 x) {
   }
 }
 
+// Complex sum and difference of a butterfly on the packed FP32x2 pipe
+// (add/sub.rn.f32x2: both components in one instruction, correctly rounded).
+MS_D void addsub_packed(float2 a, float2 b, float2& s, float2& d) {
+  unsigned long long pa, pb, ps, pd;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(pa) : "f"(a.x), "f"(a.y));
+  asm("mov.b64 %0, {%1, %2};" : "=l"(pb) : "f"(b.x), "f"(b.y));
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(ps) : "l"(pa), "l"(pb));
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(pd) : "l"(pa), "l"(pb));
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(s.x), "=f"(s.y) : "l"(ps));
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(d.x), "=f"(d.y) : "l"(pd));
+}
+
 // Radix-2 DIF network on R registers: natural-order input, bit-reversed output.
-template <int R, int SPAN, bool INV>
+// PK: butterfly sums and differences on the packed FP32x2 pipe.
+template <int R, int SPAN, bool INV, bool PK>
 struct Dif {
   template <int START, int J>
   static MS_D void bfly(float2 (&x)[R]) {
     const float2 a = x[START + J], b = x[START + J + SPAN];
-    x[START + J] = cadd(a, b);
-    x[START + J + SPAN] = twc<J, 2 * SPAN, INV>(csub(a, b));
+    if constexpr (PK) {
+      float2 s, d;
+      addsub_packed(a, b, s, d);
+      x[START + J] = s;
+      x[START + J + SPAN] = twc<J, 2 * SPAN, INV>(d);
+    } else {
+      x[START + J] = cadd(a, b);
+      x[START + J + SPAN] = twc<J, 2 * SPAN, INV>(csub(a, b));
+    }
     if constexpr (J + 1 < SPAN)
       bfly<START, J + 1>(x);
     else if constexpr (START + 2 * SPAN < R)
@@ -81,20 +101,21 @@ struct Dif {
   }
   static MS_D void run(float2 (&x)[R]) {
     bfly<0, 0>(x);
-    if constexpr (SPAN > 1) Dif<R, SPAN / 2, INV>::run(x);
+    if constexpr (SPAN > 1) Dif<R, SPAN / 2, INV, PK>::run(x);
   }
 };
 
-template <int R, bool INV>
+template <int R, bool INV, bool PK = false>
 MS_D void dft(float2 (&x)[R]) {
-  if constexpr (R > 1) Dif<R, R / 2, INV>::run(x);
+  if constexpr (R > 1) Dif<R, R / 2, INV, PK>::run(x);
 }
 
 // A factorisation N = R1 * R2 * R3 * R4 (trailing radices 1 = absent) with E
 // points per thread; every radix divides E and is at most 32.
-template <int N_, int E_, int R1_, int R2_, int R3_ = 1, int R4_ = 1>
+template <int N_, int E_, int R1_, int R2_, int R3_ = 1, int R4_ = 1, bool PK_ = false>
 struct Plan {
   static constexpr int N = N_, E = E_, P = N_ / E_;
+  static constexpr bool PK = PK_;  // butterflies on the packed FP32x2 pipe
   static constexpr int R1 = R1_, R2 = R2_, R3 = R3_, R4 = R4_;
   static constexpr int NPASS = 1 + (R2_ > 1) + (R3_ > 1) + (R4_ > 1);
   static_assert(R1_ * R2_ * R3_ * R4_ == N_, "radices must multiply to N");
@@ -200,7 +221,7 @@ MS_D void forward_pass(float2 (&v)[PL::E], float2* __restrict__ sm, int t, const
       for (int r = 0; r < R; ++r) x[r] = sm[padi<PL>(i + r * (N / R))];
 #pragma unroll
       for (int r = 1; r < R; ++r) x[r] = cmul(x[r], tr.get(tw, b, r, i));
-      dft<R, false>(x);
+      dft<R, false, PL::PK>(x);
 #pragma unroll
       for (int q = 0; q < R; ++q) v[b + q * (E / R)] = x[brev(q, LR)];
     }
@@ -223,7 +244,7 @@ MS_D void forward_pass(float2 (&v)[PL::E], float2* __restrict__ sm, int t, const
       for (int r = 0; r < R; ++r) x[r] = v[b * R + r];
 #pragma unroll
       for (int r = 1; r < R; ++r) x[r] = cmul(x[r], tr.get(tw, b, r, k));
-      dft<R, false>(x);
+      dft<R, false, PL::PK>(x);
       const int base = (i / NS) * NS * R + k;
 #pragma unroll
       for (int q = 0; q < R; ++q) sm[padi<PL>(base + q * NS)] = x[brev(q, LR)];
@@ -244,7 +265,7 @@ MS_D void line_fft(float2 (&v)[PL::E], float2* __restrict__ sm, int t, const flo
     float2 x[R1];
 #pragma unroll
     for (int r = 0; r < R1; ++r) x[r] = v[b + r * (E / R1)];
-    dft<R1, false>(x);
+    dft<R1, false, PL::PK>(x);
     const int i = t + P * b;
 #pragma unroll
     for (int q = 0; q < R1; ++q) sm[padi<PL>(i * R1 + q)] = x[brev(q, L1)];

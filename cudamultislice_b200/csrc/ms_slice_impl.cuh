@@ -11,7 +11,8 @@ namespace ms {
 
 // FFT plan variants per line length (chosen at run time by the autotuner):
 // variant 0 keeps the most points per thread (fewest exchanges), higher
-// variants spread a line over more threads (more warps in flight).
+// variants spread a line over more threads (more warps in flight); variants
+// 3..5 are 0..2 with the butterflies on the packed FP32x2 pipe.
 template <int N, int V>
 struct PlanSel;
 template <> struct PlanSel<64, 0>   { using T = fft::Plan<64, 8, 8, 8>; };
@@ -32,8 +33,26 @@ template <> struct PlanSel<1024, 2> { using T = fft::Plan<1024, 8, 8, 8, 8, 2>; 
 template <> struct PlanSel<2048, 0> { using T = fft::Plan<2048, 32, 32, 8, 8>; };
 template <> struct PlanSel<2048, 1> { using T = fft::Plan<2048, 16, 16, 16, 8>; };
 template <> struct PlanSel<2048, 2> { using T = fft::Plan<2048, 8, 8, 8, 8, 4>; };
+template <> struct PlanSel<64, 3> { using T = fft::Plan<64, 8, 8, 8, 1, 1, true>; };
+template <> struct PlanSel<64, 4> { using T = fft::Plan<64, 4, 4, 4, 4, 1, true>; };
+template <> struct PlanSel<64, 5> { using T = fft::Plan<64, 4, 4, 4, 4, 1, true>; };
+template <> struct PlanSel<128, 3> { using T = fft::Plan<128, 16, 16, 8, 1, 1, true>; };
+template <> struct PlanSel<128, 4> { using T = fft::Plan<128, 8, 8, 4, 4, 1, true>; };
+template <> struct PlanSel<128, 5> { using T = fft::Plan<128, 4, 4, 4, 4, 2, true>; };
+template <> struct PlanSel<256, 3> { using T = fft::Plan<256, 16, 16, 16, 1, 1, true>; };
+template <> struct PlanSel<256, 4> { using T = fft::Plan<256, 8, 8, 8, 4, 1, true>; };
+template <> struct PlanSel<256, 5> { using T = fft::Plan<256, 4, 4, 4, 4, 4, true>; };
+template <> struct PlanSel<512, 3> { using T = fft::Plan<512, 32, 32, 16, 1, 1, true>; };
+template <> struct PlanSel<512, 4> { using T = fft::Plan<512, 16, 16, 8, 4, 1, true>; };
+template <> struct PlanSel<512, 5> { using T = fft::Plan<512, 8, 8, 8, 8, 1, true>; };
+template <> struct PlanSel<1024, 3> { using T = fft::Plan<1024, 32, 32, 32, 1, 1, true>; };
+template <> struct PlanSel<1024, 4> { using T = fft::Plan<1024, 16, 16, 16, 4, 1, true>; };
+template <> struct PlanSel<1024, 5> { using T = fft::Plan<1024, 8, 8, 8, 8, 2, true>; };
+template <> struct PlanSel<2048, 3> { using T = fft::Plan<2048, 32, 32, 8, 8, 1, true>; };
+template <> struct PlanSel<2048, 4> { using T = fft::Plan<2048, 16, 16, 16, 8, 1, true>; };
+template <> struct PlanSel<2048, 5> { using T = fft::Plan<2048, 8, 8, 8, 8, 4, true>; };
 
-constexpr int kPlanVariants = 3;
+constexpr int kPlanVariants = 6;
 
 // Threads per CTA: rows, 256 (whole lines); columns, at least 4 columns per
 // CTA so the transposing tile access moves whole 32-byte sectors (256 threads
@@ -539,6 +558,9 @@ int twiddles_n(int variant, float2* out);
       case 0: return dispatch_a_plan<PlanSel<N, 0>::T>(a, flags, batch, s);                          \
       case 1: return dispatch_a_plan<PlanSel<N, 1>::T>(a, flags, batch, s);                          \
       case 2: return dispatch_a_plan<PlanSel<N, 2>::T>(a, flags, batch, s);                          \
+      case 3: return dispatch_a_plan<PlanSel<N, 3>::T>(a, flags, batch, s);                          \
+      case 4: return dispatch_a_plan<PlanSel<N, 4>::T>(a, flags, batch, s);                          \
+      case 5: return dispatch_a_plan<PlanSel<N, 5>::T>(a, flags, batch, s);                          \
       default: return cudaErrorInvalidValue;                                                         \
     }                                                                                                \
   }                                                                                                  \
@@ -548,6 +570,9 @@ int twiddles_n(int variant, float2* out);
       case 0: return dispatch_b_plan<PlanSel<N, 0>::T>(a, mode, batch, s);                           \
       case 1: return dispatch_b_plan<PlanSel<N, 1>::T>(a, mode, batch, s);                           \
       case 2: return dispatch_b_plan<PlanSel<N, 2>::T>(a, mode, batch, s);                           \
+      case 3: return dispatch_b_plan<PlanSel<N, 3>::T>(a, mode, batch, s);                           \
+      case 4: return dispatch_b_plan<PlanSel<N, 4>::T>(a, mode, batch, s);                           \
+      case 5: return dispatch_b_plan<PlanSel<N, 5>::T>(a, mode, batch, s);                           \
       default: return cudaErrorInvalidValue;                                                         \
     }                                                                                                \
   }                                                                                                  \
@@ -557,6 +582,9 @@ int twiddles_n(int variant, float2* out);
       case 0: fill_twiddles<PlanSel<N, 0>::T>(out); return PlanSel<N, 0>::T::TWSIZE;                 \
       case 1: fill_twiddles<PlanSel<N, 1>::T>(out); return PlanSel<N, 1>::T::TWSIZE;                 \
       case 2: fill_twiddles<PlanSel<N, 2>::T>(out); return PlanSel<N, 2>::T::TWSIZE;                 \
+      case 3: fill_twiddles<PlanSel<N, 3>::T>(out); return PlanSel<N, 3>::T::TWSIZE;                 \
+      case 4: fill_twiddles<PlanSel<N, 4>::T>(out); return PlanSel<N, 4>::T::TWSIZE;                 \
+      case 5: fill_twiddles<PlanSel<N, 5>::T>(out); return PlanSel<N, 5>::T::TWSIZE;                 \
       default: return 0;                                                                             \
     }                                                                                                \
   }

@@ -88,7 +88,7 @@ class ManagedMultisliceSimulation:
         self._chk(self._L.ms_set_option(self._h, 2, int(bool(projected))))
 
     def SetFFTPlan(self, variant: int):
-        """-1: autotuned; 0..2: force a plan variant of the fused passes."""
+        """-1: autotuned; 0..5: force a plan variant of the fused passes (3..5: packed butterflies)."""
         self._chk(self._L.ms_set_option(self._h, 3, int(variant)))
 
     def SetCheckpoint(self, stride: int):

@@ -62,8 +62,10 @@ enum {
                                xy scan of binnedAtomPKernel2 U.cu:513-578) */
   MS_OPT_FFT_PLAN = 3,      /* -1 = autotuned (default): every FFT plan variant of the
                                fused passes is timed on the device once per grid and
-                               batch size and the fastest kept; 0..2 = force a variant
-                               (0: most points per thread ... 2: most threads per line) */
+                               batch size and the fastest kept; 0..5 = force a variant
+                               (0: most points per thread ... 2: most threads per line;
+                               3..5: 0..2 with butterflies on the packed FP32x2 pipe).
+                               Variants agree to FP32 rounding, not bit for bit. */
   MS_OPT_CHECKPOINT = 4     /* focal-series gradient: slices between stored waves;
                                0 = ceil(sqrt(S)) (default), 1 = store every wave,
                                >= S = one segment recomputed from the initial wave */

@@ -87,7 +87,7 @@ def test_atom_index_large(engine_cls, oracle_mod):
 
 
 # ---------------------------------------------------------------- FFT
-@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
 @pytest.mark.parametrize("shape", [(64, 64), (128, 256), (512, 512), (1024, 1024), (256, 64), (1024, 512),
                                    (2048, 2048), (64, 2048)])
 def test_fused_fft_against_numpy(engine_cls, shape, variant):
@@ -101,7 +101,7 @@ def test_fused_fft_against_numpy(engine_cls, shape, variant):
         assert rel_l2(out, ref) < 1e-6, (shape, sign, variant, rel_l2(out, ref))
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
 def test_exit_wave_every_fft_plan(engine_cls, oracle_mod, variant):
     eng, orc = make_pair(engine_cls, oracle_mod, sto(2, 4), 256, 0.05)
     eng.SetFFTPlan(variant)
