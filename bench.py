@@ -201,8 +201,15 @@ def stem_leg(fparams, device: int, nprobes: int = 256, batch: int = 0) -> dict:
         if name == "fused":
             out["signal_mean"] = float(np.mean(sig))
     sim.close()
+    step_s = 1.0 / (out["fused"]["probes_per_s"] * nsl)
+    algo = 32 * GRID * GRID  # per probe-slice step: psi r/w in both passes (t shared, L2)
+    peak, peak_kind = measured_peaks()
     return {"value": out["fused"]["probes_per_s"], "unit": "probes/s",
             "slice_steps_per_s": out["fused"]["probes_per_s"] * nsl,
+            "roofline": {"bound": "hbm", "achieved": algo / step_s / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": algo / step_s / 1e9 / peak, "peak_source": peak_kind,
+                         "algorithmic_bytes": "32 B per pixel per probe-slice step (wave read and written by "
+                                              "the row and the column pass; the shared transmission is an L2 hit)"},
             "plain_value": out["plain"]["probes_per_s"],
             "speedup_fused_vs_plain": out["fused"]["probes_per_s"] / out["plain"]["probes_per_s"],
             "config": f"GaN [11-20] 10x6x40 cells ({len(Z)} atoms), {GRID}^2, {nsl} slices of 1.5945 A, 300 kV, "
@@ -260,6 +267,73 @@ def mixed_leg(fparams, device: int, n1024: int = 256, n512: int = 256, batch: in
                       f"({n512} probes), 1.5945 A slices, 300 kV, 25 mrad, HAADF 70-200 mrad",
             "timing": "device time of one CUDA-graph launch: both rasters as concurrent branches, or one after "
                       "the other; value = the faster arrangement"}
+
+
+def c1_leg(fparams, device: int, reps: int = 20) -> dict:
+    """The reference's own small case: SrTiO3 4 x 4 x 20 cells (1,600 atoms),
+    256^2 over 15.62 A, 40 slices of 1.9525 A, 200 kV, exit wave.  The fused
+    slice loop is one CUDA-graph launch (ms_run_conventional); the plain path
+    runs the reference's launch sequence.  Device time of the slice loop,
+    potential stack resident."""
+    from cudamultislice_b200 import ManagedMultisliceSimulation
+    from cudamultislice_b200 import structures as S
+
+    n = 256
+    Z, x, y, z = S.srtio3(4, 4, 20)
+    sim = ManagedMultisliceSimulation(device=device)
+    sim.SetAtoms(Z, x, y, z)
+    sim.UploadBinnedAtoms()
+    sim.GetParameterisation(fparams)
+    sim.ApplyMicroscopeParameters(200.0, -500.0, 0.0, 0.0, 1.0e7, 0.1, 30.0, 20.0)
+    sim.SetCalculationVariables(3.905 * 4 / n, -500.0, n, n, sim.GetSizeX(), sim.GetSizeY(), sim.GetSizeZ(),
+                                2.0, 2.0)
+    sim.PreCalculateFrequencies()
+    sim.InitialiseWavefunctions(1.9525)
+    out = {}
+    for name, path in (("fused", 0), ("plain", 1)):
+        sim.SetSlicePath(path)
+        nsl = sim.RunConventional()
+        best = None
+        for _ in range(reps):
+            sim.RunConventional()
+            t = sim.LastDeviceMs()
+            best = t if best is None else min(best, t)
+        out[name] = nsl / (best / 1000.0)
+    sim.close()
+    return {"value": out["fused"], "unit": "slice-steps/s", "plain_value": out["plain"],
+            "speedup_fused_vs_plain": out["fused"] / out["plain"],
+            "config": f"SrTiO3 4x4x20 cells (1600 atoms), {n}^2, {nsl} slices of 1.9525 A, 200 kV",
+            "timing": "device time of the slice loop (best of 20; fused: one CUDA-graph launch)"}
+
+
+def fd_leg(fparams, device: int, steps: int = 40) -> dict:
+    """Finite-difference multislice on the bench workload's specimen (a-C
+    50 x 50 x 200 A, 1024^2, 300 kV) at dz = 0.5 A (the slice thickness / 4):
+    `steps` steps of MultisliceStep (potential plane, band limit, three-level
+    update) on the fused passes against the reference's launch sequence."""
+    from cudamultislice_b200 import ManagedMultisliceSimulation
+
+    atoms = workload()
+    sim = ManagedMultisliceSimulation(device=device)
+    configure(sim, atoms, fparams)
+    out = {}
+    for name, path in (("fused", 0), ("plain", 1)):
+        sim.SetSlicePath(path)
+        sim.InitialiseWavefunctions()
+        sim.SetFDdz(SLICE_DZ / 4)
+        sim.MultisliceStepFD(1)
+        sim.ExitWave()
+        t0 = time.perf_counter()
+        for i in range(2, steps + 2):
+            sim.MultisliceStepFD(i)
+        sim.ExitWave()
+        out[name] = steps / (time.perf_counter() - t0)
+    sim.SetSlicePath(0)
+    sim.close()
+    return {"value": out["fused"], "unit": "FD steps/s", "plain_value": out["plain"],
+            "speedup_fused_vs_plain": out["fused"] / out["plain"],
+            "config": "a-C 50x50x200 A (50k atoms), 1024^2, 300 kV, FD dz 0.5 A, potential plane built per step",
+            "timing": "host clock around the synchronous step calls"}
 
 
 def focal_profile_leg(fparams, device: int) -> dict:
@@ -464,7 +538,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="profiling mode: set-up plus the timed slice loop only (no e2e, plain or CPU legs)")
-    ap.add_argument("--leg", choices=["stem", "adjoint", "tds", "mixed", "focal_profile"],
+    ap.add_argument("--leg", choices=["stem", "adjoint", "tds", "mixed", "focal_profile", "c1", "fd"],
                     help="run one secondary leg alone and print its JSON (exploration)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
@@ -475,7 +549,7 @@ def main():
         from cudamultislice_b200 import FPARAMS
 
         leg = {"stem": stem_leg, "adjoint": adjoint_leg, "tds": tds_leg, "mixed": mixed_leg,
-               "focal_profile": focal_profile_leg}[args.leg](FPARAMS, local)
+               "focal_profile": focal_profile_leg, "c1": c1_leg, "fd": fd_leg}[args.leg](FPARAMS, local)
         if rank == 0:
             print(json.dumps({"leg": args.leg, **leg}), flush=True)
         return
@@ -581,6 +655,8 @@ def main():
         out["adjoint"] = adjoint_leg(FPARAMS, local)
         out["tds"] = tds_leg(FPARAMS, local)
         out["stem_mixed"] = mixed_leg(FPARAMS, local)
+        out["c1"] = c1_leg(FPARAMS, local)
+        out["fd"] = fd_leg(FPARAMS, local)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1

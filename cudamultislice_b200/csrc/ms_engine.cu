@@ -1304,14 +1304,18 @@ class Engine {
         }
         graph_S_ = S;
       }
+      MS_TRY(cudaEventRecord(ev0_, stream_));
       MS_TRY(cudaGraphLaunch(graph_exec_, stream_));
       launches += 2LL * S;
       domain_ = 1;
     } else {
+      MS_TRY(cudaEventRecord(ev0_, stream_));
       for (int it = 1; it <= S; ++it)
         if (int rc = transmit_propagate(d_stack_.p + (size_t)(it - 1) * nx_ * ny_, it == 1)) return rc;
     }
+    MS_TRY(cudaEventRecord(ev1_, stream_));
     MS_TRY(cudaStreamSynchronize(stream_));
+    MS_TRY(cudaEventElapsedTime(&last_device_ms_, ev0_, ev1_));
     if (nslices) *nslices = S;
     return MS_OK;
   }

@@ -296,7 +296,9 @@ ms_status ms_stem_raster_concurrent(ms_sim* const* sims, int nsims, const int* c
  * FFT plan `variant`, `batch` instances. */
 ms_status ms_time_pass(ms_sim* sim, int pass, int op, int variant, int batch, int reps, float* us);
 /* Device milliseconds (CUDA events on the handle's stream) of the last
- * focal-series call, from after the target upload to before the read-back. */
+ * focal-series call (from after the target upload to before the read-back),
+ * frozen-phonon series, concurrent raster, or ms_run_conventional (the slice
+ * loop: one graph launch on the fused path). */
 ms_status ms_get_last_device_ms(ms_sim* sim, float* out);
 ms_status ms_get_binned_counts(ms_sim* sim, int* n_atoms, int* n_zbins);
 ms_status ms_copy_binned(ms_sim* sim, int* offsets, int* Z, float* x, float* y, float* z);
