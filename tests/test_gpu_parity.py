@@ -467,3 +467,41 @@ def test_non_square_grid(engine_cls, oracle_mod, shape, path):
     assert rel_l2(eng.ExitWave(), orc.Wave()) < TOL
     eng.SimulateImage(0.0)
     assert rel_l2(eng.Image(), orc.SimulateImage()) < TOL
+
+
+# ---------------------------------------------------------------- errors of the newer entry points
+def test_new_entry_point_errors(engine_cls, oracle_mod, tmp_path):
+    from cudamultislice_b200 import MultisliceError, stem_raster_concurrent
+
+    eng, _ = make_pair(engine_cls, oracle_mod, sto(2, 2), 128, 0.1)
+    with pytest.raises(MultisliceError) as e:
+        eng.FrozenPhonon(1, 0, 0, 0.076)            # no configurations
+    assert e.value.code == 1
+    with pytest.raises(MultisliceError):
+        eng.FrozenPhonon(1, 0, 2, -1.0)             # negative sigma
+    with pytest.raises(MultisliceError) as e:
+        eng.SimulateImageSeries(np.array([np.inf], np.float32))
+    assert e.value.code == 1
+    with pytest.raises(MultisliceError):
+        eng.SetDetector(np.ones(4, np.float32), np.ones(4, np.float32), binning=0)
+    with pytest.raises(MultisliceError):
+        eng.SetDetector(-np.ones(4, np.float32), np.ones(4, np.float32))
+    with pytest.raises(MultisliceError) as e:
+        eng.WriteTIFF(9, str(tmp_path / "x.tiff"))
+    assert e.value.code == 1
+    with pytest.raises(MultisliceError) as e:
+        eng.WriteTIFF(0, str(tmp_path / "x.tiff"))  # no image simulated yet
+    assert e.value.code == 2
+    with pytest.raises(MultisliceError):
+        eng.MultisliceStepRS(0)
+    with pytest.raises(MultisliceError):
+        eng.SetCheckpoint(-1)
+    with pytest.raises(MultisliceError):
+        eng.TimePass(0, 32, 0)  # the finite-difference row pass is not a timing target
+    s, _ = make_pair(engine_cls, oracle_mod, sto(2, 2), 128, 0.1, stem=True)
+    with pytest.raises(MultisliceError):
+        stem_raster_concurrent([s], [(np.array([1], np.int32), np.array([1], np.int32))], 40.0, 10.0)
+    # the handle stays usable after the failures
+    eng.RunConventional()
+    eng.SimulateImage(0.0)
+    assert np.isfinite(eng.Image()).all()
