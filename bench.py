@@ -538,6 +538,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="profiling mode: set-up plus the timed slice loop only (no e2e, plain or CPU legs)")
+    ap.add_argument("--fft-plan", type=int, default=-1,
+                    help="profiling mode: force this FFT plan variant (default: the autotuner's choice)")
     ap.add_argument("--leg", choices=["stem", "adjoint", "tds", "mixed", "focal_profile", "c1", "fd"],
                     help="run one secondary leg alone and print its JSON (exploration)")
     args = ap.parse_args()
@@ -561,6 +563,8 @@ def main():
     configure(sim, atoms, FPARAMS)
     nsl = sim.BuildPotentialStack()
     assert nsl >= 100
+    if args.profile and args.fft_plan >= 0:
+        sim.SetFFTPlan(args.fft_plan)
     fft_plan = sim.FFTPlan(1)
     steps_per = 100
     for _ in range(max(args.warmup, 3)):
