@@ -43,22 +43,34 @@ UNIT = "slice-steps/s"
 BYTES_PER_PX_STEP = 20  # read+write psi (complex64) + read V (float)
 
 
-def workload():
+def workload(size=SIZE):
     from cudamultislice_b200 import structures as S
 
-    Z, x, y, z = S.amorphous_carbon(SIZE, density=0.1, min_sep=1.2)
+    Z, x, y, z = S.amorphous_carbon(size, density=0.1, min_sep=1.2)
     return Z, x, y, z
 
 
-def configure(sim, atoms, fparams):
+FORCED_PLAN = -1  # profiling: FFT plan variant forced on every leg's engine (-1: autotuned)
+
+
+def new_sim(device: int):
+    from cudamultislice_b200 import ManagedMultisliceSimulation
+
+    sim = ManagedMultisliceSimulation(device=device)
+    if FORCED_PLAN >= 0:
+        sim.SetFFTPlan(FORCED_PLAN)
+    return sim
+
+
+def configure(sim, atoms, fparams, grid=GRID):
     Z, x, y, z = atoms
     sim.SetAtoms(Z, x, y, z)
     sim.UploadBinnedAtoms()
     sim.GetParameterisation(fparams)
     sim.ApplyMicroscopeParameters(KV, 0.0, 0.0, 0.0, CS, 0.1, 30.0, 20.0)
     # pixel 0 at the structure's corner: offset = the 2 A box padding
-    ps = SIZE[0] / GRID
-    sim.SetCalculationVariables(ps, 0.0, GRID, GRID, sim.GetSizeX(), sim.GetSizeY(), sim.GetSizeZ(), 2.0, 2.0)
+    ps = SIZE[0] / grid
+    sim.SetCalculationVariables(ps, 0.0, grid, grid, sim.GetSizeX(), sim.GetSizeY(), sim.GetSizeZ(), 2.0, 2.0)
     sim.PreCalculateFrequencies()
     sim.InitialiseWavefunctions(SLICE_DZ)
 
@@ -172,11 +184,10 @@ def stem_leg(fparams, device: int, nprobes: int = 256, batch: int = 0) -> dict:
     position through all slices, including probe generation and detection."""
     import numpy as np
 
-    from cudamultislice_b200 import ManagedMultisliceSimulation
     from cudamultislice_b200 import structures as S
 
     Z, x, y, z = S.gan_wurtzite_11_20(10, 6, 40)
-    sim = ManagedMultisliceSimulation(device=device)
+    sim = new_sim(device)
     sim.SetAtoms(Z, x, y, z)
     sim.UploadBinnedAtoms()
     sim.GetParameterisation(fparams)
@@ -227,13 +238,13 @@ def mixed_leg(fparams, device: int, n1024: int = 256, n512: int = 256, batch: in
     rasters one after the other.  Device time."""
     import numpy as np
 
-    from cudamultislice_b200 import ManagedMultisliceSimulation, stem_raster_concurrent
+    from cudamultislice_b200 import stem_raster_concurrent
     from cudamultislice_b200 import structures as S
 
     sims, pos = [], []
     for cells, grid, nr, npr in (((10, 6, 40), 1024, 128, n1024), ((5, 3, 40), 512, 64, n512)):
         Z, x, y, z = S.gan_wurtzite_11_20(*cells)
-        sim = ManagedMultisliceSimulation(device=device)
+        sim = new_sim(device)
         sim.SetAtoms(Z, x, y, z)
         sim.UploadBinnedAtoms()
         sim.GetParameterisation(fparams)
@@ -275,12 +286,11 @@ def c1_leg(fparams, device: int, reps: int = 20) -> dict:
     slice loop is one CUDA-graph launch (ms_run_conventional); the plain path
     runs the reference's launch sequence.  Device time of the slice loop,
     potential stack resident."""
-    from cudamultislice_b200 import ManagedMultisliceSimulation
     from cudamultislice_b200 import structures as S
 
     n = 256
     Z, x, y, z = S.srtio3(4, 4, 20)
-    sim = ManagedMultisliceSimulation(device=device)
+    sim = new_sim(device)
     sim.SetAtoms(Z, x, y, z)
     sim.UploadBinnedAtoms()
     sim.GetParameterisation(fparams)
@@ -306,15 +316,59 @@ def c1_leg(fparams, device: int, reps: int = 20) -> dict:
             "timing": "device time of the slice loop (best of 20; fused: one CUDA-graph launch)"}
 
 
+def grid4096_leg(fparams, device: int, steps_per: int = 20, reps: int = 3) -> dict:
+    """The bench workload's specimen (a-C 50 x 50 x 200 A, 300 kV) sampled on
+    4096^2 (0.0122 A pixels): the conventional slice loop over the resident
+    potential stack (100 slices, 6.7 GB), fused passes against the plain path
+    (cuFFT + one kernel per operation).  Device time, inputs far above L2."""
+
+    n = 4096
+    sim = new_sim(device)
+    configure(sim, workload(), fparams, grid=n)
+    nsl = sim.BuildPotentialStack()
+    out = {}
+    for name, path in (("fused", 0), ("plain", 1)):
+        sim.SetSlicePath(path)
+        sim.TimeSlices(steps_per, 1, breakdown=False)
+        ms, _, _ = sim.TimeSlices(steps_per, reps, breakdown=False)
+        out[name] = steps_per * reps / (ms / 1000.0)
+    sim.SetSlicePath(0)
+    _, row_ms, col_ms = sim.TimeSlices(steps_per, 1, breakdown=True)
+    fft_plan = sim.FFTPlan(1)
+    sim.close()
+    peak, peak_kind = measured_peaks()
+    step_gbs = BYTES_PER_PX_STEP * n * n * out["fused"] / 1e9
+    return {"value": out["fused"], "unit": "slice-steps/s", "plain_value": out["plain"],
+            "speedup_fused_vs_plain": out["fused"] / out["plain"],
+            "row_pass_ms": row_ms, "col_pass_ms": col_ms,
+            "row_pass_gbs": 20 * n * n / (row_ms / 1000.0) / 1e9, "col_pass_gbs": 16 * n * n / (col_ms / 1000.0) / 1e9,
+            "step_achieved_gbs": step_gbs, "step_frac": step_gbs / peak, "peak_source": peak_kind,
+            "fft_plan": {"row_variant": fft_plan[0], "col_variant": fft_plan[1]},
+            "config": f"a-C 50x50x200 A, {n}^2, {nsl} slices of {SLICE_DZ} A, {KV:g} kV, potential stack resident",
+            "timing": f"device time, {reps} x {steps_per} slices after one untimed pass per path"}
+
+
+def grid4096_profile_leg(fparams, device: int, reps: int = 4) -> dict:
+    """A small case of the 4096^2 slice loop for kernel captures: a-C slab
+    50 x 50 x 16 A (8 slices of 2 A, 512 MB potential stack), 300 kV, fused
+    conventional slice loop, `reps` passes over the stack."""
+    n = 4096
+    sim = new_sim(device)
+    configure(sim, workload((50.0, 50.0, 16.0)), fparams, grid=n)
+    nsl = sim.BuildPotentialStack()
+    ms, _, _ = sim.TimeSlices(nsl, reps, breakdown=False)
+    sim.close()
+    return {"slices": nsl, "slice_steps_per_s": nsl * reps / (ms / 1000.0)}
+
+
 def fd_leg(fparams, device: int, steps: int = 40) -> dict:
     """Finite-difference multislice on the bench workload's specimen (a-C
     50 x 50 x 200 A, 1024^2, 300 kV) at dz = 0.5 A (the slice thickness / 4):
     `steps` steps of MultisliceStep (potential plane, band limit, three-level
     update) on the fused passes against the reference's launch sequence."""
-    from cudamultislice_b200 import ManagedMultisliceSimulation
 
     atoms = workload()
-    sim = ManagedMultisliceSimulation(device=device)
+    sim = new_sim(device)
     configure(sim, atoms, fparams)
     out = {}
     for name, path in (("fused", 0), ("plain", 1)):
@@ -342,12 +396,11 @@ def focal_profile_leg(fparams, device: int) -> dict:
     dL/dxy) -- one potential build per slice and one potential adjoint per slice."""
     import numpy as np
 
-    from cudamultislice_b200 import ManagedMultisliceSimulation
     from cudamultislice_b200 import structures as S
 
     n = 512
     Z, x, y, z = S.srtio3(4, 4, 10)
-    sim = ManagedMultisliceSimulation(device=device)
+    sim = new_sim(device)
     sim.SetAtoms(Z, x, y, z)
     sim.UploadBinnedAtoms()
     sim.GetParameterisation(fparams)
@@ -374,7 +427,6 @@ def adjoint_leg(fparams, device: int, reps: int = 3) -> dict:
     step; and the same pair with the potential stack resident (dL/dV only)."""
     import numpy as np
 
-    from cudamultislice_b200 import ManagedMultisliceSimulation
     from cudamultislice_b200 import structures as S
 
     n, nslices = 512, 100
@@ -382,7 +434,7 @@ def adjoint_leg(fparams, device: int, reps: int = 3) -> dict:
     Z, x, y, z = S.srtio3(4, 4, 50)
     rng = np.random.default_rng(2026)
     pert = [(a + rng.normal(0.0, 0.1, a.size)).astype(np.float32) for a in (x, y, z)]
-    sim = ManagedMultisliceSimulation(device=device)
+    sim = new_sim(device)
 
     def setup(xx, yy, zz):
         sim.SetAtoms(Z, xx, yy, zz)
@@ -438,12 +490,11 @@ def tds_leg(fparams, device: int, nconf: int = 16, batch: int = 16) -> dict:
     `batch` configurations per launch on the fused path, one at a time on the
     plain path.  Reports configurations/s and slice-steps/s (potential build
     included: every configuration has its own potentials)."""
-    from cudamultislice_b200 import ManagedMultisliceSimulation
     from cudamultislice_b200 import structures as S
 
     n = 512
     Z, x, y, z = S.silicon_110(8, 6, 50)
-    sim = ManagedMultisliceSimulation(device=device)
+    sim = new_sim(device)
     sim.SetAtoms(Z, x, y, z)
     sim.UploadBinnedAtoms()
     sim.GetParameterisation(fparams)
@@ -539,8 +590,9 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="profiling mode: set-up plus the timed slice loop only (no e2e, plain or CPU legs)")
     ap.add_argument("--fft-plan", type=int, default=-1,
-                    help="profiling mode: force this FFT plan variant (default: the autotuner's choice)")
-    ap.add_argument("--leg", choices=["stem", "adjoint", "tds", "mixed", "focal_profile", "c1", "fd"],
+                    help="profiling mode and --leg runs: force this FFT plan variant (default: the autotuner's choice)")
+    ap.add_argument("--leg", choices=["stem", "adjoint", "tds", "mixed", "focal_profile", "c1", "fd", "grid4096",
+                                       "grid4096_profile"],
                     help="run one secondary leg alone and print its JSON (exploration)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
@@ -550,8 +602,12 @@ def main():
     if args.leg:
         from cudamultislice_b200 import FPARAMS
 
+        global FORCED_PLAN
+        FORCED_PLAN = args.fft_plan
+
         leg = {"stem": stem_leg, "adjoint": adjoint_leg, "tds": tds_leg, "mixed": mixed_leg,
-               "focal_profile": focal_profile_leg, "c1": c1_leg, "fd": fd_leg}[args.leg](FPARAMS, local)
+               "focal_profile": focal_profile_leg, "c1": c1_leg, "fd": fd_leg,
+               "grid4096": grid4096_leg, "grid4096_profile": grid4096_profile_leg}[args.leg](FPARAMS, local)
         if rank == 0:
             print(json.dumps({"leg": args.leg, **leg}), flush=True)
         return
@@ -661,6 +717,7 @@ def main():
         out["stem_mixed"] = mixed_leg(FPARAMS, local)
         out["c1"] = c1_leg(FPARAMS, local)
         out["fd"] = fd_leg(FPARAMS, local)
+        out["grid4096"] = grid4096_leg(FPARAMS, local)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1

@@ -1422,7 +1422,7 @@ class Engine {
     if (!defoci || !targets || !loss || nd < 1) return fail(MS_ERR_INVALID, "need defoci, targets, loss and nd >= 1");
     for (int d = 0; d < nd; ++d)
       if (!std::isfinite(defoci[d])) return fail(MS_ERR_INVALID, "non-finite defocus");
-    if (!use_fused()) return fail(MS_ERR_UNSUPPORTED, "the focal series runs on the fused passes (grid 64..2048, powers of two)");
+    if (!use_fused()) return fail(MS_ERR_UNSUPPORTED, "the focal series runs on the fused passes (grid 64..4096, powers of two)");
     if (stem_) return fail(MS_ERR_UNSUPPORTED, "the focal series needs TEM calculation variables");
     if (int rc = require_potential_inputs()) return rc;
     int Sall = 0;

@@ -14,10 +14,11 @@ cudaError_t by_length(int n, F&& f) {
     case 512: return f(std::integral_constant<int, 512>());
     case 1024: return f(std::integral_constant<int, 1024>());
     case 2048: return f(std::integral_constant<int, 2048>());
+    case 4096: return f(std::integral_constant<int, 4096>());
     default: return cudaErrorInvalidValue;
   }
 }
-bool supported_length(int n) { return n >= 64 && n <= 2048 && (n & (n - 1)) == 0; }
+bool supported_length(int n) { return n >= 64 && n <= 4096 && (n & (n - 1)) == 0; }
 }  // namespace
 
 bool fused_supported(int nx, int ny) { return supported_length(nx) && supported_length(ny); }

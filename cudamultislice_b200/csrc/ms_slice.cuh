@@ -96,7 +96,7 @@ struct PassBArgs {
   long long batch_stride_wave;
 };
 
-// Line lengths 64..2048 (powers of two) in both directions.
+// Line lengths 64..4096 (powers of two) in both directions.
 bool fused_supported(int nx, int ny);
 // Number of FFT plan variants per line length (autotuned by the engine).
 int plan_variants();

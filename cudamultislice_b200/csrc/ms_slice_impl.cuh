@@ -33,6 +33,9 @@ template <> struct PlanSel<1024, 2> { using T = fft::Plan<1024, 8, 8, 8, 8, 2>; 
 template <> struct PlanSel<2048, 0> { using T = fft::Plan<2048, 32, 32, 8, 8>; };
 template <> struct PlanSel<2048, 1> { using T = fft::Plan<2048, 16, 16, 16, 8>; };
 template <> struct PlanSel<2048, 2> { using T = fft::Plan<2048, 8, 8, 8, 8, 4>; };
+template <> struct PlanSel<4096, 0> { using T = fft::Plan<4096, 32, 32, 32, 4>; };
+template <> struct PlanSel<4096, 1> { using T = fft::Plan<4096, 16, 16, 16, 16>; };
+template <> struct PlanSel<4096, 2> { using T = fft::Plan<4096, 16, 8, 8, 8, 8>; };
 template <> struct PlanSel<64, 3> { using T = fft::Plan<64, 8, 8, 8, 1, 1, true>; };
 template <> struct PlanSel<64, 4> { using T = fft::Plan<64, 4, 4, 4, 4, 1, true>; };
 template <> struct PlanSel<64, 5> { using T = fft::Plan<64, 4, 4, 4, 4, 1, true>; };
@@ -51,16 +54,21 @@ template <> struct PlanSel<1024, 5> { using T = fft::Plan<1024, 8, 8, 8, 8, 2, t
 template <> struct PlanSel<2048, 3> { using T = fft::Plan<2048, 32, 32, 8, 8, 1, true>; };
 template <> struct PlanSel<2048, 4> { using T = fft::Plan<2048, 16, 16, 16, 8, 1, true>; };
 template <> struct PlanSel<2048, 5> { using T = fft::Plan<2048, 8, 8, 8, 8, 4, true>; };
+template <> struct PlanSel<4096, 3> { using T = fft::Plan<4096, 32, 32, 32, 4, 1, true>; };
+template <> struct PlanSel<4096, 4> { using T = fft::Plan<4096, 16, 16, 16, 16, 1, true>; };
+template <> struct PlanSel<4096, 5> { using T = fft::Plan<4096, 16, 8, 8, 8, 8, true>; };
 
 constexpr int kPlanVariants = 6;
 
 // Threads per CTA: rows, 256 (whole lines); columns, at least 4 columns per
 // CTA so the transposing tile access moves whole 32-byte sectors (256 threads
-// for lines of at most 32 threads; wider tiles measured slower).
+// for lines of at most 32 threads; wider tiles measured slower).  Lines of 4096
+// points take 2 columns per CTA: 4 would hold 131 KB of shared memory, one CTA
+// per SM, with no other CTA's loads to overlap the transforms.
 template <class PL>
 __host__ __device__ constexpr int rows_per_cta() { return PL::P >= 256 ? 1 : 256 / PL::P; }
 template <class PL>
-__host__ __device__ constexpr int cols_per_cta() { return PL::P >= 64 ? 4 : 256 / PL::P; }
+__host__ __device__ constexpr int cols_per_cta() { return PL::P < 64 ? 256 / PL::P : PL::N >= 4096 ? 2 : 4; }
 // Column slots 16/CB points (mod 16) apart for CB <= 16 columns per CTA (1 for
 // more): a 16-lane phase of the transposing tile access covers 16/CB rows of
 // CB columns, whose 8-byte points then fall in distinct bank pairs.

@@ -80,7 +80,7 @@ def worst_wavefronts(N, E, radices):
 
 def test_plan_table_parsed():
     ps = plans()
-    assert len(ps) == 18
+    assert len(ps) == 21
     for n, v, N, E, radices in ps:
         assert n == N and v in (0, 1, 2)
         prod = 1

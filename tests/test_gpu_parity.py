@@ -89,7 +89,7 @@ def test_atom_index_large(engine_cls, oracle_mod):
 # ---------------------------------------------------------------- FFT
 @pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
 @pytest.mark.parametrize("shape", [(64, 64), (128, 256), (512, 512), (1024, 1024), (256, 64), (1024, 512),
-                                   (2048, 2048), (64, 2048)])
+                                   (2048, 2048), (64, 2048), (4096, 4096), (64, 4096), (4096, 256)])
 def test_fused_fft_against_numpy(engine_cls, shape, variant):
     rng = np.random.default_rng(7)
     a = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
@@ -444,7 +444,7 @@ def test_tiff_readouts(engine_cls, oracle_mod, tmp_path):
 
 # ---------------------------------------------------------------- non-square grids
 @pytest.mark.parametrize("path", [0, 1])
-@pytest.mark.parametrize("shape", [(256, 128), (128, 512)])
+@pytest.mark.parametrize("shape", [(256, 128), (128, 512), (4096, 64), (64, 4096)])
 def test_non_square_grid(engine_cls, oracle_mod, shape, path):
     """nx != ny: the row and column passes use different line lengths (and plans)."""
     nx, ny = shape
