@@ -112,7 +112,7 @@ MS_D void dft(float2 (&x)[R]) {
 
 // A factorisation N = R1 * R2 * R3 * R4 (trailing radices 1 = absent) with E
 // points per thread; every radix divides E and is at most 32.
-template <int N_, int E_, int R1_, int R2_, int R3_ = 1, int R4_ = 1, bool PK_ = false>
+template <int N_, int E_, int R1_, int R2_, int R3_ = 1, int R4_ = 1, bool PK_ = false, bool PAD_ = false>
 struct Plan {
   static constexpr int N = N_, E = E_, P = N_ / E_;
   static constexpr bool PK = PK_;  // butterflies on the packed FP32x2 pipe
@@ -123,8 +123,9 @@ struct Plan {
   static_assert(R1_ <= 32 && R2_ <= 32 && R3_ <= 32 && R4_ <= 32, "radix above 32");
   static_assert(P <= 32 || P % 32 == 0, "multi-warp lines need whole warps");
   // Shared-memory map of a line's points (see padi): an XOR swizzle for first
-  // radices 4 and 8 on lines of at least 16 threads, else one pad point every R1.
-  static constexpr bool XOR_MAP = (R1_ == 4 || R1_ == 8) && P >= 16;
+  // radices 4 and 8 on lines of at least 16 threads, else (or with PAD_) one
+  // pad point every R1.
+  static constexpr bool XOR_MAP = !PAD_ && (R1_ == 4 || R1_ == 8) && P >= 16;
   // Points in one line slot (slots 8 apart mod 16).
   static constexpr int SLOT = XOR_MAP ? N_ + 8 : ((N_ + N_ / R1_ + 15) / 16) * 16 + 8;
   // Twiddle table: pass p >= 2 holds R_p * Ns_p entries [r][k].
@@ -133,6 +134,12 @@ struct Plan {
   static constexpr int TWSIZE = TW4 + (R4_ > 1 ? R4_ * R1_ * R2_ * R3_ : 0);
   static_assert(TWSIZE <= 2 * N_, "twiddle table larger than 2N");
 };
+
+// The same plan on the padded map (the column pass's interleaved threads read
+// runs of 16/CW consecutive points per column, which the padded map keeps in
+// consecutive banks).
+template <class PL>
+using PaddedPlan = Plan<PL::N, PL::E, PL::R1, PL::R2, PL::R3, PL::R4, PL::PK, true>;
 
 // Slot position of point n.  A 64-bit access of 16 lanes is one wavefront when
 // its points fall in 16 distinct (point mod 16) classes.  Lines read 16
@@ -158,12 +165,17 @@ MS_D int padi(int n) {
 // else named barrier 1 + (line index in the CTA) over P threads, so that the
 // lines of a CTA do not wait for one another (lines are contiguous groups of
 // P threads; at most 4 lines of P > 32 per CTA).
-template <class PL>
+//
+// GS > 0 instead names a group of GS consecutive threads that share their
+// lines' exchanges (lines interleaved across the group's warps): the warp for
+// GS <= 32, else named barrier 1 + threadIdx.x / GS over GS threads.
+template <class PL, int GS = 0>
 MS_D void line_sync() {
-  if constexpr (PL::P <= 32)
+  constexpr int G = GS > 0 ? GS : PL::P;
+  if constexpr (G <= 32)
     __syncwarp();
   else
-    asm volatile("bar.sync %0, %1;" ::"r"(1 + (int)threadIdx.x / PL::P), "n"(PL::P) : "memory");
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + (int)threadIdx.x / G), "n"(G) : "memory");
 }
 
 // Radix R of pass number IDX (0-based).
@@ -204,14 +216,14 @@ struct TwiddleRegs {
 
 // Stockham pass IDX >= 1: the previous pass has written the slot but not yet
 // synchronised.  Forward transform only; the inverse is conj(FFT(conj(x))).
-template <class PL, int IDX>
+template <class PL, int IDX, int GS = 0>
 MS_D void forward_pass(float2 (&v)[PL::E], float2* __restrict__ sm, int t, const float2* __restrict__ tw) {
   constexpr int N = PL::N, E = PL::E, P = PL::P;
   constexpr int R = PassR<PL, IDX>::R, NS = PassR<PL, IDX>::NS, LR = ilog2(R);
   constexpr bool LAST = (IDX == PL::NPASS - 1);
   TwiddleRegs<PL, IDX> tr;
   tr.load(tw, t);
-  line_sync<PL>();
+  line_sync<PL, GS>();
   if constexpr (LAST) {
 #pragma unroll
     for (int b = 0; b < E / R; ++b) {
@@ -225,7 +237,7 @@ MS_D void forward_pass(float2 (&v)[PL::E], float2* __restrict__ sm, int t, const
 #pragma unroll
       for (int q = 0; q < R; ++q) v[b + q * (E / R)] = x[brev(q, LR)];
     }
-    line_sync<PL>();
+    line_sync<PL, GS>();
   } else {
     // read every input of this thread's butterflies, then overwrite the slot
 #pragma unroll
@@ -234,7 +246,7 @@ MS_D void forward_pass(float2 (&v)[PL::E], float2* __restrict__ sm, int t, const
 #pragma unroll
       for (int r = 0; r < R; ++r) v[b * R + r] = sm[padi<PL>(i + r * (N / R))];
     }
-    line_sync<PL>();
+    line_sync<PL, GS>();
 #pragma unroll
     for (int b = 0; b < E / R; ++b) {
       const int i = t + P * b;
@@ -249,15 +261,15 @@ MS_D void forward_pass(float2 (&v)[PL::E], float2* __restrict__ sm, int t, const
 #pragma unroll
       for (int q = 0; q < R; ++q) sm[padi<PL>(base + q * NS)] = x[brev(q, LR)];
     }
-    forward_pass<PL, IDX + 1>(v, sm, t, tw);
+    forward_pass<PL, IDX + 1, GS>(v, sm, t, tw);
   }
 }
 
 // Forward N-point transform of the line held by threads t = 0..P-1 of a
 // group.  `sm` is this line's shared slot (PL::SLOT points), `tw` the plan's
-// twiddle table.  Every thread of the warp (or, for P > 32, of the CTA) must
-// call this: it synchronises.  On return the slot may be reused.
-template <class PL>
+// twiddle table.  Every thread of the line's barrier group (line_sync<PL, GS>)
+// must call this: it synchronises.  On return the slot may be reused.
+template <class PL, int GS = 0>
 MS_D void line_fft(float2 (&v)[PL::E], float2* __restrict__ sm, int t, const float2* __restrict__ tw) {
   constexpr int E = PL::E, P = PL::P, R1 = PL::R1, L1 = ilog2(R1);
 #pragma unroll
@@ -270,7 +282,7 @@ MS_D void line_fft(float2 (&v)[PL::E], float2* __restrict__ sm, int t, const flo
 #pragma unroll
     for (int q = 0; q < R1; ++q) sm[padi<PL>(i * R1 + q)] = x[brev(q, L1)];
   }
-  forward_pass<PL, 1>(v, sm, t, tw);
+  forward_pass<PL, 1, GS>(v, sm, t, tw);
 }
 
 template <int E>

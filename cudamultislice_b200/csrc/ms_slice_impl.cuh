@@ -61,21 +61,34 @@ template <> struct PlanSel<4096, 5> { using T = fft::Plan<4096, 16, 8, 8, 8, 8, 
 constexpr int kPlanVariants = 6;
 
 // Threads per CTA: rows, 256 (whole lines); columns, at least 4 columns per
-// CTA so the transposing tile access moves whole 32-byte sectors (256 threads
-// for lines of at most 32 threads; wider tiles measured slower).  Lines of 4096
-// points take 2 columns per CTA: 4 would hold 131 KB of shared memory, one CTA
-// per SM, with no other CTA's loads to overlap the transforms.
+// CTA so that a warp's accesses cover whole 32-byte sectors (256 threads for
+// lines of at most 32 threads).
 template <class PL>
 __host__ __device__ constexpr int rows_per_cta() { return PL::P >= 256 ? 1 : 256 / PL::P; }
 template <class PL>
-__host__ __device__ constexpr int cols_per_cta() { return PL::P < 64 ? 256 / PL::P : PL::N >= 4096 ? 2 : 4; }
-// Column slots 16/CB points (mod 16) apart for CB <= 16 columns per CTA (1 for
-// more): a 16-lane phase of the transposing tile access covers 16/CB rows of
-// CB columns, whose 8-byte points then fall in distinct bank pairs.
+__host__ __device__ constexpr int cols_per_cta() { return PL::P < 64 ? 256 / PL::P : 4; }
+// Column CTAs resident per SM that the register budget is sized for: two,
+// unless that would leave fewer than 64 registers per thread for 16 or more
+// points per thread.
+template <class PL>
+__host__ __device__ constexpr int col_min_ctas() {
+  return cols_per_cta<PL>() * PL::P <= (PL::E <= 8 ? 512 : 256) ? 2 : 1;
+}
+// The column pass interleaves CW adjacent columns per warp row: thread
+// (column c, index t) is thread t * CW + c of its group, so every 8-byte load
+// and store of a warp covers CW columns of 32/CW rows (CW x 8 contiguous bytes
+// per row) straight from and to registers, with no staging tile.  The CW * P
+// threads of a group share their columns' exchange barriers.
+template <class PL>
+__host__ __device__ constexpr int col_interleave() { return cols_per_cta<PL>() < 8 ? cols_per_cta<PL>() : 8; }
+template <class PL>
+__host__ __device__ constexpr int col_group() { return col_interleave<PL>() * PL::P; }
+// Column slots (padded map, fft::PaddedPlan) 16/CW points (mod 16) apart: a
+// 16-lane phase covers 16/CW consecutive points of CW columns, which then fall
+// in distinct bank pairs.
 template <class PL>
 __host__ __device__ constexpr int col_slot() {
-  return (PL::XOR_MAP ? PL::N : ((PL::N + PL::N / PL::R1 + 15) / 16) * 16) +
-         (cols_per_cta<PL>() <= 16 ? 16 / cols_per_cta<PL>() : 1);
+  return ((PL::N + PL::N / PL::R1 + 15) / 16) * 16 + 16 / col_interleave<PL>();
 }
 
 // Programmatic dependent launch: the passes are launched with programmatic
@@ -258,6 +271,13 @@ __host__ __device__ constexpr bool col_uses_ky() {
 }
 template <int MODE>
 __host__ __device__ constexpr bool col_uses_py() { return MODE == B_PROPAGATE || MODE == B_PROPAGATE_ADJ; }
+// Columns of at most 1024 points stage ky and py in shared memory; longer
+// columns read them through L1, which keeps their CTAs' shared memory to the
+// exchange slots.
+template <class PL, int MODE>
+__host__ __device__ constexpr bool col_stages_ky() { return col_uses_ky<MODE>() && PL::N <= 1024; }
+template <class PL, int MODE>
+__host__ __device__ constexpr bool col_stages_py() { return col_uses_py<MODE>() && PL::N <= 1024; }
 
 template <class PL, int MODE>
 MS_D void col_mid(float2 (&v)[PL::E], const PassBArgs& a, const float* __restrict__ sky,
@@ -330,59 +350,50 @@ MS_D void col_mid(float2 (&v)[PL::E], const PassBArgs& a, const float* __restric
 }
 
 template <class PL, int MODE>
-__global__ void __launch_bounds__(cols_per_cta<PL>() * PL::P) k_pass_b(PassBArgs a) {
+__global__ void __launch_bounds__(cols_per_cta<PL>() * PL::P, col_min_ctas<PL>()) k_pass_b(PassBArgs a) {
   constexpr int NY = PL::N, E = PL::E, P = PL::P, CB = cols_per_cta<PL>(), LS = col_slot<PL>();
-  constexpr int NT = CB * P;
+  constexpr int NT = CB * P, CW = col_interleave<PL>(), GS = col_group<PL>();
   constexpr bool TWO = MODE == B_PROPAGATE || MODE == B_CTF || MODE == B_BANDLIMIT || MODE == B_FD ||
                       MODE == B_PROPAGATE_ADJ || MODE == B_CTF_ADJ;
   extern __shared__ float2 smem[];
   const int nx = a.nx;
   const int c0 = blockIdx.x * CB;
   const long long base = (long long)blockIdx.y * a.batch_stride_wave;
-  const float2* in = a.in + base;
   const float scale = a.scale;
+  const int g = threadIdx.x / GS, gr = threadIdx.x % GS;
+  const int cl = g * CW + gr % CW, t = gr / CW;
+  const int col = c0 + cl;
+  float2* sm = smem + cl * LS;
 
   // constant frequency tables for the pointwise work (written before any pass
   // runs, so they may be read before the predecessor completes)
-  float* sky = reinterpret_cast<float*>(smem + CB * LS);
-  float2* spy = smem + CB * LS + (col_uses_ky<MODE>() ? (NY + 1) / 2 : 0);
+  constexpr bool SKY = col_stages_ky<PL, MODE>(), SPY = col_stages_py<PL, MODE>();
+  float* sky_s = reinterpret_cast<float*>(smem + CB * LS);
+  float2* spy_s = smem + CB * LS + (SKY ? (NY + 1) / 2 : 0);
   pdl_launch_dependents();
-  if constexpr (col_uses_ky<MODE>()) {
-    for (int i = threadIdx.x; i < NY; i += NT) sky[i] = a.ky[i];
+  if constexpr (SKY) {
+    for (int i = threadIdx.x; i < NY; i += NT) sky_s[i] = a.ky[i];
   }
-  if constexpr (col_uses_py<MODE>()) {
-    for (int i = threadIdx.x; i < NY; i += NT) spy[i] = a.py[i];
+  if constexpr (SPY) {
+    for (int i = threadIdx.x; i < NY; i += NT) spy_s[i] = a.py[i];
   }
-  // transposing tile load: NY rows x CB columns -> one padded slot per column,
-  // E asynchronous 8-byte copies per thread, all in flight together
+  const float* sky = SKY ? sky_s : a.ky;
+  const float2* spy = SPY ? spy_s : a.py;
+  // this thread's E points of its column, rows t + P j, all loads in flight
   pdl_wait();
-#pragma unroll
-  for (int k = 0; k < E; ++k) {
-    const int idx = threadIdx.x + k * NT;
-    const int r = idx / CB, c = idx % CB;
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem + c * LS + fft::padi<PL>(r));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(in + (long long)r * nx + c0 + c)
-                 : "memory");
-  }
-  asm volatile("cp.async.commit_group;" ::: "memory");
-  asm volatile("cp.async.wait_group 0;" ::: "memory");
-  __syncthreads();
-
-  const int lane = threadIdx.x & 31;
-  const int cl = threadIdx.x / P, t = threadIdx.x % P;
-  const int col = c0 + cl;
-  float2* sm = smem + cl * LS;
+  const float2* src = a.in + base + (long long)t * nx + col;
+  const int step = P * nx;
   float2 v[E];
 #pragma unroll
-  for (int j = 0; j < E; ++j) v[j] = sm[fft::padi<PL>(t + P * j)];
-  fft::line_sync<PL>();
+  for (int j = 0; j < E; ++j) v[j] = src[j * step];
+  if constexpr (SKY || SPY) __syncthreads();  // tables of every group
 
   // iteration 0: forward (or, for B_INV_ONLY, the conjugated inverse) and the
   // pointwise work; iteration 1: the inverse as conj(FFT(conj(.)))
 #pragma unroll 1
   for (int it = 0; it < (TWO ? 2 : 1); ++it) {
     if (MODE == B_INV_ONLY) fft::conj_all(v);
-    fft::line_fft<PL>(v, sm, t, a.tw);
+    fft::line_fft<fft::PaddedPlan<PL>, GS>(v, sm, t, a.tw);
     if (it == 0) {
       if constexpr (MODE == B_INV_ONLY) {
         fft::conj_all(v);
@@ -422,24 +433,20 @@ __global__ void __launch_bounds__(cols_per_cta<PL>() * PL::P) k_pass_b(PassBArgs
     double d = (double)acc;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) d += __shfl_down_sync(0xffffffffu, d, o);
-    if (lane == 0 && d != 0.0) atomicAdd(a.sig + blockIdx.y, d * (double)scale);
+    if ((threadIdx.x & 31) == 0 && d != 0.0) atomicAdd(a.sig + blockIdx.y, d * (double)scale);
   } else {
-    // line_fft ended with a line barrier; slots are free again
-#pragma unroll
-    for (int j = 0; j < E; ++j) sm[fft::padi<PL>(t + P * j)] = v[j];
-    __syncthreads();
-    float2* out = a.out + base;
+    // natural order: v[j] is row t + P j of this thread's column.  The row
+    // step is passed through an opaque move so that the load addresses are
+    // recomputed here rather than held in registers across the transforms.
+    int ostep;
+    asm volatile("mov.b32 %0, %1;" : "=r"(ostep) : "r"(step));
+    float2* dst = a.out + base + (long long)t * nx + col;
     if (MODE == B_CTF_ADJ && a.accumulate) {
-      for (int idx = threadIdx.x; idx < NY * CB; idx += NT) {
-        const int r = idx / CB, c = idx % CB;
-        float2* o = out + (long long)r * nx + c0 + c;
-        *o = cadd(*o, smem[c * LS + fft::padi<PL>(r)]);
-      }
+#pragma unroll
+      for (int j = 0; j < E; ++j) dst[j * ostep] = cadd(dst[j * ostep], v[j]);
     } else {
-      for (int idx = threadIdx.x; idx < NY * CB; idx += NT) {
-        const int r = idx / CB, c = idx % CB;
-        out[(long long)r * nx + c0 + c] = smem[c * LS + fft::padi<PL>(r)];
-      }
+#pragma unroll
+      for (int j = 0; j < E; ++j) dst[j * ostep] = v[j];
     }
   }
 }
@@ -485,8 +492,8 @@ template <class PL, int MODE>
 cudaError_t run_b(const PassBArgs& a, int batch, cudaStream_t s) {
   constexpr int CB = cols_per_cta<PL>();
   const size_t smem = (size_t)CB * col_slot<PL>() * sizeof(float2) +
-                      (col_uses_ky<MODE>() ? (size_t)(PL::N + 1) / 2 * sizeof(float2) : 0) +
-                      (col_uses_py<MODE>() ? (size_t)PL::N * sizeof(float2) : 0);
+                      (col_stages_ky<PL, MODE>() ? (size_t)(PL::N + 1) / 2 * sizeof(float2) : 0) +
+                      (col_stages_py<PL, MODE>() ? (size_t)PL::N * sizeof(float2) : 0);
   if (a.nx % CB) return cudaErrorInvalidValue;
   static unsigned long long done = 0;
   if (attr_once(done)) {

@@ -7,7 +7,12 @@ through its exchanges: first-pass writes (R1 apart), middle-pass reads
 half-warp (16 lanes) is one wavefront when its points fall in 16 distinct
 (point mod 16) classes; lines shorter than 16 threads share a half-warp across
 slots SLOT points apart.  The plans that use the XOR map must be
-conflict-free."""
+conflict-free.
+
+The column pass (k_pass_b) runs the same plans on the padded map with CW
+columns interleaved per warp row (thread t * CW + c of a group owns index t
+of column c; slots 16/CW points mod 16 apart): every exchange of every plan
+must be conflict-free there too."""
 import os
 import re
 from collections import Counter
@@ -110,3 +115,55 @@ def test_map_is_a_permutation():
         P = N // E
         pos = {padi(k, radices[0], P) for k in range(N)}
         assert len(pos) == N and max(pos) < slot(N, radices[0], P)
+
+
+# ---- column pass: interleaved columns on the padded map (ms_slice_impl.cuh)
+def cols_per_cta(N, P):
+    return 256 // P if P < 64 else 4
+
+
+def col_interleave(N, P):
+    return min(cols_per_cta(N, P), 8)
+
+
+def col_slot(N, R1, P):
+    return ((N + N // R1 + 15) // 16) * 16 + 16 // col_interleave(N, P)
+
+
+def col_worst_wavefronts(N, E, radices):
+    P = N // E
+    R1 = radices[0]
+    CB, CW = cols_per_cta(N, P), col_interleave(N, P)
+    GS, LS = CW * P, col_slot(N, R1, P)
+    worst = 1
+
+    def lanes(point_of):
+        nonlocal worst
+        for h in range(0, CB * P, 16):
+            banks = Counter()
+            for tid in range(h, h + 16):
+                g, gr = divmod(tid, GS)
+                c, t = g * CW + gr % CW, gr // CW
+                banks[(c * LS + point_of(t) + point_of(t) // R1) % 16] += 1
+            worst = max(worst, max(banks.values()))
+
+    NS = 1
+    for p, R in enumerate(radices):
+        for b in range(E // R):
+            if p == 0:
+                for q in range(R):
+                    lanes(lambda t: (t + P * b) * R1 + q)
+            else:
+                for r in range(R):
+                    lanes(lambda t: (t + P * b) + r * (N // R))
+                if p < len(radices) - 1:
+                    for q in range(R):
+                        lanes(lambda t: ((t + P * b) // NS) * NS * R + ((t + P * b) & (NS - 1)) + q * NS)
+        NS *= R
+    return worst
+
+
+@pytest.mark.parametrize("plan", plans(), ids=lambda p: f"N{p[0]}v{p[1]}")
+def test_column_exchanges_conflict_free(plan):
+    n, v, N, E, radices = plan
+    assert col_worst_wavefronts(N, E, radices) == 1
