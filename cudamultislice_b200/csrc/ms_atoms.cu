@@ -156,6 +156,15 @@ __global__ void k_scan_add(int* __restrict__ out, int n, const int* __restrict__
 // r^2 < 5 A^2 evaluated in non-contracted FP32.
 // ---------------------------------------------------------------------------
 constexpr int kTX = 32, kTY = 8, kPotThreads = kTX * kTY;
+
+// Pixel of thread `tid` in the 32 x 8 tile: each warp covers an 8 x 4 patch
+// (patches 4 across, 2 down), so that the lanes of a warp lie close together
+// and agree on which atoms and sub-planes pass the cut-off.
+__device__ __forceinline__ void tile_pixel(int tid, int& tx, int& ty) {
+  const int w = tid >> 5, l = tid & 31;
+  tx = (w & 3) * 8 + (l & 7);
+  ty = (w >> 2) * 4 + (l >> 3);
+}
 constexpr int kChunk = 256;
 constexpr int kMaxSeg = 512;
 
@@ -233,7 +242,8 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a) {
 
   for (int i = threadIdx.x; i < 103 * kCoefPerZ; i += kPotThreads) s_coef[i] = a.coef[i];
 
-  const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
+  int tx, ty;
+  tile_pixel(threadIdx.x, tx, ty);
   const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY;
   const int x = x0 + tx, y = y0 + ty;
   const bool inside = (x < a.nx) && (y < a.ny);
@@ -363,6 +373,10 @@ __device__ __forceinline__ f2p ex2_pair(f2p a) {
 // exp(-pi^2 rho^2 / d_i) once per atom and, per sub-plane inside the cut-off,
 // one rsqrt and three exp2 for the Lorentzian terms.  Inside r < 0.25 A (the
 // clamp) the full vatom is evaluated.  Cut-offs stay non-contracted FP32.
+// Staging drops the candidates that no pixel of the tile can reach (kept
+// atoms keep their order, so every pixel sums the same terms in the same
+// order), and each warp (an 8 x 4 pixel patch) walks only the sub-planes that
+// its nearest pixel can reach.
 constexpr int kConvChunk = 64;
 
 __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
@@ -371,6 +385,7 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
   __shared__ __align__(8) float s_g[kConvChunk][3][20];
   __shared__ int s_mlo[kConvChunk], s_mhi[kConvChunk];
   __shared__ float s_dzmin[kConvChunk];
+  __shared__ int s_wcnt[kPotThreads / 32];
   __shared__ float s_coef[103 * kCoefPerZ];
   __shared__ int s_start[kMaxSeg];
   __shared__ int s_pref[kMaxSeg + 1];
@@ -378,12 +393,21 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
 
   for (int i = threadIdx.x; i < 103 * kCoefPerZ; i += kPotThreads) s_coef[i] = a.coef[i];
 
-  const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
+  int tx, ty;
+  tile_pixel(threadIdx.x, tx, ty);
   const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY;
   const int x = x0 + tx, y = y0 + ty;
   const bool inside = (x < a.nx) && (y < a.ny);
   const float px = fadd_x(a.xoff, fmul_x((float)x, a.ps));
   const float py = fadd_x(a.yoff, fmul_x((float)y, a.ps));
+  // the tile's pixel rectangle (the extreme pixel positions, as rounded above)
+  const float tx_lo = fadd_x(a.xoff, fmul_x((float)x0, a.ps));
+  const float tx_hi = fadd_x(a.xoff, fmul_x((float)(x0 + kTX - 1), a.ps));
+  const float ty_lo = fadd_x(a.yoff, fmul_x((float)y0, a.ps));
+  const float ty_hi = fadd_x(a.yoff, fmul_x((float)(y0 + kTY - 1), a.ps));
+  // sub-plane m sits at zsub[0] - m h: its index from a height, for the
+  // per-warp sub-plane window below
+  const float zs0 = a.zsub[0], inv_h = 19.0f / (a.zsub[0] - a.zsub[19]);
   const float xlo = a.xoff + x0 * a.ps - 2.2361f, xhi = a.xoff + (x0 + kTX - 1) * a.ps + 2.2361f;
   const float ylo = a.yoff + y0 * a.ps - 2.2361f, yhi = a.yoff + (y0 + kTY - 1) * a.ps + 2.2361f;
   const int bxl = max((int)floorf(xlo / a.bw_x) - 1, 0);
@@ -418,33 +442,53 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
       __syncthreads();
 
       for (int base = 0; base < total; base += kConvChunk) {
-        const int cnt = min(kConvChunk, total - base);
-        if (threadIdx.x < cnt) {
+        const int nload = min(kConvChunk, total - base);
+        // candidates of this round, kept when some sub-plane can pass the
+        // cut-off (dz_m^2 < 5) and the atom lies within sqrt(5) A of the tile's
+        // pixel rectangle (with a margin far above FP32 rounding, so that every
+        // dropped atom fails r^2 < 5 at every pixel); kept atoms stay in order
+        bool keep = false;
+        float4 at = make_float4(0.f, 0.f, 0.f, 0.f);
+        int amlo = 20, amhi = -1;
+        float dmin = 1e30f;
+        if (threadIdx.x < nload) {
           const int gidx = base + threadIdx.x;
           int lo = 0, hi = nseg - 1;
           while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
             if (s_pref[mid] <= gidx) lo = mid; else hi = mid - 1;
           }
-          const float4 at = a.atoms[s_start[lo] + (gidx - s_pref[lo])];
-          s_at[threadIdx.x] = at;
+          at = a.atoms[s_start[lo] + (gidx - s_pref[lo])];
           // sub-planes that can pass the cut-off for some pixel (dz_m^2 < 5: an
           // interval of m, since the non-contracted dz and dz^2 are monotone in
           // the plane height) and the smallest dz_m^2 (the clamp test below)
-          int mlo = 20, mhi = -1;
-          float dmin = 1e30f;
           for (int m = 0; m < 20; ++m) {
             const float dz = fsub_x(a.zsub[m], at.z);
             const float dz2 = fmul_x(dz, dz);
             if (dz2 < 5.0f) {
-              mlo = min(mlo, m);
-              mhi = m;
+              amlo = min(amlo, m);
+              amhi = m;
             }
             dmin = fminf(dmin, dz2);
           }
-          s_mlo[threadIdx.x] = mlo;
-          s_mhi[threadIdx.x] = mhi;
-          s_dzmin[threadIdx.x] = dmin;
+          const float ddx = fmaxf(0.0f, fmaxf(tx_lo - at.x, at.x - tx_hi));
+          const float ddy = fmaxf(0.0f, fmaxf(ty_lo - at.y, at.y - ty_hi));
+          keep = amlo <= amhi && ddx * ddx + ddy * ddy < 5.0005f;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        if ((threadIdx.x & 31) == 0) s_wcnt[threadIdx.x >> 5] = __popc(bal);
+        __syncthreads();
+        int pos = 0, cnt = 0;
+        for (int w = 0; w < kConvChunk / 32; ++w) {
+          if (w < (int)(threadIdx.x >> 5)) pos += s_wcnt[w];
+          cnt += s_wcnt[w];
+        }
+        if (keep) {
+          pos += __popc(bal & ((1u << (threadIdx.x & 31)) - 1u));
+          s_at[pos] = at;
+          s_mlo[pos] = amlo;
+          s_mhi[pos] = amhi;
+          s_dzmin[pos] = dmin;
         }
         __syncthreads();
         // per (atom, sub-plane): dz^2 as the cut-off rounds it, Gaussian factors
@@ -464,11 +508,18 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
           const float4 at = s_at[i];
           const float dx = fsub_x(px, at.x), dy = fsub_x(py, at.y);
           const float dxy = fadd_x(fmul_x(dx, dx), fmul_x(dy, dy));
+          // the warp's nearest pixel bounds the sub-planes any lane can use:
+          // |zsub[m] - z| < sqrt(5 - min dxy), widened by one plane each side
+          // (dxy >= 0, so its bits order as the values do)
+          const float wmin = __int_as_float(__reduce_min_sync(0xffffffffu, __float_as_int(dxy)));
+          if (!(wmin < 5.0f)) continue;
           if (!(dxy < 5.0f)) continue;
+          const float zr = sqrtf(5.0f - wmin);
+          const int mlo = max(s_mlo[i], (int)floorf((zs0 - at.z - zr) * inv_h) - 1);
+          const int mhi = min(s_mhi[i], (int)ceilf((zs0 - at.z + zr) * inv_h) + 1);
           const float* c = s_coef + (__float_as_int(at.w) - 1) * kCoefPerZ;
           const float g0 = c[6] * ex2_fast(-c[9] * dxy), g1 = c[7] * ex2_fast(-c[10] * dxy),
                       g2 = c[8] * ex2_fast(-c[11] * dxy);
-          const int mlo = s_mlo[i], mhi = s_mhi[i];
           if (!(fadd_x(dxy, s_dzmin[i]) < 0.0625f)) {
             // No sub-plane reaches the 0.25 A clamp for this pixel: sub-planes in
             // pairs (m, m+1) on the packed FP32x2 pipe.  add.rn.f32x2 rounds each
