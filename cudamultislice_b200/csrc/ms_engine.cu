@@ -231,8 +231,7 @@ class Engine {
     box_.MinZ = hz_[mnz] - 2;
     have_atoms_ = true;
     have_index_ = false;
-    stack_valid_ = false;
-    invalidate_graph();
+    stack_valid_ = false;  // (the slice-loop graph depends on the stack's allocation only)
     return MS_OK;
   }
 
@@ -272,7 +271,6 @@ class Engine {
     have_index_ = true;
     hzoff_.clear();
     stack_valid_ = false;
-    invalidate_graph();
     return MS_OK;
   }
 
@@ -1271,7 +1269,8 @@ class Engine {
       nstack_ = S;
       stack_valid_ = true;
       tstack_valid_ = false;
-      invalidate_graph();
+      // the slice-loop graph reads the stack at replay: it stays valid while
+      // the stack keeps its allocation (checked in run_conventional)
     }
     if (nslices) *nslices = S;
     return MS_OK;
@@ -1284,7 +1283,7 @@ class Engine {
     if (int rc = ensure_prop_tables(convdz_)) return rc;
     if (use_fused()) {
       plan_for(1);  // tune outside the capture (tuning allocates and synchronises)
-      if (!graph_exec_ || graph_S_ != S) {
+      if (!graph_exec_ || graph_S_ != S || graph_stack_ != d_stack_.p) {
         invalidate_graph();
         MS_TRY(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
         int rc = MS_OK;
@@ -1303,6 +1302,7 @@ class Engine {
           return fail(MS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
         }
         graph_S_ = S;
+        graph_stack_ = d_stack_.p;
       }
       MS_TRY(cudaEventRecord(ev0_, stream_));
       MS_TRY(cudaGraphLaunch(graph_exec_, stream_));
@@ -2055,6 +2055,7 @@ class Engine {
   int nstack_ = 0;
   cudaGraphExec_t graph_exec_ = nullptr;
   int graph_S_ = -1;
+  const float* graph_stack_ = nullptr;  // stack allocation the graph was captured on
   // host read-out
   std::vector<float2> ew_;
   float ew_min_ = 0, ew_max_ = 0;

@@ -234,8 +234,13 @@ class ManagedMultisliceSimulation:
         return self._f(self._L.ms_get_image_contrast, int(t), int(l), int(b), int(r))
 
     # ---- bulk and batched (new) ----
-    def ExitWave(self) -> np.ndarray:
-        out = np.zeros((self.ny, self.nx), np.complex64)
+    def ExitWave(self, out: np.ndarray | None = None) -> np.ndarray:
+        """The exit wave (ny, nx) complex64; `out` (C-contiguous, that shape and
+        dtype, e.g. a view of pinned host memory) receives it when given."""
+        if out is None:
+            out = np.empty((self.ny, self.nx), np.complex64)
+        elif out.shape != (self.ny, self.nx) or out.dtype != np.complex64 or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous complex64 array of shape {(self.ny, self.nx)}")
         self._chk(self._L.ms_copy_exit_wave(self._h, _ptr(out)))
         return out
 

@@ -137,6 +137,34 @@ def test_exit_wave_conventional(engine_cls, oracle_mod, path):
     assert e < TOL, e
 
 
+def test_run_after_new_atoms_matches_fresh_engine(engine_cls, oracle_mod):
+    """RunConventional after SetAtoms + UploadBinnedAtoms (same grid and slice
+    count: the slice-loop graph is reused over the rebuilt potential stack)
+    equals a fresh engine's run on the new atoms; ExitWave(out=...) fills the
+    caller's buffer."""
+    Z, x, y, z = sto(2, 5)
+    eng, _ = make_pair(engine_cls, oracle_mod, (Z, x, y, z), 128, 0.1)
+    eng.SetFFTPlan(3)  # both engines on one plan: bit-identical arithmetic
+    eng.RunConventional()
+    first = eng.ExitWave()
+    inner = (x > x.min() + 0.2) & (x < x.max() - 0.2)  # the box stays as it was
+    x2 = np.where(inner, x + np.float32(0.05), x).astype(np.float32)
+    eng.SetAtoms(Z, x2, y, z)
+    eng.UploadBinnedAtoms()
+    eng.InitialiseWavefunctions(1.9525)
+    eng.RunConventional()
+    buf = np.zeros((128, 128), np.complex64)
+    got = eng.ExitWave(out=buf)
+    assert got is buf
+    fresh, _ = make_pair(engine_cls, oracle_mod, (Z, x2, y, z), 128, 0.1)
+    fresh.SetFFTPlan(3)
+    fresh.RunConventional()
+    assert np.array_equal(buf, fresh.ExitWave())
+    assert not np.array_equal(buf, first)
+    with pytest.raises(ValueError):
+        eng.ExitWave(out=np.zeros((64, 128), np.complex64))
+
+
 def test_exit_wave_c1_srtio3_256(engine_cls, oracle_mod):
     # SrTiO3 4x4x20 cells, 256^2 over 15.62 A, 1.9525 A slices, 200 kV
     eng, orc = make_pair(engine_cls, oracle_mod, sto(4, 20), 256, 15.62 / 256)
