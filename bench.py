@@ -582,7 +582,7 @@ def config_dict(natoms: int) -> dict:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-slices", type=int, default=2, help="slices in the bounded CPU-baseline sample")
@@ -692,7 +692,7 @@ def main():
     out_host, out_t = pinned(np.zeros((GRID, GRID), np.complex64))
     h2d = Z.nbytes + x.nbytes + y.nbytes + z.nbytes
     e2e_times = []
-    for k in range(args.steps + 1):
+    for k in range(min(args.steps, 20) + 1):
         t0 = time.perf_counter()
         sim.SetAtoms(Z, x, y, z)
         sim.UploadBinnedAtoms()

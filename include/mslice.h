@@ -51,7 +51,7 @@ enum {
 /* Options (ms_set_option). */
 enum {
   MS_OPT_SLICE_PATH = 0,    /* 0 = fused hand-written FFT passes (default where the
-                               grid is a power of two 64..1024), 1 = plain path:
+                               grid is a power of two 64..4096), 1 = plain path:
                                cuFFT + one kernel per operation, the reference's
                                launch sequence (U.cu:2101-2122) */
   MS_OPT_ELEMENT_TABLE = 1, /* 0 = reference symbol table, unknown -> Z=1 (U.cu:1188-1243);
