@@ -1837,6 +1837,7 @@ class Engine {
     PassBArgs b{};
     b.in = in; b.out = out; b.tw = d_twy_[variant].p; b.px = d_px_.p; b.py = d_py_.p;
     b.kx = d_kx_.p; b.ky = d_ky_.p; b.kmax = kmax_; b.nx = nx_; b.ny = ny_; b.scale = 1.0f;
+    band_limit_thresholds(kmax_, &b.k2_lt, &b.k2_le);
     return b;
   }
   // Row / column pass launchers with the plan tuned for `batch` instances.

@@ -23,6 +23,19 @@ bool supported_length(int n) { return n >= 64 && n <= 4096 && (n & (n - 1)) == 0
 
 bool fused_supported(int nx, int ny) { return supported_length(nx) && supported_length(ny); }
 
+void band_limit_thresholds(float kmax, float* k2_lt, float* k2_le) {
+  auto first = [](float m, bool strict) {
+    // smallest x >= 0 with sqrtf(x) >= m (strict: > m); sqrtf is monotone
+    auto pass = [&](float x) { return strict ? std::sqrt(x) > m : std::sqrt(x) >= m; };
+    float x = (float)((double)m * (double)m);
+    while (x > 0.0f && pass(std::nextafter(x, 0.0f))) x = std::nextafter(x, 0.0f);
+    while (!pass(x)) x = std::nextafter(x, INFINITY);
+    return x;
+  };
+  *k2_lt = first(kmax, false);
+  *k2_le = first(kmax, true);
+}
+
 int plan_variants() { return kPlanVariants; }
 
 int make_twiddles(int n, int variant, float2* host_out) {

@@ -84,6 +84,10 @@ struct PassBArgs {
   const float* kx;     // FP32 reference frequencies (decisions)
   const float* ky;
   float kmax;
+  // the band-limit decisions as thresholds on k^2 = fadd(kx^2, ky^2), set by
+  // band_limit_thresholds(): sqrt_rn(k^2) < kmax  <=>  k^2 < k2_lt and
+  // sqrt_rn(k^2) <= kmax  <=>  k^2 < k2_le (sqrt_rn is monotone)
+  float k2_lt, k2_le;
   CtfParams ctf;
   float scale;         // B_CTF: factor on the weight; B_CBED: factor on |.|
   double* sig;         // B_DETECT: one FP64 sum per instance (blockIdx.y)
@@ -95,6 +99,12 @@ struct PassBArgs {
   int nx, ny;
   long long batch_stride_wave;
 };
+
+// The smallest FP32 k^2 with sqrt_rn(k^2) >= kmax (k2_lt) and with
+// sqrt_rn(k^2) > kmax (k2_le), found from kmax^2 by stepping one ulp at a time
+// against the host's correctly rounded sqrtf, so that a comparison of k^2
+// with them takes exactly the decisions of the rounded square root.
+void band_limit_thresholds(float kmax, float* k2_lt, float* k2_le);
 
 // Line lengths 64..4096 (powers of two) in both directions.
 bool fused_supported(int nx, int ny);

@@ -293,7 +293,7 @@ MS_D void col_mid(float2 (&v)[PL::E], const PassBArgs& a, const float* __restric
       const int n = t + P * j;
       const float ky = sky[n];
       // CreatePropsKernel (U.cu:419): keep sqrtf(kx^2+ky^2) < kmax
-      const bool keep = fsqrt_x(fadd_x(kx2, fmul_x(ky, ky))) < a.kmax;
+      const bool keep = fadd_x(kx2, fmul_x(ky, ky)) < a.k2_lt;
       const float2 w = keep ? cmul(pxv, spy[n]) : make_float2(0.f, 0.f);
       v[j] = cmul(v[j], w);
     }
@@ -305,7 +305,7 @@ MS_D void col_mid(float2 (&v)[PL::E], const PassBArgs& a, const float* __restric
     for (int j = 0; j < E; ++j) {
       const int n = t + P * j;
       const float ky = sky[n];
-      const bool keep = fsqrt_x(fadd_x(kx2, fmul_x(ky, ky))) < a.kmax;
+      const bool keep = fadd_x(kx2, fmul_x(ky, ky)) < a.k2_lt;
       const float2 w = keep ? cscale(cconj(cmul(pxv, spy[n])), scale) : make_float2(0.f, 0.f);
       v[j] = cmul(v[j], w);
     }
@@ -325,7 +325,7 @@ MS_D void col_mid(float2 (&v)[PL::E], const PassBArgs& a, const float* __restric
 #pragma unroll
     for (int j = 0; j < E; ++j) {
       const float ky = sky[t + P * j];
-      const bool keep = fsqrt_x(fadd_x(kx2, fmul_x(ky, ky))) <= a.kmax;
+      const bool keep = fadd_x(kx2, fmul_x(ky, ky)) < a.k2_le;  // sqrt(k^2) <= kmax
       v[j] = keep ? cscale(v[j], scale) : make_float2(0.f, 0.f);
     }
   } else if constexpr (MODE == B_FD) {
@@ -338,7 +338,7 @@ MS_D void col_mid(float2 (&v)[PL::E], const PassBArgs& a, const float* __restric
       const int n = t + P * j;
       const float ky = sky[n];
       const float ky2 = fmul_x(ky, ky);
-      const bool keep = fsqrt_x(fadd_x(kx2, ky2)) <= a.kmax;
+      const bool keep = fadd_x(kx2, ky2) < a.k2_le;  // sqrt(k^2) <= kmax
       const long long o = (long long)col * NY + n;  // spectrum kept column-major
       const float2 s0 = sp[o];
       const float k2 = kx * kx + ky * ky;
@@ -427,7 +427,7 @@ __global__ void __launch_bounds__(cols_per_cta<PL>() * PL::P, col_min_ctas<PL>()
       const int n = t + P * j;
       const float ky = sky[n];
       const float k2 = fadd_x(kx2, fmul_x(ky, ky));
-      const bool keep = fsqrt_x(k2) < a.kmax && k2 >= a.kin2 && k2 < a.kout2;
+      const bool keep = k2 < a.k2_lt && k2 >= a.kin2 && k2 < a.kout2;  // sqrt(k^2) < kmax
       if (keep) acc += v[j].x * v[j].x + v[j].y * v[j].y;
     }
     double d = (double)acc;
