@@ -333,33 +333,6 @@ __device__ __forceinline__ float ex2_fast(float x) {
   return y;
 }
 
-// Packed FP32x2 arithmetic of sm_100 (PTX add/mul/fma.rn.f32x2: two
-// independent, correctly rounded FP32 operations in one instruction) on pairs
-// held in 64-bit registers (low half = first value).
-typedef unsigned long long f2p;
-__device__ __forceinline__ f2p pk2(float lo, float hi) {
-  f2p r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-  return r;
-}
-__device__ __forceinline__ void up2(f2p v, float& lo, float& hi) {
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
-}
-__device__ __forceinline__ f2p add2(f2p a, f2p b) {
-  f2p d;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-__device__ __forceinline__ f2p mul2(f2p a, f2p b) {
-  f2p d;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-__device__ __forceinline__ f2p fma2(f2p a, f2p b, f2p c) {
-  f2p d;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-  return d;
-}
 __device__ __forceinline__ f2p ex2_pair(f2p a) {
   float lo, hi;
   up2(a, lo, hi);

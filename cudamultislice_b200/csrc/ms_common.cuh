@@ -57,4 +57,68 @@ MS_D void sincos_red(float x, float* s, float* c) {
   *c = ((q + 1) & 2) ? -cc : cc;
 }
 
+// Packed FP32x2 arithmetic of sm_100 (PTX add/mul/fma.rn.f32x2: two
+// independent, correctly rounded FP32 operations in one instruction) on pairs
+// held in 64-bit registers (low half = first value).
+typedef unsigned long long f2p;
+MS_D f2p pk2(float lo, float hi) {
+  f2p r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+MS_D void up2(f2p v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+MS_D f2p add2(f2p a, f2p b) {
+  f2p d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+MS_D f2p mul2(f2p a, f2p b) {
+  f2p d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+MS_D f2p fma2(f2p a, f2p b, f2p c) {
+  f2p d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
+// sin and cos of two values at once: sincos_red with its polynomial and
+// reduction steps on the packed FP32x2 pipe.  Each lane rounds exactly as the
+// scalar fmaf/multiply of sincos_red does, so the results are bit-identical.
+MS_D void sincos_red2(float x0, float x1, float* s0, float* c0, float* s1, float* c1) {
+  const f2p x = pk2(x0, x1);
+  float q0, q1;
+  up2(mul2(x, pk2(0.636619772f, 0.636619772f)), q0, q1);
+  const float k0 = rintf(q0), k1 = rintf(q1);
+  const f2p nk = pk2(-k0, -k1);
+  f2p r = fma2(nk, pk2(1.5707963705062866f, 1.5707963705062866f), x);
+  r = fma2(nk, pk2(-4.371138828673793e-08f, -4.371138828673793e-08f), r);
+  r = fma2(nk, pk2(-1.7763568394002505e-15f, -1.7763568394002505e-15f), r);
+  const f2p r2 = mul2(r, r);
+  f2p ps = fma2(r2, pk2(2.7557319223985893e-06f, 2.7557319223985893e-06f),
+                pk2(-1.984126984126984e-04f, -1.984126984126984e-04f));
+  ps = fma2(r2, ps, pk2(8.333333333333333e-03f, 8.333333333333333e-03f));
+  ps = fma2(r2, ps, pk2(-0.16666666666666666f, -0.16666666666666666f));
+  const f2p sn = fma2(mul2(r, r2), ps, r);
+  f2p pc = fma2(r2, pk2(-2.755731922398589e-07f, -2.755731922398589e-07f),
+                pk2(2.48015873015873e-05f, 2.48015873015873e-05f));
+  pc = fma2(r2, pc, pk2(-1.388888888888889e-03f, -1.388888888888889e-03f));
+  pc = fma2(r2, pc, pk2(4.1666666666666664e-02f, 4.1666666666666664e-02f));
+  pc = fma2(r2, pc, pk2(-0.5f, -0.5f));
+  const f2p cs = fma2(r2, pc, pk2(1.0f, 1.0f));
+  float sa, sb, ca, cb;
+  up2(sn, sa, sb);
+  up2(cs, ca, cb);
+  const int qa = ((int)k0) & 3, qb = ((int)k1) & 3;
+  const float ssa = (qa & 1) ? ca : sa, cca = (qa & 1) ? sa : ca;
+  const float ssb = (qb & 1) ? cb : sb, ccb = (qb & 1) ? sb : cb;
+  *s0 = (qa & 2) ? -ssa : ssa;
+  *c0 = ((qa + 1) & 2) ? -cca : cca;
+  *s1 = (qb & 2) ? -ssb : ssb;
+  *c1 = ((qb + 1) & 2) ? -ccb : ccb;
+}
+
 }  // namespace ms

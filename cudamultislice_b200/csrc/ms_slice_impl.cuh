@@ -69,7 +69,8 @@ template <class PL>
 __host__ __device__ constexpr int cols_per_cta() { return PL::P < 64 ? 256 / PL::P : 4; }
 // Column CTAs resident per SM that the register budget is sized for: two,
 // unless that would leave fewer than 64 registers per thread for 16 or more
-// points per thread.
+// points per thread.  (Left free, the compiler hoists the pointwise step's
+// table loads and the next pass's twiddles far enough to hold one CTA per SM.)
 template <class PL>
 __host__ __device__ constexpr int col_min_ctas() {
   return cols_per_cta<PL>() * PL::P <= (PL::E <= 8 ? 512 : 256) ? 2 : 1;
@@ -159,11 +160,13 @@ MS_D void row_mid(float2 (&v)[PL::E], const PassAArgs& a, const RowOperands<PL, 
     for (int j = 0; j < E; ++j) o[t + P * j] = v[j];
   }
   if constexpr ((FLAGS & A_MULT_T) != 0) {
+    // two points per packed sincos (bit-identical to sincos_red per point)
 #pragma unroll
-    for (int j = 0; j < E; ++j) {
-      float sn, cs;
-      sincos_red(fmul_x(a.sigma, op.V[j]), &sn, &cs);
-      v[j] = cmul(v[j], make_float2(cs, sn));
+    for (int j = 0; j < E; j += 2) {
+      float s0, c0, s1, c1;
+      sincos_red2(fmul_x(a.sigma, op.V[j]), fmul_x(a.sigma, op.V[j + 1]), &s0, &c0, &s1, &c1);
+      v[j] = cmul(v[j], make_float2(c0, s0));
+      v[j + 1] = cmul(v[j + 1], make_float2(c1, s1));
     }
   }
   if constexpr ((FLAGS & A_MULT_TC) != 0) {
@@ -205,7 +208,7 @@ MS_D void row_mid(float2 (&v)[PL::E], const PassAArgs& a, const RowOperands<PL, 
 }
 
 template <class PL, int FLAGS>
-__global__ void __launch_bounds__(rows_per_cta<PL>() * PL::P) k_pass_a(PassAArgs a) {
+MS_D void pass_a_body(PassAArgs a) {
   constexpr int NX = PL::N, E = PL::E, P = PL::P, LS = PL::SLOT;
   constexpr bool INVF = (FLAGS & A_INV) != 0, FWDF = (FLAGS & A_FWD) != 0;
   extern __shared__ float2 smem[];
@@ -451,6 +454,30 @@ __global__ void __launch_bounds__(cols_per_cta<PL>() * PL::P, col_min_ctas<PL>()
   }
 }
 
+// The row pass kernels: k_pass_a leaves registers to the compiler (32-point
+// plans then take more than 128, one CTA per SM), k_pass_a_cap sizes them for
+// row_cap_ctas CTAs (a little spilling can cost less than the lost overlap).
+// (The column pass, k_pass_b above, sizes every plan by col_min_ctas.)
+// Row CTAs per SM a capped row plan is sized for (0: left to the compiler).
+// Fewer registers cost latency hiding at one instance while more CTAs win in
+// batches, so each plan shape keeps one free twin and one capped twin and the
+// autotuner chooses: the unpacked 32-point plan is sized for two CTAs, the
+// packed 16-point plan for three; their twins stay free.
+template <class PL>
+constexpr int row_cap_ctas() { return (PL::E >= 32 && !PL::PK) ? 2 : (PL::E == 16 && PL::PK) ? 3 : 0; }
+template <class PL>
+constexpr bool capped_plan() { return row_cap_ctas<PL>() > 0; }
+
+template <class PL, int FLAGS>
+__global__ void __launch_bounds__(rows_per_cta<PL>() * PL::P) k_pass_a(PassAArgs a) {
+  pass_a_body<PL, FLAGS>(a);
+}
+template <class PL, int FLAGS>
+__global__ void __launch_bounds__(rows_per_cta<PL>() * PL::P, row_cap_ctas<PL>()) k_pass_a_cap(PassAArgs a) {
+  pass_a_body<PL, FLAGS>(a);
+}
+
+
 inline bool attr_once(unsigned long long& mask) {
   int dev = 0;
   cudaGetDevice(&dev);
@@ -480,12 +507,16 @@ cudaError_t run_a(const PassAArgs& a, int batch, cudaStream_t s) {
   constexpr int lines = rows_per_cta<PL>();
   const size_t smem = (size_t)lines * PL::SLOT * sizeof(float2);
   if (a.ny % lines) return cudaErrorInvalidValue;
+  auto kernel = [] {
+    if constexpr (capped_plan<PL>()) return k_pass_a_cap<PL, FLAGS>;
+    else return k_pass_a<PL, FLAGS>;
+  }();
   static unsigned long long done = 0;
   if (attr_once(done)) {
-    cudaError_t e = cudaFuncSetAttribute(k_pass_a<PL, FLAGS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  return launch_pdl(k_pass_a<PL, FLAGS>, dim3(a.ny / lines, batch), lines * PL::P, smem, s, a);
+  return launch_pdl(kernel, dim3(a.ny / lines, batch), lines * PL::P, smem, s, a);
 }
 
 template <class PL, int MODE>
@@ -495,12 +526,13 @@ cudaError_t run_b(const PassBArgs& a, int batch, cudaStream_t s) {
                       (col_stages_ky<PL, MODE>() ? (size_t)(PL::N + 1) / 2 * sizeof(float2) : 0) +
                       (col_stages_py<PL, MODE>() ? (size_t)PL::N * sizeof(float2) : 0);
   if (a.nx % CB) return cudaErrorInvalidValue;
+  auto kernel = k_pass_b<PL, MODE>;
   static unsigned long long done = 0;
   if (attr_once(done)) {
-    cudaError_t e = cudaFuncSetAttribute(k_pass_b<PL, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  return launch_pdl(k_pass_b<PL, MODE>, dim3(a.nx / CB, batch), CB * PL::P, smem, s, a);
+  return launch_pdl(kernel, dim3(a.nx / CB, batch), CB * PL::P, smem, s, a);
 }
 
 template <class PL>
