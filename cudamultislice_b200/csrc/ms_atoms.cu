@@ -503,12 +503,14 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
             const f2p n3 = pk2(-c[3], -c[3]), n4 = pk2(-c[4], -c[4]), n5 = pk2(-c[5], -c[5]);
             const f2p q0 = pk2(g0, g0), q1 = pk2(g1, g1), q2 = pk2(g2, g2);
             f2p acc2 = pk2(0.0f, 0.0f);
-            for (int m = mlo & ~1; m <= mhi; m += 2) {
+            // one pair (m, m+1) into acc; pairs with no sub-plane inside the
+            // cut-off for this pixel add nothing
+            auto pair = [&](int m, f2p& acc) {
               const f2p r2 = add2(d2, *reinterpret_cast<const f2p*>(&s_dz2[i][m]));
               float ra, rb;
               up2(r2, ra, rb);
               const bool ka = ra < 5.0f, kb = rb < 5.0f;
-              if (!(ka || kb)) continue;
+              if (!(ka || kb)) return;
               const f2p ri = pk2(rsqrtf(ra), rsqrtf(rb));
               const f2p r = mul2(r2, ri);
               f2p L = mul2(c0, ex2_pair(mul2(n3, r)));
@@ -519,8 +521,18 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
               G = fma2(q2, *reinterpret_cast<const f2p*>(&s_g[i][2][m]), G);
               float va, vb;
               up2(fma2(L, ri, G), va, vb);
-              acc2 = fma2(pk2(ka ? a.wsub : 0.0f, kb ? a.wsub : 0.0f), pk2(va, vb), acc2);
+              acc = fma2(pk2(ka ? a.wsub : 0.0f, kb ? a.wsub : 0.0f), pk2(va, vb), acc);
+            };
+            // two pairs per step into two sums: independent chains for the
+            // scheduler (the even pair's sum, then the odd pair's, per lane)
+            f2p acc2b = pk2(0.0f, 0.0f);
+            int m = mlo & ~1;
+            for (; m + 2 <= mhi; m += 4) {
+              pair(m, acc2);
+              pair(m + 2, acc2b);
             }
+            if (m <= mhi) pair(m, acc2);
+            acc2 = add2(acc2, acc2b);
             float ea, eb;
             up2(acc2, ea, eb);
             acc += ea + eb;
