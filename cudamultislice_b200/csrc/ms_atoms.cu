@@ -235,12 +235,13 @@ template <int KIND>
 __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a) {
   constexpr int NSUB = (KIND == POT_CONVENTIONAL) ? 20 : (KIND == POT_RS) ? 10 : 1;
   __shared__ float4 s_at[kChunk];
-  __shared__ float s_coef[103 * kCoefPerZ];
   __shared__ int s_start[kMaxSeg];
   __shared__ int s_pref[kMaxSeg + 1];
   __shared__ int s_warp[33];
+  __shared__ int s_wcnt[kPotThreads / 32];
 
-  for (int i = threadIdx.x; i < 103 * kCoefPerZ; i += kPotThreads) s_coef[i] = a.coef[i];
+  // (coefficients are read through L1 per atom: a tile meets few elements, and
+  // staging the whole 103-element table cost more than the plane's terms)
 
   int tx, ty;
   tile_pixel(threadIdx.x, tx, ty);
@@ -251,6 +252,11 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a) {
   // pixel position, rounded exactly as the host definition (no FMA)
   const float px = fadd_x(a.xoff, fmul_x((float)x, a.ps));
   const float py = fadd_x(a.yoff, fmul_x((float)y, a.ps));
+  // the tile's pixel rectangle (the extreme pixel positions, as rounded above)
+  const float tx_lo = fadd_x(a.xoff, fmul_x((float)x0, a.ps));
+  const float tx_hi = fadd_x(a.xoff, fmul_x((float)(x0 + kTX - 1), a.ps));
+  const float ty_lo = fadd_x(a.yoff, fmul_x((float)y0, a.ps));
+  const float ty_hi = fadd_x(a.yoff, fmul_x((float)(y0 + kTY - 1), a.ps));
 
   // candidate bins of the tile (conservative: sqrt(5) + one bin)
   const float xlo = a.xoff + x0 * a.ps - 2.2361f, xhi = a.xoff + (x0 + kTX - 1) * a.ps + 2.2361f;
@@ -290,23 +296,54 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a) {
       __syncthreads();
 
       for (int base = 0; base < total; base += kChunk) {
-        const int cnt = min(kChunk, total - base);
-        if (threadIdx.x < cnt) {
+        const int nload = min(kChunk, total - base);
+        // candidates of this round, kept when some pixel of the tile can take
+        // a term from them: within sqrt(5) A of the tile's pixel rectangle
+        // with the nearest sub-plane (margin far above FP32 rounding), and in
+        // the slab for the projected form.  Kept atoms stay in order, so every
+        // pixel sums the same terms in the same order.
+        bool keep = false;
+        float4 at = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (threadIdx.x < nload) {
           const int gidx = base + threadIdx.x;
           int lo = 0, hi = nseg - 1;  // last segment with s_pref <= gidx
           while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
             if (s_pref[mid] <= gidx) lo = mid; else hi = mid - 1;
           }
-          s_at[threadIdx.x] = a.atoms[s_start[lo] + (gidx - s_pref[lo])];
+          at = a.atoms[s_start[lo] + (gidx - s_pref[lo])];
+          const float ddx = fmaxf(0.0f, fmaxf(tx_lo - at.x, at.x - tx_hi));
+          const float ddy = fmaxf(0.0f, fmaxf(ty_lo - at.y, at.y - ty_hi));
+          float reach = ddx * ddx + ddy * ddy;
+          if constexpr (KIND == POT_PROJECTED) {
+            keep = (int)floorf(fdiv_x(fsub_x(a.top, at.z), a.slab_dz)) == a.slab && reach < 5.0005f;
+          } else {
+            float dz2 = 1e30f;
+#pragma unroll
+            for (int m = 0; m < NSUB; ++m) {
+              const float dz = a.zsub[m] - at.z;
+              dz2 = fminf(dz2, dz * dz);
+            }
+            keep = reach + dz2 < 5.0005f;
+          }
         }
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        if ((threadIdx.x & 31) == 0) s_wcnt[threadIdx.x >> 5] = __popc(bal);
+        __syncthreads();
+        int pos = 0, cnt = 0;
+#pragma unroll
+        for (int w = 0; w < kPotThreads / 32; ++w) {
+          if (w < (int)(threadIdx.x >> 5)) pos += s_wcnt[w];
+          cnt += s_wcnt[w];
+        }
+        if (keep) s_at[pos + __popc(bal & ((1u << (threadIdx.x & 31)) - 1u))] = at;
         __syncthreads();
         for (int i = 0; i < cnt; ++i) {
           const float4 at = s_at[i];
           const float dx = fsub_x(px, at.x), dy = fsub_x(py, at.y);
           const float dxy = fadd_x(fmul_x(dx, dx), fmul_x(dy, dy));
           if (!(dxy < 5.0f)) continue;
-          const float* c = s_coef + (__float_as_int(at.w) - 1) * kCoefPerZ;
+          const float* c = a.coef + (__float_as_int(at.w) - 1) * kCoefPerZ;
           if constexpr (KIND == POT_PROJECTED) {
             const int slab = (int)floorf(fdiv_x(fsub_x(a.top, at.z), a.slab_dz));
             if (slab == a.slab) acc += vzatom2_f(c, dxy);
