@@ -524,9 +524,9 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
           const float wmin = __int_as_float(__reduce_min_sync(0xffffffffu, __float_as_int(dxy)));
           if (!(wmin < 5.0f)) continue;
           if (!(dxy < 5.0f)) continue;
-          const float zr = sqrtf(5.0f - wmin);
-          const int mlo = max(s_mlo[i], (int)floorf((zs0 - at.z - zr) * inv_h) - 1);
-          const int mhi = min(s_mhi[i], (int)ceilf((zs0 - at.z + zr) * inv_h) + 1);
+          const float w5 = 5.0f - wmin, zr = w5 * rsqrtf(w5);  // (approximate: one plane of margin)
+          const int mlo = max(s_mlo[i], __float2int_rd((zs0 - at.z - zr) * inv_h) - 1);
+          const int mhi = min(s_mhi[i], __float2int_ru((zs0 - at.z + zr) * inv_h) + 1);
           const float* c = s_coef + (__float_as_int(at.w) - 1) * kCoefPerZ;
           const float g0 = c[6] * ex2_fast(-c[9] * dxy), g1 = c[7] * ex2_fast(-c[10] * dxy),
                       g2 = c[8] * ex2_fast(-c[11] * dxy);
