@@ -60,13 +60,21 @@ template <> struct PlanSel<4096, 5> { using T = fft::Plan<4096, 16, 8, 8, 8, 8, 
 
 constexpr int kPlanVariants = 6;
 
-// Threads per CTA: rows, 256 (whole lines); columns, at least 4 columns per
-// CTA so that a warp's accesses cover whole 32-byte sectors (256 threads for
-// lines of at most 32 threads).
+// Threads per CTA: rows, 256 (whole lines); columns, 4 columns per CTA for
+// lines of 64 or more threads (256 threads for shorter lines), so that a
+// warp's accesses cover whole 32-byte sectors, halved for the narrow plans.
 template <class PL>
 __host__ __device__ constexpr int rows_per_cta() { return PL::P >= 256 ? 1 : 256 / PL::P; }
+// The packed 32-point column plans take half the columns per CTA: twice the
+// CTAs, which a single instance (one wave) needs, and registers enough for
+// two CTAs without spilling; their unpacked twins keep the wide tiles that
+// win in batches (the autotuner chooses per batch).
 template <class PL>
-__host__ __device__ constexpr int cols_per_cta() { return PL::P < 64 ? 256 / PL::P : 4; }
+__host__ __device__ constexpr bool narrow_cols() { return PL::PK && PL::E >= 32; }
+template <class PL>
+__host__ __device__ constexpr int cols_per_cta() {
+  return (PL::P < 64 ? 256 / PL::P : 4) / (narrow_cols<PL>() ? 2 : 1);
+}
 // Column CTAs resident per SM that the register budget is sized for: two,
 // unless that would leave fewer than 64 registers per thread for 16 or more
 // points per thread.  (Left free, the compiler hoists the pointwise step's

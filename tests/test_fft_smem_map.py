@@ -24,10 +24,14 @@ from tests.conftest import ROOT
 IMPL = os.path.join(ROOT, "cudamultislice_b200", "csrc", "ms_slice_impl.cuh")
 
 
-def plans():
+def plans(packed=False):
+    """(length, variant, N, E, radices) of every PlanSel entry; the packed
+    variants (3..5, butterflies on FP32x2) with packed=True."""
     text = open(IMPL).read()
     out = []
-    for m in re.finditer(r"PlanSel<(\d+), (\d)>\s*\{ using T = fft::Plan<([\d, ]+)>; \}", text):
+    pat = (r"PlanSel<(\d+), (\d)>\s*\{ using T = fft::Plan<([\d, ]+), true>; \}" if packed else
+           r"PlanSel<(\d+), (\d)>\s*\{ using T = fft::Plan<([\d, ]+)>; \}")
+    for m in re.finditer(pat, text):
         args = [int(v) for v in m.group(3).split(",")]
         N, E, radices = args[0], args[1], [r for r in args[2:] if r > 1]
         out.append((int(m.group(1)), int(m.group(2)), N, E, radices))
@@ -85,9 +89,9 @@ def worst_wavefronts(N, E, radices):
 
 def test_plan_table_parsed():
     ps = plans()
-    assert len(ps) == 21
-    for n, v, N, E, radices in ps:
-        assert n == N and v in (0, 1, 2)
+    assert len(ps) == 21 and len(plans(packed=True)) == 21
+    for n, v, N, E, radices in ps + plans(packed=True):
+        assert n == N and v in (0, 1, 2, 3, 4, 5)
         prod = 1
         for r in radices:
             prod *= r
@@ -118,23 +122,23 @@ def test_map_is_a_permutation():
 
 
 # ---- column pass: interleaved columns on the padded map (ms_slice_impl.cuh)
-def cols_per_cta(N, P):
-    return 256 // P if P < 64 else 4
+def cols_per_cta(N, P, narrow=False):
+    return (256 // P if P < 64 else 4) // (2 if narrow else 1)
 
 
-def col_interleave(N, P):
-    return min(cols_per_cta(N, P), 8)
+def col_interleave(N, P, narrow=False):
+    return min(cols_per_cta(N, P, narrow), 8)
 
 
-def col_slot(N, R1, P):
-    return ((N + N // R1 + 15) // 16) * 16 + 16 // col_interleave(N, P)
+def col_slot(N, R1, P, narrow=False):
+    return ((N + N // R1 + 15) // 16) * 16 + 16 // col_interleave(N, P, narrow)
 
 
-def col_worst_wavefronts(N, E, radices):
+def col_worst_wavefronts(N, E, radices, narrow=False):
     P = N // E
     R1 = radices[0]
-    CB, CW = cols_per_cta(N, P), col_interleave(N, P)
-    GS, LS = CW * P, col_slot(N, R1, P)
+    CB, CW = cols_per_cta(N, P, narrow), col_interleave(N, P, narrow)
+    GS, LS = CW * P, col_slot(N, R1, P, narrow)
     worst = 1
 
     def lanes(point_of):
@@ -163,7 +167,8 @@ def col_worst_wavefronts(N, E, radices):
     return worst
 
 
-@pytest.mark.parametrize("plan", plans(), ids=lambda p: f"N{p[0]}v{p[1]}")
+@pytest.mark.parametrize("plan", plans() + plans(packed=True), ids=lambda p: f"N{p[0]}v{p[1]}")
 def test_column_exchanges_conflict_free(plan):
+    # the packed 32-point plans run narrow (half the columns per CTA)
     n, v, N, E, radices = plan
-    assert col_worst_wavefronts(N, E, radices) == 1
+    assert col_worst_wavefronts(N, E, radices, narrow=v >= 3 and E >= 32) == 1
