@@ -203,14 +203,17 @@ MS_D void row_mid(float2 (&v)[PL::E], const PassAArgs& a, const RowOperands<PL, 
     float* dV = a.out_f + r0;
     const float m2s = -2.0f * a.sigma;
 #pragma unroll
-    for (int j = 0; j < E; ++j) {
-      const int x = t + P * j;
-      float sn, cs;
-      sincos_red(fmul_x(a.sigma, op.V[j]), &sn, &cs);
-      const float2 tt = make_float2(cs, sn);
-      const float2 q = cmul(tt, op.w(a, row0, j, t));
-      dV[x] = m2s * (v[j].x * q.y - v[j].y * q.x);
-      v[j] = cmul(cconj(tt), v[j]);
+    for (int j = 0; j < E; j += 2) {
+      float s0, c0, s1, c1;
+      sincos_red2(fmul_x(a.sigma, op.V[j]), fmul_x(a.sigma, op.V[j + 1]), &s0, &c0, &s1, &c1);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int jj = j + h, x = t + P * jj;
+        const float2 tt = h ? make_float2(c1, s1) : make_float2(c0, s0);
+        const float2 q = cmul(tt, op.w(a, row0, jj, t));
+        dV[x] = m2s * (v[jj].x * q.y - v[jj].y * q.x);
+        v[jj] = cmul(cconj(tt), v[jj]);
+      }
     }
   }
 }
