@@ -1073,7 +1073,7 @@ class Engine {
     }
     rs_n_ = n;
     rs_B_ = std::min(batch, n);
-    plan_for(rs_B_);
+    plan_for(rs_B_, true);
     MS_TRY(d_bwave_.resize((size_t)rs_B_ * N));
     MS_TRY(d_bpos_.resize(2 * (size_t)n));
     MS_TRY(d_bsig_.resize(2 * (size_t)n));
@@ -1093,7 +1093,8 @@ class Engine {
     const int B = rs_B_, n = rs_n_, S = rs_S_;
     const Grid2 g{nx_, ny_};
     const float apert = (float)((double)aperture_ * 0.001 / (double)wavel_);
-    const int vr = plan_for(B).row, vc = plan_for(B).col;
+    const PlanChoice pc = plan_for(B, true);
+    const int vr = pc.row, vc = pc.col;
     MS_TRY(cudaMemsetAsync(d_bsig_.p, 0, sizeof(double) * 2 * n, st));
     for (int start = 0; start < n; start += B) {
       const int nb = std::min(B, n - start);
@@ -1585,19 +1586,22 @@ class Engine {
     if (pass < 0 || pass > 1 || variant < 0 || variant >= plan_variants() || batch < 1 || batch > 256 || reps < 1)
       return fail(MS_ERR_INVALID, "bad pass, variant, batch or reps");
     if (pass == 0 && (op & (A_FD | A_RESID | A_ADJ | A_SAVE | A_INTENSITY | A_REAL)) != 0)
-      return fail(MS_ERR_INVALID, "row-pass timing covers A_INV, A_MULT_T and A_FWD");
+      return fail(MS_ERR_INVALID, "row-pass timing covers A_INV, A_MULT_T, A_MULT_TC and A_FWD");
     if (pass == 1 && (op == B_CBED || op == B_DETECT || op == B_FD || op == B_CTF_ADJ))
       return fail(MS_ERR_INVALID, "column-pass timing covers the wave-to-wave modes");
     if (int rc = ensure_prop_tables(convdz_)) return rc;
     const long long N = (long long)nx_ * ny_;
-    DevBuf<float2> w;
+    DevBuf<float2> w, T;
     DevBuf<float> V;
     MS_TRY(w.resize((size_t)batch * N));
     MS_TRY(V.resize((size_t)N));
+    MS_TRY(T.resize((size_t)N));  // one transmission slice shared by the instances (A_MULT_TC)
     MS_TRY(cudaMemsetAsync(w.p, 0, sizeof(float2) * batch * N, stream_));
     MS_TRY(cudaMemsetAsync(V.p, 0, sizeof(float) * N, stream_));
+    MS_TRY(cudaMemsetAsync(T.p, 0, sizeof(float2) * N, stream_));
     PassAArgs a = passa_args(w.p, w.p, variant);
     a.V = V.p;
+    a.tr = T.p;
     a.batch_stride_wave = N;
     PassBArgs b = passb_args(w.p, w.p, variant);
     b.batch_stride_wave = N;
@@ -1768,60 +1772,109 @@ class Engine {
   struct PlanChoice {
     int row = 0, col = 0;
   };
-  PlanChoice plan_for(int batch) {
+  // `tc`: the row pass multiplies by a precomputed transmission (A_MULT_TC,
+  // the batched raster) rather than forming exp(i sigma V) itself; the two
+  // load different operands and are tuned apart.
+  PlanChoice plan_for(int batch, bool tc = false) {
     if (forced_plan_ >= 0) return PlanChoice{forced_plan_, forced_plan_};
-    const int key = batch <= 1 ? 1 : (batch < 8 ? 4 : 16);
+    const int bucket = batch <= 1 ? 1 : batch < 8 ? 4 : batch < 32 ? 16 : 64;
+    const int key = bucket + (tc ? 1000 : 0);
     for (auto& kv : tuned_)
       if (kv.first == key) return kv.second;
-    PlanChoice c = autotune(key);
+    PlanChoice c = autotune(bucket, tc);
     tuned_.push_back({key, c});
     return c;
   }
 
   // Times every plan variant of the steady-state row pass and the propagating
-  // column pass on scratch waves (batch instances), on this device, and keeps
-  // the fastest.  Scratch is zero-filled so the transmission's sincos stays on
-  // its fast path.  On any launch failure the variant is skipped.
-  PlanChoice autotune(int batch) {
+  // column pass on scratch waves (batch instances), on this device, then the
+  // three fastest of each in pairs, alternating, and keeps the fastest pair.
+  // Scratch is zero-filled so the transmission's sincos stays on its fast
+  // path.  On any launch failure the variant is skipped.
+  PlanChoice autotune(int batch, bool tc) {
     PlanChoice best;
     const long long N = (long long)nx_ * ny_;
-    DevBuf<float2> w;
+    DevBuf<float2> w, T;
     DevBuf<float> V;
     if (w.resize((size_t)batch * N) != cudaSuccess || V.resize((size_t)N) != cudaSuccess) return best;
+    if (tc && T.resize((size_t)N) != cudaSuccess) return best;
     cudaMemsetAsync(w.p, 0, sizeof(float2) * batch * N, stream_);
     cudaMemsetAsync(V.p, 0, sizeof(float) * N, stream_);
+    if (tc) cudaMemsetAsync(T.p, 0, sizeof(float2) * N, stream_);
+    const int row_op = tc ? (A_INV | A_MULT_TC | A_FWD) : (A_INV | A_MULT_T | A_FWD);
     if (ensure_prop_tables(convdz_) != MS_OK) return best;
-    float best_a = INFINITY, best_b = INFINITY;
-    const int reps = 8;
-    for (int v = 0; v < plan_variants(); ++v) {
+    const int reps = 8, nv = plan_variants();
+    auto row_args = [&](int v) {
       PassAArgs a = passa_args(w.p, w.p, v);
       a.V = V.p;
+      a.tr = T.p;
       a.batch_stride_wave = N;
       a.batch_stride_V = 0;
+      return a;
+    };
+    auto col_args = [&](int v) {
       PassBArgs b = passb_args(w.p, w.p, v);
       b.batch_stride_wave = N;
+      return b;
+    };
+    auto elapsed = [&](auto&& body) {
+      float ms = INFINITY;
+      cudaEventRecord(ev0_, stream_);
+      body();
+      cudaEventRecord(ev1_, stream_);
+      if (cudaEventSynchronize(ev1_) != cudaSuccess || cudaEventElapsedTime(&ms, ev0_, ev1_) != cudaSuccess) {
+        cudaGetLastError();
+        return INFINITY;
+      }
+      return ms;
+    };
+    // each variant of each pass alone
+    std::vector<float> ta(nv, INFINITY), tb(nv, INFINITY);
+    for (int v = 0; v < nv; ++v) {
+      const PassAArgs a = row_args(v);
+      const PassBArgs b = col_args(v);
       bool ok = true;
       for (int k = 0; k < 2 && ok; ++k)  // first launches load the kernels
-        ok = launch_pass_a(a, v, A_INV | A_MULT_T | A_FWD, batch, stream_) == cudaSuccess &&
+        ok = launch_pass_a(a, v, row_op, batch, stream_) == cudaSuccess &&
              launch_pass_b(b, v, B_PROPAGATE, batch, stream_) == cudaSuccess;
       if (!ok || cudaStreamSynchronize(stream_) != cudaSuccess) {
         cudaGetLastError();
         continue;
       }
-      float ta = 0, tb = 0;
-      cudaEventRecord(ev0_, stream_);
-      for (int k = 0; k < reps; ++k) launch_pass_a(a, v, A_INV | A_MULT_T | A_FWD, batch, stream_);
-      cudaEventRecord(ev1_, stream_);
-      cudaEventSynchronize(ev1_);
-      cudaEventElapsedTime(&ta, ev0_, ev1_);
-      cudaEventRecord(ev0_, stream_);
-      for (int k = 0; k < reps; ++k) launch_pass_b(b, v, B_PROPAGATE, batch, stream_);
-      cudaEventRecord(ev1_, stream_);
-      cudaEventSynchronize(ev1_);
-      cudaEventElapsedTime(&tb, ev0_, ev1_);
+      ta[v] = elapsed([&] { for (int k = 0; k < reps; ++k) launch_pass_a(a, v, row_op, batch, stream_); });
+      tb[v] = elapsed([&] { for (int k = 0; k < reps; ++k) launch_pass_b(b, v, B_PROPAGATE, batch, stream_); });
       launches += 2LL * (reps + 2);
-      if (ta < best_a) { best_a = ta; best.row = v; }
-      if (tb < best_b) { best_b = tb; best.col = v; }
+    }
+    // the three fastest of each, paired and timed alternating as the slice
+    // loop runs them (a pass's speed depends on its neighbour: programmatic
+    // dependent launch lets the next pass's CTAs in while this one drains)
+    auto top3 = [&](const std::vector<float>& t) {
+      std::vector<int> idx(nv);
+      for (int v = 0; v < nv; ++v) idx[v] = v;
+      std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return t[x] < t[y]; });
+      idx.resize(std::min(nv, 3));
+      return idx;
+    };
+    float best_t = INFINITY;
+    for (int r : top3(ta)) {
+      if (!(ta[r] < INFINITY)) continue;
+      for (int c : top3(tb)) {
+        if (!(tb[c] < INFINITY)) continue;
+        const PassAArgs a = row_args(r);
+        const PassBArgs b = col_args(c);
+        const float t = elapsed([&] {
+          for (int k = 0; k < reps; ++k) {
+            launch_pass_a(a, r, row_op, batch, stream_);
+            launch_pass_b(b, c, B_PROPAGATE, batch, stream_);
+          }
+        });
+        launches += 2LL * reps;
+        if (t < best_t) {
+          best_t = t;
+          best.row = r;
+          best.col = c;
+        }
+      }
     }
     cudaStreamSynchronize(stream_);
     return best;

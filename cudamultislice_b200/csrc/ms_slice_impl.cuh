@@ -60,11 +60,16 @@ template <> struct PlanSel<4096, 5> { using T = fft::Plan<4096, 16, 8, 8, 8, 8, 
 
 constexpr int kPlanVariants = 6;
 
-// Threads per CTA: rows, 256 (whole lines); columns, 4 columns per CTA for
-// lines of 64 or more threads (256 threads for shorter lines), so that a
-// warp's accesses cover whole 32-byte sectors, halved for the narrow plans.
+// Threads per CTA: rows, 256 (whole lines), 128 for the unpacked 32-point
+// plans of lines of at most 64 threads (twice the CTAs, which a single
+// instance, one wave, needs; the packed twin keeps whole 256-thread CTAs);
+// columns, 4 columns per CTA for lines of 64 or more threads (256 threads for
+// shorter lines), so that a warp's accesses cover whole 32-byte sectors,
+// halved for the narrow plans.
 template <class PL>
-__host__ __device__ constexpr int rows_per_cta() { return PL::P >= 256 ? 1 : 256 / PL::P; }
+__host__ __device__ constexpr int rows_per_cta() {
+  return PL::P >= 256 ? 1 : (!PL::PK && PL::E >= 32 && PL::P <= 64) ? 128 / PL::P : 256 / PL::P;
+}
 // The packed 32-point column plans take half the columns per CTA: twice the
 // CTAs, which a single instance (one wave) needs, and registers enough for
 // two CTAs without spilling; their unpacked twins keep the wide tiles that
@@ -471,9 +476,10 @@ __global__ void __launch_bounds__(cols_per_cta<PL>() * PL::P, col_min_ctas<PL>()
 // (The column pass, k_pass_b above, sizes every plan by col_min_ctas.)
 // Row CTAs per SM a capped row plan is sized for (0: left to the compiler).
 // Fewer registers cost latency hiding at one instance while more CTAs win in
-// batches, so each plan shape keeps one free twin and one capped twin and the
-// autotuner chooses: the unpacked 32-point plan is sized for two CTAs, the
-// packed 16-point plan for three; their twins stay free.
+// batches, so plan shapes keep a free and a capped twin and the autotuner
+// chooses: the unpacked 32-point plan is sized for two CTAs (a bound only for
+// its 256-thread CTAs, lines of 128 threads), the packed 16-point plan for
+// three; their twins stay free.
 template <class PL>
 constexpr int row_cap_ctas() { return (PL::E >= 32 && !PL::PK) ? 2 : (PL::E == 16 && PL::PK) ? 3 : 0; }
 template <class PL>

@@ -291,7 +291,8 @@ ms_status ms_stem_raster_concurrent(ms_sim* const* sims, int nsims, const int* c
 /* Microseconds per launch of one fused pass on scratch waves (CUDA events,
  * `reps` back-to-back launches after two warm-up launches): pass 0 = row pass
  * with op = a combination of 1 (inverse row FFT), 2 (x exp(i sigma V)),
- * 4 (forward row FFT); pass 1 = column pass with op = 0 (forward column FFT),
+ * 512 (x a precomputed transmission, as the batched raster), 4 (forward row
+ * FFT); pass 1 = column pass with op = 0 (forward column FFT),
  * 1 (inverse), 2 (propagate), 3 (CTF), 6 (band limit), 8 (adjoint propagate);
  * FFT plan `variant`, `batch` instances. */
 ms_status ms_time_pass(ms_sim* sim, int pass, int op, int variant, int batch, int reps, float* us);
