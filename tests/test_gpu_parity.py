@@ -137,6 +137,25 @@ def test_exit_wave_conventional(engine_cls, oracle_mod, path):
     assert e < TOL, e
 
 
+@pytest.mark.parametrize("n", [128, 256])
+def test_band_limit_decisions_match_plain_path(engine_cls, oracle_mod, n):
+    """The fused column pass keeps k by comparing k^2 with thresholds derived
+    from kmax; the plain path keeps sqrtf(k^2) < kmax (CreatePropsKernel).  One
+    propagation step on each path must keep the same frequencies: their exit
+    waves' spectra agree to rounding everywhere, band edge included."""
+    specs = []
+    for path in (0, 1):
+        eng, _ = make_pair(engine_cls, oracle_mod, sto(2, 2), n, 0.1, path=path)
+        eng.MultisliceStepConventional(1)
+        specs.append(np.abs(np.fft.fft2(eng.ExitWave().astype(np.complex128))))
+    top = specs[1].max()
+    kept = specs[1] > 1e-4 * top
+    assert kept.sum() > 0 and not kept.all()
+    # a frequency kept on one path and dropped on the other would differ by its
+    # full amplitude; rounding moves the spectra by about 1e-6 of the maximum
+    assert np.abs(specs[0] - specs[1]).max() < 1e-5 * top
+
+
 def test_run_after_new_atoms_matches_fresh_engine(engine_cls, oracle_mod):
     """RunConventional after SetAtoms + UploadBinnedAtoms (same grid and slice
     count: the slice-loop graph is reused over the rebuilt potential stack)
