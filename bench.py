@@ -461,23 +461,34 @@ def adjoint_leg(fparams, device: int, reps: int = 3) -> dict:
                 best = t if best is None else min(best, t)
         return best
 
+    import torch
+
+    ksq = int(np.ceil(np.sqrt(nslices)))
     fwd = timed(lambda: sim.FocalSeries(df, T, nslices), True)
-    grad = timed(lambda: sim.FocalSeriesGrad(df, T, nslices, want_v=True, want_xy=True), True)
     fwd_res = timed(lambda: sim.FocalSeries(df, T, nslices), False)
-    grad_res = timed(lambda: sim.FocalSeriesGrad(df, T, nslices, want_v=True, want_xy=False), False)
-    sim.SetCheckpoint(1)
-    grad_res_k1 = timed(lambda: sim.FocalSeriesGrad(df, T, nslices, want_v=True, want_xy=False), False)
-    sim.SetCheckpoint(0)
+    out = {}
+    # sqrt(S) checkpoints (each segment recomputed once), then the automatic
+    # default, which stores every wave when they fit in 1/8 of free memory
+    for name, k in (("sqrt_checkpoints", ksq), ("default", 0)):
+        sim.SetCheckpoint(k)
+        grad = timed(lambda: sim.FocalSeriesGrad(df, T, nslices, want_v=True, want_xy=True), True)
+        grad_res = timed(lambda: sim.FocalSeriesGrad(df, T, nslices, want_v=True, want_xy=False), False)
+        out[name] = {"grad_ms": grad, "grad_over_forward": grad / fwd, "resident_grad_dV_ms": grad_res,
+                     "resident_grad_over_forward": grad_res / fwd_res}
+    free_b, _ = torch.cuda.mem_get_info(device)
+    auto_k = 1 if nslices * n * n * 8 <= free_b // 8 else ksq
     loss = sim.FocalSeries(df, T, nslices)
     sim.close()
+    sq = out["sqrt_checkpoints"]
     return {
         "config": f"SrTiO3 4x4x50 cells ({len(Z)} atoms), {n}^2, {nslices} slices of 1.9525 A, 200 kV, "
                   "8 defoci -80..+60 nm, targets from seeded 0.1 A position errors",
-        "forward_ms": fwd, "grad_ms": grad, "grad_over_forward": grad / fwd,
-        "potentials_resident": {"forward_ms": fwd_res, "grad_dV_ms": grad_res, "grad_over_forward": grad_res / fwd_res,
-                                "grad_dV_ms_store_all": grad_res_k1,
-                                "store_all_over_forward": grad_res_k1 / fwd_res},
-        "checkpoint_stride": int(np.ceil(np.sqrt(nslices))), "loss": loss,
+        "forward_ms": fwd, "grad_ms": sq["grad_ms"], "grad_over_forward": sq["grad_over_forward"],
+        "checkpoint_stride": ksq,
+        "potentials_resident": {"forward_ms": fwd_res, "grad_dV_ms": sq["resident_grad_dV_ms"],
+                                "grad_over_forward": sq["resident_grad_over_forward"]},
+        "default_stride": {"stride": auto_k, **out["default"]},
+        "loss": loss,
         "timing": "device time (CUDA events on the engine stream), best of 3 after a warm-up call",
     }
 

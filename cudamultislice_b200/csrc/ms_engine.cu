@@ -147,7 +147,7 @@ class Engine {
         invalidate_graph();
         return MS_OK;
       case MS_OPT_CHECKPOINT:
-        if (value < 0) return fail(MS_ERR_INVALID, "checkpoint stride must be 0 (ceil(sqrt(S))) or >= 1");
+        if (value < 0) return fail(MS_ERR_INVALID, "checkpoint stride must be 0 (automatic) or >= 1");
         ckpt_ = value;
         return MS_OK;
       case MS_OPT_FFT_PLAN:
@@ -1434,7 +1434,8 @@ class Engine {
     if (int rc = ensure_prop_tables(convdz_)) return rc;
     plan_for(1);
     const size_t N = (size_t)nx_ * ny_;
-    const int K = grad ? (ckpt_ > 0 ? std::min(ckpt_, S) : (int)std::ceil(std::sqrt((double)S))) : S;
+    int K = S;
+    if (grad) K = ckpt_ > 0 ? std::min(ckpt_, S) : auto_checkpoint_stride(S, (size_t)nx_ * ny_);
     const int nck = (S + K - 1) / K;
     MS_TRY(d_T_.resize(N * nd));
     MS_TRY(d_Phi_.resize(N));
@@ -1619,6 +1620,19 @@ class Engine {
     launches += reps + 2;
     *us = 1000.0f * ms / (float)reps;
     return MS_OK;
+  }
+
+  // Checkpoint stride when none is set: every wave stored (no recomputation)
+  // when the S waves take at most an eighth of the device's free memory, else
+  // ceil(sqrt(S)) (sqrt(S) checkpoints, each segment recomputed once).
+  static int auto_checkpoint_stride(int S, size_t N) {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+      cudaGetLastError();
+      free_b = 0;
+    }
+    if ((size_t)S * N * sizeof(float2) <= free_b / 8) return 1;
+    return (int)std::ceil(std::sqrt((double)S));
   }
 
   // ---- inspection ----

@@ -67,8 +67,10 @@ enum {
                                3..5: 0..2 with butterflies on the packed FP32x2 pipe).
                                Variants agree to FP32 rounding, not bit for bit. */
   MS_OPT_CHECKPOINT = 4     /* focal-series gradient: slices between stored waves;
-                               0 = ceil(sqrt(S)) (default), 1 = store every wave,
-                               >= S = one segment recomputed from the initial wave */
+                               0 = automatic (default): every wave when the S waves
+                               fit in an eighth of the free device memory, else
+                               ceil(sqrt(S)); 1 = store every wave; >= S = one
+                               segment recomputed from the initial wave */
 };
 
 /* ---- lifecycle ---- */
