@@ -92,7 +92,8 @@ class ManagedMultisliceSimulation:
         self._chk(self._L.ms_set_option(self._h, 3, int(variant)))
 
     def SetCheckpoint(self, stride: int):
-        """Focal-series gradient: slices between stored waves (0: ceil(sqrt(S)))."""
+        """Focal-series gradient: slices between stored waves (0: automatic, every
+        wave when they fit in an eighth of free device memory, else ceil(sqrt(S)))."""
         self._chk(self._L.ms_set_option(self._h, 4, int(stride)))
 
     # ---- structure ----
