@@ -60,15 +60,16 @@ template <> struct PlanSel<4096, 5> { using T = fft::Plan<4096, 16, 8, 8, 8, 8, 
 
 constexpr int kPlanVariants = 6;
 
-// Threads per CTA: rows, 256 (whole lines), 128 for the unpacked 32-point
-// plans of lines of at most 64 threads (twice the CTAs, which a single
-// instance, one wave, needs; the packed twin keeps whole 256-thread CTAs);
+// Threads per CTA: rows, 256 (whole lines), 64 or 128 for the unpacked
+// 32-point plans of lines of 32 or 64 threads (two lines per CTA: more CTAs,
+// which a single instance, one wave, needs; the packed twin keeps whole
+// 256-thread CTAs);
 // columns, 4 columns per CTA for lines of 64 or more threads (256 threads for
 // shorter lines), so that a warp's accesses cover whole 32-byte sectors,
 // halved for the narrow plans.
 template <class PL>
 __host__ __device__ constexpr int rows_per_cta() {
-  return PL::P >= 256 ? 1 : (!PL::PK && PL::E >= 32 && PL::P <= 64) ? 128 / PL::P : 256 / PL::P;
+  return PL::P >= 256 ? 1 : (!PL::PK && PL::E >= 32 && PL::P <= 64) ? 2 : 256 / PL::P;
 }
 // The packed 32-point column plans take half the columns per CTA: twice the
 // CTAs, which a single instance (one wave) needs, and registers enough for
