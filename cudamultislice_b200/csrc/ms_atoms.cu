@@ -297,7 +297,7 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a) {
 
       for (int base = 0; base < total; base += kChunk) {
         const int nload = min(kChunk, total - base);
-        // candidates of this round, kept when some pixel of the tile can take
+        // this chunk of candidates, kept when some pixel of the tile can take
         // a term from them: within sqrt(5) A of the tile's pixel rectangle
         // with the nearest sub-plane (margin far above FP32 rounding), and in
         // the slab for the projected form.  Kept atoms stay in order, so every
@@ -453,7 +453,7 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
 
       for (int base = 0; base < total; base += kConvChunk) {
         const int nload = min(kConvChunk, total - base);
-        // candidates of this round, kept when some sub-plane can pass the
+        // this chunk of candidates, kept when some sub-plane can pass the
         // cut-off (dz_m^2 < 5) and the atom lies within sqrt(5) A of the tile's
         // pixel rectangle (with a margin far above FP32 rounding, so that every
         // dropped atom fails r^2 < 5 at every pixel); kept atoms stay in order

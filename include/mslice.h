@@ -213,7 +213,7 @@ ms_status ms_build_potential_stack(ms_sim* sim, int* nslices);
  * captured CUDA graph); equivalent to ms_multislice_step_conventional(i)
  * for i = 1..S. */
 ms_status ms_run_conventional(ms_sim* sim, int* nslices);
-/* Annular detector (new; no reference counterpart, north-star STEM signal):
+/* Annular detector (no reference counterpart; the HAADF/ADF STEM signal):
  * sum over inner <= theta < outer (mrad) of |FFT(psi)|^2 / N. */
 ms_status ms_annular_detector(ms_sim* sim, float inner_mrad, float outer_mrad, double* out);
 
@@ -277,8 +277,8 @@ ms_status ms_focal_series(ms_sim* sim, const float* defoci, int nd, const float*
 ms_status ms_focal_series_grad(ms_sim* sim, const float* defoci, int nd, const float* targets, int nslices,
                                double* loss, float* dLdV, double* dLdxy);
 
-/* Several specimens' probe rasters in one CUDA-graph launch (north-star
- * batching of mixed grid sizes; no reference counterpart): handle k (its own
+/* Several specimens' probe rasters in one CUDA-graph launch (batching of
+ * mixed grid sizes; no reference counterpart): handle k (its own
  * specimen, grid and potentials; all handles on one device, fused path) runs
  * the raster of ms_stem_raster over its n[k] positions px[k], py[k] into
  * signal[k].  The handles' work is captured as concurrent branches of one graph

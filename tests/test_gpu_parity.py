@@ -1,7 +1,7 @@
 """Parity of the CUDA engine (through the C ABI) against the FP64 oracle.
 
 Bit-exact for the integer work (atom index); for the floating-point path the
-relative L2 error <= 1e-5 against FP64 for potentials,
+parity tolerance: relative L2 error <= 1e-5 against FP64 for potentials,
 exit waves, images and detector signals."""
 import numpy as np
 import pytest
