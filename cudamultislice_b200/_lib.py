@@ -57,6 +57,7 @@ SIGNATURES = {
     "ms_alloc_host_image": (_i, [_p]),
     "ms_simulate_image": (_i, [_p, _f]),
     "ms_get_im_value": (_i, [_p, _i, _i, _pf]),
+    "ms_get_dqe_im_value": (_i, [_p, _i, _i, _pf]),
     "ms_get_im_min": (_i, [_p, _pf]),
     "ms_get_im_max": (_i, [_p, _pf]),
     "ms_get_image_contrast": (_i, [_p, _i, _i, _i, _i, _pf]),

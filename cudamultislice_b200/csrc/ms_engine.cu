@@ -12,6 +12,7 @@
 #include <cufft.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -243,8 +244,12 @@ class Engine {
       if (!(sigma >= 0) || !std::isfinite(sigma)) return fail(MS_ERR_INVALID, "bad thermal displacement sigma");
       tds_displace(hx_.data(), hy_.data(), hz_.data(), n, seed, pass, sigma, x.data(), y.data(), z.data());
     }
-    // nSlices = ceil((MaximumZ-MinimumZ)/dz), dz = 1 (U.cu:1409-1411)
-    int nz = (int)std::ceil((box_.MaxZ - box_.MinZ) / (float)1);
+    // nSlices = ceil((MaximumZ-MinimumZ)/dz), dz = 1 (U.cu:1409-1411); the
+    // extent is range-checked before the conversion to int
+    const float zext = std::ceil((box_.MaxZ - box_.MinZ) / (float)1);
+    if (!std::isfinite(zext) || zext < 0.0f || (double)zext * kBins2 > (double)(INT_MAX - 1))
+      return fail(MS_ERR_INVALID, "structure too deep for the atom index: " + std::to_string(zext) + " z-bins");
+    int nz = (int)zext;
     nz += (nz == 0);
     const int nbins = nz * kBins2;
     MS_TRY(d_Zin_.resize(n));
@@ -913,6 +918,15 @@ class Engine {
       return MS_OK;
     }
     *out = image_[p];
+    return MS_OK;
+  }
+
+  // GetDQEImValue (U.cu:2514-2517): the magnitude of the simulated image at a
+  // pixel, without the readout noise GetImValue adds.
+  int dqe_im_value(int x, int y, float* out) {
+    if (!have_image_) return fail(MS_ERR_STATE, "image not simulated (ms_simulate_image)");
+    if (x < 0 || y < 0 || x >= nx_ || y >= ny_) return fail(MS_ERR_INVALID, "pixel index out of range");
+    *out = std::fabs(image_[(size_t)y * nx_ + x]);
     return MS_OK;
   }
 
@@ -2372,6 +2386,10 @@ ms_status ms_simulate_image(ms_sim* s, float dose) {
 ms_status ms_get_im_value(ms_sim* s, int x, int y, float* out) {
   if (ms_status r = out_check(s, out)) return r;
   return guarded(s, [&](ms::Engine& e) { return e.im_value(x, y, out); });
+}
+ms_status ms_get_dqe_im_value(ms_sim* s, int x, int y, float* out) {
+  if (ms_status rc = out_check(s, out)) return rc;
+  return guarded(s, [&](ms::Engine& e) { return e.dqe_im_value(x, y, out); });
 }
 ms_status ms_get_im_min(ms_sim* s, float* out) {
   if (ms_status r = out_check(s, out)) return r;

@@ -2,10 +2,8 @@
 //
 // Some callers cannot call cudaMalloc: a host application whose memory
 // manager owns every device allocation (a pooled allocator that forbids
-// foreign cudaMalloc/cudaFree), code that enqueues work while a CUDA graph is
-// being captured (allocation is not a capturable stream operation), or a
-// latency-critical loop that cannot afford the implicit device-wide
-// synchronisation of cudaMalloc/cudaFree.  For them this file provides
+// foreign cudaMalloc/cudaFree), or a latency-critical loop that cannot afford
+// the implicit device-wide synchronisation of cudaMalloc/cudaFree.  For them this file provides
 // ms_build_atom_index_noalloc: the bit-exact atom binning of
 // ms_upload_binned_atoms, reading the atoms from and writing the index to
 // device buffers the caller already owns.  Its scratch (bin keys, the
@@ -23,8 +21,8 @@
 //  - host code may not hand the array's name to a kernel (the name is only a
 //    host-side stand-in); the device address is looked up once per device with
 //    cudaGetSymbolAddress.  That look-up happens on the first call on each
-//    device, so the first call on a device must come before any stream
-//    capture that is meant to record later calls.
+//    device, so the first call on a device should come before any stream
+//    capture.
 #include <cmath>
 #include <cstdint>
 #include <mutex>
@@ -90,16 +88,21 @@ extern "C" ms_status ms_build_atom_index_noalloc(const int* d_Z, const float* d_
   if (reinterpret_cast<uintptr_t>(d_atoms) % 16 != 0)
     return noalloc_fail(MS_ERR_INVALID, "d_atoms must be 16-byte aligned (float4 records)");
   Box b{box[0], box[1], box[2], box[3], box[4], box[5]};
+  for (int i = 0; i < 6; ++i)
+    if (!std::isfinite(box[i])) return noalloc_fail(MS_ERR_INVALID, "box entries must be finite");
   if (!(b.MaxX > b.MinX) || !(b.MaxY > b.MinY) || !(b.MaxZ >= b.MinZ))
     return noalloc_fail(MS_ERR_INVALID, "box must satisfy Max > Min in x and y, Max >= Min in z");
-  // nSlices = ceil((MaximumZ-MinimumZ)/dz), dz = 1 (U.cu:1409-1411)
-  int nz = (int)std::ceil((b.MaxZ - b.MinZ) / (float)1);
-  nz += (nz == 0);
-  const long long nbins = (long long)nz * kBins2;
-  if (nbins > kMaxBins)
-    return noalloc_fail(MS_ERR_INVALID, "ms_build_atom_index_noalloc: " + std::to_string(nz) +
+  // nSlices = ceil((MaximumZ-MinimumZ)/dz), dz = 1 (U.cu:1409-1411); the
+  // z-bin count is checked against the scratch limit while still a float, so
+  // the conversion to int below is always in range
+  const float zext = std::ceil((b.MaxZ - b.MinZ) / (float)1);
+  if (!(zext <= (float)(kMaxBins / kBins2)))
+    return noalloc_fail(MS_ERR_INVALID, "ms_build_atom_index_noalloc: " + std::to_string(zext) +
                                             " z-bins exceed the fixed scratch limit of " +
                                             std::to_string(kMaxBins / kBins2) + "; use ms_upload_binned_atoms");
+  int nz = (int)zext;
+  nz += (nz == 0);
+  const long long nbins = (long long)nz * kBins2;
   if ((long long)offsets_capacity < nbins + 1)
     return noalloc_fail(MS_ERR_INVALID, "d_offsets holds " + std::to_string(offsets_capacity) + " ints, need " +
                                             std::to_string(nbins + 1));

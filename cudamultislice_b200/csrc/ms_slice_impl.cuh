@@ -2,6 +2,7 @@
 // line length in ms_slice_n*.cu (see ms_slice.cuh for the scheme).
 #pragma once
 #include <cmath>
+#include <mutex>
 
 #include "ms_ctf.cuh"
 #include "ms_fft.cuh"
@@ -496,12 +497,22 @@ __global__ void __launch_bounds__(rows_per_cta<PL>() * PL::P, row_cap_ctas<PL>()
 }
 
 
-inline bool attr_once(unsigned long long& mask) {
+// Raises a kernel's dynamic shared-memory limit once per device.  `mask`
+// holds one bit per device, set only after the attribute call succeeded (a
+// failed call is retried on the next launch); the mutex keeps a second host
+// thread from launching before the first one has raised the limit.
+template <class K>
+cudaError_t set_smem_once(unsigned long long& mask, K kernel, size_t smem) {
+  static std::mutex mu;
   int dev = 0;
-  cudaGetDevice(&dev);
-  if (mask >> dev & 1ull) return false;
-  mask |= 1ull << dev;
-  return true;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(mu);
+  if (mask >> dev & 1ull) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) mask |= 1ull << dev;
+  return e;
 }
 
 // Launch with programmatic stream serialisation (see pdl_wait).
@@ -530,10 +541,7 @@ cudaError_t run_a(const PassAArgs& a, int batch, cudaStream_t s) {
     else return k_pass_a<PL, FLAGS>;
   }();
   static unsigned long long done = 0;
-  if (attr_once(done)) {
-    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-  }
+  if (cudaError_t e = set_smem_once(done, kernel, smem)) return e;
   return launch_pdl(kernel, dim3(a.ny / lines, batch), lines * PL::P, smem, s, a);
 }
 
@@ -546,10 +554,7 @@ cudaError_t run_b(const PassBArgs& a, int batch, cudaStream_t s) {
   if (a.nx % CB) return cudaErrorInvalidValue;
   auto kernel = k_pass_b<PL, MODE>;
   static unsigned long long done = 0;
-  if (attr_once(done)) {
-    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-  }
+  if (cudaError_t e = set_smem_once(done, kernel, smem)) return e;
   return launch_pdl(kernel, dim3(a.nx / CB, batch), CB * PL::P, smem, s, a);
 }
 

@@ -225,6 +225,9 @@ class ManagedMultisliceSimulation:
     def GetImValue(self, x, y) -> float:
         return self._f(self._L.ms_get_im_value, int(x), int(y))
 
+    def GetDQEImValue(self, x, y) -> float:
+        return self._f(self._L.ms_get_dqe_im_value, int(x), int(y))
+
     def GetImMin(self) -> float:
         return self._f(self._L.ms_get_im_min)
 

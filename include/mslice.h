@@ -186,6 +186,10 @@ ms_status ms_get_tds_val(ms_sim* sim, int x, int y, float* out);
 ms_status ms_alloc_host_image(ms_sim* sim);
 ms_status ms_simulate_image(ms_sim* sim, float dose);
 ms_status ms_get_im_value(ms_sim* sim, int x, int y, float* out);
+/* GetDQEImValue U.cu:2514-2517 (declared unmanagedGUISimulation.cuh:191): the
+ * simulated image's magnitude at pixel (x, y), without GetImValue's readout
+ * noise. */
+ms_status ms_get_dqe_im_value(ms_sim* sim, int x, int y, float* out);
 /* Detector model for ms_simulate_image (new; the reference compiles fixed K2
  * camera tables in, MTF.h): dqe[n], ntf[n] radial tables indexed by
  * floor(|frequency-pixel distance to the nearest corner| / binning), 0.0001
@@ -326,8 +330,8 @@ ms_status ms_get_launch_count(ms_sim* sim, long long* out);
 
 /* ---- atom index without device allocation (no counterpart in the reference) ----
  * For callers that cannot call cudaMalloc: an application whose memory manager
- * owns every device allocation, work enqueued while a CUDA graph is captured, or
- * a loop that cannot take cudaMalloc's implicit device synchronisation.  Builds
+ * owns every device allocation, or a loop that cannot take cudaMalloc's
+ * implicit device synchronisation.  Builds
  * the same bit-exact atom index as ms_upload_binned_atoms from atoms already on
  * the device (d_Z, d_x, d_y, d_z: n entries each) into caller-owned device
  * buffers: d_atoms (4*n floats, 16-byte aligned: x, y, z shifted by the box
@@ -338,8 +342,8 @@ ms_status ms_get_launch_count(ms_sim* sim, long long* out);
  * Work is enqueued on `stream` (a cudaStream_t, NULL for the default stream) and
  * the call returns without waiting.  Scratch is one fixed device array of about
  * 3.1 MB inside the library, held by every GPU that loads it until exit; limits:
- * n <= 131072 atoms and nz <= 209 z-bins, larger requests fail with
- * MS_ERR_INVALID.  All calls share that array: calls whose GPU work overlaps
+ * n <= 131072 atoms and nz <= 209 z-bins, larger requests (and boxes with
+ * non-finite entries) fail with MS_ERR_INVALID before any GPU work.  All calls share that array: calls whose GPU work overlaps
  * race and corrupt each other's result.  The first call on a device looks up the
  * array's device address, so make it before any stream capture.  Errors are
  * reported by ms_last_error(NULL). */

@@ -1,6 +1,8 @@
 #!/usr/bin/env bash
 # Compiles the reference engine for the oracle-pinning build:
-#   /root/reference/GUI Simulation/UnmanagedGUISimulation.cu  (unchanged)
+#   $MS_REFERENCE_DIR/GUI Simulation/UnmanagedGUISimulation.cu  (unchanged;
+#   MS_REFERENCE_DIR defaults to the read-only checkout of the build machine,
+#   and the build is skipped where no reference sources are found)
 #   + oracle/ref_shim (empty Stdafx.h and Boost stand-ins, and the
 #     cudaMemcpyToSymbol string-name fix, force-included)
 #   + oracle/ref_driver.cpp (C entry points for the golden-vector generator)

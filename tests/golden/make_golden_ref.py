@@ -6,7 +6,7 @@ through the call sequence of its GUI, and stores inputs and outputs as .npz
 fixtures.  tests/test_golden_reference.py checks the FP64 oracle against them
 on the CPU; the reference is never needed again after generation.
 
-  python tests/golden/make_golden_ref.py [outdir]      (needs a CUDA GPU)
+  python tests/golden/make_golden_ref.py OUTDIR      (needs a CUDA GPU)
 
 Cases use only elements of the reference's symbol table, except SrTiO3, whose
 Ti the reference maps to Z = 1 (GetZNum U.cu:1241): the fixture pins that too.
@@ -135,7 +135,9 @@ def run_case(L, name, text, micro, calc, mode, dz, steps, trans_slices=(), stem_
 
 
 def main():
-    outdir = sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden_ref.py OUTDIR")
+    outdir = sys.argv[1]
     os.makedirs(outdir, exist_ok=True)
     from cudamultislice_b200 import structures as S
 

@@ -35,7 +35,7 @@ def test_header_declares_the_reference_method_list():
               "ms_stem_initialise_wavefunctions", "ms_alloc_tds", "ms_multislice_step_fd",
               "ms_multislice_step_conventional", "ms_alloc_host_image", "ms_simulate_image", "ms_get_exit_wave",
               "ms_get_stem_exit_wave", "ms_free_exit_wave", "ms_add_tds_waves", "ms_get_ew_value_abs",
-              "ms_get_ew_value_re", "ms_get_ew_value_im", "ms_get_im_value", "ms_get_tds_min", "ms_get_tds_max",
+              "ms_get_ew_value_re", "ms_get_ew_value_im", "ms_get_im_value", "ms_get_dqe_im_value", "ms_get_tds_min", "ms_get_tds_max",
               "ms_get_tds_val", "ms_get_image_contrast", "ms_get_size_x", "ms_get_size_y", "ms_get_size_z",
               "ms_get_slices", "ms_get_kmax", "ms_get_im_min", "ms_get_im_max", "ms_get_ew_min", "ms_get_ew_max"]:
         assert n in names, n

@@ -469,6 +469,8 @@ def test_detector_noise_chain(engine_cls, oracle_mod):
     z = oracle_mod.clipped_normal(int(w[0]), int(w[1]))
     v = eng.GetImValue(x, y)
     assert abs(v - (4.0 + 1.33 * z + img[y, x])) <= 1e-5 * abs(v)
+    # GetDQEImValue (U.cu:2514-2517): the same pixel without the readout noise
+    assert eng.GetDQEImValue(x, y) == abs(img[y, x])
     eng.SetDetector(None, None)
     eng.SimulateImage(dose)
     assert rel_l2(eng.Image(), I) < TOL

@@ -1,8 +1,8 @@
 """ms_build_atom_index_noalloc: the atom index without device allocation.
 
-Callers whose memory manager owns all device memory, that enqueue work during
-CUDA-graph capture, or that cannot afford cudaMalloc's device synchronisation
-pass their own device buffers; the library's scratch is a fixed device array.
+Callers whose memory manager owns all device memory, or that cannot afford
+cudaMalloc's device synchronisation, pass their own device buffers; the
+library's scratch is a fixed device array.
 This test drives the entry point through the C ABI on device buffers owned by
 the caller (allocated here with PyTorch, as such a host application would with
 its own allocator) and requires its index to equal, bit for bit, the index of
@@ -89,3 +89,11 @@ def test_noalloc_refuses_oversized_requests():
     rc = L.ms_build_atom_index_noalloc(fake, fake, fake, fake, 10, deep.ctypes.data_as(C.c_void_p), fake, fake,
                                        1 << 22, C.byref(nz), None)
     assert rc == 1 and b"z-bins" in L.ms_last_error(None)
+    # a non-finite box, and a finite one whose depth would overflow an int bin
+    # count, are refused before any launch
+    for bad in ([10, 0, 10, 0, np.inf, 0], [10, 0, 10, 0, 10, -np.inf], [10, 0, 10, 0, 1e10, 0],
+                [np.nan, 0, 10, 0, 10, 0]):
+        b = np.array(bad, np.float32)
+        rc = L.ms_build_atom_index_noalloc(fake, fake, fake, fake, 10, b.ctypes.data_as(C.c_void_p), fake, fake,
+                                           1 << 22, C.byref(nz), None)
+        assert rc == 1, bad
