@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <cmath>
 #include <complex>
+#include <map>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -323,7 +324,15 @@ struct or_sim {
     std::vector<cd> psi0, psi_minus, psi, psi_plus;
     bool have_waves = false;
     std::vector<double> tds;
+    /* optional cache of conventional potentials by iteration (tests that run
+     * many probes over one specimen); cleared whenever an input of V changes */
+    bool vcache_on = false;
+    std::map<int, std::vector<double>> vcache;
 };
+
+/* Drops cached potentials: called by every set-up step that changes an input
+ * of the potential (atoms, table, grid, offsets, slice thickness). */
+static void pot_inputs_changed(or_sim* s) { s->vcache.clear(); }
 
 extern "C" or_sim* or_create(void) { return new or_sim(); }
 extern "C" void or_destroy(or_sim* s) { delete s; }
@@ -416,6 +425,7 @@ extern "C" int or_get_box(or_sim* s, float out[6]) {
 }
 
 extern "C" int or_load_fparams(or_sim* s, const char* path) {
+    pot_inputs_changed(s);
     s->fp.assign(103 * 12, 0.0);
     int rows = 0;
     if (or_parse_fparams(path, s->fp.data(), &rows) != 0) return fail(s, "cannot read fparams");
@@ -473,12 +483,14 @@ static void bin_positions(or_sim* s, const float* X, const float* Y, const float
 
 extern "C" int or_bin_atoms(or_sim* s) {
     if (!s->have_atoms) return fail(s, "no atoms");
+    pot_inputs_changed(s);
     bin_positions(s, s->x.data(), s->y.data(), s->z.data());
     return 0;
 }
 
 extern "C" int or_bin_atoms_tds(or_sim* s, uint64_t seed, uint32_t pass, float sigma) {
     if (!s->have_atoms) return fail(s, "no atoms");
+    pot_inputs_changed(s);
     const int n = (int)s->x.size();
     std::vector<float> X(n), Y(n), Zp(n);
     or_tds_displace(s->x.data(), s->y.data(), s->z.data(), n, seed, pass, sigma,
@@ -517,6 +529,7 @@ extern "C" int or_apply_microscope(or_sim* s, float kV, float df, float A2, floa
 extern "C" int or_set_calc(or_sim* s, float ps, float df, int nx, int ny, float sx, float sy,
                            float sizeZ, float xoff, float yoff, int stem) {
     (void)sx; (void)sy;
+    pot_inputs_changed(s);
     if (nx <= 0 || ny <= 0 || !(ps > 0)) return fail(s, "bad grid");
     if (!(s->kV > 0)) return fail(s, "accelerating voltage not set");
     if (!s->have_atoms) return fail(s, "no atoms");
@@ -566,6 +579,7 @@ extern "C" int or_set_calc(or_sim* s, float ps, float df, int nx, int ny, float 
 /* PreCalculateFrequencies U.cu:1877-1964 (the unused 2x grids are not built). */
 extern "C" int or_precalc(or_sim* s) {
     if (!s->have_calc) return fail(s, "calculation variables not set");
+    pot_inputs_changed(s);
     const int nx = s->nx, ny = s->ny;
     const float ksizex = s->ps * nx, ksizey = s->ps * ny;
     const int imidx = (int)std::floor(nx / 2 + 0.5), imidy = (int)std::floor(ny / 2 + 0.5);
@@ -641,6 +655,7 @@ static void propagate_fd_level(or_sim* s) {
 
 extern "C" int or_init_waves(or_sim* s, float conv_dz) {
     if (!s->have_freq) return fail(s, "frequencies not computed");
+    pot_inputs_changed(s);
     s->convdz = conv_dz > 0 ? conv_dz : 1.0f; /* U.cu:1968 / U.cu:2005 */
     const size_t N = (size_t)s->nx * s->ny;
     s->psi_minus.assign(N, cd(1.0, 0.0));
@@ -921,10 +936,41 @@ extern "C" int or_step_rs(or_sim* s, int it) {
 
 extern "C" int or_step_conventional(or_sim* s, int it) {
     if (!s->have_waves) return fail(s, "waves not initialised");
+    std::vector<cd> in = (it == 1) ? s->psi0 : s->psi;
+    if (s->vcache_on) {
+        auto f = s->vcache.find(it);
+        if (f == s->vcache.end()) {
+            std::vector<double> V((size_t)s->nx * s->ny);
+            if (or_potential_conventional(s, it, V.data())) return -1;
+            f = s->vcache.emplace(it, std::move(V)).first;
+        }
+        tp_step(s, f->second, in);
+        return 0;
+    }
     std::vector<double> V((size_t)s->nx * s->ny);
     if (or_potential_conventional(s, it, V.data())) return -1;
-    std::vector<cd> in = (it == 1) ? s->psi0 : s->psi;
     tp_step(s, V, in);
+    return 0;
+}
+
+/* One conventional step on a caller-given potential V (N doubles, V*A): the
+ * transmission and propagation of MultisliceStepConv (U.cu:2101-2122) without
+ * the potential build, for timing the slice step alone. */
+extern "C" int or_step_given_potential(or_sim* s, int it, const double* V) {
+    if (!s->have_waves) return fail(s, "waves not initialised");
+    const size_t N = (size_t)s->nx * s->ny;
+    std::vector<double> v(V, V + N);
+    std::vector<cd> in = (it == 1) ? s->psi0 : s->psi;
+    tp_step(s, v, in);
+    return 0;
+}
+
+/* Keeps (on != 0) or drops the conventional potential of each iteration for
+ * reuse by later steps of the same specimen and set-up (many probe positions
+ * over one potential stack); off also frees the cache. */
+extern "C" int or_cache_potentials(or_sim* s, int on) {
+    s->vcache_on = on != 0;
+    if (!on) s->vcache.clear();
     return 0;
 }
 
@@ -1288,6 +1334,7 @@ extern "C" int or_focal_grad(or_sim* s, const float* defoci, int nd, const doubl
  * taken this way see no cut-off flips and measure the chain-rule gradient. */
 extern "C" int or_set_value_offset(or_sim* s, int i, double dx, double dy) {
     if (!s->have_atoms || i < 0 || i >= (int)s->x.size()) return fail(s, "bad atom index");
+    pot_inputs_changed(s);
     if (s->valdx.empty()) {
         s->valdx.assign(s->x.size(), 0.0);
         s->valdy.assign(s->x.size(), 0.0);

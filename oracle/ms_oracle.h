@@ -86,6 +86,8 @@ int or_potential_projected(or_sim*, int iteration, float dz, double* out); /* vz
 int or_potential_rs(or_sim*, int iteration, double* out);            /* binnedAtomPKernelRS U.cu:655-727 */
 
 int or_step_conventional(or_sim*, int iteration);                    /* U.cu:2085-2124 */
+int or_cache_potentials(or_sim*, int on); /* reuse conventional V across probes (test speed only) */
+int or_step_given_potential(or_sim*, int iteration, const double* V); /* the step without the potential build */
 int or_step_projected(or_sim*, int iteration);                       /* same step, projected V */
 int or_step_fd(or_sim*, int iteration);                              /* U.cu:2040-2083 */
 int or_step_rs(or_sim*, int iteration);                              /* U.cu:2126-2178, as written */

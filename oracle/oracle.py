@@ -77,6 +77,8 @@ def lib():
         "or_potential_fd": (_i, [_p, _i, _p]),
         "or_potential_projected": (_i, [_p, _i, _f, _p]),
         "or_step_conventional": (_i, [_p, _i]),
+        "or_cache_potentials": (_i, [_p, _i]),
+        "or_step_given_potential": (_i, [_p, _i, _p]),
         "or_step_projected": (_i, [_p, _i]),
         "or_step_fd": (_i, [_p, _i]),
         "or_potential_rs": (_i, [_p, _i, _p]),
@@ -297,6 +299,18 @@ class OracleSimulation:
     # ---- steps ----
     def MultisliceStepConventional(self, it: int):
         self._chk(self._L.or_step_conventional(self._h, it))
+
+    def StepGivenPotential(self, it: int, V: np.ndarray):
+        """Transmission and propagation of one conventional step on V (ny, nx)."""
+        v = np.ascontiguousarray(V, np.float64)
+        if v.size != self.nx * self.ny:
+            raise ValueError("V must hold ny * nx values")
+        self._chk(self._L.or_step_given_potential(self._h, int(it), _ptr(v)))
+
+    def CachePotentials(self, on: bool = True):
+        """Reuse each iteration's conventional potential across later steps
+        (many probe positions over one specimen); dropped on any set-up change."""
+        self._chk(self._L.or_cache_potentials(self._h, int(bool(on))))
 
     def MultisliceStepProjected(self, it: int):
         self._chk(self._L.or_step_projected(self._h, it))

@@ -5,7 +5,8 @@
 #   and the build is skipped where no reference sources are found)
 #   + oracle/ref_shim (empty Stdafx.h and Boost stand-ins, and the
 #     cudaMemcpyToSymbol string-name fix, force-included)
-#   + oracle/ref_driver.cpp (C entry points for the golden-vector generator)
+#   + oracle/ref_driver.cpp (C entry points for the golden-vector generator;
+#     it includes the reference source file, so both form one translation unit)
 # into oracle/_ref/libmsref.so.  Nothing from the reference tree is copied.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
@@ -24,8 +25,7 @@ if [ "$OUT/libmsref.so" -nt "$REF/UnmanagedGUISimulation.cu" ] && [ "$OUT/libmsr
   exit 0
 fi
 $NVCC $ARCH $COMMON -I"$REF" -include cfloat -include "$HERE/ref_shim/ref_symbol_fix.h" \
-  -c "$REF/UnmanagedGUISimulation.cu" -o "$OUT/reference_engine.o"
-$NVCC $ARCH $COMMON -I"$REF" -x cu -c "$HERE/ref_driver.cpp" -o "$OUT/ref_driver.o"
-$NVCC $ARCH -shared -o "$OUT/libmsref.so" "$OUT/reference_engine.o" "$OUT/ref_driver.o" -lcufft -lcublas \
+  -x cu -c "$HERE/ref_driver.cpp" -o "$OUT/ref_driver.o"
+$NVCC $ARCH -shared -o "$OUT/libmsref.so" "$OUT/ref_driver.o" -lcufft -lcublas \
   -Xlinker -rpath,/usr/local/cuda/lib64
 echo "$OUT/libmsref.so"

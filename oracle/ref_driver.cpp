@@ -8,13 +8,32 @@
 // copies results out so tests/golden/make_golden_ref.py can store them as
 // golden vectors.  Private members are opened only to read the atom index
 // and the per-slice transmission the class keeps on the device.
-#define private public
-#include "unmanagedGUISimulation.cuh"
-#undef private
+//
+// The reference source file is compiled inside this translation unit (it is
+// included, not copied), so that the driver can also launch two of its
+// kernels that no public method exposes on their own:
+//  - imagingKernel2 (U.cu:1044-1080), the deterministic CTF transfer that
+//    SimulateImage applies before its detector-noise chain (U.cu:2323-2333);
+//  - binnedAtomPKernel2 (U.cu:513-578), the projected-potential kernel (vzatom2
+//    over one one-angstrom z-bin), which no method of the class launches.
+#include <cuComplex.h>
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+#include <cufft.h>
 
+#include <cfloat>
 #include <cmath>
 #include <cstring>
+#include <ctime>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+#include <string>
 #include <vector>
+
+#define private public
+#include "UnmanagedGUISimulation.cu"
+#undef private
 
 extern "C" {
 
@@ -74,6 +93,51 @@ void ref_scalars(void* h, float* out) {
 
 void ref_step_conv(void* h, int i) { ((UnmanagedMultisliceSimulation*)h)->MultisliceStepConv(i); }
 void ref_step_fd(void* h, int i) { ((UnmanagedMultisliceSimulation*)h)->MultisliceStep(i); }
+// MultisliceStepRS (U.cu:2126-2178), a public method the managed wrapper does
+// not expose; afterwards devV holds the RS potential {sumz, 0} of that step.
+void ref_step_rs(void* h, int i) { ((UnmanagedMultisliceSimulation*)h)->MultisliceStepRS(i); }
+
+// binnedAtomPKernel2 (U.cu:513-578) over one-angstrom z-bin `bin`: the kernel
+// scans z-bin floor((MaxZ-MinZ-z)/dz) with an int dz, launched here with
+// dz = 1 and z = (MaxZ-MinZ) - bin - 0.5, on the 32 x 8 blocks of every
+// launch of the class.  Writes exp(i sigma2 V) as {cos, sin} to out (2n floats).
+void ref_projected(void* h, int bin, float* out, int n) {
+  auto* s = (UnmanagedMultisliceSimulation*)h;
+  dim3 dimBlock(32, 8, 1);
+  dim3 dimGrid((s->resolutionX + dimBlock.x - 1) / dimBlock.x, (s->resolutionY + dimBlock.y - 1) / dimBlock.y, 1);
+  const float top = s->MaximumZ - s->MinimumZ;
+  const float z = top - (float)bin - 0.5f;
+  binnedAtomPKernel2<<<dimGrid, dimBlock>>>(s->devV, s->PixelScale, s->atomMemories.fparamsdev,
+                                            s->atomMemories.devAtomZPos, s->atomMemories.devAtomXPos,
+                                            s->atomMemories.devAtomYPos, s->atomMemories.devAtomZNum,
+                                            s->atomMemories.devBlockStartPositions, 1, z, (int)std::ceil(top / 1.0f),
+                                            s->sigma2, s->blockxoffset, s->blockyoffset);
+  cudaMemcpy(out, s->devV, sizeof(float) * 2 * n, cudaMemcpyDeviceToHost);
+}
+
+// The deterministic part of SimulateImage (U.cu:2323-2333): FFT(Psi),
+// normalisingKernel, imagingKernel2 (objective aperture, CTF with Cs, df,
+// two- and three-fold astigmatism, spatial and temporal coherence envelopes),
+// inverse FFT, normalisingKernel.  Writes that complex image (2n floats); its
+// squared modulus is the image before the detector chain.  Psi is unchanged.
+void ref_ctf_image(void* h, float* out, int n) {
+  auto* s = (UnmanagedMultisliceSimulation*)h;
+  dim3 dimBlock(32, 8, 1);
+  dim3 dimGrid((s->resolutionX + dimBlock.x - 1) / dimBlock.x, (s->resolutionY + dimBlock.y - 1) / dimBlock.y, 1);
+  cuComplex *img = nullptr, *img2 = nullptr;
+  cudaMalloc(&img, sizeof(cuComplex) * n);
+  cudaMalloc(&img2, sizeof(cuComplex) * n);
+  cufftExecC2C(s->plan, s->Psi, s->PsiPlus, CUFFT_FORWARD);
+  normalisingKernel<<<dimGrid, dimBlock>>>(s->PsiPlus, s->normalisingfactor);
+  imagingKernel2<<<dimGrid, dimBlock>>>(s->PsiPlus, s->resolutionX, s->resolutionY, s->Cs, s->df, s->Mod2fold,
+                                        s->Arg2fold, s->Mod3fold, s->Arg3fold, s->objectiveAperture, s->wavel, img2,
+                                        s->xFrequencies, s->yFrequencies, s->beta / 1000, s->delta);
+  cufftExecC2C(s->plan, img2, img, CUFFT_INVERSE);
+  normalisingKernel<<<dimGrid, dimBlock>>>(img, s->normalisingfactor);
+  cudaMemcpy(out, img, sizeof(float) * 2 * n, cudaMemcpyDeviceToHost);
+  cudaFree(img);
+  cudaFree(img2);
+}
 
 // The transmission function the last conventional step used (devV, U.cu:2101).
 void ref_transmission(void* h, float* out, int n) {

@@ -37,6 +37,7 @@ def load():
         "ref_wave": (None, [v, p, i]), "ref_exit_wave": (None, [v, p, i, p]), "ref_alloc_tds": (None, [v]),
         "ref_add_tds": (None, [v]), "ref_tds": (None, [v, p, i]),
         "ref_binned": (None, [v, i, i, p, p, p, p, p]), "ref_sync": (i, []), "ref_last_cuda_error": (C.c_char_p, []),
+        "ref_step_rs": (None, [v, i]), "ref_projected": (None, [v, i, p, i]), "ref_ctf_image": (None, [v, p, i]),
     }
     for n, (r, a) in sig.items():
         fn = getattr(L, n)
@@ -58,7 +59,8 @@ def xyz_text(Z, x, y, z):
     return "\n".join(lines) + "\n"
 
 
-def run_case(L, name, text, micro, calc, mode, dz, steps, trans_slices=(), stem_pos=None):
+def run_case(L, name, text, micro, calc, mode, dz, steps, trans_slices=(), stem_pos=None, ctf=False,
+             projected_bins=()):
     ref = L.ref_create()
     with tempfile.TemporaryDirectory() as td:
         path = os.path.join(td, "s.xyz")
@@ -106,6 +108,12 @@ def run_case(L, name, text, micro, calc, mode, dz, steps, trans_slices=(), stem_
     for i in range(1, nsteps + 1):
         if mode == "fd":
             L.ref_step_fd(ref, i)
+        elif mode == "rs":
+            L.ref_step_rs(ref, i)
+            if i in trans_slices:  # devV = {RS potential, 0} of this step
+                t = np.zeros(2 * N, np.float32)
+                L.ref_transmission(ref, ptr(t), N)
+                out[f"rspot_{i}"] = t[0::2].reshape(ny, nx).copy()
         else:
             L.ref_step_conv(ref, i)
             if i in trans_slices:
@@ -115,6 +123,14 @@ def run_case(L, name, text, micro, calc, mode, dz, steps, trans_slices=(), stem_
     w = np.zeros(2 * N, np.float32)
     L.ref_wave(ref, ptr(w), N)
     out["wave"] = w.view(np.complex64).reshape(ny, nx)
+    if ctf:  # imagingKernel2 on this wave, as SimulateImage applies it
+        im = np.zeros(2 * N, np.float32)
+        L.ref_ctf_image(ref, ptr(im), N)
+        out["ctf_image"] = im.view(np.complex64).reshape(ny, nx)
+    for b in projected_bins:  # binnedAtomPKernel2 over one-angstrom z-bin b
+        t = np.zeros(2 * N, np.float32)
+        L.ref_projected(ref, b, ptr(t), N)
+        out[f"proj_{b}"] = t.view(np.complex64).reshape(ny, nx)
     if stem_pos is not None:
         L.ref_add_tds(ref)
         tds = np.zeros(N, np.float32)
@@ -160,6 +176,20 @@ def main():
         # finite differences with the reference's automatic stable step, 30 steps
         "ref_sto_fd_128": dict(text=sto, micro=(200.0, 0.0, 0.0, 0.0, 1e7, 0.1, 30.0, 20.0),
                                calc=(0.1, 0.0, 128, 128, 0.0, 0.0, 0), mode="fd", dz=-1.0, steps=30),
+        # MultisliceStepRS as written, 5 steps, with the RS potential of steps 2 and 4
+        "ref_sto_rs_128": dict(text=sto, micro=(200.0, 0.0, 0.0, 0.0, 1e7, 0.1, 30.0, 20.0),
+                               calc=(0.1, 0.0, 128, 128, 2.0, 2.0, 0), mode="rs", dz=1.9525, steps=5,
+                               trans_slices=(2, 4)),
+        # the CTF image (imagingKernel2) of a conventional exit wave, with two-fold
+        # astigmatism and both coherence envelopes
+        "ref_sto_ctf_128": dict(text=sto, micro=(200.0, -500.0, 30.0, 0.4, 1e7, 0.5, 30.0, 20.0),
+                                calc=(0.1, -500.0, 128, 128, 2.0, 2.0, 0), mode="conv", dz=1.9525, steps=None,
+                                ctf=True),
+        # the projected potential (binnedAtomPKernel2, vzatom2) of three z-bins of
+        # the random structure
+        "ref_rand_proj_256": dict(text=rnd, micro=(300.0, 100.0, 0.0, 0.0, 1.2e7, 0.1, 30.0, 25.0),
+                                  calc=(0.0625, 100.0, 256, 256, 1.5, 0.5, 0), mode="conv", dz=1.0, steps=1,
+                                  projected_bins=(3, 6, 9)),
     }
     for name, kw in cases.items():
         out = run_case(L, name, **kw)

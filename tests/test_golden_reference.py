@@ -16,6 +16,9 @@ import pytest
 from tests.conftest import FPARAMS, GOLDEN
 
 CASES = sorted(glob.glob(os.path.join(GOLDEN, "ref_*.npz")))
+RS_POT_TOL = 1e-6  # RS potential (FP32 vatom sums in the reference)
+CTF_TOL = 1e-5     # CTF image intensity (FP32 cuFFT and FP32 aberration phase in the reference)
+PROJ_TOL = 1e-6    # projected-potential transmission exp(i sigma V)
 
 
 def rel_l2(a, b):
@@ -75,6 +78,12 @@ def test_oracle_matches_reference(oracle_mod, path, tmp_path):
     for i in range(1, nsteps + 1):
         if str(g["mode"]) == "fd":
             o.MultisliceStepFD(i)
+        elif str(g["mode"]) == "rs":
+            key = f"rspot_{i}"
+            if key in g.files:  # binnedAtomPKernelRS (U.cu:655-727), not exponentiated
+                v = o.PotentialRS(i)
+                assert rel_l2(g[key], v) < RS_POT_TOL, (i, rel_l2(g[key], v))
+            o.MultisliceStepRS(i)
         else:
             key = f"trans_{i}"
             if key in g.files:
@@ -86,6 +95,17 @@ def test_oracle_matches_reference(oracle_mod, path, tmp_path):
     # unnormalised inverse FFT and L1 sum run in FP32 in the reference)
     tol = 1e-5 if "tds" in g.files else 2e-6
     assert e < tol, e
+    if "ctf_image" in g.files:
+        # imagingKernel2 (U.cu:1044-1080): the image before the detector chain
+        img = o.SimulateImage()
+        e_img = rel_l2(np.abs(g["ctf_image"]) ** 2, img)
+        assert e_img < CTF_TOL, e_img
+    for key in (k for k in g.files if k.startswith("proj_")):
+        # binnedAtomPKernel2 (U.cu:513-578) over one-angstrom z-bin b: the
+        # oracle's projected slab it = b + 1 of thickness 1
+        b = int(key[5:])
+        t = np.exp(1j * sc["sigma2"] * o.PotentialProjected(b + 1, 1.0))
+        assert rel_l2(g[key], t) < PROJ_TOL, (b, rel_l2(g[key], t))
     if "tds" in g.files:
         o.AddTDSWaves()
         assert rel_l2(g["tds"], o.TDS()) < 1e-5

@@ -1,0 +1,198 @@
+"""Accuracy at the benchmark configurations' own sizes and depths, against the
+FP64 oracle, through the C ABI.
+
+The engine computes in FP32 complex; its error grows with every transform, so
+agreement after a few slices on a small grid says little about a 100-slice
+run at 1024^2.  These cases run the full slice stacks of the benchmark
+workloads:
+  C2  amorphous carbon 50x50x200 A (~50k atoms), 1024^2, every 2 A slice,
+      300 kV: exit wave (fused and plain paths) and CTF images over the
+      defocus sweep (MultisliceStepConv U.cu:2085-2124 over the GUI's slice
+      loop, CUDA Simulation GUI/MainWindow.xaml.cs:258-283; imagingKernel2
+      U.cu:1044-1080);
+  C3  Si [110] 8x6x50 cells, 512^2, 1.92 A slices, 200 kV, four frozen-phonon
+      configurations: the summed diffraction pattern and mean image (the TDS
+      pass loop of MainWindow.xaml.cs:353-402);
+  C4  GaN [11-20] 10x6x40 cells, 1024^2, 1.5945 A slices, 300 kV, 25 mrad
+      probes: 16 positions of the 128x128 raster, HAADF 70-200 mrad, and one
+      probe's exit wave;
+  C5  SrTiO3 4x4x50 cells, 512^2, 1.9525 A slices, 200 kV, an 8-image focal
+      series: loss, dL/dV of every slice and dL/d(atom x, y).
+Tolerances: relative L2 error <= 1e-5 for waves and images (the north-star
+bar), <= 1e-4 for detector signals and gradients."""
+import numpy as np
+import pytest
+
+from tests.conftest import FPARAMS
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5       # waves, images, diffraction patterns
+SIG_TOL = 1e-4   # detector signals
+GRAD_TOL = 1e-4  # gradients (loss: TOL)
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.complex128)
+    b = np.asarray(b, np.complex128)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.fixture(scope="module")
+def engine_cls():
+    from cudamultislice_b200 import ManagedMultisliceSimulation, build
+
+    build.build(verbose=False)
+    return ManagedMultisliceSimulation
+
+
+def setup(s, atoms, n, ps, *, kV, df, Cs, ap, dz, stem=False, xoff=2.0, yoff=2.0):
+    s.SetAtoms(*atoms)
+    s.UploadBinnedAtoms()
+    s.GetParameterisation(FPARAMS)
+    s.ApplyMicroscopeParameters(kV, df, 0.0, 0.0, Cs, 0.1, 30.0, ap)
+    if stem:
+        s.STEMSetCalculationVariables(ps, df, n, n, s.GetSizeX(), s.GetSizeY(), s.GetSizeZ())
+    else:
+        s.SetCalculationVariables(ps, df, n, n, s.GetSizeX(), s.GetSizeY(), s.GetSizeZ(), xoff, yoff)
+    s.PreCalculateFrequencies()
+    s.InitialiseWavefunctions(dz)
+
+
+# ---------------------------------------------------------------- C2
+C2 = dict(kV=300.0, df=0.0, Cs=1.2e7, ap=20.0, dz=2.0)
+C2_DEFOCI = np.array([-1000.0, -500.0, 0.0, 500.0, 1000.0], np.float32)
+
+
+@pytest.fixture(scope="module")
+def c2_oracle(oracle_mod):
+    from cudamultislice_b200 import structures as S
+
+    atoms = S.amorphous_carbon((50.0, 50.0, 200.0), density=0.1, min_sep=1.2)
+    orc = oracle_mod.OracleSimulation()
+    setup(orc, atoms, 1024, 50.0 / 1024, **C2)
+    S_ = orc.GetSlices(True)
+    psi = orc.run_conventional()
+    imgs = []
+    for d in C2_DEFOCI:
+        orc.ApplyMicroscopeParameters(C2["kV"], float(d), 0.0, 0.0, C2["Cs"], 0.1, 30.0, C2["ap"])
+        imgs.append(orc.SimulateImage())
+    orc.close()
+    return atoms, S_, psi, np.array(imgs)
+
+
+@pytest.mark.parametrize("path", [0, 1])
+def test_c2_amorphous_carbon_1024_all_slices(engine_cls, c2_oracle, path):
+    atoms, S_, psi, imgs = c2_oracle
+    assert S_ >= 100
+    eng = engine_cls()
+    eng.SetSlicePath(path)
+    setup(eng, atoms, 1024, 50.0 / 1024, **C2)
+    assert eng.RunConventional() == S_
+    e = rel_l2(eng.ExitWave(), psi)
+    assert e < TOL, (path, e)
+    got = eng.SimulateImageSeries(C2_DEFOCI)
+    for k in range(C2_DEFOCI.size):
+        ei = rel_l2(got[k], imgs[k])
+        assert ei < TOL, (path, float(C2_DEFOCI[k]), ei)
+    eng.close()
+
+
+# ---------------------------------------------------------------- C3
+def test_c3_silicon_frozen_phonons_512_full_depth(engine_cls, oracle_mod):
+    from cudamultislice_b200 import structures as S
+
+    atoms = S.silicon_110(8, 6, 50)
+    n, ps = 512, 6 * 5.431 / 512
+    kw = dict(kV=200.0, df=0.0, Cs=1e7, ap=20.0, dz=1.92)
+    seed, first, nconf, sigma = 0x5EED2026, 0, 4, 0.076
+    eng = engine_cls()
+    setup(eng, atoms, n, ps, **kw)
+    d, im = eng.FrozenPhonon(seed, first, nconf, sigma, batch=nconf)
+    S_ = eng.GetSlices(True)
+    eng.close()
+    orc = oracle_mod.OracleSimulation()
+    setup(orc, atoms, n, ps, **kw)
+    assert orc.GetSlices(True) == S_ and S_ >= 100
+    orc.AllocTDS()
+    imgs = []
+    for p in range(first, first + nconf):
+        orc.UploadBinnedAtomsTDS(seed, p, sigma)
+        orc.run_conventional()
+        orc.AddTDSWaves()
+        imgs.append(orc.SimulateImage())
+    ed, ei = rel_l2(d, orc.TDS()), rel_l2(im, np.mean(imgs, axis=0))
+    orc.close()
+    assert ed < TOL, ed
+    assert ei < TOL, ei
+
+
+# ---------------------------------------------------------------- C4
+def test_c4_gan_haadf_raster_1024_full_depth(engine_cls, oracle_mod):
+    from cudamultislice_b200 import structures as S
+
+    atoms = S.gan_wurtzite_11_20(10, 6, 40)
+    kw = dict(kV=300.0, df=0.0, Cs=0.0, ap=25.0, dz=1.5945, stem=True)
+    eng = engine_cls()
+    orc = oracle_mod.OracleSimulation()
+    for s in (eng, orc):
+        s.SetAtoms(*atoms)
+    n = 1024
+    ps = float(eng.GetSizeX()) / n
+    setup(eng, atoms, n, ps, **kw)
+    setup(orc, atoms, n, ps, **kw)
+    S_ = orc.GetSlices(True)
+    assert eng.GetSlices(True) == S_ and S_ >= 80
+    # 16 positions spread over the 128 x 128 raster
+    g = np.linspace(0, n - 1, 128).astype(np.int32)
+    sel = np.array([5, 40, 77, 120])
+    px, py = np.meshgrid(g[sel], g[sel])
+    px, py = px.ravel().astype(np.int32), py.ravel().astype(np.int32)
+    sig = eng.StemRaster(px, py, 70.0, 200.0, batch=16)
+    orc.CachePotentials(True)
+    ref = []
+    for k, (x, y) in enumerate(zip(px, py)):
+        orc.STEMInitialiseWavefunctions(int(x), int(y))
+        orc.run_conventional()
+        ref.append(orc.AnnularDetector(70.0, 200.0))
+        if k == 5:
+            psi5 = orc.Wave()
+    ref = np.array(ref)
+    assert np.all(ref > 0)
+    err = np.abs(sig - ref) / ref
+    assert err.max() < SIG_TOL, (err.max(), sig, ref)
+    # one probe's exit wave after every slice
+    eng.STEMInitialiseWavefunctions(int(px[5]), int(py[5]))
+    eng.RunConventional()
+    e = rel_l2(eng.ExitWave(), psi5)
+    assert e < TOL, e
+    eng.close()
+    orc.close()
+
+
+# ---------------------------------------------------------------- C5
+def test_c5_focal_series_gradient_512_full_depth(engine_cls, oracle_mod):
+    """Targets: the engine's images of the crystal with seeded position errors
+    (sigma 0.1 A); the gradient is taken at the ideal positions."""
+    from cudamultislice_b200 import structures as S
+
+    Z, x, y, z = S.srtio3(4, 4, 50)
+    rng = np.random.default_rng(2026)
+    pert = [(a + rng.normal(0.0, 0.1, a.size)).astype(np.float32) for a in (x, y, z)]
+    n, nslices = 512, 100
+    kw = dict(kV=200.0, df=0.0, Cs=1.0e7, ap=20.0, dz=1.9525)
+    df = np.linspace(-800.0, 600.0, 8).astype(np.float32)
+    eng = engine_cls()
+    setup(eng, (Z, *pert), n, 3.905 * 4 / n, **kw)
+    _, T = eng.FocalSeries(df, np.zeros((8, n, n), np.float32), nslices, images=True)
+    setup(eng, (Z, x, y, z), n, 3.905 * 4 / n, **kw)
+    L, gV, gxy = eng.FocalSeriesGrad(df, T, nslices)
+    eng.close()
+    orc = oracle_mod.OracleSimulation()
+    setup(orc, (Z, x, y, z), n, 3.905 * 4 / n, **kw)
+    L0, gV0, gxy0 = orc.FocalGrad(df, T.astype(np.float64), nslices)
+    orc.close()
+    assert abs(L - L0) / L0 < TOL, (L, L0)
+    eV, exy = rel_l2(gV, gV0), rel_l2(gxy, gxy0)
+    assert eV < GRAD_TOL, eV
+    assert exy < GRAD_TOL, exy

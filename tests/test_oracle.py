@@ -180,3 +180,36 @@ def test_binning_csr_properties(oracle_mod):
     assert np.array_equal(bx, (x - MinX)[order])
     assert np.array_equal(bZ, Z[order])
     assert np.array_equal(np.bincount(key, minlength=len(off) - 1), np.diff(off))
+
+
+def test_potential_cache_gives_identical_steps(oracle_mod):
+    """CachePotentials (probe rasters over one specimen) changes no result: two
+    probe positions, cached and uncached, bit for bit; a set-up change drops
+    the cached potentials."""
+    from cudamultislice_b200 import structures
+
+    def probe_runs(cache):
+        o = oracle_mod.OracleSimulation()
+        o.SetAtoms(*structures.srtio3(2, 2, 3))
+        o.UploadBinnedAtoms()
+        o.GetParameterisation(FPARAMS)
+        o.ApplyMicroscopeParameters(300.0, 0.0, 0.0, 0.0, 0.0, 0.1, 30.0, 25.0)
+        o.STEMSetCalculationVariables(0.1, 0.0, 64, 64, o.GetSizeX(), o.GetSizeY(), o.GetSizeZ())
+        o.PreCalculateFrequencies()
+        o.InitialiseWavefunctions(1.0)
+        o.CachePotentials(cache)
+        out = []
+        for px, py in ((10, 20), (40, 33)):
+            o.STEMInitialiseWavefunctions(px, py)
+            out.append(o.run_conventional())
+        # new positions after re-binning: the cache must not serve the old slab
+        x = structures.srtio3(2, 2, 3)
+        o.SetAtoms(x[0], x[1] + np.float32(0.3), x[2], x[3])
+        o.UploadBinnedAtoms()
+        o.STEMInitialiseWavefunctions(10, 20)
+        out.append(o.run_conventional())
+        o.close()
+        return out
+
+    for a, b in zip(probe_runs(False), probe_runs(True)):
+        assert np.array_equal(a, b)
