@@ -673,7 +673,7 @@ def main():
     if args.profile and args.fft_plan >= 0:
         sim.SetFFTPlan(args.fft_plan)
     fft_plan = sim.FFTPlan(1)
-    steps_per = 100
+    steps_per = 100  # slices per bench step (the workload's 100 slices of 2 A)
     for _ in range(max(args.warmup, 3)):
         sim.TimeSlices(steps_per, 1, breakdown=False)
 
@@ -701,25 +701,57 @@ def main():
         return
     value = slice_steps / (total_ms / 1000.0)
 
-    # per-pass split of the same loop (events between passes) for the roofline
-    _, row_ms, col_ms = sim.TimeSlices(steps_per, 1, breakdown=True)
+    # roofline of the dominant kernel.  With the persistent slice loop (one
+    # cooperative launch per bench step = 100 slices) that is the loop kernel
+    # itself: its launch duration is the step time; algorithmic bytes per
+    # launch = 100 slices x 20 B per pixel (psi read + written, V read).
     N = GRID * GRID
     peak, peak_kind = measured_peaks()
     step_ms = total_ms / (steps_per * args.steps)
-    row_bytes, col_bytes = 20 * N, 16 * N  # row pass: psi r/w + V; column pass: psi r/w
-    dom = ("row pass (k_pass_a: IFFT_row, x exp(i sigma V), FFT_row)", row_ms, row_bytes) if row_ms >= col_ms else \
-          ("column pass (k_pass_b: FFT_col, x P(k), IFFT_col)", col_ms, col_bytes)
-    achieved = dom[2] / (dom[1] / 1000.0) / 1e9
-    roofline = {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
-                "launch_ms": dom[1], "row_pass_ms": row_ms, "col_pass_ms": col_ms,
-                "step_achieved_gbs": BYTES_PER_PX_STEP * N / (step_ms / 1000.0) / 1e9,
-                "step_frac": BYTES_PER_PX_STEP * N / (step_ms / 1000.0) / 1e9 / peak}
+    loop_on = launches == args.steps
+    traffic = None
     traffic_file = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(traffic_file):
         with open(traffic_file) as f:
-            tr = json.load(f)
-        roofline["traffic"] = tr.get("row_pass" if row_ms >= col_ms else "col_pass")
+            traffic = json.load(f)
+    if loop_on:
+        launch_ms = total_ms / args.steps
+        algo = steps_per * BYTES_PER_PX_STEP * N
+        achieved = algo / (launch_ms / 1000.0) / 1e9
+        roofline = {"bound": "hbm", "kernel": "k_slice_loop (persistent cooperative slice loop: per slice a row "
+                    "phase IFFT_row, x exp(i sigma V), FFT_row and a column phase FFT_col, x P(k), IFFT_col, "
+                    "grid barriers between them)", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "peak_source": peak_kind,
+                    "traffic": (traffic or {}).get("slice_loop_per_launch"),
+                    "launch_ms": launch_ms, "slices_per_launch": steps_per,
+                    "algorithmic_bytes_per_launch": algo,
+                    "timing": "CUDA events on the engine stream around the timed launches, one launch per step"}
+    else:
+        _, row_ms, col_ms = sim.TimeSlices(steps_per, 1, breakdown=True)
+        row_bytes, col_bytes = 20 * N, 16 * N
+        dom = ("row pass", row_ms, row_bytes) if row_ms >= col_ms else ("column pass", col_ms, col_bytes)
+        achieved = dom[2] / (dom[1] / 1000.0) / 1e9
+        roofline = {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "peak_source": peak_kind, "traffic": None, "launch_ms": dom[1]}
+    roofline["step_achieved_gbs"] = BYTES_PER_PX_STEP * N / (step_ms / 1000.0) / 1e9
+    roofline["step_frac"] = roofline["step_achieved_gbs"] / peak
+
+    # the same loop on one launch per pass (the fused passes without the
+    # persistent kernel), and those passes timed back to back on their own
+    sim.SetSliceLoop(False)
+    sim.TimeSlices(steps_per, 1, breakdown=False)
+    pp_ms, _, _ = sim.TimeSlices(steps_per, args.steps, breakdown=False)
+    rv, cv = sim.FFTPlan(1)
+    row_us = sim.TimePass(0, 7, rv, 1, 200)  # A_INV | A_MULT_T | A_FWD
+    col_us = sim.TimePass(1, 2, cv, 1, 200)  # B_PROPAGATE
+    sim.SetSliceLoop(True)
+    per_pass = {"value": steps_per * args.steps / (pp_ms / 1000.0), "unit": UNIT,
+                "row_pass_us_back_to_back": row_us, "col_pass_us_back_to_back": col_us,
+                "row_pass_frac": 20 * N / (row_us * 1e-6) / 1e9 / peak,
+                "col_pass_frac": 16 * N / (col_us * 1e-6) / 1e9 / peak,
+                "plan": {"row_variant": rv, "col_variant": cv},
+                "note": "k_pass_a / k_pass_b launched per pass (programmatic dependent launch); per-pass times "
+                        "from ms_time_pass, each pass launched back to back on its own"}
 
     # plain path (cuFFT + one kernel per operation) on the same GPU and stack
     sim.SetSlicePath(1)
@@ -761,9 +793,12 @@ def main():
         "warmup": max(args.warmup, 3), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "c64 (FP32 complex)", "data": "synthetic (seeded)",
         "config": config_dict(len(Z)), "clocks": clk, "gpu_launches": launches,
-        "fft_plan": {"row_variant": fft_plan[0], "col_variant": fft_plan[1], "selected_by": "on-device autotuner"},
+        "fft_plan": ({"slice_loop": "packed 32-point plan (variant 3), one warp per line, both phases"} if loop_on
+                     else {"row_variant": fft_plan[0], "col_variant": fft_plan[1],
+                           "selected_by": "on-device autotuner"}),
         "roofline": roofline,
         "plain_path": {"value": plain_value, "unit": UNIT, "speedup_fused_vs_plain": value / world / plain_value},
+        "per_pass_path": per_pass,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(psi.nbytes),
                 "note": "host clock around the synchronous C-ABI calls: atoms in from pinned host memory, "

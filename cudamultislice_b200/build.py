@@ -20,7 +20,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 SOURCES = ["ms_engine.cu", "ms_slice.cu", "ms_atoms.cu", "ms_pointwise.cu", "ms_noalloc.cu", "ms_tiff.cu",
            "ms_slice_n64.cu", "ms_slice_n128.cu", "ms_slice_n256.cu", "ms_slice_n512.cu", "ms_slice_n1024.cu",
-           "ms_slice_n2048.cu", "ms_slice_n4096.cu"]
+           "ms_slice_n2048.cu", "ms_slice_n4096.cu", "ms_slice_loop.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", f"-I{INCLUDE}"]
 

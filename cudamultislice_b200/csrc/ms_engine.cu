@@ -109,6 +109,8 @@ class Engine {
   explicit Engine(int device) : device_(device) {}
   ~Engine() {
     if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    if (fd_graph_) cudaGraphExecDestroy(fd_graph_);
+    if (h_loop_err_) cudaFreeHost(h_loop_err_);
     if (have_plan_) cufftDestroy(plan_);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
@@ -126,6 +128,9 @@ class Engine {
     MS_TRY(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     MS_TRY(cudaEventCreate(&ev0_));
     MS_TRY(cudaEventCreate(&ev1_));
+    MS_TRY(d_loop_sync_.resize(2));
+    MS_TRY(cudaHostAlloc((void**)&h_loop_err_, sizeof(unsigned int), cudaHostAllocDefault));
+    *h_loop_err_ = 0;
     return MS_OK;
   }
 
@@ -145,6 +150,7 @@ class Engine {
         if (value != 0 && value != 1) return fail(MS_ERR_INVALID, "potential mode must be 0 or 1");
         pot_mode_ = value;
         stack_valid_ = false;
+    fd_stack_valid_ = false;
         invalidate_graph();
         return MS_OK;
       case MS_OPT_CHECKPOINT:
@@ -154,6 +160,21 @@ class Engine {
       case MS_OPT_FFT_PLAN:
         if (value < -1 || value >= plan_variants()) return fail(MS_ERR_INVALID, "FFT plan must be -1 (tuned) or a variant index");
         forced_plan_ = value;
+        invalidate_graph();
+        return MS_OK;
+      case MS_OPT_SLICE_LOOP:
+        if (value != 0 && value != 1) return fail(MS_ERR_INVALID, "slice loop must be 0 (persistent) or 1 (per pass)");
+        loop_off_ = value == 1;
+        invalidate_graph();
+        return MS_OK;
+      case MS_OPT_LOOP_WAIT_US:
+        if (value < 1) return fail(MS_ERR_INVALID, "wait bound must be >= 1 microsecond");
+        loop_limit_ns_ = 1000ull * (unsigned long long)value;
+        invalidate_graph();
+        return MS_OK;
+      case MS_OPT_LOOP_WAIT_TEST:
+        if (value < 0) return fail(MS_ERR_INVALID, "test arrivals must be >= 0");
+        loop_extra_ = (unsigned int)value;
         invalidate_graph();
         return MS_OK;
       default:
@@ -232,7 +253,8 @@ class Engine {
     box_.MinZ = hz_[mnz] - 2;
     have_atoms_ = true;
     have_index_ = false;
-    stack_valid_ = false;  // (the slice-loop graph depends on the stack's allocation only)
+    stack_valid_ = false;
+    fd_stack_valid_ = false;  // (the slice-loop graph depends on the stack's allocation only)
     return MS_OK;
   }
 
@@ -276,6 +298,7 @@ class Engine {
     have_index_ = true;
     hzoff_.clear();
     stack_valid_ = false;
+    fd_stack_valid_ = false;
     return MS_OK;
   }
 
@@ -322,6 +345,7 @@ class Engine {
     MS_TRY(copy_sync(d_coef_.p, coef.data(), sizeof(float) * coef.size(), cudaMemcpyHostToDevice));
     have_fp_ = true;
     stack_valid_ = false;
+    fd_stack_valid_ = false;
     invalidate_graph();
     return MS_OK;
   }
@@ -378,6 +402,7 @@ class Engine {
     have_freq_ = false;
     have_waves_ = false;
     stack_valid_ = false;
+    fd_stack_valid_ = false;
     invalidate_graph();
     return MS_OK;
   }
@@ -435,6 +460,7 @@ class Engine {
     have_freq_ = true;
     have_waves_ = false;
     stack_valid_ = false;
+    fd_stack_valid_ = false;
     invalidate_graph();
     return MS_OK;
   }
@@ -446,6 +472,7 @@ class Engine {
     const float dz = conv_dz > 0 ? conv_dz : 1.0f;  // U.cu:1968 / U.cu:2005
     if (dz != convdz_) {
       stack_valid_ = false;
+    fd_stack_valid_ = false;
       invalidate_graph();
     }
     convdz_ = dz;
@@ -477,6 +504,8 @@ class Engine {
     int n = (int)std::ceil((box_.MaxZ - box_.MinZ) / dz);
     nFD_ = n + (n == 0);
     fd_stable_ = true;
+    fd_stack_valid_ = false;
+    invalidate_graph();
     return MS_OK;
   }
 
@@ -561,7 +590,9 @@ class Engine {
   // MultisliceStep (U.cu:2040-2083) becomes one row pass (IFFT_row, the
   // three-level stencil without its Laplacian, FFT_row) and one column pass
   // (FFT_col, + rc dz^2 4 pi^2 k^2 FFT2(psi_n), band limit, IFFT_col).
-  int step_fd_fused(int it) {
+  // `Vplane`: the step's band-limited potential plane from the FD stack
+  // (run_fd), or null to build it here.
+  int step_fd_fused(int it, const float* Vplane = nullptr) {
     const Grid2 g{nx_, ny_};
     const long long N = (long long)nx_ * ny_;
     MS_TRY(d_fdX_.resize(N));
@@ -581,23 +612,17 @@ class Engine {
       fd_state_ = true;
     }
     // V at the plane, band-limited (U.cu:2053-2063), real part kept
-    if (int rc = potential_slice(POT_FD, it, d_f_.p)) return rc;
-    MS_TRY(pw_real_to_complex(d_f_.p, d_t1_.p, g, stream_, &launches));
-    MS_TRY(pass_a(passa_args(d_t1_.p, d_t1_.p, 0), A_FWD, 1));
-    PassBArgs bl = passb_args(d_t1_.p, d_t1_.p, 0);
-    bl.scale = 1.0f / (float)N;
-    MS_TRY(pass_b(bl, B_BANDLIMIT, 1));
-    PassAArgs vr = passa_args(d_t1_.p, nullptr, 0);
-    vr.out_f = d_f_.p;
-    MS_TRY(pass_a(vr, A_INV | A_REAL, 1));
-    launches += 3;
+    if (!Vplane) {
+      if (int rc = fd_plane_fused(it, d_f_.p)) return rc;
+      Vplane = d_f_.p;
+    }
     // coefficients of finiteDifferenceKernel (U.cu:1006-1012), pi = 3.14159
     const double dz = dzFD_, lam = wavel_, aa = 2.0 * 3.14159 * dz / lam, den = 1.0 + aa * aa;
     const double rcx = 1.0 / den, rcy = -aa / den;
     PassAArgs a = passa_args(d_fdX_.p, d_fdQ_.p, 0);
     a.in2 = d_psim_.p;
     a.out2 = d_psi_.p;
-    a.V = d_f_.p;
+    a.V = Vplane;
     a.fd_rc = make_float2((float)rcx, (float)rcy);
     a.fd_ratio = make_float2((float)((1.0 - aa * aa) / den), (float)(-2.0 * aa / den));
     a.fd_kv = (float)(dz * dz * 4.0 * 3.14159 * (double)sigma2_ / lam);
@@ -611,8 +636,174 @@ class Engine {
     launches += 2;
     std::swap(d_psim_.p, d_psi_.p);  // psi_n becomes psi_{n-1}
     domain_ = 2;                      // current wave held as X
-    invalidate_graph();
+    if (!capturing_) invalidate_graph();  // a single step leaves the FD run's graph stale too
     return MS_OK;
+  }
+
+  // The band-limited FD potential plane of step `it` (binnedAtomPKernelFD,
+  // then BandLimitKernel in k-space, U.cu:2051-2063) on the fused passes, real
+  // part into out (ny x nx floats).
+  int fd_plane_fused(int it, float* out) {
+    const Grid2 g{nx_, ny_};
+    const long long N = (long long)nx_ * ny_;
+    if (int rc = potential_slice(POT_FD, it, d_f_.p)) return rc;
+    MS_TRY(pw_real_to_complex(d_f_.p, d_t1_.p, g, stream_, &launches));
+    MS_TRY(pass_a(passa_args(d_t1_.p, d_t1_.p, 0), A_FWD, 1));
+    PassBArgs bl = passb_args(d_t1_.p, d_t1_.p, 0);
+    bl.scale = 1.0f / (float)N;
+    MS_TRY(pass_b(bl, B_BANDLIMIT, 1));
+    PassAArgs vr = passa_args(d_t1_.p, nullptr, 0);
+    vr.out_f = out;
+    MS_TRY(pass_a(vr, A_INV | A_REAL, 1));
+    launches += 3;
+    return MS_OK;
+  }
+
+  // ---- finite differences as a whole run ----
+  // The band-limited potential planes of FD steps 1..S, kept resident like the
+  // conventional stack (rebuilt when the structure, grid or FD step changes):
+  // real planes for the fused passes, complex ones for the plain path (whose
+  // update kernel reads complex V, as finiteDifferenceKernel U.cu:995-1023).
+  int build_fd_stack(int S) {
+    const bool fused = use_fused();
+    if (fd_stack_valid_ && fd_nstack_ >= S && fd_stack_dz_ == dzFD_ && fd_stack_fused_ == fused) return MS_OK;
+    const size_t N = (size_t)nx_ * ny_;
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess &&
+        (double)N * S * (fused ? sizeof(float) : sizeof(float2)) > 0.5 * (double)free_b)
+      return fail(MS_ERR_NOMEM, "the FD potential stack of " + std::to_string(S) +
+                                    " planes would take more than half the free device memory");
+    fd_stack_valid_ = false;
+    if (fused) {
+      d_fdstack_c_.release();
+      MS_TRY(d_fdstack_.resize(N * S));
+      for (int it = 1; it <= S; ++it)
+        if (int rc = fd_plane_fused(it, d_fdstack_.p + (size_t)(it - 1) * N)) return rc;
+    } else {
+      d_fdstack_.release();
+      MS_TRY(d_fdstack_c_.resize(N * S));
+      const Grid2 g{nx_, ny_};
+      const float nf = 1.0f / std::sqrt((float)(nx_ * ny_));
+      for (int it = 1; it <= S; ++it) {
+        float2* plane = d_fdstack_c_.p + (size_t)(it - 1) * N;
+        if (int rc = potential_slice(POT_FD, it, d_f_.p)) return rc;
+        MS_TRY(pw_real_to_complex(d_f_.p, d_t1_.p, g, stream_, &launches));
+        MS_TRY_FFT(cufftExecC2C(plan_, d_t1_.p, d_t2_.p, CUFFT_FORWARD));
+        MS_TRY(pw_bandlimit(d_t2_.p, d_kx_.p, d_ky_.p, kmax_, nf * nf, g, stream_, &launches));
+        MS_TRY_FFT(cufftExecC2C(plan_, d_t2_.p, plane, CUFFT_INVERSE));
+      }
+    }
+    MS_TRY(cudaStreamSynchronize(stream_));
+    fd_nstack_ = S;
+    fd_stack_dz_ = dzFD_;
+    fd_stack_fused_ = fused;
+    fd_stack_valid_ = true;
+    return MS_OK;
+  }
+
+  // FD steps 1..S (S <= 0: the structure's FD step count) from the initial
+  // waves over the resident band-limited potential stack: on the fused path
+  // one captured CUDA graph (two passes per step), replayed while the stack,
+  // the step count and the wave buffers stay the same; on the plain path the
+  // reference's per-step launch sequence without the potential build.  Device
+  // time in ms_get_last_device_ms.
+  int run_fd(int nsteps, int* out_steps) {
+    if (!have_waves_) return fail(MS_ERR_STATE, "wavefunctions not initialised");
+    if (!fd_stable_) return fail(MS_ERR_NUMERIC, "no stable finite-difference step for these conditions");
+    if (int rc = require_potential_inputs()) return rc;
+    const int S = nsteps > 0 ? nsteps : nFD_;
+    if (S < 1 || S > 100000) return fail(MS_ERR_INVALID, "need 1 <= steps <= 100000");
+    if (int rc = build_fd_stack(S)) return rc;
+    const size_t N = (size_t)nx_ * ny_;
+    if (use_fused()) {
+      if (int rc = ensure_real()) return rc;
+      plan_for(1);  // tune outside the capture
+      MS_TRY(d_fdX_.resize(N));
+      MS_TRY(d_fdQ_.resize(N));
+      MS_TRY(d_fdS_.resize(N));
+      if (!fd_graph_ || fd_graph_S_ != S || fd_graph_stack_ != d_fdstack_.p || fd_graph_psi_ != d_psi_.p ||
+          fd_graph_psim_ != d_psim_.p) {
+        drop_fd_graph();
+        float2* psi0 = d_psi_.p;
+        float2* psim0 = d_psim_.p;
+        fd_state_ = false;
+        capturing_ = true;
+        MS_TRY(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        int rc = MS_OK;
+        for (int it = 1; it <= S && rc == MS_OK; ++it) rc = step_fd_fused(it, d_fdstack_.p + (size_t)(it - 1) * N);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(stream_, &graph);
+        capturing_ = false;
+        // nothing ran: the waves are still in the buffers the capture started on
+        fd_graph_psi_end_ = d_psi_.p;
+        fd_graph_psim_end_ = d_psim_.p;
+        d_psi_.p = psi0;
+        d_psim_.p = psim0;
+        domain_ = 0;
+        fd_state_ = false;
+        if (rc != MS_OK) {
+          if (graph) cudaGraphDestroy(graph);
+          return rc;
+        }
+        if (e != cudaSuccess) return fail(MS_ERR_CUDA, std::string("FD graph capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&fd_graph_, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+          fd_graph_ = nullptr;
+          return fail(MS_ERR_CUDA, std::string("FD graph instantiate: ") + cudaGetErrorString(e));
+        }
+        fd_graph_S_ = S;
+        fd_graph_stack_ = d_fdstack_.p;
+        fd_graph_psi_ = psi0;
+        fd_graph_psim_ = psim0;
+      }
+      MS_TRY(cudaEventRecord(ev0_, stream_));
+      MS_TRY(cudaGraphLaunch(fd_graph_, stream_));
+      MS_TRY(cudaEventRecord(ev1_, stream_));
+      launches += 4 + 2LL * S;
+      d_psi_.p = fd_graph_psi_end_;
+      d_psim_.p = fd_graph_psim_end_;
+      fd_state_ = true;
+      domain_ = 2;
+    } else {
+      if (int rc = ensure_real()) return rc;
+      MS_TRY(cudaEventRecord(ev0_, stream_));
+      for (int it = 1; it <= S; ++it)
+        if (int rc = step_fd_plain(d_fdstack_c_.p + (size_t)(it - 1) * N)) return rc;
+      MS_TRY(cudaEventRecord(ev1_, stream_));
+    }
+    MS_TRY(cudaStreamSynchronize(stream_));
+    MS_TRY(cudaEventElapsedTime(&last_device_ms_, ev0_, ev1_));
+    drop_conv_graph();  // the conventional loop's graph holds the old wave buffers
+    if (out_steps) *out_steps = S;
+    return MS_OK;
+  }
+
+  // One plain-path FD step on a band-limited complex potential plane: the
+  // spectral Laplacian, the three-level update and the band limit of psi+
+  // (U.cu:2066-2082), cuFFT plus one kernel per operation.
+  int step_fd_plain(const float2* Vc) {
+    const Grid2 g{nx_, ny_};
+    const float nf = 1.0f / std::sqrt((float)(nx_ * ny_));
+    MS_TRY_FFT(cufftExecC2C(plan_, d_psi_.p, d_t2_.p, CUFFT_FORWARD));
+    MS_TRY(pw_laplacian(d_t2_.p, d_kx_.p, d_ky_.p, nf * nf, g, stream_, &launches));
+    MS_TRY_FFT(cufftExecC2C(plan_, d_t2_.p, d_grad_.p, CUFFT_INVERSE));
+    MS_TRY(pw_fd_update(d_grad_.p, d_psim_.p, d_t2_.p, d_psi_.p, Vc, sigma2_, wavel_, dzFD_, g, stream_,
+                        &launches));
+    MS_TRY_FFT(cufftExecC2C(plan_, d_t2_.p, d_t1_.p, CUFFT_FORWARD));
+    MS_TRY(pw_bandlimit(d_t1_.p, d_kx_.p, d_ky_.p, kmax_, nf * nf, g, stream_, &launches));
+    MS_TRY_FFT(cufftExecC2C(plan_, d_t1_.p, d_t2_.p, CUFFT_INVERSE));
+    std::swap(d_psim_.p, d_psi_.p);
+    std::swap(d_psi_.p, d_t2_.p);
+    domain_ = 0;
+    fd_state_ = false;
+    return MS_OK;
+  }
+
+  void drop_fd_graph() {
+    if (fd_graph_) cudaGraphExecDestroy(fd_graph_);
+    fd_graph_ = nullptr;
+    fd_graph_S_ = -1;
   }
 
   // ---- queries ----
@@ -1296,13 +1487,28 @@ class Engine {
     int S = 0;
     if (int rc = build_stack(&S)) return rc;
     if (int rc = ensure_prop_tables(convdz_)) return rc;
+    const bool loop = use_loop();
     if (use_fused()) {
-      plan_for(1);  // tune outside the capture (tuning allocates and synchronises)
+      if (loop) {
+        if (int rc = prepare_loop()) return rc;
+      } else {
+        plan_for(1);  // tune outside the capture (tuning allocates and synchronises)
+      }
       if (!graph_exec_ || graph_S_ != S || graph_stack_ != d_stack_.p) {
         invalidate_graph();
         MS_TRY(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
         int rc = MS_OK;
-        for (int it = 1; it <= S && rc == MS_OK; ++it) rc = enqueue_fused_step(d_stack_.p + (size_t)(it - 1) * nx_ * ny_, it == 1);
+        if (loop) {
+          // the whole slice loop: one cooperative launch, its barrier state
+          // cleared before it and its error word read back after it
+          rc = enqueue_loop(d_stack_.p, S, true);
+          if (rc == MS_OK && cudaMemcpyAsync(h_loop_err_, d_loop_sync_.p + 1, sizeof(unsigned int),
+                                             cudaMemcpyDeviceToHost, stream_) != cudaSuccess)
+            rc = fail(MS_ERR_CUDA, "loop error read-back");
+        } else {
+          for (int it = 1; it <= S && rc == MS_OK; ++it)
+            rc = enqueue_fused_step(d_stack_.p + (size_t)(it - 1) * nx_ * ny_, it == 1);
+        }
         cudaGraph_t graph = nullptr;
         cudaError_t e = cudaStreamEndCapture(stream_, &graph);
         if (rc != MS_OK) {
@@ -1319,9 +1525,10 @@ class Engine {
         graph_S_ = S;
         graph_stack_ = d_stack_.p;
       }
+      *h_loop_err_ = 0;
       MS_TRY(cudaEventRecord(ev0_, stream_));
       MS_TRY(cudaGraphLaunch(graph_exec_, stream_));
-      launches += 2LL * S;
+      launches += loop ? 1 : 2LL * S;
       domain_ = 1;
     } else {
       MS_TRY(cudaEventRecord(ev0_, stream_));
@@ -1331,8 +1538,57 @@ class Engine {
     MS_TRY(cudaEventRecord(ev1_, stream_));
     MS_TRY(cudaStreamSynchronize(stream_));
     MS_TRY(cudaEventElapsedTime(&last_device_ms_, ev0_, ev1_));
+    if (loop && use_fused() && *h_loop_err_ != 0) return loop_timeout_fail();
     if (nslices) *nslices = S;
     return MS_OK;
+  }
+
+  // The persistent slice loop runs the conventional loop where it is provided
+  // (square 256, 512, 1024 grids), unless MS_OPT_SLICE_LOOP turns it off or an
+  // FFT plan variant is forced (MS_OPT_FFT_PLAN selects per-pass kernels).
+  bool use_loop() const {
+    return use_fused() && !loop_off_ && forced_plan_ < 0 && slice_loop_variant(nx_, ny_) >= 0;
+  }
+  int prepare_loop() {
+    if (loop_grid_ > 0 && loop_grid_n_ == nx_) return MS_OK;
+    int grid = 0;
+    MS_TRY(slice_loop_prepare(nx_, &grid));
+    loop_grid_ = grid;
+    loop_grid_n_ = nx_;
+    return MS_OK;
+  }
+  LoopArgs loop_args(const float* Vstack, int S) {
+    const int v = slice_loop_variant(nx_, ny_);
+    LoopArgs L{};
+    L.a = passa_args(d_psi0_.p, d_psi_.p, v);
+    L.b = passb_args(d_psi_.p, d_psi_.p, v);
+    L.psi0 = d_psi0_.p;
+    L.wave = d_psi_.p;
+    L.Vstack = Vstack;
+    L.vstride = (long long)nx_ * ny_;
+    L.S = S;
+    L.sync.count = d_loop_sync_.p;
+    L.sync.error = reinterpret_cast<int*>(d_loop_sync_.p + 1);
+    L.sync.limit_ns = loop_limit_ns_;
+    L.sync.expect_extra = loop_extra_;
+    return L;
+  }
+  // Enqueues the slice loop over S slices of Vstack (no host sync, no
+  // allocation): the arrival counter is cleared first, and the error word too
+  // when `clear_error` (the first launch of a sequence).
+  int enqueue_loop(const float* Vstack, int S, bool clear_error) {
+    fd_state_ = false;
+    MS_TRY(cudaMemsetAsync(d_loop_sync_.p, 0, (clear_error ? 2 : 1) * sizeof(unsigned int), stream_));
+    MS_TRY(launch_slice_loop(loop_args(Vstack, S), loop_grid_, stream_));
+    domain_ = 1;
+    return MS_OK;
+  }
+  int loop_timeout_fail() {
+    domain_ = 0;
+    have_waves_ = false;
+    return fail(MS_ERR_CUDA,
+                "persistent slice loop: a grid-barrier wait ran out (MS_OPT_LOOP_WAIT_US); the wave is undefined, "
+                "initialise the wavefunctions again");
   }
 
   int time_slices(int steps, int reps, float* total_ms, float* row_ms, float* col_ms) {
@@ -1342,17 +1598,32 @@ class Engine {
     if (int rc = build_stack(&S)) return rc;
     if (int rc = ensure_prop_tables(convdz_)) return rc;
     const size_t N = (size_t)nx_ * ny_;
+    const bool loop = use_loop() && steps <= S;
+    if (loop) {
+      if (int rc = prepare_loop()) return rc;
+    }
     MS_TRY(cudaStreamSynchronize(stream_));
-    // whole steps, back to back
+    // whole steps, back to back (the persistent loop: one launch per repetition)
+    *h_loop_err_ = 0;
     MS_TRY(cudaEventRecord(ev0_, stream_));
-    for (int r = 0; r < reps; ++r)
-      for (int k = 0; k < steps; ++k)
-        if (int rc = transmit_propagate(d_stack_.p + (size_t)(k % S) * N, k == 0)) return rc;
+    for (int r = 0; r < reps; ++r) {
+      if (loop) {
+        if (int rc = enqueue_loop(d_stack_.p, steps, r == 0)) return rc;
+        ++launches;
+      } else {
+        for (int k = 0; k < steps; ++k)
+          if (int rc = transmit_propagate(d_stack_.p + (size_t)(k % S) * N, k == 0)) return rc;
+      }
+    }
     MS_TRY(cudaEventRecord(ev1_, stream_));
-    MS_TRY(cudaEventSynchronize(ev1_));
+    if (loop)
+      MS_TRY(cudaMemcpyAsync(h_loop_err_, d_loop_sync_.p + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, stream_));
+    MS_TRY(cudaStreamSynchronize(stream_));
+    if (loop && *h_loop_err_ != 0) return loop_timeout_fail();
     MS_TRY(cudaEventElapsedTime(total_ms, ev0_, ev1_));
     if (!row_ms || !col_ms) return MS_OK;  // no per-pass breakdown requested
     *row_ms = *col_ms = 0.0f;
+    if (loop) return MS_OK;  // one launch per repetition: no per-pass split
     if (use_fused()) {
       // the same sequence with an event between every pass: per-launch averages
       std::vector<cudaEvent_t> ev(2 * steps + 1, nullptr);
@@ -1732,12 +2003,20 @@ class Engine {
   bool use_fused() const { return fused_ok_ && !force_plain_; }
 
 
-  void invalidate_graph() {
+  // Drops the captured slice-loop graph (it holds the wave buffers, tables and
+  // set-up scalars as kernel arguments).
+  void drop_conv_graph() {
     if (graph_exec_) {
       cudaGraphExecDestroy(graph_exec_);
       graph_exec_ = nullptr;
     }
     graph_S_ = -1;
+  }
+  // Every change of the grid, structure, parameters or options drops both
+  // captured graphs (conventional loop and FD run).
+  void invalidate_graph() {
+    drop_conv_graph();
+    drop_fd_graph();
   }
 
   int require_potential_inputs() {
@@ -2136,6 +2415,24 @@ class Engine {
   bool have_waves_ = false, stack_valid_ = false, have_tds_ = false, tds_host_valid_ = false;
   int nstack_ = 0;
   cudaGraphExec_t graph_exec_ = nullptr;
+  // whole FD runs: resident band-limited planes and the captured step graph
+  DevBuf<float> d_fdstack_;
+  DevBuf<float2> d_fdstack_c_;
+  bool fd_stack_valid_ = false, fd_stack_fused_ = false, capturing_ = false;
+  int fd_nstack_ = 0;
+  float fd_stack_dz_ = -1.0f;
+  cudaGraphExec_t fd_graph_ = nullptr;
+  int fd_graph_S_ = -1;
+  const float* fd_graph_stack_ = nullptr;
+  float2 *fd_graph_psi_ = nullptr, *fd_graph_psim_ = nullptr, *fd_graph_psi_end_ = nullptr,
+         *fd_graph_psim_end_ = nullptr;
+  // persistent slice loop: barrier state [count, error], pinned error copy
+  DevBuf<unsigned int> d_loop_sync_;
+  unsigned int* h_loop_err_ = nullptr;
+  int loop_grid_ = 0, loop_grid_n_ = 0;
+  bool loop_off_ = false;
+  unsigned int loop_extra_ = 0;
+  unsigned long long loop_limit_ns_ = 1000000000ull;
   int graph_S_ = -1;
   const float* graph_stack_ = nullptr;  // stack allocation the graph was captured on
   // host read-out
@@ -2435,6 +2732,9 @@ ms_status ms_build_potential_stack(ms_sim* s, int* nslices) {
 }
 ms_status ms_run_conventional(ms_sim* s, int* nslices) {
   return guarded(s, [&](ms::Engine& e) { return e.run_conventional(nslices); });
+}
+ms_status ms_run_fd(ms_sim* s, int nsteps, int* nsteps_out) {
+  return guarded(s, [&](ms::Engine& e) { return e.run_fd(nsteps, nsteps_out); });
 }
 ms_status ms_annular_detector(ms_sim* s, float inner, float outer, double* out) {
   if (ms_status r = out_check(s, out)) return r;

@@ -116,4 +116,33 @@ int make_twiddles(int n, int variant, float2* host_out);
 cudaError_t launch_pass_a(const PassAArgs& a, int variant, int flags, int batch, cudaStream_t s);
 cudaError_t launch_pass_b(const PassBArgs& a, int variant, int mode, int batch, cudaStream_t s);
 
+// ---- persistent slice loop (ms_slice_loop.cuh) ----
+struct LoopSync {
+  unsigned int* count;          // grid-barrier arrivals, zeroed before the launch
+  int* error;                   // 0, or kLoopTimeout after a wait ran out
+  unsigned long long limit_ns;  // bound on each wait
+  unsigned int expect_extra;    // added to every barrier's target: a target the
+                                // grid cannot reach (tests of the bound)
+};
+constexpr int kLoopTimeout = 1;
+
+struct LoopArgs {
+  PassAArgs a;          // row phase (twiddles, sigma; the wave set below)
+  PassBArgs b;          // column phase (twiddles, propagator, band limit)
+  const float2* psi0;   // initial wave (real space), read by slice 1
+  float2* wave;         // the wave, left in row-frequency form
+  const float* Vstack;  // potentials [S][ny][nx]
+  long long vstride;    // floats between slices of the stack
+  int S;                // slices
+  LoopSync sync;
+};
+// FFT plan variant whose twiddle tables the persistent loop uses on an nx x ny
+// grid, or -1 where it is not provided (non-square, or not 256/512/1024).
+int slice_loop_variant(int nx, int ny);
+// Raises the loop kernel's shared-memory limit and returns its grid (one CTA
+// per SM, all resident).
+cudaError_t slice_loop_prepare(int n, int* grid);
+// Cooperative launch of the whole slice loop.
+cudaError_t launch_slice_loop(const LoopArgs& L, int grid, cudaStream_t s);
+
 }  // namespace ms

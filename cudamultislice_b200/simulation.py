@@ -96,6 +96,20 @@ class ManagedMultisliceSimulation:
         wave when they fit in an eighth of free device memory, else ceil(sqrt(S)))."""
         self._chk(self._L.ms_set_option(self._h, 4, int(stride)))
 
+    def SetSliceLoop(self, persistent: bool):
+        """Conventional slice loop on square 256/512/1024 grids: one persistent
+        cooperative launch for all slices (True, the default) or one launch per
+        row and column pass (False)."""
+        self._chk(self._L.ms_set_option(self._h, 5, 0 if persistent else 1))
+
+    def SetLoopWaitUs(self, us: int):
+        """Bound on each grid-barrier wait of the persistent loop (microseconds)."""
+        self._chk(self._L.ms_set_option(self._h, 6, int(us)))
+
+    def SetLoopWaitTest(self, extra: int):
+        """Test hook: every grid barrier waits for `extra` arrivals that never come."""
+        self._chk(self._L.ms_set_option(self._h, 7, int(extra)))
+
     # ---- structure ----
     def ImportAtoms(self, filename: str):
         self._chk(self._L.ms_import_atoms(self._h, filename.encode()))
@@ -266,6 +280,13 @@ class ManagedMultisliceSimulation:
     def RunConventional(self) -> int:
         out = C.c_int()
         self._chk(self._L.ms_run_conventional(self._h, C.byref(out)))
+        return out.value
+
+    def RunFD(self, nsteps: int = 0) -> int:
+        """Finite-difference steps 1..nsteps (0: GetSlices(False)) from the
+        initial waves; returns the step count (device time: LastDeviceMs)."""
+        out = C.c_int()
+        self._chk(self._L.ms_run_fd(self._h, int(nsteps), C.byref(out)))
         return out.value
 
     def AnnularDetector(self, inner_mrad: float, outer_mrad: float) -> float:

@@ -66,11 +66,22 @@ enum {
                                (0: most points per thread ... 2: most threads per line;
                                3..5: 0..2 with butterflies on the packed FP32x2 pipe).
                                Variants agree to FP32 rounding, not bit for bit. */
-  MS_OPT_CHECKPOINT = 4     /* focal-series gradient: slices between stored waves;
+  MS_OPT_CHECKPOINT = 4,    /* focal-series gradient: slices between stored waves;
                                0 = automatic (default): every wave when the S waves
                                fit in an eighth of the free device memory, else
                                ceil(sqrt(S)); 1 = store every wave; >= S = one
                                segment recomputed from the initial wave */
+  MS_OPT_SLICE_LOOP = 5,    /* fused conventional slice loop (ms_run_conventional,
+                               ms_time_slices) on square 256, 512 and 1024 grids:
+                               0 = one persistent cooperative launch for all slices,
+                               the phases separated by grid barriers (default);
+                               1 = one launch per row and per column pass */
+  MS_OPT_LOOP_WAIT_US = 6,  /* bound on each grid-barrier wait of the persistent slice
+                               loop, microseconds (default 1,000,000); a wait that runs
+                               out ends the launch and the call fails with MS_ERR_CUDA */
+  MS_OPT_LOOP_WAIT_TEST = 7 /* test hook: > 0 makes every grid barrier wait for that many
+                               arrivals more than the grid has, so the wait bound runs out
+                               (0 = off, the default) */
 };
 
 /* ---- lifecycle ---- */
@@ -214,9 +225,20 @@ ms_status ms_get_grid(ms_sim* sim, int* nx, int* ny);
 /* Builds the potentials of slices 1..S into a device-resident stack. */
 ms_status ms_build_potential_stack(ms_sim* sim, int* nslices);
 /* Runs conventional slices 1..S from the initial wave (replayed as one
- * captured CUDA graph); equivalent to ms_multislice_step_conventional(i)
- * for i = 1..S. */
+ * captured CUDA graph: on square 256, 512 and 1024 grids a single persistent
+ * cooperative launch for all slices, MS_OPT_SLICE_LOOP); equivalent to
+ * ms_multislice_step_conventional(i) for i = 1..S, the GUI's step loop
+ * (CUDA Simulation GUI/MainWindow.xaml.cs:258-283). */
 ms_status ms_run_conventional(ms_sim* sim, int* nslices);
+/* Runs finite-difference steps 1..nsteps (nsteps <= 0: ms_get_slices(sim, 0,
+ * ...)) from the initial waves: MultisliceStep (U.cu:2040-2083) as the GUI
+ * loops over it (MainWindow.xaml.cs:258-283), equivalent to
+ * ms_multislice_step_fd(i) for i = 1..nsteps.  The band-limited potential
+ * planes are built once into a device-resident stack (rebuilt when the
+ * structure, grid or FD step changes); the fused path then replays one
+ * captured CUDA graph of two passes per step.  *nsteps_out (may be NULL)
+ * receives the step count; device time in ms_get_last_device_ms. */
+ms_status ms_run_fd(ms_sim* sim, int nsteps, int* nsteps_out);
 /* Annular detector (no reference counterpart; the HAADF/ADF STEM signal):
  * sum over inner <= theta < outer (mrad) of |FFT(psi)|^2 / N. */
 ms_status ms_annular_detector(ms_sim* sim, float inner_mrad, float outer_mrad, double* out);

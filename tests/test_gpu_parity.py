@@ -554,3 +554,40 @@ def test_new_entry_point_errors(engine_cls, oracle_mod, tmp_path):
     eng.RunConventional()
     eng.SimulateImage(0.0)
     assert np.isfinite(eng.Image()).all()
+
+
+# ---------------------------------------------------------------- whole FD runs
+@pytest.mark.parametrize("path", [0, 1])
+def test_run_fd_equals_step_loop_and_oracle(engine_cls, oracle_mod, path):
+    """ms_run_fd (band-limited potential planes resident, fused steps replayed
+    as one graph) equals ms_multislice_step_fd(1..n) and the oracle's
+    MultisliceStep loop (U.cu:2040-2083); odd and even step counts, repeated
+    runs (graph replay, and the recapture an odd count's buffer parity needs)."""
+    eng, orc = make_pair(engine_cls, oracle_mod, sto(2, 2), 128, 0.1, kV=200.0, path=path)
+    for s in (eng, orc):
+        s.InitialiseWavefunctions()
+        s.SetFDdz(0.05)
+    for i in range(1, 42):
+        orc.MultisliceStepFD(i)
+    ref = orc.Wave()
+    for i in range(1, 42):
+        eng.MultisliceStepFD(i)
+    steps = eng.ExitWave()
+    for rep in range(3):
+        eng.InitialiseWavefunctions()
+        assert eng.RunFD(41) == 41
+        w = eng.ExitWave()
+        assert rel_l2(w, ref) < 5 * TOL, (rep, rel_l2(w, ref))
+        assert rel_l2(w, steps.astype(np.complex128)) < 1e-6, rep
+        assert eng.LastDeviceMs() > 0
+    eng.InitialiseWavefunctions()
+    assert eng.RunFD(40) == 40
+    orc.InitialiseWavefunctions()
+    orc.SetFDdz(0.05)
+    for i in range(1, 41):
+        orc.MultisliceStepFD(i)
+    assert rel_l2(eng.ExitWave(), orc.Wave()) < 5 * TOL
+    # a step after a whole run continues from its state
+    eng.MultisliceStepFD(41)
+    orc.MultisliceStepFD(41)
+    assert rel_l2(eng.ExitWave(), orc.Wave()) < 5 * TOL

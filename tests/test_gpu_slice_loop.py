@@ -1,0 +1,146 @@
+"""The persistent slice loop (one cooperative launch for all slices, grid
+barriers between the row and column phases) against the per-pass kernels
+and the FP64 oracle, and the bound on its grid-barrier waits.
+
+Reference being replaced: the per-slice launch sequence of
+MultisliceStepConv (GUI Simulation/UnmanagedGUISimulation.cu:2085-2124) as
+the GUI drives it (CUDA Simulation GUI/MainWindow.xaml.cs:258-283)."""
+import numpy as np
+import pytest
+
+from tests.conftest import FPARAMS
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.complex128)
+    b = np.asarray(b, np.complex128)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.fixture(scope="module")
+def engine_cls():
+    from cudamultislice_b200 import ManagedMultisliceSimulation, build
+
+    build.build(verbose=False)
+    return ManagedMultisliceSimulation
+
+
+def setup(s, atoms, n, ps, kV=200.0, df=-500.0, stem=False):
+    s.SetAtoms(*atoms)
+    s.UploadBinnedAtoms()
+    s.GetParameterisation(FPARAMS)
+    s.ApplyMicroscopeParameters(kV, df, 0.0, 0.0, 1e7, 0.1, 30.0, 20.0)
+    if stem:
+        s.STEMSetCalculationVariables(ps, df, n, n, s.GetSizeX(), s.GetSizeY(), s.GetSizeZ())
+    else:
+        s.SetCalculationVariables(ps, df, n, n, s.GetSizeX(), s.GetSizeY(), s.GetSizeZ(), 2.0, 2.0)
+    s.PreCalculateFrequencies()
+    s.InitialiseWavefunctions(1.9525)
+
+
+@pytest.mark.parametrize("n", [256, 512, 1024])
+def test_loop_matches_passes_and_oracle(engine_cls, oracle_mod, n):
+    from cudamultislice_b200 import structures as S
+
+    atoms = S.srtio3(4, 4, 6)
+    ps = 3.905 * 4 / n
+    eng = engine_cls()
+    setup(eng, atoms, n, ps)
+    nsl = eng.RunConventional()  # persistent loop (default)
+    w_loop = eng.ExitWave()
+    launches_loop = eng.LaunchCount()
+    eng.SetSliceLoop(False)
+    eng.InitialiseWavefunctions(1.9525)
+    eng.RunConventional()
+    w_pass = eng.ExitWave()
+    eng.close()
+    orc = oracle_mod.OracleSimulation()
+    setup(orc, atoms, n, ps)
+    psi = orc.run_conventional()
+    orc.close()
+    assert nsl == orc.GetSlices(True)
+    assert rel_l2(w_loop, psi) < TOL, rel_l2(w_loop, psi)
+    assert rel_l2(w_pass, psi) < TOL
+    # same arithmetic per point as the per-pass kernels of the same plan, up to
+    # the plan variant the per-pass path was tuned to
+    assert rel_l2(w_loop, w_pass) < 3e-6
+    assert launches_loop > 0
+
+
+def test_loop_repeated_runs_and_step_calls_agree(engine_cls, oracle_mod):
+    """Replaying the captured loop gives the same wave every time, and equals
+    the per-slice MultisliceStepConventional calls."""
+    from cudamultislice_b200 import structures as S
+
+    atoms = S.srtio3(4, 4, 5)
+    eng = engine_cls()
+    setup(eng, atoms, 512, 3.905 * 4 / 512)
+    runs = []
+    for _ in range(3):
+        eng.InitialiseWavefunctions(1.9525)
+        eng.RunConventional()
+        runs.append(eng.ExitWave())
+    assert np.array_equal(runs[0], runs[1]) and np.array_equal(runs[1], runs[2])
+    eng.InitialiseWavefunctions(1.9525)
+    for i in range(1, eng.GetSlices(True) + 1):
+        eng.MultisliceStepConventional(i)
+    assert rel_l2(eng.ExitWave(), runs[0]) < 2e-6
+    eng.close()
+
+
+def test_loop_stem_probe(engine_cls, oracle_mod):
+    from cudamultislice_b200 import structures as S
+
+    atoms = S.srtio3(4, 4, 4)
+    n = 256
+    eng, orc = engine_cls(), oracle_mod.OracleSimulation()
+    for s in (eng, orc):
+        setup(s, atoms, n, 3.905 * 4 / n, kV=300.0, df=0.0, stem=True)
+        s.STEMInitialiseWavefunctions(100, 37)
+    eng.RunConventional()
+    psi = orc.run_conventional()
+    assert rel_l2(eng.ExitWave(), psi) < TOL
+    eng.close()
+    orc.close()
+
+
+def test_loop_time_slices(engine_cls):
+    from cudamultislice_b200 import structures as S
+
+    eng = engine_cls()
+    setup(eng, S.srtio3(4, 4, 6), 1024, 3.905 * 4 / 1024)
+    nsl = eng.BuildPotentialStack()
+    l0 = eng.LaunchCount()
+    ms, row, col = eng.TimeSlices(nsl, 3, breakdown=True)
+    assert ms > 0 and row == 0 and col == 0  # one launch per repetition, no per-pass split
+    assert eng.LaunchCount() - l0 == 3
+    eng.close()
+
+
+def test_loop_wait_bound_ends_the_launch_with_an_error(engine_cls, oracle_mod):
+    """A grid barrier whose arrivals never come (the test hook asks for one
+    more than the grid has) runs out its 20 ms bound: the call fails with a
+    status, the context stays usable, and the next run is correct."""
+    from cudamultislice_b200 import MultisliceError
+    from cudamultislice_b200 import structures as S
+
+    atoms = S.srtio3(2, 2, 3)
+    eng = engine_cls()
+    setup(eng, atoms, 256, 0.06)
+    eng.SetLoopWaitUs(20000)
+    eng.SetLoopWaitTest(1)
+    with pytest.raises(MultisliceError) as e:
+        eng.RunConventional()
+    assert e.value.code == 3 and "grid-barrier wait ran out" in str(e.value)
+    eng.SetLoopWaitTest(0)
+    eng.InitialiseWavefunctions(1.9525)
+    eng.RunConventional()
+    orc = oracle_mod.OracleSimulation()
+    setup(orc, atoms, 256, 0.06)
+    assert rel_l2(eng.ExitWave(), orc.run_conventional()) < TOL
+    eng.close()
+    orc.close()
