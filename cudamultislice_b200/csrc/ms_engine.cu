@@ -445,6 +445,7 @@ class Engine {
     have_plan_ = true;
     fused_ok_ = fused_supported(nx, ny);
     tuned_.clear();
+    raster_batch_.clear();
     if (fused_ok_) {
       std::vector<float2> tw(2 * (size_t)std::max(nx, ny));
       for (int v = 0; v < plan_variants(); ++v) {
@@ -1256,14 +1257,7 @@ class Engine {
     if (batch > 1024) return fail(MS_ERR_INVALID, "batch must be at most 1024 (<= 0: automatic)");
     if (!(inner >= 0) || !(outer > inner)) return fail(MS_ERR_INVALID, "need 0 <= inner < outer");
     if (batch <= 0) {
-      // automatic: 64 probes per launch (measured near the optimum on B200 for
-      // 512^2 and 1024^2), fewer when a quarter of the free memory cannot hold them
-      size_t free_b = 0, total_b = 0;
-      batch = 64;
-      if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
-        const size_t per = (size_t)nx_ * ny_ * sizeof(float2);
-        batch = (int)std::max<size_t>(1, std::min<size_t>(64, free_b / 4 / per));
-      }
+      if (int rc = tune_raster_batch(px[0], py[0], inner, outer, &batch)) return rc;
     }
     if (int rc = build_stack(&rs_S_)) return rc;
     if (int rc = ensure_prop_tables(convdz_)) return rc;
@@ -1290,6 +1284,49 @@ class Engine {
     const float kin = (inner * 0.001f) / wavel_, kout = (outer * 0.001f) / wavel_;
     rs_kin2_ = kin * kin;
     rs_kout2_ = kout * kout;
+    return MS_OK;
+  }
+
+  // Probes per launch of the raster, tuned on the device once per grid: each
+  // candidate batch (8 ... 64, at most what a quarter of the free memory
+  // holds) runs one batch of probes through every slice, and the fastest per
+  // probe is kept.  Batches whose waves fit in L2 (about 12 at 1024^2) keep
+  // the passes' wave traffic on chip; larger ones stream it from HBM.
+  int tune_raster_batch(int px0, int py0, float inner, float outer, int* out) {
+    for (auto& kv : raster_batch_)
+      if (kv.first == (long long)nx_ * 100000 + ny_) {
+        *out = kv.second;
+        return MS_OK;
+      }
+    size_t free_b = 0, total_b = 0;
+    int cap = 64;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+      const size_t per = (size_t)nx_ * ny_ * sizeof(float2);
+      cap = (int)std::max<size_t>(1, std::min<size_t>(64, free_b / 4 / per));
+    }
+    const int cands[] = {8, 12, 16, 24, 32, 48, 64};
+    int best = std::min(cap, 64);
+    float best_t = INFINITY;
+    for (int B : cands) {
+      if (B > cap) break;
+      std::vector<int> qx(B, px0), qy(B, py0);
+      for (int rep = 0; rep < 2; ++rep) {  // the first run tunes the plans and loads the kernels
+        if (int rc = raster_prepare(qx.data(), qy.data(), B, inner, outer, B)) return rc;
+        MS_TRY(cudaEventRecord(ev0_, stream_));
+        if (int rc = raster_enqueue(stream_)) return rc;
+        MS_TRY(cudaEventRecord(ev1_, stream_));
+        MS_TRY(cudaEventSynchronize(ev1_));
+      }
+      float ms = 0.0f;
+      MS_TRY(cudaEventElapsedTime(&ms, ev0_, ev1_));
+      const float per_probe = ms / (float)B;
+      if (per_probe < best_t) {
+        best_t = per_probe;
+        best = B;
+      }
+    }
+    raster_batch_.push_back({(long long)nx_ * 100000 + ny_, best});
+    *out = best;
     return MS_OK;
   }
 
@@ -2397,6 +2434,7 @@ class Engine {
   DevBuf<float> d_T_, d_dV_, d_img_, d_fpstack_, d_fpdiff_, d_fpsum_, d_fpimg_;
   DevBuf<double> d_loss_, d_dxy_;
   std::vector<std::pair<int, PlanChoice>> tuned_;
+  std::vector<std::pair<long long, int>> raster_batch_;  // tuned probes per launch by grid
   float prop_dz_ = -1.0f;
   cufftHandle plan_ = 0;
   bool have_plan_ = false;

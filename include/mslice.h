@@ -249,7 +249,8 @@ ms_status ms_annular_detector(ms_sim* sim, float inner_mrad, float outer_mrad, d
  * STEMInitialiseWavefunctions (U.cu:2672-2705), conventional slices 1..S over
  * the potential stack, and the annular-detector signal of ms_annular_detector,
  * written to signal[i].  Probes run `batch` at a time in one set of launches
- * (batch <= 0: automatic, 64 or what a quarter of the free memory holds). */
+ * (batch <= 0: automatic, tuned on the device once per grid size among 8 ... 64
+ * probes per launch, at most what a quarter of the free memory holds). */
 ms_status ms_stem_raster(ms_sim* sim, const int* px, const int* py, int n, float inner_mrad,
                          float outer_mrad, int batch, double* signal);
 

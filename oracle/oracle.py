@@ -179,12 +179,20 @@ class OracleSimulation:
 
     def __init__(self):
         self._L = lib()
-        self._h = self._L.or_create()
+        self._handle = self._L.or_create()
+
+    @property
+    def _h(self):
+        # every call passes the handle through here: a closed simulation raises
+        # instead of handing a freed pointer to the C library
+        if not self._handle:
+            raise OracleError("oracle simulation used after close()")
+        return self._handle
 
     def close(self):
-        if self._h:
-            self._L.or_destroy(self._h)
-            self._h = None
+        if self._handle:
+            self._L.or_destroy(self._handle)
+            self._handle = None
 
     def __del__(self):
         try:

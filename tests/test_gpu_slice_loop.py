@@ -61,8 +61,9 @@ def test_loop_matches_passes_and_oracle(engine_cls, oracle_mod, n):
     orc = oracle_mod.OracleSimulation()
     setup(orc, atoms, n, ps)
     psi = orc.run_conventional()
+    S_ = orc.GetSlices(True)
     orc.close()
-    assert nsl == orc.GetSlices(True)
+    assert nsl == S_
     assert rel_l2(w_loop, psi) < TOL, rel_l2(w_loop, psi)
     assert rel_l2(w_pass, psi) < TOL
     # same arithmetic per point as the per-pass kernels of the same plan, up to
@@ -114,6 +115,7 @@ def test_loop_time_slices(engine_cls):
     eng = engine_cls()
     setup(eng, S.srtio3(4, 4, 6), 1024, 3.905 * 4 / 1024)
     nsl = eng.BuildPotentialStack()
+    eng.TimeSlices(nsl, 1, breakdown=False)  # builds the propagator tables (one launch)
     l0 = eng.LaunchCount()
     ms, row, col = eng.TimeSlices(nsl, 3, breakdown=True)
     assert ms > 0 and row == 0 and col == 0  # one launch per repetition, no per-pass split
