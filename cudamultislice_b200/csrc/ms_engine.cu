@@ -172,6 +172,12 @@ class Engine {
         loop_limit_ns_ = 1000ull * (unsigned long long)value;
         invalidate_graph();
         return MS_OK;
+      case MS_OPT_LOOP_VARIANT:
+        if (value < -1 || value >= slice_loop_variants())
+          return fail(MS_ERR_INVALID, "loop variant must be -1 (tuned) or a variant index");
+        forced_loop_ = value;
+        invalidate_graph();
+        return MS_OK;
       case MS_OPT_LOOP_WAIT_TEST:
         if (value < 0) return fail(MS_ERR_INVALID, "test arrivals must be >= 0");
         loop_extra_ = (unsigned int)value;
@@ -446,6 +452,7 @@ class Engine {
     fused_ok_ = fused_supported(nx, ny);
     tuned_.clear();
     raster_batch_.clear();
+    loop_grid_ = 0;
     if (fused_ok_) {
       std::vector<float2> tw(2 * (size_t)std::max(nx, ny));
       for (int v = 0; v < plan_variants(); ++v) {
@@ -1527,7 +1534,7 @@ class Engine {
     const bool loop = use_loop();
     if (use_fused()) {
       if (loop) {
-        if (int rc = prepare_loop()) return rc;
+        if (int rc = prepare_loop(S)) return rc;
       } else {
         plan_for(1);  // tune outside the capture (tuning allocates and synchronises)
       }
@@ -1586,12 +1593,71 @@ class Engine {
   bool use_loop() const {
     return use_fused() && !loop_off_ && forced_plan_ < 0 && slice_loop_variant(nx_, ny_) >= 0;
   }
-  int prepare_loop() {
-    if (loop_grid_ > 0 && loop_grid_n_ == nx_) return MS_OK;
-    int grid = 0;
-    MS_TRY(slice_loop_prepare(nx_, &grid));
-    loop_grid_ = grid;
+  // Chooses the loop kernel variant for this grid (forced by
+  // MS_OPT_LOOP_VARIANT, else tuned once: every variant runs a short loop of
+  // up to 16 slices over the resident stack, three times after two warm-up
+  // launches, and the fastest is kept).  Needs the potential stack; outside
+  // stream capture (it synchronises).
+  int prepare_loop(int S) {
+    if (loop_grid_ > 0 && loop_grid_n_ == nx_ && loop_tuned_for_ == forced_loop_) return MS_OK;
+    int best_v = -1, best_grid = 0;
+    float best_t = INFINITY;
+    const int St = std::min(S, 16);
+    for (int v = 0; v < slice_loop_variants(); ++v) {
+      if (forced_loop_ >= 0 && v != forced_loop_) continue;
+      int grid = 0;
+      if (slice_loop_prepare(nx_, v, &grid) != cudaSuccess) {
+        cudaGetLastError();
+        continue;
+      }
+      if (forced_loop_ >= 0) {
+        best_v = v;
+        best_grid = grid;
+        break;
+      }
+      loop_v_ = v;
+      loop_grid_ = grid;
+      for (int k = 0; k < 2; ++k)
+        if (int rc = enqueue_loop(d_stack_.p, St, k == 0)) return rc;
+      MS_TRY(cudaEventRecord(ev0_, stream_));
+      for (int k = 0; k < 3; ++k)
+        if (int rc = enqueue_loop(d_stack_.p, St, false)) return rc;
+      MS_TRY(cudaEventRecord(ev1_, stream_));
+      MS_TRY(cudaMemcpyAsync(h_loop_err_, d_loop_sync_.p + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, stream_));
+      MS_TRY(cudaStreamSynchronize(stream_));
+      launches += 5;
+      if (*h_loop_err_ != 0) return loop_timeout_fail();
+      float ms = 0.0f;
+      MS_TRY(cudaEventElapsedTime(&ms, ev0_, ev1_));
+      if (ms < best_t) {
+        best_t = ms;
+        best_v = v;
+        best_grid = grid;
+      }
+    }
+    if (best_v < 0) return fail(MS_ERR_CUDA, "no persistent slice-loop variant could be prepared on this device");
+    loop_v_ = best_v;
+    loop_grid_ = best_grid;
     loop_grid_n_ = nx_;
+    loop_tuned_for_ = forced_loop_;
+    domain_ = 0;  // tuning left scratch in the wave; every run starts from psi0
+    return MS_OK;
+  }
+  int slice_loop_info(int* variant, int* columns, int* grid) {
+    if (!variant || !columns || !grid) return fail(MS_ERR_INVALID, "null output");
+    if (!use_loop()) {
+      *variant = -1;
+      *columns = 0;
+      *grid = 0;
+      return MS_OK;
+    }
+    int S = 0;
+    if (int rc = build_stack(&S)) return rc;
+    if (int rc = ensure_prop_tables(convdz_)) return rc;
+    if (int rc = prepare_loop(S)) return rc;
+    *variant = loop_v_;
+    *columns = slice_loop_columns(loop_v_);
+    *grid = loop_grid_;
     return MS_OK;
   }
   LoopArgs loop_args(const float* Vstack, int S) {
@@ -1616,7 +1682,7 @@ class Engine {
   int enqueue_loop(const float* Vstack, int S, bool clear_error) {
     fd_state_ = false;
     MS_TRY(cudaMemsetAsync(d_loop_sync_.p, 0, (clear_error ? 2 : 1) * sizeof(unsigned int), stream_));
-    MS_TRY(launch_slice_loop(loop_args(Vstack, S), loop_grid_, stream_));
+    MS_TRY(launch_slice_loop(loop_args(Vstack, S), loop_v_, loop_grid_, stream_));
     domain_ = 1;
     return MS_OK;
   }
@@ -1637,7 +1703,7 @@ class Engine {
     const size_t N = (size_t)nx_ * ny_;
     const bool loop = use_loop() && steps <= S;
     if (loop) {
-      if (int rc = prepare_loop()) return rc;
+      if (int rc = prepare_loop(S)) return rc;
     }
     MS_TRY(cudaStreamSynchronize(stream_));
     // whole steps, back to back (the persistent loop: one launch per repetition)
@@ -2467,7 +2533,7 @@ class Engine {
   // persistent slice loop: barrier state [count, error], pinned error copy
   DevBuf<unsigned int> d_loop_sync_;
   unsigned int* h_loop_err_ = nullptr;
-  int loop_grid_ = 0, loop_grid_n_ = 0;
+  int loop_grid_ = 0, loop_grid_n_ = 0, loop_v_ = 0, forced_loop_ = -1, loop_tuned_for_ = -2;
   bool loop_off_ = false;
   unsigned int loop_extra_ = 0;
   unsigned long long loop_limit_ns_ = 1000000000ull;
@@ -2770,6 +2836,9 @@ ms_status ms_build_potential_stack(ms_sim* s, int* nslices) {
 }
 ms_status ms_run_conventional(ms_sim* s, int* nslices) {
   return guarded(s, [&](ms::Engine& e) { return e.run_conventional(nslices); });
+}
+ms_status ms_get_slice_loop(ms_sim* s, int* variant, int* columns, int* grid) {
+  return guarded(s, [&](ms::Engine& e) { return e.slice_loop_info(variant, columns, grid); });
 }
 ms_status ms_run_fd(ms_sim* s, int nsteps, int* nsteps_out) {
   return guarded(s, [&](ms::Engine& e) { return e.run_fd(nsteps, nsteps_out); });

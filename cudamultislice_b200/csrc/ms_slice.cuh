@@ -139,10 +139,14 @@ struct LoopArgs {
 // FFT plan variant whose twiddle tables the persistent loop uses on an nx x ny
 // grid, or -1 where it is not provided (non-square, or not 256/512/1024).
 int slice_loop_variant(int nx, int ny);
-// Raises the loop kernel's shared-memory limit and returns its grid (one CTA
+// Kernel variants of the loop (column unit width, grid-barrier form), and the
+// columns per unit of one variant.
+int slice_loop_variants();
+int slice_loop_columns(int variant);
+// Raises a loop variant's shared-memory limit and returns its grid (one CTA
 // per SM, all resident).
-cudaError_t slice_loop_prepare(int n, int* grid);
-// Cooperative launch of the whole slice loop.
-cudaError_t launch_slice_loop(const LoopArgs& L, int grid, cudaStream_t s);
+cudaError_t slice_loop_prepare(int n, int variant, int* grid);
+// Cooperative launch of the whole slice loop (kernel variant `variant`).
+cudaError_t launch_slice_loop(const LoopArgs& L, int variant, int grid, cudaStream_t s);
 
 }  // namespace ms

@@ -9,12 +9,13 @@ namespace {
 template <int N>
 using LoopPL = typename PlanSel<N, LoopPlan<N>::V>::T;
 
-template <int N>
+template <int N, int V>
 cudaError_t loop_prepare(int* grid) {
   using PL = LoopPL<N>;
-  using SH = LoopShape<PL, kLoopCW>;
+  using LV = LoopVariant<V>;
+  using SH = LoopShape<PL, LV::CW>;
   static_assert(PL::P == 32, "loop plan must run one warp per line");
-  auto kernel = k_slice_loop<PL, kLoopCW>;
+  auto kernel = k_slice_loop<PL, LV::CW, LV::TIGHT>;
   static unsigned long long done = 0;
   if (cudaError_t e = set_smem_once(done, kernel, SH::SMEM)) return e;
   int dev = 0, sms = 0, per_sm = 0;
@@ -26,10 +27,11 @@ cudaError_t loop_prepare(int* grid) {
   return cudaSuccess;
 }
 
-template <int N>
+template <int N, int V>
 cudaError_t loop_launch(const LoopArgs& L, int grid, cudaStream_t s) {
   using PL = LoopPL<N>;
-  using SH = LoopShape<PL, kLoopCW>;
+  using LV = LoopVariant<V>;
+  using SH = LoopShape<PL, LV::CW>;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(SH::NT);
@@ -40,7 +42,26 @@ cudaError_t loop_launch(const LoopArgs& L, int grid, cudaStream_t s) {
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_slice_loop<PL, kLoopCW>, L);
+  return cudaLaunchKernelEx(&cfg, k_slice_loop<PL, LV::CW, LV::TIGHT>, L);
+}
+
+template <int V>
+cudaError_t prepare_v(int n, int* grid) {
+  switch (n) {
+    case 256: return loop_prepare<256, V>(grid);
+    case 512: return loop_prepare<512, V>(grid);
+    case 1024: return loop_prepare<1024, V>(grid);
+    default: return cudaErrorInvalidValue;
+  }
+}
+template <int V>
+cudaError_t launch_v(const LoopArgs& L, int grid, cudaStream_t s) {
+  switch (L.a.nx) {
+    case 256: return loop_launch<256, V>(L, grid, s);
+    case 512: return loop_launch<512, V>(L, grid, s);
+    case 1024: return loop_launch<1024, V>(L, grid, s);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace
@@ -55,22 +76,39 @@ int slice_loop_variant(int nx, int ny) {
   }
 }
 
-cudaError_t slice_loop_prepare(int n, int* grid) {
-  switch (n) {
-    case 256: return loop_prepare<256>(grid);
-    case 512: return loop_prepare<512>(grid);
-    case 1024: return loop_prepare<1024>(grid);
+int slice_loop_variants() { return kLoopVariants; }
+
+int slice_loop_columns(int variant) {
+  switch (variant) {
+    case 0: return LoopVariant<0>::CW;
+    case 1: return LoopVariant<1>::CW;
+    case 2: return LoopVariant<2>::CW;
+    case 3: return LoopVariant<3>::CW;
+    case 4: return LoopVariant<4>::CW;
+    default: return 0;
+  }
+}
+
+cudaError_t slice_loop_prepare(int n, int variant, int* grid) {
+  switch (variant) {
+    case 0: return prepare_v<0>(n, grid);
+    case 1: return prepare_v<1>(n, grid);
+    case 2: return prepare_v<2>(n, grid);
+    case 3: return prepare_v<3>(n, grid);
+    case 4: return prepare_v<4>(n, grid);
     default: return cudaErrorInvalidValue;
   }
 }
 
-cudaError_t launch_slice_loop(const LoopArgs& L, int grid, cudaStream_t s) {
+cudaError_t launch_slice_loop(const LoopArgs& L, int variant, int grid, cudaStream_t s) {
   if (L.a.nx != L.a.ny || L.b.nx != L.a.nx || L.b.ny != L.a.ny || L.S < 1 || grid < 1)
     return cudaErrorInvalidValue;
-  switch (L.a.nx) {
-    case 256: return loop_launch<256>(L, grid, s);
-    case 512: return loop_launch<512>(L, grid, s);
-    case 1024: return loop_launch<1024>(L, grid, s);
+  switch (variant) {
+    case 0: return launch_v<0>(L, grid, s);
+    case 1: return launch_v<1>(L, grid, s);
+    case 2: return launch_v<2>(L, grid, s);
+    case 3: return launch_v<3>(L, grid, s);
+    case 4: return launch_v<4>(L, grid, s);
     default: return cudaErrorInvalidValue;
   }
 }

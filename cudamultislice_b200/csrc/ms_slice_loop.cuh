@@ -34,29 +34,38 @@ MS_D unsigned long long global_ns() {
 
 // Grid barrier number `epoch` (1, 2, ...).  Returns false (in every thread of
 // the CTA) when the grid must stop: this CTA's wait ran out or another CTA
-// reported an error.
+// reported an error.  TIGHT = false: the arrival is an atomic add and the
+// wait polls with a short sleep; TIGHT = true: the arrival is a release
+// reduction (no round trip) and the wait polls back to back, checking the
+// clock and the error word every 32 polls.
+template <bool TIGHT>
 MS_D bool loop_barrier(const LoopSync& s, unsigned int epoch) {
   __syncthreads();
   int ok = 1;
   if (threadIdx.x == 0) {
     __threadfence();
-    atomicAdd(s.count, 1u);
+    if constexpr (TIGHT)
+      asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(s.count) : "memory");
+    else
+      atomicAdd(s.count, 1u);
     const unsigned int target = epoch * gridDim.x + s.expect_extra;
     const unsigned long long t0 = global_ns();
-    while (true) {
+    for (unsigned int it = 0;; ++it) {
       unsigned int v;
       asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(s.count) : "memory");
       if (v >= target) break;
-      if (*reinterpret_cast<volatile int*>(s.error) != 0) {
-        ok = 0;
-        break;
+      if (!TIGHT || (it & 31) == 31) {
+        if (*reinterpret_cast<volatile int*>(s.error) != 0) {
+          ok = 0;
+          break;
+        }
+        if (global_ns() - t0 > s.limit_ns) {
+          atomicExch(s.error, kLoopTimeout);
+          ok = 0;
+          break;
+        }
       }
-      if (global_ns() - t0 > s.limit_ns) {
-        atomicExch(s.error, kLoopTimeout);
-        ok = 0;
-        break;
-      }
-      __nanosleep(32);
+      if constexpr (!TIGHT) __nanosleep(32);
     }
     __threadfence();
   }
@@ -153,7 +162,7 @@ MS_D void prefetch_rows(const float* V, int G) {
   }
 }
 
-template <class PL, int CW>
+template <class PL, int CW, bool TIGHT>
 __global__ void __launch_bounds__(256, 1) k_slice_loop(LoopArgs L) {
   using SH = LoopShape<PL, CW>;
   constexpr int N = PL::N, GS = SH::GS, GROUPS = SH::GROUPS;
@@ -181,12 +190,12 @@ __global__ void __launch_bounds__(256, 1) k_slice_loop(LoopArgs L) {
       else
         loop_row<PL, true>(L.a, L.wave, L.wave, V, line, lane, sm);
     }
-    if (!loop_barrier(L.sync, ++epoch)) return;
+    if (!loop_barrier<TIGHT>(L.sync, ++epoch)) return;
     // ---- column phase ----
     if (s + 1 < L.S) prefetch_rows<PL>(V + L.vstride, G);
     for (int u = g * G + blockIdx.x; u < L.b.nx / CW; u += GROUPS * G)
       loop_col<PL, CW>(L.b, L.wave, u * CW, cl, t, smem + (g * CW + cl) * SH::COL_SLOT, sky, spy);
-    if (s + 1 < L.S && !loop_barrier(L.sync, ++epoch)) return;
+    if (s + 1 < L.S && !loop_barrier<TIGHT>(L.sync, ++epoch)) return;
   }
 }
 
@@ -197,6 +206,14 @@ struct LoopPlan;
 template <> struct LoopPlan<256> { static constexpr int V = 4; };
 template <> struct LoopPlan<512> { static constexpr int V = 4; };
 template <> struct LoopPlan<1024> { static constexpr int V = 3; };
-constexpr int kLoopCW = 4;
+// Variants of the loop kernel (chosen per grid by the engine's autotuner):
+// the column unit width CW and the barrier form.
+constexpr int kLoopVariants = 5;
+template <int V> struct LoopVariant;
+template <> struct LoopVariant<0> { static constexpr int CW = 4; static constexpr bool TIGHT = false; };
+template <> struct LoopVariant<1> { static constexpr int CW = 8; static constexpr bool TIGHT = false; };
+template <> struct LoopVariant<2> { static constexpr int CW = 4; static constexpr bool TIGHT = true; };
+template <> struct LoopVariant<3> { static constexpr int CW = 8; static constexpr bool TIGHT = true; };
+template <> struct LoopVariant<4> { static constexpr int CW = 2; static constexpr bool TIGHT = true; };
 
 }  // namespace ms

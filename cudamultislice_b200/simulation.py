@@ -102,6 +102,16 @@ class ManagedMultisliceSimulation:
         row and column pass (False)."""
         self._chk(self._L.ms_set_option(self._h, 5, 0 if persistent else 1))
 
+    def SetLoopVariant(self, variant: int):
+        """Persistent slice loop kernel variant: -1 tuned (default), 0..4 forced."""
+        self._chk(self._L.ms_set_option(self._h, 8, int(variant)))
+
+    def SliceLoop(self):
+        """(variant, columns per unit, CTAs) of the persistent loop on this grid (variant -1: not used)."""
+        v, c, g = C.c_int(), C.c_int(), C.c_int()
+        self._chk(self._L.ms_get_slice_loop(self._h, C.byref(v), C.byref(c), C.byref(g)))
+        return v.value, c.value, g.value
+
     def SetLoopWaitUs(self, us: int):
         """Bound on each grid-barrier wait of the persistent loop (microseconds)."""
         self._chk(self._L.ms_set_option(self._h, 6, int(us)))

@@ -79,9 +79,13 @@ enum {
   MS_OPT_LOOP_WAIT_US = 6,  /* bound on each grid-barrier wait of the persistent slice
                                loop, microseconds (default 1,000,000); a wait that runs
                                out ends the launch and the call fails with MS_ERR_CUDA */
-  MS_OPT_LOOP_WAIT_TEST = 7 /* test hook: > 0 makes every grid barrier wait for that many
+  MS_OPT_LOOP_WAIT_TEST = 7, /* test hook: > 0 makes every grid barrier wait for that many
                                arrivals more than the grid has, so the wait bound runs out
                                (0 = off, the default) */
+  MS_OPT_LOOP_VARIANT = 8   /* persistent slice loop kernel variant: -1 = tuned on the
+                               device once per grid (default); 0..4 = force one (column
+                               unit width 4, 8, 4, 8, 2 columns; barrier form sleep-poll for
+                               0-1, release reduction with tight poll for 2-4) */
 };
 
 /* ---- lifecycle ---- */
@@ -348,6 +352,10 @@ ms_status ms_time_slices(ms_sim* sim, int steps, int reps, float* ms_total, floa
 /* FFT plan variants (row pass, column pass) used for `batch` instances, tuning
  * them first if needed (MS_OPT_FFT_PLAN). */
 ms_status ms_get_fft_plan(ms_sim* sim, int batch, int* row_variant, int* col_variant);
+/* The persistent slice loop this grid runs: kernel variant (-1 when the loop
+ * does not run here), columns per column unit, CTAs (one per SM); tunes the
+ * variant first if needed (MS_OPT_LOOP_VARIANT). */
+ms_status ms_get_slice_loop(ms_sim* sim, int* variant, int* columns, int* grid);
 /* Number of this library's kernels launched by the handle so far. */
 ms_status ms_get_launch_count(ms_sim* sim, long long* out);
 

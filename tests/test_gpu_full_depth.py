@@ -28,6 +28,13 @@ Tolerances:
     1e-6 of its norm; a 70-200 mrad ring that the band limit cuts to its
     inner edge holds a small fraction of the beam, so the same absolute error
     is a larger fraction of the ring signal (bounded here by 1e-3);
+  - a STEM probe's exit wave through 80 slices of the GaN crystal: <= 2e-5.
+    This case sits at the FP32 floor itself: the same multislice with an
+    ideal single-precision FFT (scipy's pocketfft in complex64, potentials and
+    propagator exact) is 1.0e-5 from FP64 at 1024^2 (tests/fp32_floor_model.py).
+    A crystal repeats the same slices, so the transform's rounding adds up
+    coherently, and a probe's energy sits where the propagator is not 1;
+    the amorphous plane-wave workload stays near 2e-6;
   - gradients: relative L2 error <= 1e-4; the focal-series loss <= 1e-4 (it
     sums squared residuals I - T that are small against I, so its relative
     error is the images' error magnified by I / (I - T)), the images
@@ -44,6 +51,7 @@ INT_TOL = 2e-5    # intensities (CTF images)
 BEAM_TOL = 1e-6   # detector signal error / total probe intensity
 RING_TOL = 1e-3   # detector signal error / ring signal
 GRAD_TOL = 1e-4   # gradients and the focal-series loss
+PROBE_TOL = 2e-5  # probe exit wave through a crystal (twice the FP32 floor of that case)
 
 
 def rel_l2(a, b):
@@ -190,7 +198,7 @@ def test_c4_gan_haadf_raster_1024_full_depth(engine_cls, oracle_mod):
     eng.STEMInitialiseWavefunctions(int(px[5]), int(py[5]))
     eng.RunConventional()
     e = rel_l2(eng.ExitWave(), psi5)
-    assert e < TOL, e
+    assert e < PROBE_TOL, e
     eng.close()
     orc.close()
 
@@ -221,7 +229,7 @@ def test_c5_focal_series_gradient_512_full_depth(engine_cls, oracle_mod):
     setup(orc, (Z, x, y, z), n, 3.905 * 4 / n, **kw)
     L0, gV0, gxy0 = orc.FocalGrad(df, T.astype(np.float64), nslices)
     _, imgs0 = orc.FocalForward(df, T.astype(np.float64), nslices)
-    psi = orc.run_conventional(nslices)
+    psi = orc.run_conventional()  # every slice, as RunConventional
     orc.close()
     ew = rel_l2(w, psi)
     assert ew < TOL, ew

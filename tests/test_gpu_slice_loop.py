@@ -146,3 +146,27 @@ def test_loop_wait_bound_ends_the_launch_with_an_error(engine_cls, oracle_mod):
     assert rel_l2(eng.ExitWave(), orc.run_conventional()) < TOL
     eng.close()
     orc.close()
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+def test_every_loop_variant(engine_cls, oracle_mod, variant):
+    """Each kernel variant of the loop (column unit width, barrier form) gives
+    the oracle's exit wave; the tuner's choice is one of them."""
+    from cudamultislice_b200 import structures as S
+
+    atoms = S.srtio3(4, 4, 4)
+    n = 1024
+    eng = engine_cls()
+    setup(eng, atoms, n, 3.905 * 4 / n)
+    v, cols, grid = eng.SliceLoop()
+    assert 0 <= v <= 4 and cols in (2, 4, 8) and grid > 0
+    eng.SetLoopVariant(variant)
+    assert eng.SliceLoop()[0] == variant
+    eng.RunConventional()
+    w = eng.ExitWave()
+    eng.close()
+    orc = oracle_mod.OracleSimulation()
+    setup(orc, atoms, n, 3.905 * 4 / n)
+    psi = orc.run_conventional()
+    orc.close()
+    assert rel_l2(w, psi) < TOL
