@@ -1244,8 +1244,12 @@ class Engine {
       return MS_OK;
     }
     if (int rc = raster_prepare(px, py, n, inner, outer, batch)) return rc;
-    if (int rc = raster_enqueue(stream_)) return rc;
-    return raster_finish(signal);
+    MS_TRY(cudaEventRecord(ev0_, stream_));
+    if (int rc = raster_enqueue(stream_, true)) return rc;
+    MS_TRY(cudaEventRecord(ev1_, stream_));
+    if (int rc = raster_finish(signal)) return rc;
+    MS_TRY(cudaEventElapsedTime(&last_device_ms_, ev0_, ev1_));
+    return MS_OK;
   }
 
   // Probe raster in three phases so that several handles can be captured into
@@ -1320,9 +1324,13 @@ class Engine {
       for (int rep = 0; rep < 2; ++rep) {  // the first run tunes the plans and loads the kernels
         if (int rc = raster_prepare(qx.data(), qy.data(), B, inner, outer, B)) return rc;
         MS_TRY(cudaEventRecord(ev0_, stream_));
-        if (int rc = raster_enqueue(stream_)) return rc;
+        if (int rc = raster_enqueue(stream_, true)) return rc;
         MS_TRY(cudaEventRecord(ev1_, stream_));
         MS_TRY(cudaEventSynchronize(ev1_));
+        if (rs_loop_) {
+          MS_TRY(copy_sync(h_loop_err_, d_loop_sync_.p + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost));
+          if (*h_loop_err_ != 0) return loop_timeout_fail();
+        }
       }
       float ms = 0.0f;
       MS_TRY(cudaEventElapsedTime(&ms, ev0_, ev1_));
@@ -1337,26 +1345,117 @@ class Engine {
     return MS_OK;
   }
 
-  int raster_enqueue(cudaStream_t st) {
+  // Probes of raster positions start .. start+nb-1 into the batch buffer (real
+  // space, unnormalised) and their L1 norms (STEMInitialiseWavefunctions,
+  // U.cu:2672-2705), enqueued on `st`.
+  int raster_probes(cudaStream_t st, int start, int nb) {
     const long long N = (long long)nx_ * ny_;
-    const int B = rs_B_, n = rs_n_, S = rs_S_;
+    const int n = rs_n_;
     const Grid2 g{nx_, ny_};
     const float apert = (float)((double)aperture_ * 0.001 / (double)wavel_);
+    const PlanChoice pc = plan_for(rs_B_, true);
+    const int vr = pc.row, vc = pc.col;
+    MS_TRY(pw_probe_batch(d_bwave_.p, N, nb, d_kx_.p, d_ky_.p, d_bpos_.p + start, d_bpos_.p + n + start, apert,
+                          ps_, df_, Cs_, wavel_, g, st, &launches));
+    PassBArgs bi = passb_args(d_bwave_.p, d_bwave_.p, vc);
+    bi.batch_stride_wave = N;
+    MS_TRY(launch_pass_b(bi, vc, B_INV_ONLY, nb, st));
+    PassAArgs ai = passa_args(d_bwave_.p, d_bwave_.p, vr);
+    ai.batch_stride_wave = N;
+    MS_TRY(launch_pass_a(ai, vr, A_INV, nb, st));
+    launches += 2;
+    MS_TRY(pw_sum_abs_batch(d_bwave_.p, N, N, nb, d_bpart_.p, d_bsig_.p + n + start, st, &launches));
+    return MS_OK;
+  }
+
+  // The batched persistent loop serves this handle's batches (square 256, 512
+  // or 1024 grids, no forced plan, MS_OPT_SLICE_LOOP on).
+  bool use_batch_loop() const {
+    return use_fused() && !loop_off_ && forced_plan_ < 0 && nx_ == ny_ && batch_loop_supported(nx_, 0);
+  }
+  // One group of the batched loop over the raster batch at `start`: the
+  // probes through the transmission stack, the detector on the last slice.
+  LoopGroup raster_group(int start, int nb) {
+    const long long N = (long long)nx_ * ny_;
+    const int v = batch_loop_plan(nx_);
+    LoopGroup g{};
+    g.n = nx_;
+    g.B = nb;
+    g.wave = d_bwave_.p;
+    g.tstack = d_tstack_.p;
+    g.inst_stride = 0;
+    g.slice_stride = N;
+    g.a = passa_args(d_bwave_.p, d_bwave_.p, v);
+    g.b = passb_args(d_bwave_.p, d_bwave_.p, v);
+    g.b.kin2 = rs_kin2_;
+    g.b.kout2 = rs_kout2_;
+    g.b.scale = 1.0f / (float)N;
+    g.sig = d_bsig_.p + start;
+    return g;
+  }
+  // Launch of the batched loop over one or two groups (g1 may be null), with
+  // this handle's barrier state (the counter cleared first; the error word is
+  // cleared by the caller at the start of a sequence).
+  int enqueue_batch_loop(cudaStream_t st, const LoopGroup& g0, const LoopGroup* g1, int S) {
+    BatchLoopArgs L{};
+    L.g[0] = g0;
+    if (g1) L.g[1] = *g1;
+    L.S = S;
+    L.sync.count = d_loop_sync_.p;
+    L.sync.error = reinterpret_cast<int*>(d_loop_sync_.p + 1);
+    L.sync.limit_ns = loop_limit_ns_;
+    L.sync.expect_extra = loop_extra_;
+    int grid = 0;
+    MS_TRY(batch_loop_prepare(g0.n, g1 ? g1->n : 0, &grid));
+    MS_TRY(cudaMemsetAsync(d_loop_sync_.p, 0, sizeof(unsigned int), st));
+    MS_TRY(launch_batch_loop(L, grid, st));
+    ++launches;
+    return MS_OK;
+  }
+  int raster_slices() const { return rs_S_; }
+  int raster_batch() const { return rs_B_; }
+  int raster_count() const { return rs_n_; }
+  int grid_n() const { return nx_; }
+  // Clears the raster's signal sums on `st` (its batches then run through
+  // raster_probes and another handle's batched-loop launches).
+  int raster_begin(cudaStream_t st) {
+    MS_TRY(cudaMemsetAsync(d_bsig_.p, 0, sizeof(double) * 2 * rs_n_, st));
+    rs_loop_ = false;
+    return MS_OK;
+  }
+  int loop_begin(cudaStream_t st) {
+    *h_loop_err_ = 0;
+    MS_TRY(cudaMemsetAsync(d_loop_sync_.p, 0, 2 * sizeof(unsigned int), st));
+    return MS_OK;
+  }
+  int loop_check(cudaStream_t st) {
+    MS_TRY(cudaMemcpyAsync(h_loop_err_, d_loop_sync_.p + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+    MS_TRY(cudaStreamSynchronize(st));
+    if (*h_loop_err_ != 0) return loop_timeout_fail();
+    return MS_OK;
+  }
+
+  // `allow_loop`: the slices of each batch run in the batched persistent loop
+  // (one launch per batch) where it is provided; otherwise, and always when
+  // several handles' rasters run as concurrent graph branches, one launch per
+  // pass.
+  int raster_enqueue(cudaStream_t st, bool allow_loop = false) {
+    const long long N = (long long)nx_ * ny_;
+    const int B = rs_B_, n = rs_n_, S = rs_S_;
     const PlanChoice pc = plan_for(B, true);
     const int vr = pc.row, vc = pc.col;
+    const bool loop = allow_loop && use_batch_loop();
     MS_TRY(cudaMemsetAsync(d_bsig_.p, 0, sizeof(double) * 2 * n, st));
+    if (loop) MS_TRY(cudaMemsetAsync(d_loop_sync_.p, 0, 2 * sizeof(unsigned int), st));
+    rs_loop_ = loop;
     for (int start = 0; start < n; start += B) {
       const int nb = std::min(B, n - start);
-      MS_TRY(pw_probe_batch(d_bwave_.p, N, nb, d_kx_.p, d_ky_.p, d_bpos_.p + start, d_bpos_.p + n + start, apert,
-                            ps_, df_, Cs_, wavel_, g, st, &launches));
-      PassBArgs bi = passb_args(d_bwave_.p, d_bwave_.p, vc);
-      bi.batch_stride_wave = N;
-      MS_TRY(launch_pass_b(bi, vc, B_INV_ONLY, nb, st));
-      PassAArgs ai = passa_args(d_bwave_.p, d_bwave_.p, vr);
-      ai.batch_stride_wave = N;
-      MS_TRY(launch_pass_a(ai, vr, A_INV, nb, st));
-      launches += 2;
-      MS_TRY(pw_sum_abs_batch(d_bwave_.p, N, N, nb, d_bpart_.p, d_bsig_.p + n + start, st, &launches));
+      if (int rc = raster_probes(st, start, nb)) return rc;
+      if (loop) {
+        const LoopGroup g = raster_group(start, nb);
+        if (int rc = enqueue_batch_loop(st, g, nullptr, S)) return rc;
+        continue;
+      }
       for (int it = 1; it <= S; ++it) {
         PassAArgs a = passa_args(d_bwave_.p, d_bwave_.p, vr);
         a.batch_stride_wave = N;
@@ -1384,6 +1483,10 @@ class Engine {
     const int n = rs_n_;
     std::vector<double> host(2 * (size_t)n);
     MS_TRY(copy_sync(host.data(), d_bsig_.p, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost));
+    if (rs_loop_) {
+      MS_TRY(copy_sync(h_loop_err_, d_loop_sync_.p + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost));
+      if (*h_loop_err_ != 0) return loop_timeout_fail();
+    }
     for (int i = 0; i < n; ++i) {
       const double l1 = host[n + i];
       if (!(l1 > 0)) return fail(MS_ERR_NUMERIC, "probe is empty (aperture smaller than one frequency pixel)");
@@ -1436,6 +1539,7 @@ class Engine {
       plan_for(B);
     }
     invalidate_graph();
+    bool fp_loop = false;
     MS_TRY(cudaEventRecord(ev0_, stream_));
     for (int start = 0; start < nconf; start += B) {
       const int nb = std::min(B, nconf - start);
@@ -1462,16 +1566,33 @@ class Engine {
         MS_TRY(cudaMemcpyAsync(d_bwave_.p + (size_t)k * N, d_psi0_.p, sizeof(float2) * N, cudaMemcpyDeviceToDevice,
                                stream_));
       }
-      for (int it = 1; it <= S; ++it) {
-        PassAArgs a = passa_args(d_bwave_.p, d_bwave_.p, 0);
-        a.batch_stride_wave = N;
-        a.batch_stride_V = (long long)S * N;
-        a.V = d_fpstack_.p + (size_t)(it - 1) * N;
-        MS_TRY(pass_a(a, it == 1 ? (A_MULT_T | A_FWD) : (A_INV | A_MULT_T | A_FWD), nb));
-        PassBArgs b = passb_args(d_bwave_.p, d_bwave_.p, 0);
-        b.batch_stride_wave = N;
-        MS_TRY(pass_b(b, B_PROPAGATE, nb));
-        launches += 2;
+      if (use_batch_loop()) {
+        // the nb configurations through every slice in one persistent launch
+        const int v = batch_loop_plan(nx_);
+        LoopGroup lg{};
+        lg.n = nx_;
+        lg.B = nb;
+        lg.wave = d_bwave_.p;
+        lg.Vstack = d_fpstack_.p;
+        lg.inst_stride = (long long)S * N;
+        lg.slice_stride = N;
+        lg.a = passa_args(d_bwave_.p, d_bwave_.p, v);
+        lg.b = passb_args(d_bwave_.p, d_bwave_.p, v);
+        if (start == 0) MS_TRY(cudaMemsetAsync(d_loop_sync_.p, 0, 2 * sizeof(unsigned int), stream_));
+        if (int rc = enqueue_batch_loop(stream_, lg, nullptr, S)) return rc;
+        fp_loop = true;
+      } else {
+        for (int it = 1; it <= S; ++it) {
+          PassAArgs a = passa_args(d_bwave_.p, d_bwave_.p, 0);
+          a.batch_stride_wave = N;
+          a.batch_stride_V = (long long)S * N;
+          a.V = d_fpstack_.p + (size_t)(it - 1) * N;
+          MS_TRY(pass_a(a, it == 1 ? (A_MULT_T | A_FWD) : (A_INV | A_MULT_T | A_FWD), nb));
+          PassBArgs b = passb_args(d_bwave_.p, d_bwave_.p, 0);
+          b.batch_stride_wave = N;
+          MS_TRY(pass_b(b, B_PROPAGATE, nb));
+          launches += 2;
+        }
       }
       if (diff) {
         PassBArgs b = passb_args(d_bwave_.p, d_bwave_.p, 0);
@@ -1498,7 +1619,10 @@ class Engine {
     MS_TRY(cudaEventRecord(ev1_, stream_));
     if (diff) MS_TRY(cudaMemcpyAsync(diff, d_fpdiff_.p, sizeof(float) * N, cudaMemcpyDeviceToHost, stream_));
     if (image) MS_TRY(cudaMemcpyAsync(image, d_fpsum_.p, sizeof(float) * N, cudaMemcpyDeviceToHost, stream_));
+    if (fp_loop)
+      MS_TRY(cudaMemcpyAsync(h_loop_err_, d_loop_sync_.p + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, stream_));
     MS_TRY(cudaStreamSynchronize(stream_));
+    if (fp_loop && *h_loop_err_ != 0) return loop_timeout_fail();
     MS_TRY(cudaEventElapsedTime(&last_device_ms_, ev0_, ev1_));
     return MS_OK;
   }
@@ -1591,7 +1715,7 @@ class Engine {
   // (square 256, 512, 1024 grids), unless MS_OPT_SLICE_LOOP turns it off or an
   // FFT plan variant is forced (MS_OPT_FFT_PLAN selects per-pass kernels).
   bool use_loop() const {
-    return use_fused() && !loop_off_ && forced_plan_ < 0 && slice_loop_variant(nx_, ny_) >= 0;
+    return use_fused() && !loop_off_ && forced_plan_ < 0 && slice_loop_supported(nx_, ny_);
   }
   // Chooses the loop kernel variant for this grid (forced by
   // MS_OPT_LOOP_VARIANT, else tuned once: every variant runs a short loop of
@@ -1661,7 +1785,7 @@ class Engine {
     return MS_OK;
   }
   LoopArgs loop_args(const float* Vstack, int S) {
-    const int v = slice_loop_variant(nx_, ny_);
+    const int v = slice_loop_plan(nx_, loop_v_);
     LoopArgs L{};
     L.a = passa_args(d_psi0_.p, d_psi_.p, v);
     L.b = passb_args(d_psi_.p, d_psi_.p, v);
@@ -2158,13 +2282,17 @@ class Engine {
     if (dz == prop_dz_ && d_px_.p) return MS_OK;
     std::vector<float2> px(nx_), py(ny_);
     const double invN = 1.0 / ((double)nx_ * ny_);
+    // unit factors nearest modulus 1 (unit_fp32); the 1/N of the fused
+    // passes is a power of two, so scaling px by it is exact
+    const float fN = (float)invN;
     for (int i = 0; i < nx_; ++i) {
       const double ph = 3.14159265 * (double)dz * (double)wavel_ * (double)hkx_[i] * (double)hkx_[i];
-      px[i] = make_float2((float)(std::cos(ph) * invN), (float)(-std::sin(ph) * invN));
+      const float2 u = unit_fp32(std::cos(ph), -std::sin(ph));
+      px[i] = make_float2(u.x * fN, u.y * fN);
     }
     for (int j = 0; j < ny_; ++j) {
       const double ph = 3.14159265 * (double)dz * (double)wavel_ * (double)hky_[j] * (double)hky_[j];
-      py[j] = make_float2((float)std::cos(ph), (float)(-std::sin(ph)));
+      py[j] = unit_fp32(std::cos(ph), -std::sin(ph));
     }
     MS_TRY(d_px_.resize(nx_));
     MS_TRY(d_py_.resize(ny_));
@@ -2494,6 +2622,7 @@ class Engine {
   uint32_t det_serial_ = 0;
   bool image_noisy_ = false;
   int rs_n_ = 0, rs_B_ = 1, rs_S_ = 0;  // prepared probe raster
+  bool rs_loop_ = false;                 // its slices ran in the batched persistent loop
   float rs_kin2_ = 0, rs_kout2_ = 0;
   std::vector<int> hzoff_;  // first sorted atom per z-bin (focal-series atom gradient)
   DevBuf<float2> d_ck_, d_seg_, d_G_, d_U_, d_Phi_;
@@ -2945,6 +3074,58 @@ ms_status ms_stem_raster_concurrent(ms_sim* const* sims, int nsims, const int* c
         return e0.fail(rc, "handle " + std::to_string(k) + ": " + e.err);
     }
     cudaStream_t st0 = e0.stream();
+    // Two handles whose grids the batched persistent loop serves, with equal
+    // slice counts: each round takes the next batch of both rasters through
+    // every slice in ONE cooperative launch (group 0 the larger grid), on the
+    // first handle's stream.
+    if (nsims == 2 && sims[0]->e->use_batch_loop() && sims[1]->e->use_batch_loop() &&
+        sims[0]->e->raster_slices() == sims[1]->e->raster_slices()) {
+      const int big = sims[0]->e->grid_n() >= sims[1]->e->grid_n() ? 0 : 1;
+      ms::Engine& ea = *sims[big]->e;
+      ms::Engine& eb = *sims[1 - big]->e;
+      if (ms::batch_loop_supported(ea.grid_n(), eb.grid_n())) {
+        cudaEvent_t t0 = nullptr, t1 = nullptr;
+        if (cudaEventCreate(&t0) != cudaSuccess || cudaEventCreate(&t1) != cudaSuccess) {
+          if (t0) cudaEventDestroy(t0);
+          return e0.fail(MS_ERR_CUDA, "cudaEventCreate failed");
+        }
+        int rc = MS_OK;
+        cudaError_t ce = cudaEventRecord(t0, st0);
+        if (ce == cudaSuccess) rc = ea.raster_begin(st0);
+        if (rc == MS_OK) rc = eb.raster_begin(st0);
+        if (rc == MS_OK) rc = e0.loop_begin(st0);
+        const int na = ea.raster_count(), nb = eb.raster_count(), Ba = ea.raster_batch(), Bb = eb.raster_batch();
+        for (int r = 0; ce == cudaSuccess && rc == MS_OK; ++r) {
+          const int sa = r * Ba, sb = r * Bb;
+          const int ka = std::max(0, std::min(Ba, na - sa)), kb = std::max(0, std::min(Bb, nb - sb));
+          if (ka == 0 && kb == 0) break;
+          if (ka > 0) rc = ea.raster_probes(st0, sa, ka);
+          if (rc == MS_OK && kb > 0) rc = eb.raster_probes(st0, sb, kb);
+          if (rc != MS_OK) break;
+          if (ka > 0 && kb > 0) {
+            const ms::LoopGroup g0 = ea.raster_group(sa, ka), g1 = eb.raster_group(sb, kb);
+            rc = e0.enqueue_batch_loop(st0, g0, &g1, ea.raster_slices());
+          } else {
+            const ms::LoopGroup g0 = ka > 0 ? ea.raster_group(sa, ka) : eb.raster_group(sb, kb);
+            rc = e0.enqueue_batch_loop(st0, g0, nullptr, ea.raster_slices());
+          }
+        }
+        if (ce == cudaSuccess && rc == MS_OK) ce = cudaEventRecord(t1, st0);
+        if (ce == cudaSuccess && rc == MS_OK) rc = e0.loop_check(st0);
+        float ms = 0.0f;
+        if (ce == cudaSuccess && rc == MS_OK && cudaEventElapsedTime(&ms, t0, t1) == cudaSuccess)
+          e0.set_last_device_ms(ms);
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        if (rc != MS_OK) return rc;
+        if (ce != cudaSuccess) return e0.fail(MS_ERR_CUDA, std::string("mixed raster: ") + cudaGetErrorString(ce));
+        for (int k = 0; k < nsims; ++k) {
+          ms::Engine& e = *sims[k]->e;
+          if (int r2 = e.raster_finish(signal[k])) return e0.fail(r2, "handle " + std::to_string(k) + ": " + e.err);
+        }
+        return (int)MS_OK;
+      }
+    }
     std::vector<cudaEvent_t> ev(nsims + 2, nullptr);
     for (auto& x : ev)
       if (cudaEventCreate(&x) != cudaSuccess) {

@@ -13,7 +13,9 @@
 //     operation that follows (transmission, propagator) needs no reordering.
 // The slot is padded by one point every R1 points so the stride-R1 writes of
 // pass 1 hit distinct banks.  In-register butterflies are radix-2 DIF networks
-// with compile-time twiddle constants; trivial twiddles cost no multiply.
+// with compile-time twiddles applied as exact quarter turns plus three-shear
+// rotations (twc); trivial twiddles cost no multiply.  Table twiddles are the
+// FP32 pairs nearest unit modulus (unit_fp32).
 // Forward = exp(-2 pi i jk/N) (cuFFT CUFFT_FORWARD); the inverse is computed as
 // conj(FFT(conj(x))) so that a kernel holds one copy of the transform code
 // (instruction-cache footprint); both directions unnormalised.
@@ -23,23 +25,6 @@
 namespace ms {
 namespace fft {
 
-// cos(2 pi j / 32) for j = 0..8 (first quadrant); the rest follows by symmetry.
-MS_HD constexpr float cos32_q(int j) {
-  return j == 0 ? 1.0f
-       : j == 1 ? 0.98078528040323043f
-       : j == 2 ? 0.92387953251128674f
-       : j == 3 ? 0.83146961230254524f
-       : j == 4 ? 0.70710678118654757f
-       : j == 5 ? 0.55557023301960229f
-       : j == 6 ? 0.38268343236508984f
-       : j == 7 ? 0.19509032201612833f
-                : 0.0f;
-}
-MS_HD constexpr float cos32(int j) {
-  return j <= 8 ? cos32_q(j) : j <= 16 ? -cos32_q(16 - j) : j <= 24 ? -cos32_q(j - 16) : cos32_q(32 - j);
-}
-MS_HD constexpr float sin32(int j) { return cos32((j + 24) & 31); }  // sin(a) = cos(a - pi/2)
-
 MS_HD constexpr int brev(int v, int bits) {
   int r = 0;
   for (int i = 0; i < bits; ++i) r |= ((v >> i) & 1) << (bits - 1 - i);
@@ -47,22 +32,51 @@ MS_HD constexpr int brev(int v, int bits) {
 }
 MS_HD constexpr int ilog2(int v) { return v <= 1 ? 0 : 1 + ilog2(v >> 1); }
 
+// tan(k pi / 32) and sin(k pi / 16), k = 1..4: the shear coefficients of a
+// rotation by k/32 of a turn.
+MS_HD constexpr float shear_t(int k) {
+  return k == 1 ? 0.098491403357164248f : k == 2 ? 0.19891236737965801f : k == 3 ? 0.3033466836073424f
+                                                                                  : 0.41421356237309503f;
+}
+MS_HD constexpr float shear_s(int k) {
+  return k == 1 ? 0.19509032201612825f : k == 2 ? 0.38268343236508978f : k == 3 ? 0.55557023301960218f
+                                                                                 : 0.70710678118654746f;
+}
+
 // x * W_M^J, W = exp(-2 pi i / M) forward, exp(+2 pi i / M) inverse; M divides 32.
+// The rotation is an exact quarter turn (a swap and negation) followed, for
+// the remaining angle r (|r| <= 1/8 turn), by three shears
+//   x1 = x - tan(r/2) y,  y1 = y + sin(r) x1,  x2 = x1 - tan(r/2) y1
+// (Paeth's decomposition).  Each shear has determinant exactly 1 whatever the
+// FP32 rounding of its coefficient, so the rotation does not change the norm
+// systematically: a rotation by rounded (cos, sin) scales by |(c, s)| != 1,
+// an error that repeats in every transform of every slice and adds up
+// coherently over a slice stack.  Three FMAs instead of a complex multiply.
 template <int J, int M, bool INV>
 MS_D float2 twc(float2 x) {
   constexpr int j = ((J % M) + M) % M * (32 / M);
   if constexpr (j == 0) {
     return x;
-  } else if constexpr (j == 16) {
-    return make_float2(-x.x, -x.y);
-  } else if constexpr (j == 8) {  // -i forward, +i inverse
-    return INV ? make_float2(-x.y, x.x) : make_float2(x.y, -x.x);
-  } else if constexpr (j == 24) {  // +i forward, -i inverse
-    return INV ? make_float2(x.y, -x.x) : make_float2(-x.y, x.x);
   } else {
-    constexpr float c = cos32(j);
-    constexpr float s = INV ? sin32(j) : -sin32(j);
-    return make_float2(x.x * c - x.y * s, x.x * s + x.y * c);
+    // angle in 32nds of a turn, counter-clockwise: -j forward, +j inverse
+    constexpr int a = INV ? j : (32 - j) % 32;
+    constexpr int q = ((a + 4) / 8) % 4;   // nearest quarter turn
+    constexpr int rem = a - 8 * ((a + 4) / 8);  // -4 .. 3
+    float2 y = x;
+    if constexpr (q == 1) y = make_float2(-x.y, x.x);
+    else if constexpr (q == 2) y = make_float2(-x.x, -x.y);
+    else if constexpr (q == 3) y = make_float2(x.y, -x.x);
+    if constexpr (rem == 0) {
+      return y;
+    } else {
+      constexpr int k = rem > 0 ? rem : -rem;
+      constexpr float t = rem > 0 ? shear_t(k) : -shear_t(k);
+      constexpr float sn = rem > 0 ? shear_s(k) : -shear_s(k);
+      const float x1 = fmaf(-t, y.y, y.x);
+      const float y1 = fmaf(sn, x1, y.y);
+      const float x2 = fmaf(-t, y1, x1);
+      return make_float2(x2, y1);
+    }
   }
 }
 

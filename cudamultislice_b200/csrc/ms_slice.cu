@@ -36,6 +36,27 @@ void band_limit_thresholds(float kmax, float* k2_lt, float* k2_le) {
   *k2_le = first(kmax, true);
 }
 
+float2 unit_fp32(double c, double s) {
+  const float c0 = (float)c, s0 = (float)s;
+  float bc = c0, bs = s0;
+  double bn = INFINITY, ba = INFINITY;
+  const double ang = std::atan2(s, c);
+  for (int dc = -1; dc <= 1; ++dc)
+    for (int ds = -1; ds <= 1; ++ds) {
+      const float cc = dc == 0 ? c0 : std::nextafter(c0, dc > 0 ? INFINITY : -INFINITY);
+      const float ss = ds == 0 ? s0 : std::nextafter(s0, ds > 0 ? INFINITY : -INFINITY);
+      const double n = std::fabs((double)cc * cc + (double)ss * ss - 1.0);
+      const double a = std::fabs(std::atan2((double)ss, (double)cc) - ang);
+      if (n < bn || (n == bn && a < ba)) {
+        bn = n;
+        ba = a;
+        bc = cc;
+        bs = ss;
+      }
+    }
+  return make_float2(bc, bs);
+}
+
 int plan_variants() { return kPlanVariants; }
 
 int make_twiddles(int n, int variant, float2* host_out) {

@@ -106,6 +106,13 @@ struct PassBArgs {
 // with them takes exactly the decisions of the rounded square root.
 void band_limit_thresholds(float kmax, float* k2_lt, float* k2_le);
 
+// (cos, sin) as the FP32 pair within one ulp of each component whose modulus
+// is nearest 1 (ties: nearest angle).  Unit factors applied once per transform
+// or per slice (twiddles, propagator) then scale the wave by |(c, s)|^S over a
+// stack of S slices only to that pair's remaining modulus error, far below the
+// plain rounding's, which adds up coherently when the slices repeat (crystals).
+float2 unit_fp32(double c, double s);
+
 // Line lengths 64..4096 (powers of two) in both directions.
 bool fused_supported(int nx, int ny);
 // Number of FFT plan variants per line length (autotuned by the engine).
@@ -136,9 +143,37 @@ struct LoopArgs {
   int S;                // slices
   LoopSync sync;
 };
-// FFT plan variant whose twiddle tables the persistent loop uses on an nx x ny
-// grid, or -1 where it is not provided (non-square, or not 256/512/1024).
-int slice_loop_variant(int nx, int ny);
+// Batched persistent loop: B instances of one or two square grid sizes
+// stepped through the same S slices by one cooperative launch.
+struct LoopGroup {
+  int n;                   // grid (n x n): 256, 512 or 1024; 0 = group absent
+  int B;                   // instances
+  float2* wave;            // [B][n][n]: real space on entry, row-frequency form after the loop
+  const float* Vstack;     // per-instance potentials (x exp(i sigma V) on the fly), or null
+  const float2* tstack;    // transmissions (x t), used when Vstack is null
+  long long inst_stride;   // elements between instances' stacks (0: one stack shared by all)
+  long long slice_stride;  // elements between slices of a stack
+  PassAArgs a;             // row tables (twiddles, sigma)
+  PassBArgs b;             // column tables (twiddles, propagator, band limit; detector annulus)
+  double* sig;             // last slice: annular-detector sum per instance (then no propagation)
+};
+struct BatchLoopArgs {
+  LoopGroup g[2];
+  int S;
+  LoopSync sync;
+};
+// Grids (n0 >= n1; n1 = 0 for one group, n1 = n0 for two of one size) the
+// batched loop is provided for.
+bool batch_loop_supported(int n0, int n1);
+// FFT plan variant (twiddle tables) of the batched loop for lines of n points.
+int batch_loop_plan(int n);
+cudaError_t batch_loop_prepare(int n0, int n1, int* grid);
+cudaError_t launch_batch_loop(const BatchLoopArgs& L, int grid, cudaStream_t s);
+
+// Grids the persistent loop is provided for (square 256, 512, 1024), and the
+// FFT plan variant (twiddle tables) that loop kernel variant `variant` uses.
+bool slice_loop_supported(int nx, int ny);
+int slice_loop_plan(int n, int variant);
 // Kernel variants of the loop (column unit width, grid-barrier form), and the
 // columns per unit of one variant.
 int slice_loop_variants();

@@ -315,8 +315,8 @@ MS_D void col_mid(float2 (&v)[PL::E], const PassBArgs& a, const float* __restric
       const float ky = sky[n];
       // CreatePropsKernel (U.cu:419): keep sqrtf(kx^2+ky^2) < kmax
       const bool keep = fadd_x(kx2, fmul_x(ky, ky)) < a.k2_lt;
-      const float2 w = keep ? cmul(pxv, spy[n]) : make_float2(0.f, 0.f);
-      v[j] = cmul(v[j], w);
+      // the two unit factors one after the other (no rounded product table)
+      v[j] = keep ? cmul(cmul(v[j], pxv), spy[n]) : make_float2(0.f, 0.f);
     }
   } else if constexpr (MODE == B_PROPAGATE_ADJ) {
     const float kx = a.kx[col];
@@ -327,8 +327,7 @@ MS_D void col_mid(float2 (&v)[PL::E], const PassBArgs& a, const float* __restric
       const int n = t + P * j;
       const float ky = sky[n];
       const bool keep = fadd_x(kx2, fmul_x(ky, ky)) < a.k2_lt;
-      const float2 w = keep ? cscale(cconj(cmul(pxv, spy[n])), scale) : make_float2(0.f, 0.f);
-      v[j] = cmul(v[j], w);
+      v[j] = keep ? cscale(cmul(cmul(v[j], cconj(pxv)), cconj(spy[n])), scale) : make_float2(0.f, 0.f);
     }
   } else if constexpr (MODE == B_CTF || MODE == B_CTF_ADJ) {
     const float kx = a.kx[col];
@@ -606,7 +605,7 @@ void fill_twiddles(float2* out) {
     for (int r = 0; r < R[p]; ++r)
       for (int k = 0; k < ns; ++k) {
         const long double ang = twopi * (long double)(((long long)r * k) % m) / (long double)m;
-        out[off + r * ns + k] = make_float2((float)std::cos(ang), (float)(-std::sin(ang)));
+        out[off + r * ns + k] = unit_fp32((double)std::cos(ang), (double)(-std::sin(ang)));
       }
     off += m;
     ns = m;

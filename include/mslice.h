@@ -83,9 +83,11 @@ enum {
                                arrivals more than the grid has, so the wait bound runs out
                                (0 = off, the default) */
   MS_OPT_LOOP_VARIANT = 8   /* persistent slice loop kernel variant: -1 = tuned on the
-                               device once per grid (default); 0..4 = force one (column
-                               unit width 4, 8, 4, 8, 2 columns; barrier form sleep-poll for
-                               0-1, release reduction with tight poll for 2-4) */
+                               device once per grid (default); 0..7 = force one: 0-4 run
+                               lines of one warp in 256-thread CTAs (column units of 4, 8,
+                               4, 8, 2 columns; barrier sleep-poll for 0-1, release
+                               reduction with tight poll for 2-4); 5-7 lines of two warps
+                               in 512-thread CTAs (units of 4, 2, 8 columns, tight poll) */
 };
 
 /* ---- lifecycle ---- */

@@ -148,7 +148,7 @@ def test_loop_wait_bound_ends_the_launch_with_an_error(engine_cls, oracle_mod):
     orc.close()
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7])
 def test_every_loop_variant(engine_cls, oracle_mod, variant):
     """Each kernel variant of the loop (column unit width, barrier form) gives
     the oracle's exit wave; the tuner's choice is one of them."""
@@ -159,7 +159,7 @@ def test_every_loop_variant(engine_cls, oracle_mod, variant):
     eng = engine_cls()
     setup(eng, atoms, n, 3.905 * 4 / n)
     v, cols, grid = eng.SliceLoop()
-    assert 0 <= v <= 4 and cols in (2, 4, 8) and grid > 0
+    assert 0 <= v <= 7 and cols in (2, 4, 8) and grid > 0
     eng.SetLoopVariant(variant)
     assert eng.SliceLoop()[0] == variant
     eng.RunConventional()
@@ -170,3 +170,99 @@ def test_every_loop_variant(engine_cls, oracle_mod, variant):
     psi = orc.run_conventional()
     orc.close()
     assert rel_l2(w, psi) < TOL
+
+
+# ---------------------------------------------------------------- batched persistent loop
+def stem_pair(engine_cls, oracle_mod, atoms, n, ps):
+    eng, orc = engine_cls(), oracle_mod.OracleSimulation()
+    for s in (eng, orc):
+        setup(s, atoms, n, ps, kV=300.0, df=-50.0, stem=True)
+    return eng, orc
+
+
+def test_batched_loop_raster_matches_passes_and_oracle(engine_cls, oracle_mod):
+    """ms_stem_raster with every batch's slices in one persistent launch (256^2,
+    batches of 3 over 7 probes) equals the per-pass raster and the oracle's
+    per-probe HAADF signal (AnnularDetector after each probe's slice loop)."""
+    from cudamultislice_b200 import structures as S
+
+    atoms = S.srtio3(4, 4, 3)
+    eng, orc = stem_pair(engine_cls, oracle_mod, atoms, 256, 3.905 * 4 / 256)
+    px = np.array([10, 128, 200, 3, 77, 250, 50], np.int32)
+    py = np.array([20, 128, 7, 199, 33, 110, 50], np.int32)
+    l0 = eng.LaunchCount()
+    sig = eng.StemRaster(px, py, 10.0, 40.0, batch=3)
+    loop_launches = eng.LaunchCount() - l0
+    eng.SetSliceLoop(False)
+    sig_pass = eng.StemRaster(px, py, 10.0, 40.0, batch=3)
+    ref = []
+    for x, y in zip(px, py):
+        orc.STEMInitialiseWavefunctions(int(x), int(y))
+        orc.run_conventional()
+        ref.append(orc.AnnularDetector(10.0, 40.0))
+    ref = np.array(ref)
+    S_ = orc.GetSlices(True)
+    eng.close()
+    orc.close()
+    assert np.max(np.abs(sig - ref) / ref) < 1e-4, (sig, ref)
+    assert np.max(np.abs(sig - sig_pass) / sig_pass) < 1e-5
+    # three batches: probe preparation launches plus one loop launch each, far
+    # fewer than two launches per slice
+    assert loop_launches < 3 * (2 * S_)
+
+
+def test_batched_loop_frozen_phonons(engine_cls, oracle_mod):
+    """ms_frozen_phonon with each batch of configurations in one persistent
+    launch (per-configuration potential stacks, exp(i sigma V) on the fly)."""
+    from cudamultislice_b200 import structures as S
+
+    atoms = S.srtio3(4, 4, 3)
+    n = 256
+    eng = engine_cls()
+    setup(eng, atoms, n, 3.905 * 4 / n)
+    seed, sigma, first, nconf = 0x5EED2026, 0.076, 2, 3
+    d, im = eng.FrozenPhonon(seed, first, nconf, sigma, batch=2)
+    eng.SetSliceLoop(False)
+    d2, im2 = eng.FrozenPhonon(seed, first, nconf, sigma, batch=2)
+    eng.close()
+    orc = oracle_mod.OracleSimulation()
+    setup(orc, atoms, n, 3.905 * 4 / n)
+    orc.AllocTDS()
+    imgs = []
+    for p in range(first, first + nconf):
+        orc.UploadBinnedAtomsTDS(seed, p, sigma)
+        orc.run_conventional()
+        orc.AddTDSWaves()
+        imgs.append(orc.SimulateImage())
+    td = orc.TDS()
+    orc.close()
+    assert rel_l2(d, td) < TOL
+    assert rel_l2(im, np.mean(imgs, axis=0)) < 2 * TOL
+    assert rel_l2(d, d2) < 2e-6 and rel_l2(im, im2) < 4e-6
+
+
+def test_mixed_grids_in_one_persistent_launch(engine_cls, oracle_mod):
+    """Two specimens on 512^2 and 256^2: each round takes the next batch of
+    both rasters through every slice in one cooperative launch; the signals
+    equal each handle's own raster (same per-instance arithmetic; only the
+    order of the FP64 detector sums differs) and the oracle's."""
+    from cudamultislice_b200 import stem_raster_concurrent
+    from cudamultislice_b200 import structures as S
+
+    atoms = S.srtio3(4, 4, 3)
+    a, orc_a = stem_pair(engine_cls, oracle_mod, atoms, 512, 3.905 * 4 / 512)
+    b, _ = stem_pair(engine_cls, oracle_mod, atoms, 256, 3.905 * 4 / 256)
+    pa = (np.array([10, 256, 400, 3, 77], np.int32), np.array([20, 256, 7, 399, 33], np.int32))
+    pb = (np.array([0, 128, 200, 17, 90, 250, 31], np.int32), np.array([5, 128, 60, 240, 90, 1, 140], np.int32))
+    (sa, sb), ms = stem_raster_concurrent([a, b], [pa, pb], 10.0, 40.0, batch=3)
+    ra = a.StemRaster(*pa, 10.0, 40.0, batch=3)
+    rb = b.StemRaster(*pb, 10.0, 40.0, batch=3)
+    assert ms > 0
+    np.testing.assert_allclose(sa, ra, rtol=1e-10)
+    np.testing.assert_allclose(sb, rb, rtol=1e-10)
+    orc_a.STEMInitialiseWavefunctions(int(pa[0][1]), int(pa[1][1]))
+    orc_a.run_conventional()
+    ref = orc_a.AnnularDetector(10.0, 40.0)
+    assert abs(sa[1] - ref) / ref < 1e-4
+    for s in (a, b, orc_a):
+        s.close()
