@@ -252,6 +252,14 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a) {
   // pixel position, rounded exactly as the host definition (no FMA)
   const float px = fadd_x(a.xoff, fmul_x((float)x, a.ps));
   const float py = fadd_x(a.yoff, fmul_x((float)y, a.ps));
+  // Values are evaluated at the exact positions (the cut-off decisions use the
+  // FP32 ones above, as the reference rounds them): the pixel's offset from
+  // its rounded position, and per sub-plane the height's (zsub_lo).  Deep in a
+  // thick slab or far across the grid the rounding is 1e-6..1e-5 A, which next
+  // to a core moves V by ~1e-5 of its value -- the same in every repeat of a
+  // crystal's slices, so it would add up over the stack.
+  const float px_lo = (float)(((double)a.xoff + (double)x * (double)a.ps) - (double)px);
+  const float py_lo = (float)(((double)a.yoff + (double)y * (double)a.ps) - (double)py);
   // the tile's pixel rectangle (the extreme pixel positions, as rounded above)
   const float tx_lo = fadd_x(a.xoff, fmul_x((float)x0, a.ps));
   const float tx_hi = fadd_x(a.xoff, fmul_x((float)(x0 + kTX - 1), a.ps));
@@ -342,6 +350,8 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a) {
           const float4 at = s_at[i];
           const float dx = fsub_x(px, at.x), dy = fsub_x(py, at.y);
           const float dxy = fadd_x(fmul_x(dx, dx), fmul_x(dy, dy));
+          const float dxv = dx + px_lo, dyv = dy + py_lo;
+          const float dxyv = fmaf(dxv, dxv, dyv * dyv);
           if (!(dxy < 5.0f)) continue;
           const float* c = a.coef + (__float_as_int(at.w) - 1) * kCoefPerZ;
           if constexpr (KIND == POT_PROJECTED) {
@@ -392,6 +402,7 @@ constexpr int kConvChunk = 64;
 __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
   __shared__ float4 s_at[kConvChunk];
   __shared__ __align__(8) float s_dz2[kConvChunk][20];
+  __shared__ __align__(8) float s_dz2v[kConvChunk][20];
   __shared__ __align__(8) float s_g[kConvChunk][3][20];
   __shared__ int s_mlo[kConvChunk], s_mhi[kConvChunk];
   __shared__ float s_dzmin[kConvChunk];
@@ -410,6 +421,14 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
   const bool inside = (x < a.nx) && (y < a.ny);
   const float px = fadd_x(a.xoff, fmul_x((float)x, a.ps));
   const float py = fadd_x(a.yoff, fmul_x((float)y, a.ps));
+  // Values are evaluated at the exact positions (the cut-off decisions use the
+  // FP32 ones above, as the reference rounds them): the pixel's offset from
+  // its rounded position, and per sub-plane the height's (zsub_lo).  Deep in a
+  // thick slab or far across the grid the rounding is 1e-6..1e-5 A, which next
+  // to a core moves V by ~1e-5 of its value -- the same in every repeat of a
+  // crystal's slices, so it would add up over the stack.
+  const float px_lo = (float)(((double)a.xoff + (double)x * (double)a.ps) - (double)px);
+  const float py_lo = (float)(((double)a.yoff + (double)y * (double)a.ps) - (double)py);
   // the tile's pixel rectangle (the extreme pixel positions, as rounded above)
   const float tx_lo = fadd_x(a.xoff, fmul_x((float)x0, a.ps));
   const float tx_hi = fadd_x(a.xoff, fmul_x((float)(x0 + kTX - 1), a.ps));
@@ -501,23 +520,29 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
           s_dzmin[pos] = dmin;
         }
         __syncthreads();
-        // per (atom, sub-plane): dz^2 as the cut-off rounds it, Gaussian factors
+        // per (atom, sub-plane): dz^2 as the cut-off rounds it, the exact
+        // height's dz^2 for the values, Gaussian factors
         for (int q = threadIdx.x; q < cnt * 20; q += kPotThreads) {
           const int i = q / 20, m = q % 20;
           const float4 at = s_at[i];
           const float dz = fsub_x(a.zsub[m], at.z);
           const float dz2 = fmul_x(dz, dz);
           s_dz2[i][m] = dz2;
+          const float dzv = dz + a.zsub_lo[m];
+          const float dz2v = dzv * dzv;
+          s_dz2v[i][m] = dz2v;
           const float* c = s_coef + (__float_as_int(at.w) - 1) * kCoefPerZ;
-          s_g[i][0][m] = ex2_fast(-c[9] * dz2);
-          s_g[i][1][m] = ex2_fast(-c[10] * dz2);
-          s_g[i][2][m] = ex2_fast(-c[11] * dz2);
+          s_g[i][0][m] = ex2_fast(-c[9] * dz2v);
+          s_g[i][1][m] = ex2_fast(-c[10] * dz2v);
+          s_g[i][2][m] = ex2_fast(-c[11] * dz2v);
         }
         __syncthreads();
         for (int i = 0; i < cnt; ++i) {
           const float4 at = s_at[i];
           const float dx = fsub_x(px, at.x), dy = fsub_x(py, at.y);
           const float dxy = fadd_x(fmul_x(dx, dx), fmul_x(dy, dy));
+          const float dxv = dx + px_lo, dyv = dy + py_lo;
+          const float dxyv = fmaf(dxv, dxv, dyv * dyv);
           // the warp's nearest pixel bounds the sub-planes any lane can use:
           // |zsub[m] - z| < sqrt(5 - min dxy), widened by one plane each side
           // (dxy >= 0, so its bits order as the values do)
@@ -528,14 +553,16 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
           const int mlo = max(s_mlo[i], __float2int_rd((zs0 - at.z - zr) * inv_h) - 1);
           const int mhi = min(s_mhi[i], __float2int_ru((zs0 - at.z + zr) * inv_h) + 1);
           const float* c = s_coef + (__float_as_int(at.w) - 1) * kCoefPerZ;
-          const float g0 = c[6] * ex2_fast(-c[9] * dxy), g1 = c[7] * ex2_fast(-c[10] * dxy),
-                      g2 = c[8] * ex2_fast(-c[11] * dxy);
-          if (!(fadd_x(dxy, s_dzmin[i]) < 0.0625f)) {
+          const float g0 = c[6] * ex2_fast(-c[9] * dxyv), g1 = c[7] * ex2_fast(-c[10] * dxyv),
+                      g2 = c[8] * ex2_fast(-c[11] * dxyv);
+          // (a margin over 0.0625: the clamp is decided on the exact-position
+          // value r^2 in the sub-plane loop below)
+          if (!(fadd_x(dxy, s_dzmin[i]) < 0.0627f)) {
             // No sub-plane reaches the 0.25 A clamp for this pixel: sub-planes in
             // pairs (m, m+1) on the packed FP32x2 pipe.  add.rn.f32x2 rounds each
             // lane as fadd_x does, so the r^2 < 5 decisions are unchanged; sub-
             // planes outside [mlo, mhi] have dz^2 >= 5 and fail the test.
-            const f2p d2 = pk2(dxy, dxy);
+            const f2p d2 = pk2(dxy, dxy), d2v = pk2(dxyv, dxyv);
             const f2p c0 = pk2(c[0], c[0]), c1 = pk2(c[1], c[1]), c2 = pk2(c[2], c[2]);
             const f2p n3 = pk2(-c[3], -c[3]), n4 = pk2(-c[4], -c[4]), n5 = pk2(-c[5], -c[5]);
             const f2p q0 = pk2(g0, g0), q1 = pk2(g1, g1), q2 = pk2(g2, g2);
@@ -548,8 +575,11 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
               up2(r2, ra, rb);
               const bool ka = ra < 5.0f, kb = rb < 5.0f;
               if (!(ka || kb)) return;
-              const f2p ri = pk2(rsqrtf(ra), rsqrtf(rb));
-              const f2p r = mul2(r2, ri);
+              const f2p r2v = add2(d2v, *reinterpret_cast<const f2p*>(&s_dz2v[i][m]));
+              float va2, vb2;
+              up2(r2v, va2, vb2);
+              const f2p ri = pk2(rsqrtf(va2), rsqrtf(vb2));
+              const f2p r = mul2(r2v, ri);
               f2p L = mul2(c0, ex2_pair(mul2(n3, r)));
               L = fma2(c1, ex2_pair(mul2(n4, r)), L);
               L = fma2(c2, ex2_pair(mul2(n5, r)), L);
@@ -577,11 +607,12 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
             for (int m = mlo; m <= mhi; ++m) {
               const float r2 = fadd_x(dxy, s_dz2[i][m]);
               if (!(r2 < 5.0f)) continue;
+              const float r2v = dxyv + s_dz2v[i][m];
               float v;
-              if (r2 < 0.0625f) {
-                v = vatom_f(c, r2);  // inside the 0.25 A clamp
+              if (r2v < 0.0625f) {
+                v = vatom_f(c, r2v);  // inside the 0.25 A clamp
               } else {
-                const float ri = rsqrtf(r2), r = r2 * ri;
+                const float ri = rsqrtf(r2v), r = r2v * ri;
                 const float L =
                     c[0] * ex2_fast(-c[3] * r) + c[1] * ex2_fast(-c[4] * r) + c[2] * ex2_fast(-c[5] * r);
                 const float G = g0 * s_g[i][0][m] + g1 * s_g[i][1][m] + g2 * s_g[i][2][m];

@@ -48,6 +48,8 @@ struct PotArgs {
   int kt, kb;            // inclusive z-bin window
   int nsub;              // sub-planes (20 conventional, 1 finite difference)
   float zsub[20];        // sub-plane z (shifted frame), FP32 as the reference
+  float zsub_lo[20];     // exact height minus zsub (values only; the cut-off
+                         // decisions use zsub as the reference rounds it)
   float wsub;            // weight per sub-plane
   // projected mode: atoms with floorf((top - z)/dz) == slab
   float top, slab_dz;

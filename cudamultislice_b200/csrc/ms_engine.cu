@@ -1306,7 +1306,8 @@ class Engine {
   int tune_raster_batch(int px0, int py0, float inner, float outer, int* out) {
     for (auto& kv : raster_batch_)
       if (kv.first == (long long)nx_ * 100000 + ny_) {
-        *out = kv.second;
+        *out = kv.second & 0xFFFF;
+        rs_prefer_loop_ = (kv.second >> 16) != 0;
         return MS_OK;
       }
     size_t free_b = 0, total_b = 0;
@@ -1317,9 +1318,12 @@ class Engine {
     }
     const int cands[] = {8, 12, 16, 24, 32, 48, 64};
     int best = std::min(cap, 64);
+    bool best_loop = false;
     float best_t = INFINITY;
-    for (int B : cands) {
+    for (int B : cands)
+      for (int lp = 0; lp < (use_batch_loop() ? 2 : 1); ++lp) {
       if (B > cap) break;
+      rs_prefer_loop_ = lp == 1;  // slices in the batched persistent loop, or per pass
       std::vector<int> qx(B, px0), qy(B, py0);
       for (int rep = 0; rep < 2; ++rep) {  // the first run tunes the plans and loads the kernels
         if (int rc = raster_prepare(qx.data(), qy.data(), B, inner, outer, B)) return rc;
@@ -1338,9 +1342,11 @@ class Engine {
       if (per_probe < best_t) {
         best_t = per_probe;
         best = B;
+        best_loop = rs_prefer_loop_;
       }
-    }
-    raster_batch_.push_back({(long long)nx_ * 100000 + ny_, best});
+      }
+    rs_prefer_loop_ = best_loop;
+    raster_batch_.push_back({(long long)nx_ * 100000 + ny_, best | (best_loop ? 1 << 16 : 0)});
     *out = best;
     return MS_OK;
   }
@@ -1406,7 +1412,7 @@ class Engine {
     L.sync.limit_ns = loop_limit_ns_;
     L.sync.expect_extra = loop_extra_;
     int grid = 0;
-    MS_TRY(batch_loop_prepare(g0.n, g1 ? g1->n : 0, &grid));
+    MS_TRY(batch_loop_prepare(g0.n, g1 ? g1->n : 0, g0.Vstack == nullptr, &grid));
     MS_TRY(cudaMemsetAsync(d_loop_sync_.p, 0, sizeof(unsigned int), st));
     MS_TRY(launch_batch_loop(L, grid, st));
     ++launches;
@@ -1444,7 +1450,7 @@ class Engine {
     const int B = rs_B_, n = rs_n_, S = rs_S_;
     const PlanChoice pc = plan_for(B, true);
     const int vr = pc.row, vc = pc.col;
-    const bool loop = allow_loop && use_batch_loop();
+    const bool loop = allow_loop && use_batch_loop() && rs_prefer_loop_;
     MS_TRY(cudaMemsetAsync(d_bsig_.p, 0, sizeof(double) * 2 * n, st));
     if (loop) MS_TRY(cudaMemsetAsync(d_loop_sync_.p, 0, 2 * sizeof(unsigned int), st));
     rs_loop_ = loop;
@@ -2530,7 +2536,10 @@ class Engine {
       a.xoff = xoff_;
       a.yoff = yoff_;
       a.nsub = 20;
-      for (int m = 1; m <= 20; ++m) a.zsub[m - 1] = z - m * convdz_ / 20.0f;
+      for (int m = 1; m <= 20; ++m) {
+        a.zsub[m - 1] = z - m * convdz_ / 20.0f;
+        a.zsub_lo[m - 1] = (float)(((double)z - m * (double)convdz_ / 20.0) - (double)a.zsub[m - 1]);
+      }
       a.wsub = convdz_ / 20.0f;
     } else if (kind == POT_RS) {
       // binnedAtomPKernelRS U.cu:655-727 at z = top - dz*it, dz = 1 (int) (U.cu:2129-2137)
@@ -2541,7 +2550,10 @@ class Engine {
       a.xoff = xoff_;
       a.yoff = yoff_;
       a.nsub = 10;
-      for (int m = 1; m <= 10; ++m) a.zsub[m - 1] = z - (float)(m * 1) / 10.0f;
+      for (int m = 1; m <= 10; ++m) {
+        a.zsub[m - 1] = z - (float)(m * 1) / 10.0f;
+        a.zsub_lo[m - 1] = (float)(((double)z - m / 10.0) - (double)a.zsub[m - 1]);
+      }
       a.wsub = 1 / 10.0f;
     } else if (kind == POT_FD) {
       // binnedAtomPKernelFD U.cu:883-946 at z = top - dzFD*it, no offsets
@@ -2623,6 +2635,7 @@ class Engine {
   bool image_noisy_ = false;
   int rs_n_ = 0, rs_B_ = 1, rs_S_ = 0;  // prepared probe raster
   bool rs_loop_ = false;                 // its slices ran in the batched persistent loop
+  bool rs_prefer_loop_ = true;           // tuned: batched loop (or per pass) for this grid's rasters
   float rs_kin2_ = 0, rs_kout2_ = 0;
   std::vector<int> hzoff_;  // first sorted atom per z-bin (focal-series atom gradient)
   DevBuf<float2> d_ck_, d_seg_, d_G_, d_U_, d_Phi_;

@@ -167,7 +167,8 @@ struct BatchLoopArgs {
 bool batch_loop_supported(int n0, int n1);
 // FFT plan variant (twiddle tables) of the batched loop for lines of n points.
 int batch_loop_plan(int n);
-cudaError_t batch_loop_prepare(int n0, int n1, int* grid);
+// tc: the groups multiply by stored transmissions (else exp(i sigma V) from V).
+cudaError_t batch_loop_prepare(int n0, int n1, bool tc, int* grid);
 cudaError_t launch_batch_loop(const BatchLoopArgs& L, int grid, cudaStream_t s);
 
 // Grids the persistent loop is provided for (square 256, 512, 1024), and the

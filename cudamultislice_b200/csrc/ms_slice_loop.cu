@@ -130,12 +130,12 @@ template <int N>
 using NarrowPL = typename PlanSel<N, LoopPlan<N, false>::V>::T;
 constexpr int kBatchCW = 4;
 
-template <int N0, int N1>
+template <int N0, int N1, bool TC>
 cudaError_t batch_prepare_t(int* grid) {
   using PL0 = NarrowPL<N0>;
   using PL1 = NarrowPL<N1>;
   using SH = BatchShape<PL0, PL1, kBatchCW>;
-  auto kernel = k_batch_loop<PL0, PL1, kBatchCW>;
+  auto kernel = k_batch_loop<PL0, PL1, kBatchCW, TC>;
   static unsigned long long done = 0;
   if (cudaError_t e = set_smem_once(done, kernel, SH::SMEM)) return e;
   int dev = 0, sms = 0, per_sm = 0;
@@ -147,7 +147,7 @@ cudaError_t batch_prepare_t(int* grid) {
   return cudaSuccess;
 }
 
-template <int N0, int N1>
+template <int N0, int N1, bool TC>
 cudaError_t batch_launch_t(const BatchLoopArgs& L, int grid, cudaStream_t s) {
   using PL0 = NarrowPL<N0>;
   using PL1 = NarrowPL<N1>;
@@ -162,7 +162,7 @@ cudaError_t batch_launch_t(const BatchLoopArgs& L, int grid, cudaStream_t s) {
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_batch_loop<PL0, PL1, kBatchCW>, L);
+  return cudaLaunchKernelEx(&cfg, k_batch_loop<PL0, PL1, kBatchCW, TC>, L);
 }
 
 // (n0, n1) -> instantiation; n1 = 0: one group (the second plan repeats the first)
@@ -195,19 +195,28 @@ int batch_loop_plan(int n) {
   }
 }
 
-cudaError_t batch_loop_prepare(int n0, int n1, int* grid) {
-  return by_pair(n0, n1, [&](auto a, auto b) { return batch_prepare_t<decltype(a)::value, decltype(b)::value>(grid); });
+cudaError_t batch_loop_prepare(int n0, int n1, bool tc, int* grid) {
+  return by_pair(n0, n1, [&](auto a, auto b) {
+    return tc ? batch_prepare_t<decltype(a)::value, decltype(b)::value, true>(grid)
+              : batch_prepare_t<decltype(a)::value, decltype(b)::value, false>(grid);
+  });
 }
 
 cudaError_t launch_batch_loop(const BatchLoopArgs& L, int grid, cudaStream_t s) {
   const int n0 = L.g[0].n, n1 = (L.g[1].n > 0 && L.g[1].B > 0) ? L.g[1].n : 0;
   if (L.S < 1 || grid < 1 || L.g[0].B < 1 || !batch_loop_supported(n0, n1)) return cudaErrorInvalidValue;
+  const bool tc = L.g[0].Vstack == nullptr;
   for (int k = 0; k < (n1 ? 2 : 1); ++k) {
     const LoopGroup& g = L.g[k];
-    if (!g.wave || (!g.Vstack && !g.tstack) || g.a.nx != g.n || g.a.ny != g.n || g.b.nx != g.n || g.b.ny != g.n)
+    // every group of a launch takes the same potential source
+    if (!g.wave || (tc ? !g.tstack : !g.Vstack) || (tc && g.Vstack) || g.a.nx != g.n || g.a.ny != g.n ||
+        g.b.nx != g.n || g.b.ny != g.n)
       return cudaErrorInvalidValue;
   }
-  return by_pair(n0, n1, [&](auto a, auto b) { return batch_launch_t<decltype(a)::value, decltype(b)::value>(L, grid, s); });
+  return by_pair(n0, n1, [&](auto a, auto b) {
+    return tc ? batch_launch_t<decltype(a)::value, decltype(b)::value, true>(L, grid, s)
+              : batch_launch_t<decltype(a)::value, decltype(b)::value, false>(L, grid, s);
+  });
 }
 
 }  // namespace ms

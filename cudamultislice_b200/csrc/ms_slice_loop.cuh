@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(NT, 1) k_slice_loop(LoopArgs L) {
 
 // Row phase of one line of a batched instance: [IFFT_row] -> x t -> FFT_row
 // in place, t = exp(i sigma V) from V on the fly or a stored transmission.
-template <class PL>
+template <class PL, bool TC>
 MS_D void batch_row(const LoopGroup& G, int s, int inst, int line, int t, float2* sm, bool first) {
   constexpr int NX = PL::N, E = PL::E, P = PL::P;
   const long long nn = (long long)NX * NX;
@@ -219,7 +219,7 @@ MS_D void batch_row(const LoopGroup& G, int s, int inst, int line, int t, float2
   float2 v[E];
 #pragma unroll
   for (int j = 0; j < E; ++j) v[j] = w[t + P * j];
-  if (G.Vstack) {
+  if constexpr (!TC) {
     float vv[E];
 #pragma unroll
     for (int j = 0; j < E; ++j) vv[j] = G.Vstack[q0 + t + P * j];
@@ -308,6 +308,7 @@ struct BatchShape {
   using A = LoopShape<PL0, CW, 256>;
   using B = LoopShape<PL1, CW, 256>;
   static constexpr int NT = 256;
+  static constexpr int LINES_ROWS = NT / 32;  // row lines in flight per CTA
   static constexpr int EXCH = A::EXCH > B::EXCH ? A::EXCH : B::EXCH;
   static constexpr int N0 = PL0::N, N1 = PL1::N;
   // exchange slots, then ky0 | ky1 (floats, padded to float2) and py0 | py1
@@ -315,7 +316,9 @@ struct BatchShape {
   static constexpr size_t SMEM = ((size_t)EXCH + KY + N0 + N1) * sizeof(float2);
 };
 
-template <class PL0, class PL1, int CW>
+// TC: the groups multiply by stored transmissions (tstack) rather than
+// forming exp(i sigma V) from Vstack.
+template <class PL0, class PL1, int CW, bool TC>
 __global__ void __launch_bounds__(256, 1) k_batch_loop(BatchLoopArgs L) {
   using SH = BatchShape<PL0, PL1, CW>;
   using SA = typename SH::A;
@@ -344,6 +347,11 @@ __global__ void __launch_bounds__(256, 1) k_batch_loop(BatchLoopArgs L) {
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   const int g = threadIdx.x / GS, gr = threadIdx.x % GS;
   const int cl = gr % CW, t = gr / CW;
+  // one slot size for both grids: the CTA's column groups may hold units of
+  // different grids at the same time (N0 >= N1, so group 0's slots are the larger)
+  constexpr int CSLOT = SA::COL_SLOT > SB::COL_SLOT ? SA::COL_SLOT : SB::COL_SLOT;
+  constexpr int RSLOT = SA::ROW_SLOT > SB::ROW_SLOT ? SA::ROW_SLOT : SB::ROW_SLOT;
+  static_assert(SH::LINES_ROWS * RSLOT <= SH::EXCH && GROUPS * CW * CSLOT <= SH::EXCH, "exchange slots overflow");
   const long long rows0 = (long long)G0.B * N0, rows1 = has1 ? (long long)G1.B * N1 : 0;
   const long long units0 = (long long)G0.B * (N0 / CW), units1 = has1 ? (long long)G1.B * (N1 / CW) : 0;
   unsigned int epoch = 0;
@@ -351,23 +359,21 @@ __global__ void __launch_bounds__(256, 1) k_batch_loop(BatchLoopArgs L) {
     const bool first = s == 0, last = s + 1 == L.S;
     // ---- row phase: every line of every instance ----
     for (long long r = (long long)warp * G + blockIdx.x; r < rows0 + rows1; r += (long long)SA::LINES * G) {
-      float2* sm = smem + warp * (SA::ROW_SLOT > SB::ROW_SLOT ? SA::ROW_SLOT : SB::ROW_SLOT);
+      float2* sm = smem + warp * RSLOT;
       if (r < rows0)
-        batch_row<PL0>(G0, s, (int)(r / N0), (int)(r % N0), lane, sm, first);
+        batch_row<PL0, TC>(G0, s, (int)(r / N0), (int)(r % N0), lane, sm, first);
       else
-        batch_row<PL1>(G1, s, (int)((r - rows0) / N1), (int)((r - rows0) % N1), lane, sm, first);
+        batch_row<PL1, TC>(G1, s, (int)((r - rows0) / N1), (int)((r - rows0) % N1), lane, sm, first);
     }
     if (!loop_barrier<true>(L.sync, ++epoch)) return;
     // ---- column phase: every column unit of every instance ----
     for (long long u = (long long)g * G + blockIdx.x; u < units0 + units1; u += (long long)GROUPS * G) {
-      const int slot = g * CW + cl;
+      float2* sm = smem + (g * CW + cl) * CSLOT;
       if (u < units0) {
-        float2* sm = smem + slot * SA::COL_SLOT;
         batch_col<PL0, CW>(G0, (int)(u / (N0 / CW)), (int)(u % (N0 / CW)) * CW, cl, t, sm, sky0, spy0,
                            last && G0.sig != nullptr);
       } else {
         const long long v = u - units0;
-        float2* sm = smem + slot * SB::COL_SLOT;
         batch_col<PL1, CW>(G1, (int)(v / (N1 / CW)), (int)(v % (N1 / CW)) * CW, cl, t, sm, sky1, spy1,
                            last && G1.sig != nullptr);
       }
