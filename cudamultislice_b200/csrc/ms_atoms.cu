@@ -399,7 +399,21 @@ __device__ __forceinline__ f2p ex2_pair(f2p a) {
 // its nearest pixel can reach.
 constexpr int kConvChunk = 64;
 
+// Tile shapes of the conventional kernel (TX x TY pixels, 256 threads, warps
+// on 8 x 4 patches): 32 x 8, 16 x 16, 64 x 4 -- tuned per specimen and grid by
+// the engine (a squarer tile stages fewer candidate atoms per pixel, a wider
+// one fewer bins per row of CTAs).
+template <int TX, int TY>
+__device__ __forceinline__ void tile_pixel_t(int tid, int& tx, int& ty) {
+  constexpr int PX = TX / 8;  // patches across
+  const int w = tid >> 5, l = tid & 31;
+  tx = (w % PX) * 8 + (l & 7);
+  ty = (w / PX) * 4 + (l >> 3);
+}
+
+template <int TX, int TY>
 __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
+  static_assert(TX * TY == kPotThreads && TX % 8 == 0 && TY % 4 == 0, "tile of 8 x 4 warp patches");
   __shared__ float4 s_at[kConvChunk];
   __shared__ __align__(8) float s_dz2[kConvChunk][20];
   __shared__ __align__(8) float s_dz2v[kConvChunk][20];
@@ -415,8 +429,8 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
   for (int i = threadIdx.x; i < 103 * kCoefPerZ; i += kPotThreads) s_coef[i] = a.coef[i];
 
   int tx, ty;
-  tile_pixel(threadIdx.x, tx, ty);
-  const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY;
+  tile_pixel_t<TX, TY>(threadIdx.x, tx, ty);
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
   const int x = x0 + tx, y = y0 + ty;
   const bool inside = (x < a.nx) && (y < a.ny);
   const float px = fadd_x(a.xoff, fmul_x((float)x, a.ps));
@@ -431,14 +445,14 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
   const float py_lo = (float)(((double)a.yoff + (double)y * (double)a.ps) - (double)py);
   // the tile's pixel rectangle (the extreme pixel positions, as rounded above)
   const float tx_lo = fadd_x(a.xoff, fmul_x((float)x0, a.ps));
-  const float tx_hi = fadd_x(a.xoff, fmul_x((float)(x0 + kTX - 1), a.ps));
+  const float tx_hi = fadd_x(a.xoff, fmul_x((float)(x0 + TX - 1), a.ps));
   const float ty_lo = fadd_x(a.yoff, fmul_x((float)y0, a.ps));
-  const float ty_hi = fadd_x(a.yoff, fmul_x((float)(y0 + kTY - 1), a.ps));
+  const float ty_hi = fadd_x(a.yoff, fmul_x((float)(y0 + TY - 1), a.ps));
   // sub-plane m sits at zsub[0] - m h: its index from a height, for the
   // per-warp sub-plane window below
   const float zs0 = a.zsub[0], inv_h = 19.0f / (a.zsub[0] - a.zsub[19]);
-  const float xlo = a.xoff + x0 * a.ps - 2.2361f, xhi = a.xoff + (x0 + kTX - 1) * a.ps + 2.2361f;
-  const float ylo = a.yoff + y0 * a.ps - 2.2361f, yhi = a.yoff + (y0 + kTY - 1) * a.ps + 2.2361f;
+  const float xlo = a.xoff + x0 * a.ps - 2.2361f, xhi = a.xoff + (x0 + TX - 1) * a.ps + 2.2361f;
+  const float ylo = a.yoff + y0 * a.ps - 2.2361f, yhi = a.yoff + (y0 + TY - 1) * a.ps + 2.2361f;
   const int bxl = max((int)floorf(xlo / a.bw_x) - 1, 0);
   const int bxh = min((int)floorf(xhi / a.bw_x) + 1, kBins - 1);
   const int byl = max((int)floorf(ylo / a.bw_y) - 1, 0);
@@ -759,10 +773,20 @@ cudaError_t build_atom_index(const int* dZ, const float* dx, const float* dy, co
   return cudaGetLastError();
 }
 
-cudaError_t launch_potential(const PotArgs& a, int kind, cudaStream_t s) {
+int potential_tiles() { return 3; }
+
+cudaError_t launch_potential(const PotArgs& a, int kind, cudaStream_t s, int tile) {
   dim3 grid((a.nx + kTX - 1) / kTX, (a.ny + kTY - 1) / kTY);
+  if (kind == POT_CONVENTIONAL) {
+    switch (tile) {
+      case 0: k_potential_conv<32, 8><<<grid, kPotThreads, 0, s>>>(a); break;
+      case 1: k_potential_conv<16, 16><<<dim3((a.nx + 15) / 16, (a.ny + 15) / 16), kPotThreads, 0, s>>>(a); break;
+      case 2: k_potential_conv<64, 4><<<dim3((a.nx + 63) / 64, (a.ny + 3) / 4), kPotThreads, 0, s>>>(a); break;
+      default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+  }
   switch (kind) {
-    case POT_CONVENTIONAL: k_potential_conv<<<grid, kPotThreads, 0, s>>>(a); break;
     case POT_FD: k_potential<POT_FD><<<grid, kPotThreads, 0, s>>>(a); break;
     case POT_PROJECTED: k_potential<POT_PROJECTED><<<grid, kPotThreads, 0, s>>>(a); break;
     case POT_RS: k_potential<POT_RS><<<grid, kPotThreads, 0, s>>>(a); break;

@@ -57,7 +57,10 @@ struct PotArgs {
   long long batch_stride_V;
 };
 
-cudaError_t launch_potential(const PotArgs& a, int kind, cudaStream_t s);
+// tile: the conventional kernel's tile shape variant (0: 32 x 8, 1: 16 x 16,
+// 2: 64 x 4 pixels; other kinds take 32 x 8).
+cudaError_t launch_potential(const PotArgs& a, int kind, cudaStream_t s, int tile = 0);
+int potential_tiles();
 
 // Adjoint of the conventional potential of one slice with respect to atom x, y:
 // dxy[2 perm[l] + {0,1}] += dL/d{x,y} of sorted atoms l in [a0, a1) (the CSR

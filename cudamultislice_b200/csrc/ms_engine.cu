@@ -178,6 +178,13 @@ class Engine {
         forced_loop_ = value;
         invalidate_graph();
         return MS_OK;
+      case MS_OPT_POTENTIAL_TILE:
+        if (value < -1 || value >= potential_tiles()) return fail(MS_ERR_INVALID, "tile must be -1 (tuned) or 0..2");
+        pot_tile_ = value;
+        stack_valid_ = false;
+        fd_stack_valid_ = false;
+        invalidate_graph();
+        return MS_OK;
       case MS_OPT_LOOP_WAIT_TEST:
         if (value < 0) return fail(MS_ERR_INVALID, "test arrivals must be >= 0");
         loop_extra_ = (unsigned int)value;
@@ -453,6 +460,7 @@ class Engine {
     tuned_.clear();
     raster_batch_.clear();
     loop_grid_ = 0;
+    pot_tile_ = -1;
     if (fused_ok_) {
       std::vector<float2> tw(2 * (size_t)std::max(nx, ny));
       for (int v = 0; v < plan_variants(); ++v) {
@@ -2508,9 +2516,41 @@ class Engine {
 
   // Potential of one slice into out (ny x nx floats).
   int potential_slice(int kind, int it, float* out) {
+    if (kind == POT_CONVENTIONAL && pot_tile_ < 0 && !capturing_)
+      if (int rc = tune_pot_tile()) return rc;
     const PotArgs a = pot_args(kind, it, out);
-    MS_TRY(launch_potential(a, kind, stream_));
+    MS_TRY(launch_potential(a, kind, stream_, kind == POT_CONVENTIONAL ? std::max(pot_tile_, 0) : 0));
     ++launches;
+    return MS_OK;
+  }
+
+  // Tile shape of the conventional potential kernel for this grid, tuned on
+  // the device the first time it is needed: each shape builds the mid-slab
+  // slice (one warm-up launch, then three timed) and the fastest is kept.
+  int tune_pot_tile() {
+    int S = 0;
+    if (int rc = get_slices(true, &S)) return rc;
+    const int it = std::max(1, S / 2);
+    const size_t N = (size_t)nx_ * ny_;
+    MS_TRY(d_V_.resize(N));
+    float best_t = INFINITY;
+    int best = 0;
+    for (int t = 0; t < potential_tiles(); ++t) {
+      const PotArgs a = pot_args(POT_CONVENTIONAL, it, d_V_.p);
+      MS_TRY(launch_potential(a, POT_CONVENTIONAL, stream_, t));
+      MS_TRY(cudaEventRecord(ev0_, stream_));
+      for (int k = 0; k < 3; ++k) MS_TRY(launch_potential(a, POT_CONVENTIONAL, stream_, t));
+      MS_TRY(cudaEventRecord(ev1_, stream_));
+      MS_TRY(cudaEventSynchronize(ev1_));
+      float ms = 0.0f;
+      MS_TRY(cudaEventElapsedTime(&ms, ev0_, ev1_));
+      launches += 4;
+      if (ms < best_t) {
+        best_t = ms;
+        best = t;
+      }
+    }
+    pot_tile_ = best;
     return MS_OK;
   }
 
@@ -2633,6 +2673,7 @@ class Engine {
   uint64_t det_seed_ = 0;
   uint32_t det_serial_ = 0;
   bool image_noisy_ = false;
+  int pot_tile_ = -1;                    // tuned tile shape of the conventional potential (-1: not yet)
   int rs_n_ = 0, rs_B_ = 1, rs_S_ = 0;  // prepared probe raster
   bool rs_loop_ = false;                 // its slices ran in the batched persistent loop
   bool rs_prefer_loop_ = true;           // tuned: batched loop (or per pass) for this grid's rasters

@@ -112,6 +112,10 @@ class ManagedMultisliceSimulation:
         self._chk(self._L.ms_get_slice_loop(self._h, C.byref(v), C.byref(c), C.byref(g)))
         return v.value, c.value, g.value
 
+    def SetPotentialTile(self, tile: int):
+        """Conventional potential kernel tile: -1 tuned (default), 0/1/2 = 32x8, 16x16, 64x4 pixels."""
+        self._chk(self._L.ms_set_option(self._h, 9, int(tile)))
+
     def SetLoopWaitUs(self, us: int):
         """Bound on each grid-barrier wait of the persistent loop (microseconds)."""
         self._chk(self._L.ms_set_option(self._h, 6, int(us)))

@@ -82,12 +82,14 @@ enum {
   MS_OPT_LOOP_WAIT_TEST = 7, /* test hook: > 0 makes every grid barrier wait for that many
                                arrivals more than the grid has, so the wait bound runs out
                                (0 = off, the default) */
-  MS_OPT_LOOP_VARIANT = 8   /* persistent slice loop kernel variant: -1 = tuned on the
+  MS_OPT_LOOP_VARIANT = 8,  /* persistent slice loop kernel variant: -1 = tuned on the
                                device once per grid (default); 0..7 = force one: 0-4 run
                                lines of one warp in 256-thread CTAs (column units of 4, 8,
                                4, 8, 2 columns; barrier sleep-poll for 0-1, release
                                reduction with tight poll for 2-4); 5-7 lines of two warps
                                in 512-thread CTAs (units of 4, 2, 8 columns, tight poll) */
+  MS_OPT_POTENTIAL_TILE = 9 /* conventional potential kernel tile: -1 = tuned on the device
+                               per grid (default); 0, 1, 2 = 32 x 8, 16 x 16, 64 x 4 pixels */
 };
 
 /* ---- lifecycle ---- */

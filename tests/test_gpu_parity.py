@@ -111,6 +111,23 @@ def test_exit_wave_every_fft_plan(engine_cls, oracle_mod, variant):
 
 
 # ---------------------------------------------------------------- potentials
+@pytest.mark.parametrize("tile", [0, 1, 2])
+def test_potential_tile_shapes(engine_cls, oracle_mod, tile):
+    """Every tile shape of the conventional potential kernel (32x8, 16x16, 64x4)
+    gives the oracle's potential; the shapes differ only in summation order."""
+    from cudamultislice_b200 import structures as S
+
+    atoms = S.random_atoms(3000, size=(30.0, 27.0, 12.0), seed=21)
+    eng, orc = make_pair(engine_cls, oracle_mod, atoms, 256, 0.12)
+    eng.SetPotentialTile(tile)
+    for it in (3, 5):
+        v = eng.PotentialSlice(0, it)
+        ref = orc.PotentialConventional(it)
+        assert rel_l2(v, ref) < 1e-6, (tile, it, rel_l2(v, ref))
+    eng.SetPotentialTile(-1)  # tuned
+    assert rel_l2(eng.PotentialSlice(0, 5), orc.PotentialConventional(5)) < 1e-6
+
+
 @pytest.mark.parametrize("kind", [0, 1, 2])
 def test_potential_slices(engine_cls, oracle_mod, kind):
     eng, orc = make_pair(engine_cls, oracle_mod, sto(2, 4), 128, 0.1)
@@ -411,8 +428,11 @@ def test_stem_raster_concurrent_mixed_grids(engine_cls, oracle_mod):
     ra = a.StemRaster(*pa, 10.0, 40.0, batch=3)
     rb = b.StemRaster(*pb, 10.0, 40.0, batch=3)
     assert ms > 0
+    # the 128^2 handle runs per-pass kernels in both arrangements (same
+    # arithmetic); the 256^2 handle's own raster runs its slices in the batched
+    # persistent loop, the graph branch per pass (FP32 rounding apart)
     np.testing.assert_allclose(sa, ra, rtol=1e-12)
-    np.testing.assert_allclose(sb, rb, rtol=1e-12)
+    np.testing.assert_allclose(sb, rb, rtol=1e-6)
     orc_a.STEMInitialiseWavefunctions(int(pa[0][1]), int(pa[1][1]))
     for i in range(1, orc_a.GetSlices(True) + 1):
         orc_a.MultisliceStepConventional(i)
