@@ -121,4 +121,27 @@ MS_D void sincos_red2(float x0, float x1, float* s0, float* c0, float* s1, float
   *c1 = ((qb + 1) & 2) ? -ccb : ccb;
 }
 
+// sincos_red2 for arguments whose quarter-turn count is 0 (|x * 2/pi| <= 0.5
+// as sincos_red2 rounds the product, so rint gives 0): the reduction steps are
+// then exact identities and the quadrant swap does nothing, so the polynomials
+// alone give bit-identical results.
+MS_D bool sincos_small_ok(float x) { return fabsf(x * 0.636619772f) <= 0.5f; }
+MS_D void sincos_small2(float x0, float x1, float* s0, float* c0, float* s1, float* c1) {
+  const f2p r = pk2(x0, x1);
+  const f2p r2 = mul2(r, r);
+  f2p ps = fma2(r2, pk2(2.7557319223985893e-06f, 2.7557319223985893e-06f),
+                pk2(-1.984126984126984e-04f, -1.984126984126984e-04f));
+  ps = fma2(r2, ps, pk2(8.333333333333333e-03f, 8.333333333333333e-03f));
+  ps = fma2(r2, ps, pk2(-0.16666666666666666f, -0.16666666666666666f));
+  const f2p sn = fma2(mul2(r, r2), ps, r);
+  f2p pc = fma2(r2, pk2(-2.755731922398589e-07f, -2.755731922398589e-07f),
+                pk2(2.48015873015873e-05f, 2.48015873015873e-05f));
+  pc = fma2(r2, pc, pk2(-1.388888888888889e-03f, -1.388888888888889e-03f));
+  pc = fma2(r2, pc, pk2(4.1666666666666664e-02f, 4.1666666666666664e-02f));
+  pc = fma2(r2, pc, pk2(-0.5f, -0.5f));
+  const f2p cs = fma2(r2, pc, pk2(1.0f, 1.0f));
+  up2(sn, *s0, *s1);
+  up2(cs, *c0, *c1);
+}
+
 }  // namespace ms

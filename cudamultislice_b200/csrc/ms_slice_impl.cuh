@@ -175,13 +175,28 @@ MS_D void row_mid(float2 (&v)[PL::E], const PassAArgs& a, const RowOperands<PL, 
     for (int j = 0; j < E; ++j) o[t + P * j] = v[j];
   }
   if constexpr ((FLAGS & A_MULT_T) != 0) {
-    // two points per packed sincos (bit-identical to sincos_red per point)
+    // two points per packed sincos (bit-identical to sincos_red per point);
+    // the polynomial-only form when every phase of the warp is within a
+    // quarter turn of 0 (bit-identical too)
+    bool small = true;
 #pragma unroll
-    for (int j = 0; j < E; j += 2) {
-      float s0, c0, s1, c1;
-      sincos_red2(fmul_x(a.sigma, op.V[j]), fmul_x(a.sigma, op.V[j + 1]), &s0, &c0, &s1, &c1);
-      v[j] = cmul(v[j], make_float2(c0, s0));
-      v[j + 1] = cmul(v[j + 1], make_float2(c1, s1));
+    for (int j = 0; j < E; ++j) small = small && sincos_small_ok(fmul_x(a.sigma, op.V[j]));
+    if (__all_sync(0xffffffffu, small)) {
+#pragma unroll
+      for (int j = 0; j < E; j += 2) {
+        float s0, c0, s1, c1;
+        sincos_small2(fmul_x(a.sigma, op.V[j]), fmul_x(a.sigma, op.V[j + 1]), &s0, &c0, &s1, &c1);
+        v[j] = cmul(v[j], make_float2(c0, s0));
+        v[j + 1] = cmul(v[j + 1], make_float2(c1, s1));
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < E; j += 2) {
+        float s0, c0, s1, c1;
+        sincos_red2(fmul_x(a.sigma, op.V[j]), fmul_x(a.sigma, op.V[j + 1]), &s0, &c0, &s1, &c1);
+        v[j] = cmul(v[j], make_float2(c0, s0));
+        v[j + 1] = cmul(v[j + 1], make_float2(c1, s1));
+      }
     }
   }
   if constexpr ((FLAGS & A_MULT_TC) != 0) {

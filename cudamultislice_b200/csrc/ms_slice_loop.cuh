@@ -26,6 +26,36 @@
 
 namespace ms {
 
+// v *= exp(i sigma V) over a thread's E points: the polynomial-only sincos
+// when every phase of the warp is within a quarter turn of 0 (bit-identical,
+// the usual case for slices of a few angstroms), else the reduced one.
+template <int E>
+MS_D void transmit_line(float2 (&v)[E], float (&vv)[E], float sigma) {
+  bool small = true;
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    vv[j] = fmul_x(sigma, vv[j]);
+    small = small && sincos_small_ok(vv[j]);
+  }
+  if (__all_sync(0xffffffffu, small)) {
+#pragma unroll
+    for (int j = 0; j < E; j += 2) {
+      float s0, c0, s1, c1;
+      sincos_small2(vv[j], vv[j + 1], &s0, &c0, &s1, &c1);
+      v[j] = cmul(v[j], make_float2(c0, s0));
+      v[j + 1] = cmul(v[j + 1], make_float2(c1, s1));
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < E; j += 2) {
+      float s0, c0, s1, c1;
+      sincos_red2(vv[j], vv[j + 1], &s0, &c0, &s1, &c1);
+      v[j] = cmul(v[j], make_float2(c0, s0));
+      v[j + 1] = cmul(v[j + 1], make_float2(c1, s1));
+    }
+  }
+}
+
 MS_D unsigned long long global_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -106,13 +136,7 @@ MS_D void loop_row(const PassAArgs& a, const float2* in, float2* out, const floa
     fft::line_fft<PL>(v, sm, t, a.tw);
     fft::conj_all(v);
   }
-#pragma unroll
-  for (int j = 0; j < E; j += 2) {
-    float s0, c0, s1, c1;
-    sincos_red2(fmul_x(a.sigma, vv[j]), fmul_x(a.sigma, vv[j + 1]), &s0, &c0, &s1, &c1);
-    v[j] = cmul(v[j], make_float2(c0, s0));
-    v[j + 1] = cmul(v[j + 1], make_float2(c1, s1));
-  }
+  transmit_line<E>(v, vv, a.sigma);
   fft::line_fft<PL>(v, sm, t, a.tw);
 #pragma unroll
   for (int j = 0; j < E; ++j) out[row0 + t + P * j] = v[j];
@@ -228,13 +252,7 @@ MS_D void batch_row(const LoopGroup& G, int s, int inst, int line, int t, float2
       fft::line_fft<PL>(v, sm, t, G.a.tw);
       fft::conj_all(v);
     }
-#pragma unroll
-    for (int j = 0; j < E; j += 2) {
-      float s0, c0, s1, c1;
-      sincos_red2(fmul_x(G.a.sigma, vv[j]), fmul_x(G.a.sigma, vv[j + 1]), &s0, &c0, &s1, &c1);
-      v[j] = cmul(v[j], make_float2(c0, s0));
-      v[j + 1] = cmul(v[j + 1], make_float2(c1, s1));
-    }
+    transmit_line<E>(v, vv, G.a.sigma);
   } else {
     float2 tc[E];
 #pragma unroll

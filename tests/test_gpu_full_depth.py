@@ -112,6 +112,7 @@ def test_c2_amorphous_carbon_1024_all_slices(engine_cls, c2_oracle, path):
     setup(eng, atoms, 1024, 50.0 / 1024, **C2)
     assert eng.RunConventional() == S_
     e = rel_l2(eng.ExitWave(), psi)
+    print(f"C2 path {path}: exit wave {e:.3e}")
     assert e < TOL, (path, e)
     got = eng.SimulateImageSeries(C2_DEFOCI)
     for k in range(C2_DEFOCI.size):
@@ -153,6 +154,7 @@ def test_c3_silicon_frozen_phonons_512_full_depth(engine_cls, oracle_mod):
     ed, ei = rel_l2(d, orc.TDS()), rel_l2(im, np.mean(imgs, axis=0))
     orc.close()
     ew = rel_l2(w0, psi0)
+    print(f"C3: exit wave {ew:.3e}, diffraction {ed:.3e}, image {ei:.3e}")
     assert ew < TOL, ew
     assert ed < TOL, ed
     assert ei < INT_TOL, ei
@@ -198,6 +200,7 @@ def test_c4_gan_haadf_raster_1024_full_depth(engine_cls, oracle_mod):
     eng.STEMInitialiseWavefunctions(int(px[5]), int(py[5]))
     eng.RunConventional()
     e = rel_l2(eng.ExitWave(), psi5)
+    print(f"C4: HAADF error / beam {err.max() / beam:.3e}, probe exit wave {e:.3e}")
     assert e < PROBE_TOL, e
     eng.close()
     orc.close()
@@ -232,6 +235,8 @@ def test_c5_focal_series_gradient_512_full_depth(engine_cls, oracle_mod):
     psi = orc.run_conventional()  # every slice, as RunConventional
     orc.close()
     ew = rel_l2(w, psi)
+    eV, exy = rel_l2(gV, gV0), rel_l2(gxy, gxy0)
+    print(f"C5: exit wave {ew:.3e}, loss {abs(L - L0) / L0:.3e}, dL/dV {eV:.3e}, dL/dxy {exy:.3e}")
     assert ew < TOL, ew
     for k in range(df.size):
         ei = rel_l2(imgs[k], imgs0[k])
