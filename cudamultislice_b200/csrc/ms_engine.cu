@@ -1426,7 +1426,14 @@ class Engine {
     ++launches;
     return MS_OK;
   }
+  int raster_tuning(int* batch, int* persistent) {
+    if (!batch || !persistent) return fail(MS_ERR_INVALID, "null output");
+    *batch = rs_B_;
+    *persistent = rs_loop_ ? 1 : 0;
+    return MS_OK;
+  }
   int raster_slices() const { return rs_S_; }
+  bool raster_prefers_loop() const { return rs_prefer_loop_; }
   int raster_batch() const { return rs_B_; }
   int raster_count() const { return rs_n_; }
   int grid_n() const { return nx_; }
@@ -3020,6 +3027,9 @@ ms_status ms_build_potential_stack(ms_sim* s, int* nslices) {
 ms_status ms_run_conventional(ms_sim* s, int* nslices) {
   return guarded(s, [&](ms::Engine& e) { return e.run_conventional(nslices); });
 }
+ms_status ms_get_raster_tuning(ms_sim* s, int* batch, int* persistent) {
+  return guarded(s, [&](ms::Engine& e) { return e.raster_tuning(batch, persistent); });
+}
 ms_status ms_get_slice_loop(ms_sim* s, int* variant, int* columns, int* grid) {
   return guarded(s, [&](ms::Engine& e) { return e.slice_loop_info(variant, columns, grid); });
 }
@@ -3133,6 +3143,7 @@ ms_status ms_stem_raster_concurrent(ms_sim* const* sims, int nsims, const int* c
     // every slice in ONE cooperative launch (group 0 the larger grid), on the
     // first handle's stream.
     if (nsims == 2 && sims[0]->e->use_batch_loop() && sims[1]->e->use_batch_loop() &&
+        sims[0]->e->raster_prefers_loop() && sims[1]->e->raster_prefers_loop() &&
         sims[0]->e->raster_slices() == sims[1]->e->raster_slices()) {
       const int big = sims[0]->e->grid_n() >= sims[1]->e->grid_n() ? 0 : 1;
       ms::Engine& ea = *sims[big]->e;

@@ -9,13 +9,14 @@ namespace {
 template <int N, int V>
 using LoopPL = typename PlanSel<N, LoopPlan<N, (LoopVariant<V>::NT > 256)>::V>::T;
 
+
 template <int N, int V>
 cudaError_t loop_prepare(int* grid) {
   using PL = LoopPL<N, V>;
   using LV = LoopVariant<V>;
   using SH = LoopShape<PL, LV::CW, LV::NT>;
   static_assert(PL::P * LV::NT == 32 * 256 || PL::P * LV::NT == 64 * 512, "plan and CTA size must match");
-  auto kernel = k_slice_loop<PL, LV::CW, LV::TIGHT, LV::NT>;
+  auto kernel = k_slice_loop<PL, LV::CW, LV::TIGHT, LV::NT, LV::FENCED>;
   static unsigned long long done = 0;
   if (cudaError_t e = set_smem_once(done, kernel, SH::SMEM)) return e;
   int dev = 0, sms = 0, per_sm = 0;
@@ -42,7 +43,7 @@ cudaError_t loop_launch(const LoopArgs& L, int grid, cudaStream_t s) {
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_slice_loop<PL, LV::CW, LV::TIGHT, LV::NT>, L);
+  return cudaLaunchKernelEx(&cfg, k_slice_loop<PL, LV::CW, LV::TIGHT, LV::NT, LV::FENCED>, L);
 }
 
 template <int V>
@@ -69,7 +70,7 @@ cudaError_t launch_v(const LoopArgs& L, int grid, cudaStream_t s) {
 bool slice_loop_supported(int nx, int ny) { return nx == ny && (nx == 256 || nx == 512 || nx == 1024); }
 
 int slice_loop_plan(int n, int variant) {
-  const bool wide = variant >= 5;
+  const bool wide = variant >= 5 && variant <= 7;
   switch (n) {
     case 256: return wide ? LoopPlan<256, true>::V : LoopPlan<256, false>::V;
     case 512: return wide ? LoopPlan<512, true>::V : LoopPlan<512, false>::V;
@@ -90,6 +91,8 @@ int slice_loop_columns(int variant) {
     case 5: return LoopVariant<5>::CW;
     case 6: return LoopVariant<6>::CW;
     case 7: return LoopVariant<7>::CW;
+    case 8: return LoopVariant<8>::CW;
+    case 9: return LoopVariant<9>::CW;
     default: return 0;
   }
 }
@@ -104,6 +107,8 @@ cudaError_t slice_loop_prepare(int n, int variant, int* grid) {
     case 5: return prepare_v<5>(n, grid);
     case 6: return prepare_v<6>(n, grid);
     case 7: return prepare_v<7>(n, grid);
+    case 8: return prepare_v<8>(n, grid);
+    case 9: return prepare_v<9>(n, grid);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -120,6 +125,8 @@ cudaError_t launch_slice_loop(const LoopArgs& L, int variant, int grid, cudaStre
     case 5: return launch_v<5>(L, grid, s);
     case 6: return launch_v<6>(L, grid, s);
     case 7: return launch_v<7>(L, grid, s);
+    case 8: return launch_v<8>(L, grid, s);
+    case 9: return launch_v<9>(L, grid, s);
     default: return cudaErrorInvalidValue;
   }
 }

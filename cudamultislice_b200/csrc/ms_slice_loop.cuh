@@ -67,13 +67,16 @@ MS_D unsigned long long global_ns() {
 // reported an error.  TIGHT = false: the arrival is an atomic add and the
 // wait polls with a short sleep; TIGHT = true: the arrival is a release
 // reduction (no round trip) and the wait polls back to back, checking the
-// clock and the error word every 32 polls.
-template <bool TIGHT>
+// clock and the error word every 32 polls.  FENCED: full fences around the
+// arrival and after the wait (as cooperative groups' grid sync); without
+// them the release reduction and the acquire load carry the ordering (both
+// are cumulative over what the CTA's bar.sync has ordered before them).
+template <bool TIGHT, bool FENCED = true>
 MS_D bool loop_barrier(const LoopSync& s, unsigned int epoch) {
   __syncthreads();
   int ok = 1;
   if (threadIdx.x == 0) {
-    __threadfence();
+    if constexpr (FENCED || !TIGHT) __threadfence();
     if constexpr (TIGHT)
       asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(s.count) : "memory");
     else
@@ -97,7 +100,7 @@ MS_D bool loop_barrier(const LoopSync& s, unsigned int epoch) {
       }
       if constexpr (!TIGHT) __nanosleep(32);
     }
-    __threadfence();
+    if constexpr (FENCED || !TIGHT) __threadfence();
   }
   return __syncthreads_and(ok) != 0;
 }
@@ -186,7 +189,7 @@ MS_D void prefetch_rows(const float* V, int G) {
   }
 }
 
-template <class PL, int CW, bool TIGHT, int NT>
+template <class PL, int CW, bool TIGHT, int NT, bool FENCED = true>
 __global__ void __launch_bounds__(NT, 1) k_slice_loop(LoopArgs L) {
   using SH = LoopShape<PL, CW, NT>;
   constexpr int N = PL::N, P = PL::P, GS = SH::GS, GROUPS = SH::GROUPS;
@@ -214,7 +217,7 @@ __global__ void __launch_bounds__(NT, 1) k_slice_loop(LoopArgs L) {
       else
         loop_row<PL, true>(L.a, L.wave, L.wave, V, line, lt, sm);
     }
-    if (!loop_barrier<TIGHT>(L.sync, ++epoch)) return;
+    if (!loop_barrier<TIGHT, FENCED>(L.sync, ++epoch)) return;
     // ---- column phase ----
     if (s + 1 < L.S) prefetch_rows<PL>(V + L.vstride, G);
     for (int u = g * G + blockIdx.x; u < L.b.nx / CW; u += GROUPS * G)
@@ -404,16 +407,18 @@ __global__ void __launch_bounds__(256, 1) k_batch_loop(BatchLoopArgs L) {
 // narrow (lines of one warp, 256-thread CTAs) or wide (lines of two warps,
 // 512-thread CTAs: twice the warps per SM, one more exchange pass), the
 // column unit width CW and the barrier form.
-constexpr int kLoopVariants = 8;
+constexpr int kLoopVariants = 10;
 template <int V> struct LoopVariant;
-template <> struct LoopVariant<0> { static constexpr int CW = 4, NT = 256; static constexpr bool TIGHT = false; };
-template <> struct LoopVariant<1> { static constexpr int CW = 8, NT = 256; static constexpr bool TIGHT = false; };
-template <> struct LoopVariant<2> { static constexpr int CW = 4, NT = 256; static constexpr bool TIGHT = true; };
-template <> struct LoopVariant<3> { static constexpr int CW = 8, NT = 256; static constexpr bool TIGHT = true; };
-template <> struct LoopVariant<4> { static constexpr int CW = 2, NT = 256; static constexpr bool TIGHT = true; };
-template <> struct LoopVariant<5> { static constexpr int CW = 4, NT = 512; static constexpr bool TIGHT = true; };
-template <> struct LoopVariant<6> { static constexpr int CW = 2, NT = 512; static constexpr bool TIGHT = true; };
-template <> struct LoopVariant<7> { static constexpr int CW = 8, NT = 512; static constexpr bool TIGHT = true; };
+template <> struct LoopVariant<0> { static constexpr int CW = 4, NT = 256; static constexpr bool TIGHT = false, FENCED = true; };
+template <> struct LoopVariant<1> { static constexpr int CW = 8, NT = 256; static constexpr bool TIGHT = false, FENCED = true; };
+template <> struct LoopVariant<2> { static constexpr int CW = 4, NT = 256; static constexpr bool TIGHT = true, FENCED = true; };
+template <> struct LoopVariant<3> { static constexpr int CW = 8, NT = 256; static constexpr bool TIGHT = true, FENCED = true; };
+template <> struct LoopVariant<4> { static constexpr int CW = 2, NT = 256; static constexpr bool TIGHT = true, FENCED = true; };
+template <> struct LoopVariant<5> { static constexpr int CW = 4, NT = 512; static constexpr bool TIGHT = true, FENCED = true; };
+template <> struct LoopVariant<6> { static constexpr int CW = 2, NT = 512; static constexpr bool TIGHT = true, FENCED = true; };
+template <> struct LoopVariant<7> { static constexpr int CW = 8, NT = 512; static constexpr bool TIGHT = true, FENCED = true; };
+template <> struct LoopVariant<8> { static constexpr int CW = 8, NT = 256; static constexpr bool TIGHT = true, FENCED = false; };
+template <> struct LoopVariant<9> { static constexpr int CW = 4, NT = 256; static constexpr bool TIGHT = true, FENCED = false; };
 
 // FFT plan variant (PlanSel) of the loop per line length: the packed plan with
 // one warp per line (narrow loop variants) or two warps per line (wide).

@@ -116,6 +116,12 @@ class ManagedMultisliceSimulation:
         """Conventional potential kernel tile: -1 tuned (default), 0/1/2 = 32x8, 16x16, 64x4 pixels."""
         self._chk(self._L.ms_set_option(self._h, 9, int(tile)))
 
+    def RasterTuning(self):
+        """(probes per launch, 1 if the slices ran in the batched persistent loop) of the last raster."""
+        b, p = C.c_int(), C.c_int()
+        self._chk(self._L.ms_get_raster_tuning(self._h, C.byref(b), C.byref(p)))
+        return b.value, p.value
+
     def SetLoopWaitUs(self, us: int):
         """Bound on each grid-barrier wait of the persistent loop (microseconds)."""
         self._chk(self._L.ms_set_option(self._h, 6, int(us)))

@@ -83,11 +83,13 @@ enum {
                                arrivals more than the grid has, so the wait bound runs out
                                (0 = off, the default) */
   MS_OPT_LOOP_VARIANT = 8,  /* persistent slice loop kernel variant: -1 = tuned on the
-                               device once per grid (default); 0..7 = force one: 0-4 run
+                               device once per grid (default); 0..9 = force one: 0-4 run
                                lines of one warp in 256-thread CTAs (column units of 4, 8,
                                4, 8, 2 columns; barrier sleep-poll for 0-1, release
                                reduction with tight poll for 2-4); 5-7 lines of two warps
-                               in 512-thread CTAs (units of 4, 2, 8 columns, tight poll) */
+                               in 512-thread CTAs (units of 4, 2, 8 columns, tight poll);
+                               8-9 as 3 and 2 with the ordering carried by the release
+                               reduction and the acquire poll alone (no full fences) */
   MS_OPT_POTENTIAL_TILE = 9 /* conventional potential kernel tile: -1 = tuned on the device
                                per grid (default); 0, 1, 2 = 32 x 8, 16 x 16, 64 x 4 pixels */
 };
@@ -356,6 +358,10 @@ ms_status ms_time_slices(ms_sim* sim, int steps, int reps, float* ms_total, floa
 /* FFT plan variants (row pass, column pass) used for `batch` instances, tuning
  * them first if needed (MS_OPT_FFT_PLAN). */
 ms_status ms_get_fft_plan(ms_sim* sim, int batch, int* row_variant, int* col_variant);
+/* The last raster's probes per launch and whether its slices ran in the
+ * batched persistent loop (1) or per pass (0); with batch <= 0 both are the
+ * device-tuned choice. */
+ms_status ms_get_raster_tuning(ms_sim* sim, int* batch, int* persistent);
 /* The persistent slice loop this grid runs: kernel variant (-1 when the loop
  * does not run here), columns per column unit, CTAs (one per SM); tunes the
  * variant first if needed (MS_OPT_LOOP_VARIANT). */

@@ -19,26 +19,20 @@ workloads:
   C5  SrTiO3 4x4x50 cells, 512^2, 1.9525 A slices, 200 kV, an 8-image focal
       series: loss, dL/dV of every slice and dL/d(atom x, y).
 Tolerances:
-  - waves (exit waves, diffraction amplitudes |FFT(psi)|): relative L2 error
-    <= 1e-5, the north-star bar;
-  - intensities (CTF images |.|^2): <= 2e-5, the same bar carried through the
-    square (a relative amplitude error e gives about 2e in intensity);
-  - the HAADF ring: its error relative to the probe's total intensity
-    <= 1e-6.  The FP32 error of a wave is spread over all of k-space at about
-    1e-6 of its norm; a 70-200 mrad ring that the band limit cuts to its
-    inner edge holds a small fraction of the beam, so the same absolute error
-    is a larger fraction of the ring signal (bounded here by 1e-3);
-  - a STEM probe's exit wave through 80 slices of the GaN crystal: <= 2e-5.
-    This case sits at the FP32 floor itself: the same multislice with an
-    ideal single-precision FFT (scipy's pocketfft in complex64, potentials and
-    propagator exact) is 1.0e-5 from FP64 at 1024^2 (tests/fp32_floor_model.py).
-    A crystal repeats the same slices, so the transform's rounding adds up
-    coherently, and a probe's energy sits where the propagator is not 1;
-    the amorphous plane-wave workload stays near 2e-6;
-  - gradients: relative L2 error <= 1e-4; the focal-series loss <= 1e-4 (it
-    sums squared residuals I - T that are small against I, so its relative
-    error is the images' error magnified by I / (I - T)), the images
-    themselves at the intensity bar."""
+  - waves (exit waves, diffraction amplitudes |FFT(psi)|) and intensities (CTF
+    images): relative L2 error <= 1e-5, the north-star bar.  Measured: C2
+    9.0e-7 (plain cuFFT path 4.0e-6), C3 2.4e-6 / 1.4e-6 / 2.5e-6, C4 probe
+    2.7e-6, C5 1.8e-6.  An ideal single-precision FFT (tests/fp32_floor_model.py)
+    lands at 1.0e-5 on the C4 probe: crystals repeat their slices, so rounding
+    that is the same in every slice adds up coherently.  The engine stays well
+    below it because its rotations cannot change the norm (three-shear
+    twiddles, unit-modulus tables) and its potential values are taken at exact
+    positions;
+  - the HAADF ring: its error relative to the probe's total intensity <= 1e-6
+    (measured 1.7e-11), and relative to the ring signal <= 1e-3 (the ring holds
+    a small fraction of the beam);
+  - gradients: relative L2 error <= 1e-4 (measured 3.3e-6 and 7.6e-6); the loss
+    <= 1e-5."""
 import numpy as np
 import pytest
 
@@ -46,12 +40,10 @@ from tests.conftest import FPARAMS
 
 pytestmark = pytest.mark.gpu
 
-TOL = 1e-5        # waves, diffraction amplitudes
-INT_TOL = 2e-5    # intensities (CTF images)
+TOL = 1e-5        # waves, diffraction amplitudes, images, the loss
 BEAM_TOL = 1e-6   # detector signal error / total probe intensity
 RING_TOL = 1e-3   # detector signal error / ring signal
-GRAD_TOL = 1e-4   # gradients and the focal-series loss
-PROBE_TOL = 2e-5  # probe exit wave through a crystal (twice the FP32 floor of that case)
+GRAD_TOL = 1e-4   # gradients
 
 
 def rel_l2(a, b):
@@ -115,9 +107,12 @@ def test_c2_amorphous_carbon_1024_all_slices(engine_cls, c2_oracle, path):
     print(f"C2 path {path}: exit wave {e:.3e}")
     assert e < TOL, (path, e)
     got = eng.SimulateImageSeries(C2_DEFOCI)
+    # the plain path keeps the reference's arithmetic (cuFFT, plainly rounded
+    # propagator): its wave error (4.0e-6) doubles in the intensity
+    itol = TOL if path == 0 else 2 * TOL
     for k in range(C2_DEFOCI.size):
         ei = rel_l2(got[k], imgs[k])
-        assert ei < INT_TOL, (path, float(C2_DEFOCI[k]), ei)
+        assert ei < itol, (path, float(C2_DEFOCI[k]), ei)
     eng.close()
 
 
@@ -157,7 +152,7 @@ def test_c3_silicon_frozen_phonons_512_full_depth(engine_cls, oracle_mod):
     print(f"C3: exit wave {ew:.3e}, diffraction {ed:.3e}, image {ei:.3e}")
     assert ew < TOL, ew
     assert ed < TOL, ed
-    assert ei < INT_TOL, ei
+    assert ei < TOL, ei
 
 
 # ---------------------------------------------------------------- C4
@@ -201,7 +196,7 @@ def test_c4_gan_haadf_raster_1024_full_depth(engine_cls, oracle_mod):
     eng.RunConventional()
     e = rel_l2(eng.ExitWave(), psi5)
     print(f"C4: HAADF error / beam {err.max() / beam:.3e}, probe exit wave {e:.3e}")
-    assert e < PROBE_TOL, e
+    assert e < TOL, e
     eng.close()
     orc.close()
 
@@ -240,9 +235,9 @@ def test_c5_focal_series_gradient_512_full_depth(engine_cls, oracle_mod):
     assert ew < TOL, ew
     for k in range(df.size):
         ei = rel_l2(imgs[k], imgs0[k])
-        assert ei < INT_TOL, (k, ei)
-    assert abs(Lf - L0) / L0 < GRAD_TOL, (Lf, L0)
-    assert abs(L - L0) / L0 < GRAD_TOL, (L, L0)
+        assert ei < TOL, (k, ei)
+    assert abs(Lf - L0) / L0 < TOL, (Lf, L0)
+    assert abs(L - L0) / L0 < TOL, (L, L0)
     eV, exy = rel_l2(gV, gV0), rel_l2(gxy, gxy0)
     assert eV < GRAD_TOL, eV
     assert exy < GRAD_TOL, exy
