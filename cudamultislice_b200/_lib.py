@@ -69,6 +69,7 @@ SIGNATURES = {
     "ms_run_conventional": (_i, [_p, _pi]),
     "ms_run_fd": (_i, [_p, _i, _pi]),
     "ms_get_slice_loop": (_i, [_p, _pi, _pi, _pi]),
+    "ms_get_potential_sum": (_i, [_p, _pi, _pi]),
     "ms_get_raster_tuning": (_i, [_p, _pi, _pi]),
     "ms_annular_detector": (_i, [_p, _f, _f, _pd]),
     "ms_stem_raster": (_i, [_p, _p, _p, _i, _f, _f, _i, _p]),

@@ -643,6 +643,234 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
   if (inside) a.V[(long long)y * a.nx + x] = acc;
 }
 
+// ---------------------------------------------------------------------------
+// Separable conventional potential.  Each Gaussian of an element's expansion
+// v(r) ~= sum_j w_j exp(-alpha_j r^2) factorises over r^2 = rho^2 + dz_m^2, so
+// an atom's sub-plane sum at a pixel is
+//   sum_{m valid} wsub v(rho^2 + dz_m^2) ~= sum_j exp(-alpha_j rho^2) T_K[j],
+//   T_K[j] = wsub sum_{k < K} w_j exp(-alpha_j dz_(k)^2),
+// where the valid sub-planes (r^2 < 5 in the reference's FP32 rounding) are the
+// K with the smallest dz^2: for a fixed pixel the decision is monotone in dz^2.
+// k_atom_tables forms the T rows once per atom and slice; the pixel kernel
+// finds K with a five-step search over the atom's ascending thresholds (the
+// reference's own FP32 test, sub-plane by sub-plane) and takes kGaussJ
+// exponentials per (pixel, atom) instead of four per (pixel, atom, sub-plane).
+// Inside the 0.25 A clamp, where v is constant and the expansion does not
+// hold, the pixel sums vatom over its K sub-planes directly.
+// ---------------------------------------------------------------------------
+constexpr int kTabAtoms = 16;  // atoms per CTA of the table kernel, 16 threads each
+
+__global__ void __launch_bounds__(256) k_atom_tables(PotArgs a) {
+  __shared__ float s_d2[kTabAtoms][20];
+  __shared__ float s_qv[kTabAtoms][20];
+  if (a.kt > a.kb || a.kt < 0 || a.kb >= a.nz) return;  // (no z-bin in the window)
+  const int a0 = a.off[a.kt * kBins2], na = a.off[(a.kb + 1) * kBins2] - a0;
+  const int la = threadIdx.x >> 4, j = threadIdx.x & 15;
+  for (int base = blockIdx.x * kTabAtoms; base < na; base += gridDim.x * kTabAtoms) {
+    const bool valid = base + la < na;
+    float* tab = a.tab + (size_t)(base + la) * kTabStride;
+    float4 at = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (valid) {
+      at = a.atoms[a0 + base + la];
+      // dz_m^2 as the cut-off rounds it (16 lanes, two planes for the first 4)
+      for (int m = j; m < 20; m += 16) {
+        const float dz = fsub_x(a.zsub[m], at.z);
+        s_d2[la][m] = fmul_x(dz, dz);
+      }
+    }
+    __syncthreads();
+    int n = 0;
+    if (valid && j == 0) {
+      // sub-planes in ascending dz^2: dz is monotone in the plane height, so
+      // dz^2 rises on both sides of its minimum; merge the two sides
+      int m0 = 0;
+      for (int m = 1; m < 20; ++m)
+        if (s_d2[la][m] < s_d2[la][m0]) m0 = m;
+      int lo = m0 - 1, hi = m0 + 1, m = m0;
+      while (n < 20 && s_d2[la][m] < 5.0f) {
+        tab[kTabQ + n] = s_d2[la][m];
+        const float dzv = fsub_x(a.zsub[m], at.z) + a.zsub_lo[m];
+        const float qv = dzv * dzv;
+        tab[kTabQV + n] = qv;
+        s_qv[la][n] = qv;
+        ++n;
+        const float dl = lo >= 0 ? s_d2[la][lo] : 1e30f, dh = hi < 20 ? s_d2[la][hi] : 1e30f;
+        if (dl <= dh) m = lo--; else m = hi++;
+        if (m < 0 || m >= 20) break;
+      }
+      for (int k = n; k < 32; ++k) tab[kTabQ + k] = 1e30f;
+      s_d2[la][0] = __int_as_float(n);  // (the count, for the T rows below)
+    }
+    __syncthreads();
+    if (valid && j < kGaussJ) {
+      const int nk = __float_as_int(s_d2[la][0]);
+      const float* g = a.gauss + (__float_as_int(at.w) - 1) * 2 * kGaussJ;
+      const float al = g[j], w = g[kGaussJ + j];
+      double s = 0.0;
+      for (int k = 0; k < nk; ++k) {
+        s += (double)w * (double)exp2f(-al * s_qv[la][k]);
+        tab[kTabT + k * kGaussJ + j] = (float)((double)a.wsub * s);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <int TX, int TY>
+__global__ void __launch_bounds__(kPotThreads) k_potential_sep(PotArgs a) {
+  static_assert(TX * TY == kPotThreads && TX % 8 == 0 && TY % 4 == 0, "tile of 8 x 4 warp patches");
+  __shared__ float4 s_at[kConvChunk];
+  __shared__ __align__(16) float s_q[kConvChunk][32];
+  __shared__ __align__(16) float s_al[kConvChunk][kGaussJ];
+  __shared__ int s_l[kConvChunk];
+  __shared__ int s_wcnt[kPotThreads / 32];
+  __shared__ int s_start[kMaxSeg];
+  __shared__ int s_pref[kMaxSeg + 1];
+  __shared__ int s_warp[33];
+
+  int tx, ty;
+  tile_pixel_t<TX, TY>(threadIdx.x, tx, ty);
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int x = x0 + tx, y = y0 + ty;
+  const bool inside = (x < a.nx) && (y < a.ny);
+  const float px = fadd_x(a.xoff, fmul_x((float)x, a.ps));
+  const float py = fadd_x(a.yoff, fmul_x((float)y, a.ps));
+  // values at the exact positions, decisions at the reference's FP32 ones (as
+  // in k_potential_conv)
+  const float px_lo = (float)(((double)a.xoff + (double)x * (double)a.ps) - (double)px);
+  const float py_lo = (float)(((double)a.yoff + (double)y * (double)a.ps) - (double)py);
+  const float tx_lo = fadd_x(a.xoff, fmul_x((float)x0, a.ps));
+  const float tx_hi = fadd_x(a.xoff, fmul_x((float)(x0 + TX - 1), a.ps));
+  const float ty_lo = fadd_x(a.yoff, fmul_x((float)y0, a.ps));
+  const float ty_hi = fadd_x(a.yoff, fmul_x((float)(y0 + TY - 1), a.ps));
+  const float xlo = a.xoff + x0 * a.ps - 2.2361f, xhi = a.xoff + (x0 + TX - 1) * a.ps + 2.2361f;
+  const float ylo = a.yoff + y0 * a.ps - 2.2361f, yhi = a.yoff + (y0 + TY - 1) * a.ps + 2.2361f;
+  const int bxl = max((int)floorf(xlo / a.bw_x) - 1, 0);
+  const int bxh = min((int)floorf(xhi / a.bw_x) + 1, kBins - 1);
+  const int byl = max((int)floorf(ylo / a.bw_y) - 1, 0);
+  const int byh = min((int)floorf(yhi / a.bw_y) + 1, kBins - 1);
+  const int nyb = byh - byl + 1;
+  const bool window = a.kt <= a.kb && a.kt >= 0 && a.kb < a.nz;
+  const int a0 = window ? a.off[a.kt * kBins2] : 0;
+
+  float acc = 0.0f;
+  if (bxl <= bxh && byl <= byh && window) {
+    const int kstep = max(kMaxSeg / nyb, 1);
+    for (int kg = a.kt; kg <= a.kb; kg += kstep) {
+      const int kend = min(kg + kstep - 1, a.kb);
+      const int nseg = (kend - kg + 1) * nyb;
+      int len0 = 0, len1 = 0, st0 = 0, st1 = 0;
+      const int s0 = threadIdx.x, s1 = threadIdx.x + kPotThreads;
+      if (s0 < nseg) {
+        const int b = (kg + s0 / nyb) * kBins2 + (byl + s0 % nyb) * kBins;
+        st0 = a.off[b + bxl];
+        len0 = a.off[b + bxh + 1] - st0;
+      }
+      if (s1 < nseg) {
+        const int b = (kg + s1 / nyb) * kBins2 + (byl + s1 % nyb) * kBins;
+        st1 = a.off[b + bxl];
+        len1 = a.off[b + bxh + 1] - st1;
+      }
+      int total;
+      const int ex = block_exclusive_scan(len0 + len1, s_warp, &total);
+      if (s0 < nseg) { s_start[s0] = st0; s_pref[s0] = ex; }
+      if (s1 < nseg) { s_start[s1] = st1; s_pref[s1] = ex + len0; }
+      if (threadIdx.x == 0) s_pref[nseg] = total;
+      __syncthreads();
+
+      for (int base = 0; base < total; base += kConvChunk) {
+        const int nload = min(kConvChunk, total - base);
+        // candidates kept when the nearest sub-plane can pass the cut-off
+        // within sqrt(5) A of the tile's pixel rectangle (margin far above
+        // FP32 rounding); kept atoms stay in CSR order
+        bool keep = false;
+        float4 at = make_float4(0.f, 0.f, 0.f, 0.f);
+        int li = 0;
+        if (threadIdx.x < nload) {
+          const int gidx = base + threadIdx.x;
+          int lo = 0, hi = nseg - 1;
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (s_pref[mid] <= gidx) lo = mid; else hi = mid - 1;
+          }
+          const int l = s_start[lo] + (gidx - s_pref[lo]);
+          at = a.atoms[l];
+          li = l - a0;
+          const float q0 = a.tab[(size_t)li * kTabStride + kTabQ];
+          const float ddx = fmaxf(0.0f, fmaxf(tx_lo - at.x, at.x - tx_hi));
+          const float ddy = fmaxf(0.0f, fmaxf(ty_lo - at.y, at.y - ty_hi));
+          keep = q0 < 5.0f && ddx * ddx + ddy * ddy + q0 < 5.0005f;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        if ((threadIdx.x & 31) == 0) s_wcnt[threadIdx.x >> 5] = __popc(bal);
+        __syncthreads();
+        int pos = 0, cnt = 0;
+        for (int w = 0; w < kConvChunk / 32; ++w) {
+          if (w < (int)(threadIdx.x >> 5)) pos += s_wcnt[w];
+          cnt += s_wcnt[w];
+        }
+        if (keep) {
+          pos += __popc(bal & ((1u << (threadIdx.x & 31)) - 1u));
+          s_at[pos] = at;
+          s_l[pos] = li;
+        }
+        __syncthreads();
+        for (int q = threadIdx.x; q < cnt * 32; q += kPotThreads)
+          s_q[q >> 5][q & 31] = a.tab[(size_t)s_l[q >> 5] * kTabStride + kTabQ + (q & 31)];
+        for (int q = threadIdx.x; q < cnt * kGaussJ; q += kPotThreads) {
+          const int i = q / kGaussJ, jj = q - i * kGaussJ;
+          s_al[i][jj] = a.gauss[(__float_as_int(s_at[i].w) - 1) * 2 * kGaussJ + jj];
+        }
+        __syncthreads();
+        for (int i = 0; i < cnt; ++i) {
+          const float4 at = s_at[i];
+          const float dx = fsub_x(px, at.x), dy = fsub_x(py, at.y);
+          const float dxy = fadd_x(fmul_x(dx, dx), fmul_x(dy, dy));
+          const float q0 = s_q[i][0];
+          // no lane takes a term from this atom: dxy >= 0, so its bits order
+          // as the values do
+          const float wmin = __int_as_float(__reduce_min_sync(0xffffffffu, __float_as_int(dxy)));
+          if (!(fadd_x(wmin, q0) < 5.0f)) continue;
+          // K = the sub-planes with r^2 = dxy + dz^2 < 5 (the reference's test)
+          int K = 0;
+#pragma unroll
+          for (int st = 16; st >= 1; st >>= 1)
+            if (fadd_x(dxy, s_q[i][K + st - 1]) < 5.0f) K += st;
+          if (K == 0) continue;
+          const float dxv = dx + px_lo, dyv = dy + py_lo;
+          const float dxyv = fmaf(dxv, dxv, dyv * dyv);
+          const float* tab = a.tab + (size_t)s_l[i] * kTabStride;
+          if (fadd_x(dxy, q0) < 0.0627f) {
+            // a sub-plane reaches the 0.25 A clamp (decided on the exact r^2
+            // inside vatom_f): the direct sum
+            const float* c = a.coef + (__float_as_int(at.w) - 1) * kCoefPerZ;
+            float v = 0.0f;
+            for (int k = 0; k < K; ++k) v += vatom_f(c, dxyv + __ldg(tab + kTabQV + k));
+            acc += a.wsub * v;
+          } else {
+            const float4* T = reinterpret_cast<const float4*>(tab + kTabT + (K - 1) * kGaussJ);
+            const float4* A = reinterpret_cast<const float4*>(&s_al[i][0]);
+            const f2p nr = pk2(-dxyv, -dxyv);
+            f2p s2 = pk2(0.0f, 0.0f);
+#pragma unroll
+            for (int g = 0; g < kGaussJ / 4; ++g) {
+              const float4 al = A[g];
+              const float4 t = __ldg(T + g);
+              s2 = fma2(ex2_pair(mul2(pk2(al.x, al.y), nr)), pk2(t.x, t.y), s2);
+              s2 = fma2(ex2_pair(mul2(pk2(al.z, al.w), nr)), pk2(t.z, t.w), s2);
+            }
+            float e0, e1;
+            up2(s2, e0, e1);
+            acc += e0 + e1;
+          }
+        }
+        __syncthreads();
+      }
+    }
+  }
+  if (inside) a.V[(long long)y * a.nx + x] = acc;
+}
+
 // Adjoint of k_potential_conv with respect to the atoms' x and y.  For slice
 // potential V(p) = sum_atoms sum_m wsub v(r^2), r^2 = (p - X)^2 + dz_m^2, and
 // the slice's dL/dV field G:
@@ -775,8 +1003,20 @@ cudaError_t build_atom_index(const int* dZ, const float* dx, const float* dy, co
 
 int potential_tiles() { return 3; }
 
-cudaError_t launch_potential(const PotArgs& a, int kind, cudaStream_t s, int tile) {
+cudaError_t launch_potential(const PotArgs& a, int kind, cudaStream_t s, int tile, bool separable) {
   dim3 grid((a.nx + kTX - 1) / kTX, (a.ny + kTY - 1) / kTY);
+  if (kind == POT_CONVENTIONAL && separable) {
+    if (!a.tab || !a.gauss) return cudaErrorInvalidValue;
+    // the window's atoms (read on the device) in 16-atom rounds
+    k_atom_tables<<<148 * 8, 256, 0, s>>>(a);
+    switch (tile) {
+      case 0: k_potential_sep<32, 8><<<grid, kPotThreads, 0, s>>>(a); break;
+      case 1: k_potential_sep<16, 16><<<dim3((a.nx + 15) / 16, (a.ny + 15) / 16), kPotThreads, 0, s>>>(a); break;
+      case 2: k_potential_sep<64, 4><<<dim3((a.nx + 63) / 64, (a.ny + 3) / 4), kPotThreads, 0, s>>>(a); break;
+      default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+  }
   if (kind == POT_CONVENTIONAL) {
     switch (tile) {
       case 0: k_potential_conv<32, 8><<<grid, kPotThreads, 0, s>>>(a); break;

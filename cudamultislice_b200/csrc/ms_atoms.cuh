@@ -55,11 +55,28 @@ struct PotArgs {
   float top, slab_dz;
   int slab;
   long long batch_stride_V;
+  // separable conventional kernel: per-atom tables of the slice (written by
+  // the table kernel, kTabStride floats per atom of the z-window, in CSR
+  // order) and the Gaussian expansions [103][2][kGaussJ] (alpha_j log2(e),
+  // then w_j)
+  float* tab;
+  const float* gauss;
 };
+
+// Gaussian expansion of vatom per element: v(r) ~= sum_j w_j exp(-alpha_j r^2)
+// for 0.25 A <= r <= 2.2365 A (positive weights).
+constexpr int kGaussJ = 12;
+// Per-atom table of one slice (floats): the reference-rounded dz_m^2 of the
+// sub-planes that can pass the cut-off, ascending, padded with 1e30 to 32
+// (the cut-off thresholds); the exact-height dz_m^2 in the same order; then
+// row k = 0..19: wsub sum_{k' <= k} w_j exp(-alpha_j dzv_k'^2), j < kGaussJ.
+constexpr int kTabQ = 0, kTabQV = 32, kTabT = 56, kTabStride = 304;
 
 // tile: the conventional kernel's tile shape variant (0: 32 x 8, 1: 16 x 16,
 // 2: 64 x 4 pixels; other kinds take 32 x 8).
-cudaError_t launch_potential(const PotArgs& a, int kind, cudaStream_t s, int tile = 0);
+// separable: conventional kind only, through the per-atom tables (a.tab,
+// a.gauss set) instead of the per-sub-plane sum.
+cudaError_t launch_potential(const PotArgs& a, int kind, cudaStream_t s, int tile = 0, bool separable = false);
 int potential_tiles();
 
 // Adjoint of the conventional potential of one slice with respect to atom x, y:

@@ -44,6 +44,11 @@
 
 namespace ms {
 
+// Gaussian expansions of vatom per element for the separable potential kernel
+// (kGaussFit[Z-1] = {J, alpha_j..., w_j...}), fitted offline to the stock
+// fparams.dat and re-checked against the loaded table before use.
+#include "ms_gauss_fit.inc"
+
 // ---------------------------------------------------------------------------
 // small utilities
 // ---------------------------------------------------------------------------
@@ -181,6 +186,15 @@ class Engine {
       case MS_OPT_POTENTIAL_TILE:
         if (value < -1 || value >= potential_tiles()) return fail(MS_ERR_INVALID, "tile must be -1 (tuned) or 0..2");
         pot_tile_ = value;
+        pot_tile_forced_ = value >= 0;
+        stack_valid_ = false;
+        fd_stack_valid_ = false;
+        invalidate_graph();
+        return MS_OK;
+      case MS_OPT_POTENTIAL_SUM:
+        if (value < 0 || value > 2) return fail(MS_ERR_INVALID, "potential sum must be 0 (auto), 1 or 2");
+        pot_sum_ = value;
+        if (!pot_tile_forced_) pot_tile_ = -1;  // (the tile is tuned per kernel)
         stack_valid_ = false;
         fd_stack_valid_ = false;
         invalidate_graph();
@@ -245,6 +259,8 @@ class Engine {
         return fail(MS_ERR_INVALID, "non-finite atom position");
     }
     hZ_.assign(Z, Z + n);
+    zpresent_.assign(104, 0);
+    for (int i = 0; i < n; ++i) zpresent_[Z[i]] = 1;
     hx_.assign(x, x + n);
     hy_.assign(y, y + n);
     hz_.assign(z, z + n);
@@ -292,6 +308,7 @@ class Engine {
     MS_TRY(d_yin_.resize(n));
     MS_TRY(d_zin_.resize(n));
     MS_TRY(d_atoms_.resize(n));
+    MS_TRY(d_tab_.resize((size_t)n * kTabStride));
     MS_TRY(d_off_.resize(nbins + 1));
     MS_TRY(d_key_.resize(n));
     MS_TRY(d_idx_.resize(n));
@@ -356,6 +373,20 @@ class Engine {
     }
     MS_TRY(d_coef_.resize(coef.size()));
     MS_TRY(copy_sync(d_coef_.p, coef.data(), sizeof(float) * coef.size(), cudaMemcpyHostToDevice));
+    // the Gaussian expansions, in the kernel's FP32 form (alpha_j log2(e), w_j)
+    std::vector<float> gauss(103 * 2 * kGaussJ, 0.0f);
+    for (int r = 0; r < 103; ++r) {
+      if ((int)kGaussFit[r][0] != kGaussJ) continue;
+      for (int j = 0; j < kGaussJ; ++j) {
+        gauss[(r * 2) * kGaussJ + j] = (float)(kGaussFit[r][1 + j] * log2e);
+        gauss[(r * 2 + 1) * kGaussJ + j] = (float)kGaussFit[r][1 + kGaussJ + j];
+      }
+    }
+    MS_TRY(d_gauss_.resize(gauss.size()));
+    MS_TRY(copy_sync(d_gauss_.p, gauss.data(), sizeof(float) * gauss.size(), cudaMemcpyHostToDevice));
+    hfp_ = fp;
+    hgauss_ = gauss;
+    gauss_row_ok_.assign(103, -1);
     have_fp_ = true;
     stack_valid_ = false;
     fd_stack_valid_ = false;
@@ -460,7 +491,7 @@ class Engine {
     tuned_.clear();
     raster_batch_.clear();
     loop_grid_ = 0;
-    pot_tile_ = -1;
+    if (!pot_tile_forced_) pot_tile_ = -1;
     if (fused_ok_) {
       std::vector<float2> tw(2 * (size_t)std::max(nx, ny));
       for (int v = 0; v < plan_variants(); ++v) {
@@ -1657,10 +1688,16 @@ class Engine {
     if (!stack_valid_ || nstack_ != S) {
       const size_t N = (size_t)nx_ * ny_;
       MS_TRY(d_stack_.resize(N * S));
+      const int kind = pot_mode_ == 1 ? POT_PROJECTED : POT_CONVENTIONAL;
+      if (kind == POT_CONVENTIONAL && pot_tile_ < 0 && !capturing_)
+        if (int rc = tune_pot_tile()) return rc;
+      // device time of the stack (ms_get_last_device_ms)
+      MS_TRY(cudaEventRecord(ev0_, stream_));
       for (int it = 1; it <= S; ++it)
-        if (int rc = potential_slice(pot_mode_ == 1 ? POT_PROJECTED : POT_CONVENTIONAL, it, d_stack_.p + (it - 1) * N))
-          return rc;
+        if (int rc = potential_slice(kind, it, d_stack_.p + (it - 1) * N)) return rc;
+      MS_TRY(cudaEventRecord(ev1_, stream_));
       MS_TRY(cudaStreamSynchronize(stream_));
+      MS_TRY(cudaEventElapsedTime(&last_device_ms_, ev0_, ev1_));
       nstack_ = S;
       stack_valid_ = true;
       tstack_valid_ = false;
@@ -1788,6 +1825,12 @@ class Engine {
     domain_ = 0;  // tuning left scratch in the wave; every run starts from psi0
     return MS_OK;
   }
+  int potential_sum_info(int* last, int* next) {
+    if (last) *last = last_pot_sum_;
+    if (next) *next = separable_ok() ? 2 : 1;
+    return MS_OK;
+  }
+
   int slice_loop_info(int* variant, int* columns, int* grid) {
     if (!variant || !columns || !grid) return fail(MS_ERR_INVALID, "null output");
     if (!use_loop()) {
@@ -2521,13 +2564,52 @@ class Engine {
     return MS_OK;
   }
 
+  // Whether element row r's Gaussian expansion holds for the loaded table:
+  // checked once per row in FP64, with the kernel's FP32-rounded exponents and
+  // weights, against vatom (U.cu:160-193) on 0.25 <= r <= 2.2365 A.
+  bool gauss_row_ok(int r) {
+    if (r < 0 || r >= 103 || r >= nrows_fp_) return false;
+    if (gauss_row_ok_[r] >= 0) return gauss_row_ok_[r] == 1;
+    bool ok = (int)kGaussFit[r][0] == kGaussJ;
+    const double pi = 3.141592654;
+    const double* f = &hfp_[r * 12];
+    const float* al = &hgauss_[(r * 2) * kGaussJ];
+    const float* w = &hgauss_[(r * 2 + 1) * kGaussJ];
+    for (int i = 0; ok && i < 1000; ++i) {
+      const double rad = 0.25 * std::pow(2.2365 / 0.25, i / 999.0), r2 = rad * rad;
+      double L = 0.0, G = 0.0;
+      for (int k = 0; k < 3; ++k) {
+        L += f[2 * k] * std::exp(-2.0 * pi * rad * std::sqrt(f[2 * k + 1]));
+        G += f[6 + 2 * k] * std::exp(-(pi * rad) * (pi * rad) / f[7 + 2 * k]) * std::pow(f[7 + 2 * k], -1.5);
+      }
+      const double v = 150.4121417 * L / rad + 266.5157269 * G;
+      double e = 0.0;
+      for (int j = 0; j < kGaussJ; ++j) e += (double)w[j] * std::exp2(-(double)al[j] * r2);
+      ok = v > 0.0 && std::fabs(e - v) <= kGaussTol * v;
+    }
+    gauss_row_ok_[r] = ok ? 1 : 0;
+    return ok;
+  }
+  // The separable conventional kernel applies when every element of the
+  // specimen has a valid expansion (MS_OPT_POTENTIAL_SUM 0 or 2).
+  bool separable_ok() {
+    if (pot_sum_ == 1 || !have_fp_) return false;
+    for (int z = 1; z <= 103; ++z)
+      if (z < (int)zpresent_.size() && zpresent_[z] && !gauss_row_ok(z - 1)) return false;
+    return true;
+  }
+
   // Potential of one slice into out (ny x nx floats).
   int potential_slice(int kind, int it, float* out) {
+    const bool sep = kind == POT_CONVENTIONAL && separable_ok();
+    if (kind == POT_CONVENTIONAL && pot_sum_ == 2 && !sep)
+      return fail(MS_ERR_UNSUPPORTED, "an element of the specimen has no valid Gaussian expansion");
     if (kind == POT_CONVENTIONAL && pot_tile_ < 0 && !capturing_)
       if (int rc = tune_pot_tile()) return rc;
     const PotArgs a = pot_args(kind, it, out);
-    MS_TRY(launch_potential(a, kind, stream_, kind == POT_CONVENTIONAL ? std::max(pot_tile_, 0) : 0));
-    ++launches;
+    MS_TRY(launch_potential(a, kind, stream_, kind == POT_CONVENTIONAL ? std::max(pot_tile_, 0) : 0, sep));
+    launches += sep ? 2 : 1;
+    last_pot_sum_ = kind == POT_CONVENTIONAL ? (sep ? 2 : 1) : last_pot_sum_;
     return MS_OK;
   }
 
@@ -2542,16 +2624,17 @@ class Engine {
     MS_TRY(d_V_.resize(N));
     float best_t = INFINITY;
     int best = 0;
+    const bool sep = separable_ok();
     for (int t = 0; t < potential_tiles(); ++t) {
       const PotArgs a = pot_args(POT_CONVENTIONAL, it, d_V_.p);
-      MS_TRY(launch_potential(a, POT_CONVENTIONAL, stream_, t));
+      MS_TRY(launch_potential(a, POT_CONVENTIONAL, stream_, t, sep));
       MS_TRY(cudaEventRecord(ev0_, stream_));
-      for (int k = 0; k < 3; ++k) MS_TRY(launch_potential(a, POT_CONVENTIONAL, stream_, t));
+      for (int k = 0; k < 3; ++k) MS_TRY(launch_potential(a, POT_CONVENTIONAL, stream_, t, sep));
       MS_TRY(cudaEventRecord(ev1_, stream_));
       MS_TRY(cudaEventSynchronize(ev1_));
       float ms = 0.0f;
       MS_TRY(cudaEventElapsedTime(&ms, ev0_, ev1_));
-      launches += 4;
+      launches += sep ? 8 : 4;
       if (ms < best_t) {
         best_t = ms;
         best = t;
@@ -2566,6 +2649,8 @@ class Engine {
     a.atoms = d_atoms_.p;
     a.off = d_off_.p;
     a.coef = d_coef_.p;
+    a.tab = d_tab_.p;
+    a.gauss = d_gauss_.p;
     a.V = out;
     a.nx = nx_;
     a.ny = ny_;
@@ -2661,6 +2746,15 @@ class Engine {
   DevBuf<float> d_coef_;
   int nrows_fp_ = 0;
   bool have_fp_ = false;
+  // separable potential: expansions [103][2][kGaussJ], per-atom tables of the
+  // current slice, the loaded rows (FP64), per-row check (-1 not yet checked)
+  static constexpr double kGaussTol = 2e-7;
+  DevBuf<float> d_gauss_, d_tab_;
+  std::vector<double> hfp_;
+  std::vector<float> hgauss_;
+  std::vector<int> gauss_row_ok_;
+  std::vector<char> zpresent_;
+  int pot_sum_ = 0, last_pot_sum_ = 0;
   // microscope
   float kV_ = 0, df_ = 0, A2_ = 0, phi2_ = 0, Cs_ = 0, beta_ = 0, delta_ = 0, aperture_ = 0;
   bool have_micro_ = false;
@@ -2681,6 +2775,7 @@ class Engine {
   uint32_t det_serial_ = 0;
   bool image_noisy_ = false;
   int pot_tile_ = -1;                    // tuned tile shape of the conventional potential (-1: not yet)
+  bool pot_tile_forced_ = false;
   int rs_n_ = 0, rs_B_ = 1, rs_S_ = 0;  // prepared probe raster
   bool rs_loop_ = false;                 // its slices ran in the batched persistent loop
   bool rs_prefer_loop_ = true;           // tuned: batched loop (or per pass) for this grid's rasters
@@ -3029,6 +3124,9 @@ ms_status ms_run_conventional(ms_sim* s, int* nslices) {
 }
 ms_status ms_get_raster_tuning(ms_sim* s, int* batch, int* persistent) {
   return guarded(s, [&](ms::Engine& e) { return e.raster_tuning(batch, persistent); });
+}
+ms_status ms_get_potential_sum(ms_sim* s, int* last, int* next) {
+  return guarded(s, [&](ms::Engine& e) { return e.potential_sum_info(last, next); });
 }
 ms_status ms_get_slice_loop(ms_sim* s, int* variant, int* columns, int* grid) {
   return guarded(s, [&](ms::Engine& e) { return e.slice_loop_info(variant, columns, grid); });

@@ -116,6 +116,18 @@ class ManagedMultisliceSimulation:
         """Conventional potential kernel tile: -1 tuned (default), 0/1/2 = 32x8, 16x16, 64x4 pixels."""
         self._chk(self._L.ms_set_option(self._h, 9, int(tile)))
 
+    def SetPotentialSum(self, mode: int):
+        """Conventional potential's sub-plane sum: 0 separable where it applies
+        (default), 1 per (pixel, atom, sub-plane), 2 separable or an error."""
+        self._chk(self._L.ms_set_option(self._h, 10, int(mode)))
+
+    def PotentialSum(self):
+        """(last, next): how the last conventional potential was summed and how
+        the next would be (1 per sub-plane, 2 separable; last 0: none yet)."""
+        a, b = C.c_int(), C.c_int()
+        self._chk(self._L.ms_get_potential_sum(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def RasterTuning(self):
         """(probes per launch, 1 if the slices ran in the batched persistent loop) of the last raster."""
         b, p = C.c_int(), C.c_int()

@@ -90,8 +90,17 @@ enum {
                                in 512-thread CTAs (units of 4, 2, 8 columns, tight poll);
                                8-9 as 3 and 2 with the ordering carried by the release
                                reduction and the acquire poll alone (no full fences) */
-  MS_OPT_POTENTIAL_TILE = 9 /* conventional potential kernel tile: -1 = tuned on the device
+  MS_OPT_POTENTIAL_TILE = 9, /* conventional potential kernel tile: -1 = tuned on the device
                                per grid (default); 0, 1, 2 = 32 x 8, 16 x 16, 64 x 4 pixels */
+  MS_OPT_POTENTIAL_SUM = 10 /* how the conventional potential sums an atom's 20 sub-planes
+                               (binnedAtomPKernel3, U.cu:582-653): 0 = separable where it
+                               applies (default), else per sub-plane; 1 = per (pixel, atom,
+                               sub-plane), vatom evaluated term by term; 2 = separable, or
+                               MS_ERR_UNSUPPORTED.  Separable: each element's vatom as 12
+                               Gaussians in r^2 (checked against the loaded parameterisation
+                               to 2e-7 of v on 0.25..2.2365 A), so that an atom's sub-plane
+                               sum costs 12 exponentials per pixel; the same sub-planes pass
+                               the reference's FP32 cut-off test as term by term. */
 };
 
 /* ---- lifecycle ---- */
@@ -232,7 +241,8 @@ ms_status ms_copy_tds(ms_sim* sim, float* dst /* nx*ny */);
 ms_status ms_get_grid(ms_sim* sim, int* nx, int* ny);
 
 /* ---- whole-run entry points (new) ---- */
-/* Builds the potentials of slices 1..S into a device-resident stack. */
+/* Builds the potentials of slices 1..S into a device-resident stack (device
+ * time of a build that ran in ms_get_last_device_ms). */
 ms_status ms_build_potential_stack(ms_sim* sim, int* nslices);
 /* Runs conventional slices 1..S from the initial wave (replayed as one
  * captured CUDA graph: on square 256, 512 and 1024 grids a single persistent
@@ -337,8 +347,8 @@ ms_status ms_stem_raster_concurrent(ms_sim* const* sims, int nsims, const int* c
 ms_status ms_time_pass(ms_sim* sim, int pass, int op, int variant, int batch, int reps, float* us);
 /* Device milliseconds (CUDA events on the handle's stream) of the last
  * focal-series call (from after the target upload to before the read-back),
- * frozen-phonon series, concurrent raster, or ms_run_conventional (the slice
- * loop: one graph launch on the fused path). */
+ * frozen-phonon series, concurrent raster, ms_run_conventional (the slice
+ * loop: one graph launch on the fused path) or potential-stack build. */
 ms_status ms_get_last_device_ms(ms_sim* sim, float* out);
 ms_status ms_get_binned_counts(ms_sim* sim, int* n_atoms, int* n_zbins);
 ms_status ms_copy_binned(ms_sim* sim, int* offsets, int* Z, float* x, float* y, float* z);
@@ -368,6 +378,10 @@ ms_status ms_get_raster_tuning(ms_sim* sim, int* batch, int* persistent);
 ms_status ms_get_slice_loop(ms_sim* sim, int* variant, int* columns, int* grid);
 /* Number of this library's kernels launched by the handle so far. */
 ms_status ms_get_launch_count(ms_sim* sim, long long* out);
+/* How the last conventional potential was summed (1 = per sub-plane,
+ * 2 = separable, 0 = none built yet) and how the next one would be
+ * (MS_OPT_POTENTIAL_SUM and the specimen's elements). */
+ms_status ms_get_potential_sum(ms_sim* sim, int* last, int* next);
 
 /* ---- atom index without device allocation (no counterpart in the reference) ----
  * For callers that cannot call cudaMalloc: an application whose memory manager
