@@ -283,7 +283,9 @@ __global__ void __launch_bounds__(kPotThreads) k_potential(PotArgs a) {
       const int nseg = (kend - kg + 1) * nyb;
       // segment lengths and their exclusive prefix
       int len0 = 0, len1 = 0, st0 = 0, st1 = 0;
-      const int s0 = threadIdx.x, s1 = threadIdx.x + kPotThreads;
+      // thread t holds the adjacent segments 2t and 2t + 1, so that the scan of
+      // their summed lengths gives every segment its prefix in segment order
+      const int s0 = 2 * (int)threadIdx.x, s1 = s0 + 1;
       if (s0 < nseg) {
         const int k = kg + s0 / nyb, j = byl + s0 % nyb;
         const int b = k * kBins2 + j * kBins;
@@ -466,7 +468,9 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
       const int kend = min(kg + kstep - 1, a.kb);
       const int nseg = (kend - kg + 1) * nyb;
       int len0 = 0, len1 = 0, st0 = 0, st1 = 0;
-      const int s0 = threadIdx.x, s1 = threadIdx.x + kPotThreads;
+      // thread t holds the adjacent segments 2t and 2t + 1, so that the scan of
+      // their summed lengths gives every segment its prefix in segment order
+      const int s0 = 2 * (int)threadIdx.x, s1 = s0 + 1;
       if (s0 < nseg) {
         const int b = (kg + s0 / nyb) * kBins2 + (byl + s0 % nyb) * kBins;
         st0 = a.off[b + bxl];
@@ -660,18 +664,34 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_conv(PotArgs a) {
 // ---------------------------------------------------------------------------
 constexpr int kTabAtoms = 16;  // atoms per CTA of the table kernel, 16 threads each
 
+// The cut-off test fadd(dxy, q) < 5 (round to nearest even) holds exactly when
+// the real sum dxy + q < 5 - 2^-22 (the midpoint below 5 rounds up to the even
+// 5); for a float dxy that is dxy < t with t the FP32 value of 5 - 2^-22 - q
+// rounded up (the difference is exact in FP64 wherever it can decide the
+// rounding).  So one comparison per search step decides as the reference does.
+__device__ __forceinline__ float cutoff_threshold(float q) {
+  return __double2float_ru(4.999999761581421 - (double)q);
+}
+
 __global__ void __launch_bounds__(256) k_atom_tables(PotArgs a) {
   __shared__ float s_d2[kTabAtoms][20];
   __shared__ float s_qv[kTabAtoms][20];
+  __shared__ float s_e[kTabAtoms][20][kGaussJ];
+  __shared__ int s_n[kTabAtoms];
   if (a.kt > a.kb || a.kt < 0 || a.kb >= a.nz) return;  // (no z-bin in the window)
-  const int a0 = a.off[a.kt * kBins2], na = a.off[(a.kb + 1) * kBins2] - a0;
+  // (this instance's index and tables; a itself stays in parameter space,
+  // where a.zsub is read)
+  const float4* atoms = a.atoms + blockIdx.y * a.b_atoms;
+  const int* off = a.off + blockIdx.y * a.b_off;
+  float* tabs = a.tab + blockIdx.y * a.b_tab;
+  const int a0 = off[a.kt * kBins2], na = off[(a.kb + 1) * kBins2] - a0;
   const int la = threadIdx.x >> 4, j = threadIdx.x & 15;
   for (int base = blockIdx.x * kTabAtoms; base < na; base += gridDim.x * kTabAtoms) {
     const bool valid = base + la < na;
-    float* tab = a.tab + (size_t)(base + la) * kTabStride;
+    float* tab = tabs + (size_t)(base + la) * kTabStride;
     float4 at = make_float4(0.f, 0.f, 0.f, 0.f);
     if (valid) {
-      at = a.atoms[a0 + base + la];
+      at = atoms[a0 + base + la];
       // dz_m^2 as the cut-off rounds it (16 lanes, two planes for the first 4)
       for (int m = j; m < 20; m += 16) {
         const float dz = fsub_x(a.zsub[m], at.z);
@@ -679,48 +699,61 @@ __global__ void __launch_bounds__(256) k_atom_tables(PotArgs a) {
       }
     }
     __syncthreads();
-    int n = 0;
-    if (valid && j == 0) {
-      // sub-planes in ascending dz^2: dz is monotone in the plane height, so
-      // dz^2 rises on both sides of its minimum; merge the two sides
-      int m0 = 0;
-      for (int m = 1; m < 20; ++m)
-        if (s_d2[la][m] < s_d2[la][m0]) m0 = m;
-      int lo = m0 - 1, hi = m0 + 1, m = m0;
-      while (n < 20 && s_d2[la][m] < 5.0f) {
-        tab[kTabQ + n] = s_d2[la][m];
+    const float* g = a.gauss + (valid ? __float_as_int(at.w) - 1 : 0) * 2 * kGaussJ;
+    if (valid) {
+      // each lane places its sub-planes by rank (ascending dz^2, ties by m);
+      // the planes with dz^2 < 5 are the first n of that order
+      int cnt = 0;
+      for (int m = 0; m < 20; ++m) cnt += s_d2[la][m] < 5.0f;
+      if (j == 0) s_n[la] = cnt;
+      for (int m = j; m < 20; m += 16) {
+        const float d = s_d2[la][m];
+        if (!(d < 5.0f)) continue;
+        int r = 0;
+        for (int k = 0; k < 20; ++k) {
+          const float e = s_d2[la][k];
+          r += (e < d) || (e == d && k < m);
+        }
         const float dzv = fsub_x(a.zsub[m], at.z) + a.zsub_lo[m];
         const float qv = dzv * dzv;
-        tab[kTabQV + n] = qv;
-        s_qv[la][n] = qv;
-        ++n;
-        const float dl = lo >= 0 ? s_d2[la][lo] : 1e30f, dh = hi < 20 ? s_d2[la][hi] : 1e30f;
-        if (dl <= dh) m = lo--; else m = hi++;
-        if (m < 0 || m >= 20) break;
+        tab[kTabQ + r] = cutoff_threshold(d);
+        tab[kTabQV + r] = qv;
+        s_qv[la][r] = qv;
       }
-      for (int k = n; k < 32; ++k) tab[kTabQ + k] = 1e30f;
-      s_d2[la][0] = __int_as_float(n);  // (the count, for the T rows below)
+      for (int k = cnt + j; k < 32; k += 16) tab[kTabQ + k] = -1e30f;
+    }
+    __syncthreads();
+    if (valid) {
+      // w_j exp(-alpha_j dzv_k^2) for every (sub-plane, Gaussian), independent
+      const int nk = s_n[la];
+      for (int q = j; q < nk * kGaussJ; q += 16) {
+        const int k = q / kGaussJ, jj = q - k * kGaussJ;
+        s_e[la][k][jj] = g[kGaussJ + jj] * exp2f(-g[jj] * s_qv[la][k]);
+      }
     }
     __syncthreads();
     if (valid && j < kGaussJ) {
-      const int nk = __float_as_int(s_d2[la][0]);
-      const float* g = a.gauss + (__float_as_int(at.w) - 1) * 2 * kGaussJ;
-      const float al = g[j], w = g[kGaussJ + j];
-      double s = 0.0;
+      // running sums over the sub-planes in ascending dz^2 (FP64, rounded once)
+      const int nk = s_n[la];
+      double sum = 0.0;
       for (int k = 0; k < nk; ++k) {
-        s += (double)w * (double)exp2f(-al * s_qv[la][k]);
-        tab[kTabT + k * kGaussJ + j] = (float)((double)a.wsub * s);
+        sum += (double)s_e[la][k][j];
+        tab[kTabT + k * kGaussJ + j] = (float)((double)a.wsub * sum);
       }
     }
     __syncthreads();
   }
 }
 
-template <int TX, int TY>
-__global__ void __launch_bounds__(kPotThreads) k_potential_sep(PotArgs a) {
-  static_assert(TX * TY == kPotThreads && TX % 8 == 0 && TY % 4 == 0, "tile of 8 x 4 warp patches");
+// Each thread sums RY pixels of one column (rows y, y + 4, ...): a warp covers
+// an 8 x 4RY patch, and the per-atom work of a warp (staged atom, element,
+// table row base, loop) is shared by RY pixels per lane.  Each warp walks
+// only the staged atoms that can reach its own patch.
+template <int TX, int TY, int RY>
+__global__ void __launch_bounds__(kPotThreads, RY >= 4 ? 5 : 6) k_potential_sep(PotArgs a) {
+  static_assert(TX * TY == kPotThreads * RY && TX % 8 == 0 && TY % (4 * RY) == 0, "tile of 8 x 4RY warp patches");
   __shared__ float4 s_at[kConvChunk];
-  __shared__ __align__(16) float s_q[kConvChunk][32];
+  __shared__ __align__(16) float s_t[kConvChunk][32];
   __shared__ __align__(16) float s_al[kConvChunk][kGaussJ];
   __shared__ int s_l[kConvChunk];
   __shared__ int s_wcnt[kPotThreads / 32];
@@ -728,21 +761,35 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_sep(PotArgs a) {
   __shared__ int s_pref[kMaxSeg + 1];
   __shared__ int s_warp[33];
 
-  int tx, ty;
-  tile_pixel_t<TX, TY>(threadIdx.x, tx, ty);
+  constexpr int PX = TX / 8;  // patches across
+  // (this instance's index, tables and output)
+  const float4* atoms = a.atoms + blockIdx.z * a.b_atoms;
+  const int* off = a.off + blockIdx.z * a.b_off;
+  const float* tabs = a.tab + blockIdx.z * a.b_tab;
+  float* V = a.V + blockIdx.z * a.b_V;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-  const int x = x0 + tx, y = y0 + ty;
-  const bool inside = (x < a.nx) && (y < a.ny);
+  const int wx0 = x0 + (w % PX) * 8, wy0 = y0 + (w / PX) * 4 * RY;  // this warp's patch
+  const int x = wx0 + (lane & 7);
   const float px = fadd_x(a.xoff, fmul_x((float)x, a.ps));
-  const float py = fadd_x(a.yoff, fmul_x((float)y, a.ps));
   // values at the exact positions, decisions at the reference's FP32 ones (as
   // in k_potential_conv)
   const float px_lo = (float)(((double)a.xoff + (double)x * (double)a.ps) - (double)px);
-  const float py_lo = (float)(((double)a.yoff + (double)y * (double)a.ps) - (double)py);
+  float py[RY], py_lo[RY], acc[RY];
+#pragma unroll
+  for (int r = 0; r < RY; ++r) {
+    const int y = wy0 + (lane >> 3) + 4 * r;
+    py[r] = fadd_x(a.yoff, fmul_x((float)y, a.ps));
+    py_lo[r] = (float)(((double)a.yoff + (double)y * (double)a.ps) - (double)py[r]);
+    acc[r] = 0.0f;
+  }
   const float tx_lo = fadd_x(a.xoff, fmul_x((float)x0, a.ps));
   const float tx_hi = fadd_x(a.xoff, fmul_x((float)(x0 + TX - 1), a.ps));
   const float ty_lo = fadd_x(a.yoff, fmul_x((float)y0, a.ps));
   const float ty_hi = fadd_x(a.yoff, fmul_x((float)(y0 + TY - 1), a.ps));
+  const float wx_lo = fadd_x(a.xoff, fmul_x((float)wx0, a.ps)), wx_hi = fadd_x(a.xoff, fmul_x((float)(wx0 + 7), a.ps));
+  const float wy_lo = fadd_x(a.yoff, fmul_x((float)wy0, a.ps));
+  const float wy_hi = fadd_x(a.yoff, fmul_x((float)(wy0 + 4 * RY - 1), a.ps));
   const float xlo = a.xoff + x0 * a.ps - 2.2361f, xhi = a.xoff + (x0 + TX - 1) * a.ps + 2.2361f;
   const float ylo = a.yoff + y0 * a.ps - 2.2361f, yhi = a.yoff + (y0 + TY - 1) * a.ps + 2.2361f;
   const int bxl = max((int)floorf(xlo / a.bw_x) - 1, 0);
@@ -751,25 +798,26 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_sep(PotArgs a) {
   const int byh = min((int)floorf(yhi / a.bw_y) + 1, kBins - 1);
   const int nyb = byh - byl + 1;
   const bool window = a.kt <= a.kb && a.kt >= 0 && a.kb < a.nz;
-  const int a0 = window ? a.off[a.kt * kBins2] : 0;
+  const int a0 = window ? off[a.kt * kBins2] : 0;
 
-  float acc = 0.0f;
   if (bxl <= bxh && byl <= byh && window) {
     const int kstep = max(kMaxSeg / nyb, 1);
     for (int kg = a.kt; kg <= a.kb; kg += kstep) {
       const int kend = min(kg + kstep - 1, a.kb);
       const int nseg = (kend - kg + 1) * nyb;
       int len0 = 0, len1 = 0, st0 = 0, st1 = 0;
-      const int s0 = threadIdx.x, s1 = threadIdx.x + kPotThreads;
+      // thread t holds the adjacent segments 2t and 2t + 1, so that the scan of
+      // their summed lengths gives every segment its prefix in segment order
+      const int s0 = 2 * (int)threadIdx.x, s1 = s0 + 1;
       if (s0 < nseg) {
         const int b = (kg + s0 / nyb) * kBins2 + (byl + s0 % nyb) * kBins;
-        st0 = a.off[b + bxl];
-        len0 = a.off[b + bxh + 1] - st0;
+        st0 = off[b + bxl];
+        len0 = off[b + bxh + 1] - st0;
       }
       if (s1 < nseg) {
         const int b = (kg + s1 / nyb) * kBins2 + (byl + s1 % nyb) * kBins;
-        st1 = a.off[b + bxl];
-        len1 = a.off[b + bxh + 1] - st1;
+        st1 = off[b + bxl];
+        len1 = off[b + bxh + 1] - st1;
       }
       int total;
       const int ex = block_exclusive_scan(len0 + len1, s_warp, &total);
@@ -794,81 +842,105 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_sep(PotArgs a) {
             if (s_pref[mid] <= gidx) lo = mid; else hi = mid - 1;
           }
           const int l = s_start[lo] + (gidx - s_pref[lo]);
-          at = a.atoms[l];
+          at = atoms[l];
           li = l - a0;
-          const float q0 = a.tab[(size_t)li * kTabStride + kTabQ];
+          const float t0 = tabs[(size_t)li * kTabStride + kTabQ];
           const float ddx = fmaxf(0.0f, fmaxf(tx_lo - at.x, at.x - tx_hi));
           const float ddy = fmaxf(0.0f, fmaxf(ty_lo - at.y, at.y - ty_hi));
-          keep = q0 < 5.0f && ddx * ddx + ddy * ddy + q0 < 5.0005f;
+          keep = ddx * ddx + ddy * ddy < t0 + 0.0005f;
         }
         const unsigned bal = __ballot_sync(0xffffffffu, keep);
-        if ((threadIdx.x & 31) == 0) s_wcnt[threadIdx.x >> 5] = __popc(bal);
+        if (lane == 0) s_wcnt[w] = __popc(bal);
         __syncthreads();
         int pos = 0, cnt = 0;
-        for (int w = 0; w < kConvChunk / 32; ++w) {
-          if (w < (int)(threadIdx.x >> 5)) pos += s_wcnt[w];
-          cnt += s_wcnt[w];
+        for (int ww = 0; ww < kConvChunk / 32; ++ww) {
+          if (ww < w) pos += s_wcnt[ww];
+          cnt += s_wcnt[ww];
         }
         if (keep) {
-          pos += __popc(bal & ((1u << (threadIdx.x & 31)) - 1u));
+          pos += __popc(bal & ((1u << lane) - 1u));
           s_at[pos] = at;
           s_l[pos] = li;
         }
         __syncthreads();
         for (int q = threadIdx.x; q < cnt * 32; q += kPotThreads)
-          s_q[q >> 5][q & 31] = a.tab[(size_t)s_l[q >> 5] * kTabStride + kTabQ + (q & 31)];
+          s_t[q >> 5][q & 31] = tabs[(size_t)s_l[q >> 5] * kTabStride + kTabQ + (q & 31)];
         for (int q = threadIdx.x; q < cnt * kGaussJ; q += kPotThreads) {
           const int i = q / kGaussJ, jj = q - i * kGaussJ;
-          s_al[i][jj] = a.gauss[(__float_as_int(s_at[i].w) - 1) * 2 * kGaussJ + jj];
+          s_al[i][jj] = -a.gauss[(__float_as_int(s_at[i].w) - 1) * 2 * kGaussJ + jj];
         }
         __syncthreads();
-        for (int i = 0; i < cnt; ++i) {
-          const float4 at = s_at[i];
-          const float dx = fsub_x(px, at.x), dy = fsub_x(py, at.y);
-          const float dxy = fadd_x(fmul_x(dx, dx), fmul_x(dy, dy));
-          const float q0 = s_q[i][0];
-          // no lane takes a term from this atom: dxy >= 0, so its bits order
-          // as the values do
-          const float wmin = __int_as_float(__reduce_min_sync(0xffffffffu, __float_as_int(dxy)));
-          if (!(fadd_x(wmin, q0) < 5.0f)) continue;
-          // K = the sub-planes with r^2 = dxy + dz^2 < 5 (the reference's test)
-          int K = 0;
-#pragma unroll
-          for (int st = 16; st >= 1; st >>= 1)
-            if (fadd_x(dxy, s_q[i][K + st - 1]) < 5.0f) K += st;
-          if (K == 0) continue;
-          const float dxv = dx + px_lo, dyv = dy + py_lo;
-          const float dxyv = fmaf(dxv, dxv, dyv * dyv);
-          const float* tab = a.tab + (size_t)s_l[i] * kTabStride;
-          if (fadd_x(dxy, q0) < 0.0627f) {
-            // a sub-plane reaches the 0.25 A clamp (decided on the exact r^2
-            // inside vatom_f): the direct sum
-            const float* c = a.coef + (__float_as_int(at.w) - 1) * kCoefPerZ;
-            float v = 0.0f;
-            for (int k = 0; k < K; ++k) v += vatom_f(c, dxyv + __ldg(tab + kTabQV + k));
-            acc += a.wsub * v;
-          } else {
-            const float4* T = reinterpret_cast<const float4*>(tab + kTabT + (K - 1) * kGaussJ);
+        // each warp walks the staged atoms that can reach its own patch
+        for (int c0 = 0; c0 < cnt; c0 += 32) {
+          bool reach = false;
+          if (c0 + lane < cnt) {
+            const float4 ar = s_at[c0 + lane];
+            const float ddx = fmaxf(0.0f, fmaxf(wx_lo - ar.x, ar.x - wx_hi));
+            const float ddy = fmaxf(0.0f, fmaxf(wy_lo - ar.y, ar.y - wy_hi));
+            reach = ddx * ddx + ddy * ddy < s_t[c0 + lane][0] + 0.0005f;
+          }
+          unsigned mask = __ballot_sync(0xffffffffu, reach);
+          while (mask) {
+            const int i = c0 + __ffs(mask) - 1;
+            mask &= mask - 1u;
+            const float4 at = s_at[i];
+            const float* t = s_t[i];
+            const float* tab = tabs + (size_t)s_l[i] * kTabStride;
             const float4* A = reinterpret_cast<const float4*>(&s_al[i][0]);
-            const f2p nr = pk2(-dxyv, -dxyv);
-            f2p s2 = pk2(0.0f, 0.0f);
+            const float dx = fsub_x(px, at.x);
+            const float dx2 = fmul_x(dx, dx);
+            const float dxv = dx + px_lo;
 #pragma unroll
-            for (int g = 0; g < kGaussJ / 4; ++g) {
-              const float4 al = A[g];
-              const float4 t = __ldg(T + g);
-              s2 = fma2(ex2_pair(mul2(pk2(al.x, al.y), nr)), pk2(t.x, t.y), s2);
-              s2 = fma2(ex2_pair(mul2(pk2(al.z, al.w), nr)), pk2(t.z, t.w), s2);
+            for (int r = 0; r < RY; ++r) {
+              const float dy = fsub_x(py[r], at.y);
+              const float dxy = fadd_x(dx2, fmul_x(dy, dy));
+              // K = the sub-planes with r^2 = dxy + dz^2 < 5 (the reference's test)
+              int K = 0;
+#pragma unroll
+              for (int st = 16; st >= 1; st >>= 1)
+                if (dxy < t[K + st - 1]) K += st;
+              if (K == 0) continue;
+              const float dyv = dy + py_lo[r];
+              const float dxyv = fmaf(dxv, dxv, dyv * dyv);
+              if (dxy < t[0] - 4.9373f) {
+                // a sub-plane can reach the 0.25 A clamp (dxy + dz^2 < 0.0627;
+                // the clamp itself is decided on the exact r^2 inside vatom_f):
+                // the direct sum
+                const float* c = a.coef + (__float_as_int(at.w) - 1) * kCoefPerZ;
+                float v = 0.0f;
+                for (int k = 0; k < K; ++k) v += vatom_f(c, dxyv + __ldg(tab + kTabQV + k));
+                acc[r] += a.wsub * v;
+              } else {
+                // sum_j exp(-alpha_j rho^2) T_K[j] (each term one multiply,
+                // one ex2, one fused multiply-add)
+                const float4* T = reinterpret_cast<const float4*>(tab + kTabT + (K - 1) * kGaussJ);
+                float e0 = 0.0f, e1 = 0.0f;
+#pragma unroll
+                for (int g = 0; g < kGaussJ / 4; ++g) {
+                  const float4 al = A[g];
+                  const float4 tt = __ldg(T + g);
+                  e0 = fmaf(ex2_fast(al.x * dxyv), tt.x, e0);
+                  e1 = fmaf(ex2_fast(al.y * dxyv), tt.y, e1);
+                  e0 = fmaf(ex2_fast(al.z * dxyv), tt.z, e0);
+                  e1 = fmaf(ex2_fast(al.w * dxyv), tt.w, e1);
+                }
+                acc[r] += e0 + e1;
+              }
             }
-            float e0, e1;
-            up2(s2, e0, e1);
-            acc += e0 + e1;
           }
         }
-        __syncthreads();
+        // (no barrier here: the next round writes the staged arrays only after
+        // its first barrier, which every warp reaches after this loop)
       }
     }
   }
-  if (inside) a.V[(long long)y * a.nx + x] = acc;
+  if (x < a.nx) {
+#pragma unroll
+    for (int r = 0; r < RY; ++r) {
+      const int y = wy0 + (lane >> 3) + 4 * r;
+      if (y < a.ny) V[(long long)y * a.nx + x] = acc[r];
+    }
+  }
 }
 
 // Adjoint of k_potential_conv with respect to the atoms' x and y.  For slice
@@ -965,14 +1037,132 @@ __global__ void __launch_bounds__(kPotThreads) k_potential_conv_adjoint(PotArgs 
   }
 }
 
+// v'(r^2) of vatom_f, as k_potential_conv_adjoint evaluates it term by term
+// (zero inside the 0.25 A clamp, where v is constant).
+__device__ __forceinline__ float vatom_deriv_f(const float* __restrict__ c, float r2) {
+  if (r2 < 0.0625f) return 0.0f;
+  constexpr float kLn2 = 0.6931471805599453f;
+  const float ri = rsqrtf(r2), r = r2 * ri;
+  const float L = c[0] * ex2_fast(-c[3] * r) * fmaf(-c[3] * kLn2, r, -1.0f) +
+                  c[1] * ex2_fast(-c[4] * r) * fmaf(-c[4] * kLn2, r, -1.0f) +
+                  c[2] * ex2_fast(-c[5] * r) * fmaf(-c[5] * kLn2, r, -1.0f);
+  const float G = c[9] * c[6] * ex2_fast(-c[9] * r2) + c[10] * c[7] * ex2_fast(-c[10] * r2) +
+                  c[11] * c[8] * ex2_fast(-c[11] * r2);
+  return 0.5f * L * ri * ri * ri - kLn2 * G;
+}
+
+// Adjoint of the separable potential with respect to the atoms' x and y: for
+// the slice's dL/dV field G and V(p) = sum_atoms sum_j exp(-alpha_j rho^2)
+// T_K(p)[j] (the same K, the same exact-position values as k_potential_sep),
+//   dL/dX = 2 sum_p G(p) (px - X) sum_j alpha_j exp(-alpha_j rho^2) T_K[j],
+// likewise for Y (the cut-off decisions are not differentiated, as in the
+// per-sub-plane adjoint).  Pixels with a sub-plane inside the 0.25 A clamp
+// take the per-sub-plane derivative.  blockIdx.x: the atom of the window (its
+// table row), blockIdx.y: one of gridDim.y interleaved row sets of its
+// +-2.3 A pixel square; FP64 block sums, added atomically in input order.
+__global__ void __launch_bounds__(kPotThreads) k_potential_sep_adjoint(PotArgs a, const float* __restrict__ G,
+                                                                       const int* __restrict__ perm, int a0,
+                                                                       double* __restrict__ dxy) {
+  __shared__ float s_t[32];
+  __shared__ float s_qv[20];
+  __shared__ __align__(16) float s_al[kGaussJ];
+  __shared__ double s_red[2][kPotThreads / 32];
+  constexpr float kLn2 = 0.6931471805599453f;
+  const int l = a0 + blockIdx.x;
+  const float4 at = a.atoms[l];
+  const float* tab = a.tab + (size_t)blockIdx.x * kTabStride;
+  const float* c = a.coef + (__float_as_int(at.w) - 1) * kCoefPerZ;
+  if (threadIdx.x < 32) s_t[threadIdx.x] = tab[kTabQ + threadIdx.x];
+  if (threadIdx.x < 20) s_qv[threadIdx.x] = tab[kTabQV + threadIdx.x];
+  if (threadIdx.x < kGaussJ) s_al[threadIdx.x] = a.gauss[(__float_as_int(at.w) - 1) * 2 * kGaussJ + threadIdx.x];
+  __syncthreads();
+  const int xl = max((int)floorf((at.x - 2.3f - a.xoff) / a.ps), 0);
+  const int xh = min((int)ceilf((at.x + 2.3f - a.xoff) / a.ps), a.nx - 1);
+  const int yl = max((int)floorf((at.y - 2.3f - a.yoff) / a.ps), 0);
+  const int yh = min((int)ceilf((at.y + 2.3f - a.yoff) / a.ps), a.ny - 1);
+  const int wx = xh - xl + 1, wy = yh - yl + 1;
+  const int ns = gridDim.y, js = blockIdx.y;
+  const float t0 = s_t[0];
+  float gx = 0.0f, gy = 0.0f;
+  if (wx > 0 && wy > js) {
+    const int npx = wx * ((wy - js + ns - 1) / ns);
+    for (int w = threadIdx.x; w < npx; w += kPotThreads) {
+      const int x = xl + w % wx, y = yl + js + (w / wx) * ns;
+      const float px = fadd_x(a.xoff, fmul_x((float)x, a.ps));
+      const float py = fadd_x(a.yoff, fmul_x((float)y, a.ps));
+      const float dx = fsub_x(px, at.x), dy = fsub_x(py, at.y);
+      const float dxy2 = fadd_x(fmul_x(dx, dx), fmul_x(dy, dy));
+      int K = 0;
+#pragma unroll
+      for (int st = 16; st >= 1; st >>= 1)
+        if (dxy2 < s_t[K + st - 1]) K += st;
+      if (K == 0) continue;
+      const float dxv = dx + (float)(((double)a.xoff + (double)x * (double)a.ps) - (double)px);
+      const float dyv = dy + (float)(((double)a.yoff + (double)y * (double)a.ps) - (double)py);
+      const float dxyv = fmaf(dxv, dxv, dyv * dyv);
+      const float gp = G[(long long)y * a.nx + x];
+      float D;  // d/d(rho^2) of the atom's value at this pixel
+      if (dxy2 < t0 - 4.9373f) {
+        D = 0.0f;
+        for (int k = 0; k < K; ++k) D += vatom_deriv_f(c, dxyv + s_qv[k]);
+        D *= a.wsub;
+      } else {
+        const float4* T = reinterpret_cast<const float4*>(tab + kTabT + (K - 1) * kGaussJ);
+        float e0 = 0.0f, e1 = 0.0f;
+#pragma unroll
+        for (int g = 0; g < kGaussJ / 4; ++g) {
+          const float4 al = *reinterpret_cast<const float4*>(&s_al[4 * g]);
+          const float4 tt = __ldg(T + g);
+          e0 = fmaf(al.x * ex2_fast(-al.x * dxyv), tt.x, e0);
+          e1 = fmaf(al.y * ex2_fast(-al.y * dxyv), tt.y, e1);
+          e0 = fmaf(al.z * ex2_fast(-al.z * dxyv), tt.z, e0);
+          e1 = fmaf(al.w * ex2_fast(-al.w * dxyv), tt.w, e1);
+        }
+        D = -kLn2 * (e0 + e1);  // (s_al holds alpha_j log2(e))
+      }
+      gx += gp * D * dxv;
+      gy += gp * D * dyv;
+    }
+  }
+  double sx = gx, sy = gy;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    sx += __shfl_down_sync(0xffffffffu, sx, o);
+    sy += __shfl_down_sync(0xffffffffu, sy, o);
+  }
+  const int warp = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    s_red[0][warp] = sx;
+    s_red[1][warp] = sy;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tx = 0.0, ty = 0.0;
+    for (int k = 0; k < kPotThreads / 32; ++k) {
+      tx += s_red[0][k];
+      ty += s_red[1][k];
+    }
+    const int i = perm[l];
+    atomicAdd(dxy + 2 * i, -2.0 * tx);
+    atomicAdd(dxy + 2 * i + 1, -2.0 * ty);
+  }
+}
+
 }  // namespace
 
 cudaError_t launch_potential_adjoint(const PotArgs& a, const float* G, const int* perm, int a0, int a1, double* dxy,
-                                     cudaStream_t s) {
+                                     cudaStream_t s, bool separable) {
   if (a1 <= a0) return cudaSuccess;
   // about 8 CTAs per SM (148 SMs) in all, at most 16 row sets per atom
   const int na = a1 - a0;
   const int ns = std::min(16, std::max(1, (8 * 148 + na - 1) / na));
+  if (separable) {
+    if (!a.tab || !a.gauss) return cudaErrorInvalidValue;
+    // the slice's per-atom tables (a0 is the window's first atom, as there)
+    k_atom_tables<<<148 * 8, 256, 0, s>>>(a);
+    k_potential_sep_adjoint<<<dim3(na, ns), kPotThreads, 0, s>>>(a, G, perm, a0, dxy);
+    return cudaGetLastError();
+  }
   k_potential_conv_adjoint<<<dim3(na, ns), kPotThreads, 0, s>>>(a, G, perm, a0, dxy);
   return cudaGetLastError();
 }
@@ -1002,21 +1192,26 @@ cudaError_t build_atom_index(const int* dZ, const float* dx, const float* dy, co
 }
 
 int potential_tiles() { return 3; }
+int potential_tiles_separable() { return 4; }
 
-cudaError_t launch_potential(const PotArgs& a, int kind, cudaStream_t s, int tile, bool separable) {
+cudaError_t launch_potential(const PotArgs& a, int kind, cudaStream_t s, int tile, bool separable, int nbatch) {
   dim3 grid((a.nx + kTX - 1) / kTX, (a.ny + kTY - 1) / kTY);
   if (kind == POT_CONVENTIONAL && separable) {
-    if (!a.tab || !a.gauss) return cudaErrorInvalidValue;
+    if (!a.tab || !a.gauss || nbatch < 1 || nbatch > 65535) return cudaErrorInvalidValue;
     // the window's atoms (read on the device) in 16-atom rounds
-    k_atom_tables<<<148 * 8, 256, 0, s>>>(a);
+    k_atom_tables<<<dim3(nbatch > 1 ? 296 : 148 * 8, nbatch), 256, 0, s>>>(a);
+    // tiles of two or four pixels per thread: 16 x 32, 32 x 16, 16 x 64, 32 x 32
+    const int nb = nbatch;
     switch (tile) {
-      case 0: k_potential_sep<32, 8><<<grid, kPotThreads, 0, s>>>(a); break;
-      case 1: k_potential_sep<16, 16><<<dim3((a.nx + 15) / 16, (a.ny + 15) / 16), kPotThreads, 0, s>>>(a); break;
-      case 2: k_potential_sep<64, 4><<<dim3((a.nx + 63) / 64, (a.ny + 3) / 4), kPotThreads, 0, s>>>(a); break;
+      case 0: k_potential_sep<16, 32, 2><<<dim3((a.nx + 15) / 16, (a.ny + 31) / 32, nb), kPotThreads, 0, s>>>(a); break;
+      case 1: k_potential_sep<32, 16, 2><<<dim3((a.nx + 31) / 32, (a.ny + 15) / 16, nb), kPotThreads, 0, s>>>(a); break;
+      case 2: k_potential_sep<16, 64, 4><<<dim3((a.nx + 15) / 16, (a.ny + 63) / 64, nb), kPotThreads, 0, s>>>(a); break;
+      case 3: k_potential_sep<32, 32, 4><<<dim3((a.nx + 31) / 32, (a.ny + 31) / 32, nb), kPotThreads, 0, s>>>(a); break;
       default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
   }
+  if (nbatch != 1) return cudaErrorInvalidValue;
   if (kind == POT_CONVENTIONAL) {
     switch (tile) {
       case 0: k_potential_conv<32, 8><<<grid, kPotThreads, 0, s>>>(a); break;

@@ -61,28 +61,37 @@ struct PotArgs {
   // then w_j)
   float* tab;
   const float* gauss;
+  // batched separable builds (one instance per blockIdx.z of the pixel kernel,
+  // blockIdx.y of the table kernel): element strides of atoms, off, tab and V
+  // between instances (0 for one instance)
+  long long b_atoms, b_off, b_tab, b_V;
 };
 
 // Gaussian expansion of vatom per element: v(r) ~= sum_j w_j exp(-alpha_j r^2)
 // for 0.25 A <= r <= 2.2365 A (positive weights).
 constexpr int kGaussJ = 12;
-// Per-atom table of one slice (floats): the reference-rounded dz_m^2 of the
-// sub-planes that can pass the cut-off, ascending, padded with 1e30 to 32
-// (the cut-off thresholds); the exact-height dz_m^2 in the same order; then
-// row k = 0..19: wsub sum_{k' <= k} w_j exp(-alpha_j dzv_k'^2), j < kGaussJ.
+// Per-atom table of one slice (floats): for the sub-planes that can pass the
+// cut-off, in ascending reference-rounded dz_m^2, the thresholds t_k with
+// "fadd(dxy, dz_k^2) < 5 exactly when dxy < t_k", padded with -1e30 to 32;
+// the exact-height dz_m^2 in the same order; then row k = 0..19:
+// wsub sum_{k' <= k} w_j exp(-alpha_j dzv_k'^2), j < kGaussJ.
 constexpr int kTabQ = 0, kTabQV = 32, kTabT = 56, kTabStride = 304;
 
 // tile: the conventional kernel's tile shape variant (0: 32 x 8, 1: 16 x 16,
 // 2: 64 x 4 pixels; other kinds take 32 x 8).
 // separable: conventional kind only, through the per-atom tables (a.tab,
 // a.gauss set) instead of the per-sub-plane sum.
-cudaError_t launch_potential(const PotArgs& a, int kind, cudaStream_t s, int tile = 0, bool separable = false);
+cudaError_t launch_potential(const PotArgs& a, int kind, cudaStream_t s, int tile = 0, bool separable = false,
+                             int nbatch = 1);
 int potential_tiles();
+int potential_tiles_separable();
 
 // Adjoint of the conventional potential of one slice with respect to atom x, y:
 // dxy[2 perm[l] + {0,1}] += dL/d{x,y} of sorted atoms l in [a0, a1) (the CSR
 // range of the slice's z-window), G = dL/dV of the slice [ny][nx].
+// separable: through the per-atom tables of the separable kernel (a.tab,
+// a.gauss set; a0 must be the first atom of the slice's z-window).
 cudaError_t launch_potential_adjoint(const PotArgs& a, const float* G, const int* perm, int a0, int a1, double* dxy,
-                                     cudaStream_t s);
+                                     cudaStream_t s, bool separable = false);
 
 }  // namespace ms

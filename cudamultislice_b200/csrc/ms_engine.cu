@@ -184,7 +184,8 @@ class Engine {
         invalidate_graph();
         return MS_OK;
       case MS_OPT_POTENTIAL_TILE:
-        if (value < -1 || value >= potential_tiles()) return fail(MS_ERR_INVALID, "tile must be -1 (tuned) or 0..2");
+        if (value < -1 || value >= std::max(potential_tiles(), potential_tiles_separable()))
+          return fail(MS_ERR_INVALID, "tile must be -1 (tuned) or a tile index of the potential kernels");
         pot_tile_ = value;
         pot_tile_forced_ = value >= 0;
         stack_valid_ = false;
@@ -1551,6 +1552,66 @@ class Engine {
   bool fused() const { return use_fused(); }
   void set_last_device_ms(float ms) { last_device_ms_ = ms; }
 
+  // z-bins of the atom index for the loaded box (U.cu:1409-1411), range-checked.
+  int index_zbins(int* nz) {
+    const float zext = std::ceil((box_.MaxZ - box_.MinZ) / (float)1);
+    if (!std::isfinite(zext) || zext < 0.0f || (double)zext * kBins2 > (double)(INT_MAX - 1))
+      return fail(MS_ERR_INVALID, "structure too deep for the atom index: " + std::to_string(zext) + " z-bins");
+    *nz = (int)zext;
+    *nz += (*nz == 0);
+    return MS_OK;
+  }
+
+  // Potential stacks of nb frozen-phonon configurations (passes pass0 ..
+  // pass0 + nb - 1, displaced as ms_upload_binned_atoms_tds): every
+  // configuration binned into its own index (the same bit-exact binning),
+  // then per slice one table launch and one separable-potential launch over
+  // all nb (instance = blockIdx), into d_fpstack_ [config][slice][ny][nx].
+  int tds_potential_batch(uint64_t seed, uint32_t pass0, int nb, float sigma, int S) {
+    const int n = (int)hx_.size();
+    int nz = 0;
+    if (int rc = index_zbins(&nz)) return rc;
+    if (nz != nzb_) return fail(MS_ERR_STATE, "atom index out of date");
+    const long long nbins = (long long)nz * kBins2;
+    const size_t N = (size_t)nx_ * ny_;
+    std::vector<float> hx((size_t)nb * n), hy((size_t)nb * n), hz((size_t)nb * n);
+    for (int k = 0; k < nb; ++k)
+      tds_displace(hx_.data(), hy_.data(), hz_.data(), n, seed, pass0 + (uint32_t)k, sigma, hx.data() + (size_t)k * n,
+                   hy.data() + (size_t)k * n, hz.data() + (size_t)k * n);
+    MS_TRY(d_tdsx_.resize((size_t)nb * n));
+    MS_TRY(d_tdsy_.resize((size_t)nb * n));
+    MS_TRY(d_tdsz_.resize((size_t)nb * n));
+    MS_TRY(d_tds_atoms_.resize((size_t)nb * n));
+    MS_TRY(d_tds_off_.resize((size_t)nb * (nbins + 1)));
+    if (d_tab_.n < (size_t)nb * n * kTabStride) MS_TRY(d_tab_.resize((size_t)nb * n * kTabStride));
+    // (copies from pageable memory return once the data is staged, so the
+    // host vectors may go out of scope when this returns)
+    MS_TRY(cudaMemcpyAsync(d_tdsx_.p, hx.data(), sizeof(float) * hx.size(), cudaMemcpyHostToDevice, stream_));
+    MS_TRY(cudaMemcpyAsync(d_tdsy_.p, hy.data(), sizeof(float) * hy.size(), cudaMemcpyHostToDevice, stream_));
+    MS_TRY(cudaMemcpyAsync(d_tdsz_.p, hz.data(), sizeof(float) * hz.size(), cudaMemcpyHostToDevice, stream_));
+    BinScratch scr{d_key_.p, d_idx_.p, d_cursor_.p, d_blocksum_.p};
+    for (int k = 0; k < nb; ++k) {
+      AtomIndex idx{d_tds_atoms_.p + (size_t)k * n, d_tds_off_.p + (size_t)k * (nbins + 1), 0, 0};
+      MS_TRY(build_atom_index(d_Zin_.p, d_tdsx_.p + (size_t)k * n, d_tdsy_.p + (size_t)k * n,
+                              d_tdsz_.p + (size_t)k * n, n, box_, nz, idx, scr, stream_));
+      launches += 8;
+    }
+    const int tile = std::min(std::max(pot_tile_, 0), potential_tiles_separable() - 1);
+    for (int it = 1; it <= S; ++it) {
+      PotArgs a = pot_args(POT_CONVENTIONAL, it, d_fpstack_.p + (size_t)(it - 1) * N);
+      a.atoms = d_tds_atoms_.p;
+      a.off = d_tds_off_.p;
+      a.b_atoms = n;
+      a.b_off = nbins + 1;
+      a.b_tab = (long long)n * kTabStride;
+      a.b_V = (long long)S * N;
+      MS_TRY(launch_potential(a, POT_CONVENTIONAL, stream_, tile, true, nb));
+      launches += 2;
+    }
+    last_pot_sum_ = 2;
+    return MS_OK;
+  }
+
   // ---- frozen-phonon series (the GUI's pass loop, MainWindow.xaml.cs:353-402) ----
   // Configurations first_pass .. first_pass + nconf - 1, each displaced as
   // ms_upload_binned_atoms_tds(seed, pass, sigma), through conventional slices
@@ -1592,6 +1653,13 @@ class Engine {
     }
     invalidate_graph();
     bool fp_loop = false;
+    // the fused path bins every configuration of a batch into its own index
+    // and builds their potentials slice by slice in one launch each
+    // (separable kernel); the handle's index is the last configuration's
+    // afterwards, as one upload at a time leaves it
+    const bool batch_pot = fused && kind == POT_CONVENTIONAL && separable_ok();
+    if (batch_pot && pot_tile_ < 0)
+      if (int rc = tune_pot_tile()) return rc;
     MS_TRY(cudaEventRecord(ev0_, stream_));
     for (int start = 0; start < nconf; start += B) {
       const int nb = std::min(B, nconf - start);
@@ -1611,13 +1679,18 @@ class Engine {
         continue;
       }
       // potential stacks of the nb configurations: [config][slice][ny][nx]
-      for (int k = 0; k < nb; ++k) {
-        if (int rc = upload_binned(true, seed, first_pass + (uint32_t)(start + k), sigma)) return rc;
-        for (int it = 1; it <= S; ++it)
-          if (int rc = potential_slice(kind, it, d_fpstack_.p + ((size_t)k * S + (it - 1)) * N)) return rc;
+      if (batch_pot) {
+        if (int rc = tds_potential_batch(seed, first_pass + (uint32_t)start, nb, sigma, S)) return rc;
+      } else {
+        for (int k = 0; k < nb; ++k) {
+          if (int rc = upload_binned(true, seed, first_pass + (uint32_t)(start + k), sigma)) return rc;
+          for (int it = 1; it <= S; ++it)
+            if (int rc = potential_slice(kind, it, d_fpstack_.p + ((size_t)k * S + (it - 1)) * N)) return rc;
+        }
+      }
+      for (int k = 0; k < nb; ++k)
         MS_TRY(cudaMemcpyAsync(d_bwave_.p + (size_t)k * N, d_psi0_.p, sizeof(float2) * N, cudaMemcpyDeviceToDevice,
                                stream_));
-      }
       if (use_batch_loop()) {
         // the nb configurations through every slice in one persistent launch
         const int v = batch_loop_plan(nx_);
@@ -1669,6 +1742,8 @@ class Engine {
       }
     }
     MS_TRY(cudaEventRecord(ev1_, stream_));
+    if (batch_pot)
+      if (int rc = upload_binned(true, seed, first_pass + (uint32_t)(nconf - 1), sigma)) return rc;
     if (diff) MS_TRY(cudaMemcpyAsync(diff, d_fpdiff_.p, sizeof(float) * N, cudaMemcpyDeviceToHost, stream_));
     if (image) MS_TRY(cudaMemcpyAsync(image, d_fpsum_.p, sizeof(float) * N, cudaMemcpyDeviceToHost, stream_));
     if (fp_loop)
@@ -2120,8 +2195,9 @@ class Engine {
           if (dLdxy) {
             const PotArgs pa = pot_args(POT_CONVENTIONAL, n, nullptr);
             const int a0 = hzoff_[pa.kt], a1 = hzoff_[pa.kb + 1];
-            MS_TRY(launch_potential_adjoint(pa, dV, d_idx_.p, a0, a1, d_dxy_.p, stream_));
-            ++launches;
+            const bool sep = separable_ok();
+            MS_TRY(launch_potential_adjoint(pa, dV, d_idx_.p, a0, a1, d_dxy_.p, stream_, sep));
+            launches += sep ? 2 : 1;
           }
         }
       }
@@ -2607,7 +2683,9 @@ class Engine {
     if (kind == POT_CONVENTIONAL && pot_tile_ < 0 && !capturing_)
       if (int rc = tune_pot_tile()) return rc;
     const PotArgs a = pot_args(kind, it, out);
-    MS_TRY(launch_potential(a, kind, stream_, kind == POT_CONVENTIONAL ? std::max(pot_tile_, 0) : 0, sep));
+    const int ntile = sep ? potential_tiles_separable() : potential_tiles();
+    MS_TRY(launch_potential(a, kind, stream_, kind == POT_CONVENTIONAL ? std::min(std::max(pot_tile_, 0), ntile - 1) : 0,
+                            sep));
     launches += sep ? 2 : 1;
     last_pot_sum_ = kind == POT_CONVENTIONAL ? (sep ? 2 : 1) : last_pot_sum_;
     return MS_OK;
@@ -2625,7 +2703,7 @@ class Engine {
     float best_t = INFINITY;
     int best = 0;
     const bool sep = separable_ok();
-    for (int t = 0; t < potential_tiles(); ++t) {
+    for (int t = 0; t < (sep ? potential_tiles_separable() : potential_tiles()); ++t) {
       const PotArgs a = pot_args(POT_CONVENTIONAL, it, d_V_.p);
       MS_TRY(launch_potential(a, POT_CONVENTIONAL, stream_, t, sep));
       MS_TRY(cudaEventRecord(ev0_, stream_));
@@ -2750,6 +2828,9 @@ class Engine {
   // current slice, the loaded rows (FP64), per-row check (-1 not yet checked)
   static constexpr double kGaussTol = 2e-7;
   DevBuf<float> d_gauss_, d_tab_;
+  DevBuf<float> d_tdsx_, d_tdsy_, d_tdsz_;  // displaced positions of a frozen-phonon batch
+  DevBuf<float4> d_tds_atoms_;              // their atom indices [config][n], [config][nbins + 1]
+  DevBuf<int> d_tds_off_;
   std::vector<double> hfp_;
   std::vector<float> hgauss_;
   std::vector<int> gauss_row_ok_;

@@ -91,7 +91,9 @@ enum {
                                8-9 as 3 and 2 with the ordering carried by the release
                                reduction and the acquire poll alone (no full fences) */
   MS_OPT_POTENTIAL_TILE = 9, /* conventional potential kernel tile: -1 = tuned on the device
-                               per grid (default); 0, 1, 2 = 32 x 8, 16 x 16, 64 x 4 pixels */
+                               per grid (default); per-sub-plane kernel 0, 1, 2 = 32 x 8,
+                               16 x 16, 64 x 4 pixels; separable kernel 0..3 = 16 x 32,
+                               32 x 16 (two pixels per thread), 16 x 64, 32 x 32 (four) */
   MS_OPT_POTENTIAL_SUM = 10 /* how the conventional potential sums an atom's 20 sub-planes
                                (binnedAtomPKernel3, U.cu:582-653): 0 = separable where it
                                applies (default), else per sub-plane; 1 = per (pixel, atom,

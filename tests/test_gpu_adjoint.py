@@ -87,6 +87,26 @@ def test_focal_series_gradient_vs_oracle(engine_cls, oracle_mod):
     assert rel_l2(gxy, gxy0) < GRAD_TOL, rel_l2(gxy, gxy0)
 
 
+@pytest.mark.parametrize("mode", [1, 2])
+def test_focal_gradient_both_potential_sums(engine_cls, oracle_mod, mode):
+    """The gradient through the per-sub-plane potential (and its per-sub-plane
+    adjoint) and through the separable one (and its adjoint) both match the
+    oracle, and each other to well inside the tolerance."""
+    eng, orc, S = focal_pair(engine_cls, oracle_mod, nc=3, nzc=3, n=128, ps=0.09, seed=6)
+    T = targets(3, 128, seed=5)
+    eng.SetPotentialSum(mode)
+    L, gV, gxy = eng.FocalSeriesGrad(DEFOCI, T, S)
+    assert eng.PotentialSum()[0] == mode
+    L0, gV0, gxy0 = orc.FocalGrad(DEFOCI, T.astype(np.float64), S)
+    assert abs(L - L0) / L0 < 1e-5
+    assert rel_l2(gV, gV0) < GRAD_TOL, rel_l2(gV, gV0)
+    assert rel_l2(gxy, gxy0) < GRAD_TOL, rel_l2(gxy, gxy0)
+    eng.SetPotentialSum(3 - mode)
+    L1, gV1, gxy1 = eng.FocalSeriesGrad(DEFOCI, T, S)
+    assert rel_l2(gxy, gxy1) < GRAD_TOL / 2, rel_l2(gxy, gxy1)
+    assert rel_l2(gV, gV1) < GRAD_TOL / 2, rel_l2(gV, gV1)
+
+
 @pytest.mark.parametrize("stride", [1, 2, 4, 0, 1000])
 def test_checkpoint_strides_agree(engine_cls, oracle_mod, stride):
     """Every checkpoint stride recomputes the same waves: results agree with

@@ -56,11 +56,17 @@ def _cases():
         "gan": (S.gan_wurtzite_11_20(2, 2, 3), 128, 0.1, 1.5945),
         "random_thin": (S.random_atoms(800, size=(12.0, 12.0, 9.0), seed=7), 128, 0.1, 0.5),
         "on_pixels": (onpix, 128, 0.1, 2.0),
+        # coarse pixels over a small box (bins of 0.24 A): a tile's candidate
+        # bins exceed 256 segments
+        "coarse_small_box": (S.srtio3(2, 2, 4), 64, 0.25, 1.9525),
     }
 
 
+@pytest.mark.parametrize("tile", [-1, 0, 1, 2, 3])
 @pytest.mark.parametrize("case", list(_cases().keys()))
-def test_separable_potential(engine_cls, oracle_mod, case):
+def test_separable_potential(engine_cls, oracle_mod, case, tile):
+    """tile -1: the shape the engine tunes; 0..3: each tile shape (two and four
+    pixels per thread) forced.  The per-sub-plane kernel is checked alongside."""
     atoms, n, ps, dz = _cases()[case]
     eng = engine_cls()
     orc = oracle_mod.OracleSimulation()
@@ -75,7 +81,9 @@ def test_separable_potential(engine_cls, oracle_mod, case):
         if np.abs(ref).max() == 0:
             continue
         eng.SetPotentialSum(2)
+        eng.SetPotentialTile(tile)
         vs = eng.PotentialSlice(0, it)
+        eng.SetPotentialTile(-1)
         assert eng.PotentialSum() == (2, 2)
         eng.SetPotentialSum(1)
         vp = eng.PotentialSlice(0, it)
@@ -84,6 +92,7 @@ def test_separable_potential(engine_cls, oracle_mod, case):
         ep = np.linalg.norm(vp - ref) / np.linalg.norm(ref)
         worst = max(worst, es)
         assert es < TOL_SEP, (case, it, es, ep)
+        assert ep < TOL_SEP, (case, it, es, ep)
         assert np.abs(vs - ref).max() < 5 * TOL_SEP * np.abs(ref).max(), (case, it)
         # zero exactly where no atom reaches (the same cut-off decisions)
         assert np.array_equal(vs == 0, vp == 0), (case, it)
