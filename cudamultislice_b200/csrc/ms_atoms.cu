@@ -911,19 +911,21 @@ __global__ void __launch_bounds__(kPotThreads, RY >= 4 ? 5 : 6) k_potential_sep(
                 for (int k = 0; k < K; ++k) v += vatom_f(c, dxyv + __ldg(tab + kTabQV + k));
                 acc[r] += a.wsub * v;
               } else {
-                // sum_j exp(-alpha_j rho^2) T_K[j] (each term one multiply,
-                // one ex2, one fused multiply-add)
-                const float4* T = reinterpret_cast<const float4*>(tab + kTabT + (K - 1) * kGaussJ);
-                float e0 = 0.0f, e1 = 0.0f;
+                // sum_j exp(-alpha_j rho^2) T_K[j]: per pair of Gaussians one
+                // packed multiply, two ex2, one packed fused multiply-add
+                const ulonglong2* T = reinterpret_cast<const ulonglong2*>(tab + kTabT + (K - 1) * kGaussJ);
+                const ulonglong2* A2 = reinterpret_cast<const ulonglong2*>(A);
+                const f2p rr = pk2(dxyv, dxyv);
+                f2p s2 = pk2(0.0f, 0.0f);
 #pragma unroll
                 for (int g = 0; g < kGaussJ / 4; ++g) {
-                  const float4 al = A[g];
-                  const float4 tt = __ldg(T + g);
-                  e0 = fmaf(ex2_fast(al.x * dxyv), tt.x, e0);
-                  e1 = fmaf(ex2_fast(al.y * dxyv), tt.y, e1);
-                  e0 = fmaf(ex2_fast(al.z * dxyv), tt.z, e0);
-                  e1 = fmaf(ex2_fast(al.w * dxyv), tt.w, e1);
+                  const ulonglong2 al = A2[g];
+                  const ulonglong2 tt = __ldg(T + g);
+                  s2 = fma2(ex2_pair(mul2(al.x, rr)), tt.x, s2);
+                  s2 = fma2(ex2_pair(mul2(al.y, rr)), tt.y, s2);
                 }
+                float e0, e1;
+                up2(s2, e0, e1);
                 acc[r] += e0 + e1;
               }
             }
