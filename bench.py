@@ -563,6 +563,33 @@ def tds_leg(fparams, device: int, nconf: int = 16, batch: int = 16) -> dict:
 MID_SLICES = 10  # CPU-baseline sample: this many slices from the middle of the slab
 
 
+def potential_leg(fparams, device: int, reps: int = 3) -> dict:
+    """The workload's potential stack (102 slices, 1024^2, 50k atoms) built by
+    the separable kernel (the default) and by the per-sub-plane kernel: device
+    time of ms_build_potential_stack, best of `reps` rebuilds after a first
+    build that tunes each kernel's tile shape."""
+    atoms = workload()
+    out = {}
+    for mode, name in ((2, "separable"), (1, "per_subplane")):
+        sim = new_sim(device)
+        sim.SetPotentialSum(mode)
+        configure(sim, atoms, fparams)
+        nsl = sim.BuildPotentialStack()
+        best = float("inf")
+        for _ in range(reps):
+            sim.UploadBinnedAtoms()
+            sim.BuildPotentialStack()
+            best = min(best, sim.LastDeviceMs())
+        out[name] = {"stack_ms": best, "us_per_slice": 1000.0 * best / nsl, "slices": nsl,
+                     "kernel_ran": {1: "per sub-plane", 2: "separable"}[sim.PotentialSum()[0]]}
+        sim.close()
+    return {"value": out["separable"]["us_per_slice"], "unit": "us per slice",
+            "speedup_separable_vs_per_subplane": out["per_subplane"]["stack_ms"] / out["separable"]["stack_ms"],
+            "config": "a-C 50x50x200 A (50k atoms), 1024^2, 102 slices of 2 A (binnedAtomPKernel3 semantics)",
+            "timing": "device time (CUDA events) of ms_build_potential_stack, best of 3 rebuilds",
+            "detail": out}
+
+
 def mid_range(S: int, k: int = MID_SLICES) -> range:
     """Iterations of the k slices centred in an S-slice stack."""
     a = max(1, S // 2 - k // 2 + 1)
@@ -668,7 +695,7 @@ def main():
     ap.add_argument("--fft-plan", type=int, default=-1,
                     help="profiling mode and --leg runs: force this FFT plan variant (default: the autotuner's choice)")
     ap.add_argument("--leg", choices=["stem", "adjoint", "tds", "mixed", "focal_profile", "c1", "fd", "grid4096",
-                                       "grid4096_profile"],
+                                       "grid4096_profile", "potential"],
                     help="run one secondary leg alone and print its JSON (exploration)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
@@ -683,7 +710,8 @@ def main():
 
         leg = {"stem": stem_leg, "adjoint": adjoint_leg, "tds": tds_leg, "mixed": mixed_leg,
                "focal_profile": focal_profile_leg, "c1": c1_leg, "fd": fd_leg,
-               "grid4096": grid4096_leg, "grid4096_profile": grid4096_profile_leg}[args.leg](FPARAMS, local)
+               "grid4096": grid4096_leg, "grid4096_profile": grid4096_profile_leg,
+               "potential": potential_leg}[args.leg](FPARAMS, local)
         if rank == 0:
             print(json.dumps({"leg": args.leg, **leg}), flush=True)
         return
@@ -838,6 +866,7 @@ def main():
         out["c1"] = c1_leg(FPARAMS, local)
         out["fd"] = fd_leg(FPARAMS, local)
         out["grid4096"] = grid4096_leg(FPARAMS, local)
+        out["potential"] = potential_leg(FPARAMS, local)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
