@@ -1196,6 +1196,27 @@ cudaError_t build_atom_index(const int* dZ, const float* dx, const float* dy, co
 int potential_tiles() { return 3; }
 int potential_tiles_separable() { return 4; }
 
+cudaError_t launch_atom_tables(const PotArgs& a, cudaStream_t s, int nbatch) {
+  if (!a.tab || !a.gauss || nbatch < 1 || nbatch > 65535) return cudaErrorInvalidValue;
+  // the window's atoms (read on the device) in 16-atom rounds
+  k_atom_tables<<<dim3(nbatch > 1 ? 296 : 148 * 8, nbatch), 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_potential_from_tables(const PotArgs& a, cudaStream_t s, int tile, int nbatch) {
+  if (!a.tab || !a.gauss || nbatch < 1 || nbatch > 65535) return cudaErrorInvalidValue;
+  // tiles of two or four pixels per thread: 16 x 32, 32 x 16, 16 x 64, 32 x 32
+  const int nb = nbatch;
+  switch (tile) {
+    case 0: k_potential_sep<16, 32, 2><<<dim3((a.nx + 15) / 16, (a.ny + 31) / 32, nb), kPotThreads, 0, s>>>(a); break;
+    case 1: k_potential_sep<32, 16, 2><<<dim3((a.nx + 31) / 32, (a.ny + 15) / 16, nb), kPotThreads, 0, s>>>(a); break;
+    case 2: k_potential_sep<16, 64, 4><<<dim3((a.nx + 15) / 16, (a.ny + 63) / 64, nb), kPotThreads, 0, s>>>(a); break;
+    case 3: k_potential_sep<32, 32, 4><<<dim3((a.nx + 31) / 32, (a.ny + 31) / 32, nb), kPotThreads, 0, s>>>(a); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t launch_potential(const PotArgs& a, int kind, cudaStream_t s, int tile, bool separable, int nbatch) {
   dim3 grid((a.nx + kTX - 1) / kTX, (a.ny + kTY - 1) / kTY);
   if (kind == POT_CONVENTIONAL && separable) {

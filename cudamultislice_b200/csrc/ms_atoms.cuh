@@ -85,6 +85,11 @@ cudaError_t launch_potential(const PotArgs& a, int kind, cudaStream_t s, int til
                              int nbatch = 1);
 int potential_tiles();
 int potential_tiles_separable();
+// The separable conventional kernel's two launches apart (launch_potential
+// with separable = true enqueues both on one stream): the per-atom tables of
+// the slice into a.tab, then the potential from them.
+cudaError_t launch_atom_tables(const PotArgs& a, cudaStream_t s, int nbatch = 1);
+cudaError_t launch_potential_from_tables(const PotArgs& a, cudaStream_t s, int tile, int nbatch = 1);
 
 // Adjoint of the conventional potential of one slice with respect to atom x, y:
 // dxy[2 perm[l] + {0,1}] += dL/d{x,y} of sorted atoms l in [a0, a1) (the CSR

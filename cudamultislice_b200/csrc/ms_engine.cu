@@ -119,6 +119,9 @@ class Engine {
     if (have_plan_) cufftDestroy(plan_);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
+    for (cudaEvent_t e : {ev_tab_[0], ev_tab_[1], ev_pix_[0], ev_pix_[1], ev_fork_})
+      if (e) cudaEventDestroy(e);
+    if (side_) cudaStreamDestroy(side_);
     if (stream_) cudaStreamDestroy(stream_);
   }
 
@@ -133,6 +136,11 @@ class Engine {
     MS_TRY(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     MS_TRY(cudaEventCreate(&ev0_));
     MS_TRY(cudaEventCreate(&ev1_));
+    // the side stream of the potential stack (tables of the next slice while
+    // the current slice's potential runs) and its ordering events
+    MS_TRY(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&ev_tab_[0], &ev_tab_[1], &ev_pix_[0], &ev_pix_[1], &ev_fork_})
+      MS_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     MS_TRY(d_loop_sync_.resize(2));
     MS_TRY(cudaHostAlloc((void**)&h_loop_err_, sizeof(unsigned int), cudaHostAllocDefault));
     *h_loop_err_ = 0;
@@ -309,7 +317,7 @@ class Engine {
     MS_TRY(d_yin_.resize(n));
     MS_TRY(d_zin_.resize(n));
     MS_TRY(d_atoms_.resize(n));
-    MS_TRY(d_tab_.resize((size_t)n * kTabStride));
+    if (d_tab_.n < (size_t)n * kTabStride) MS_TRY(d_tab_.resize((size_t)n * kTabStride));
     MS_TRY(d_off_.resize(nbins + 1));
     MS_TRY(d_key_.resize(n));
     MS_TRY(d_idx_.resize(n));
@@ -1583,7 +1591,6 @@ class Engine {
     MS_TRY(d_tdsz_.resize((size_t)nb * n));
     MS_TRY(d_tds_atoms_.resize((size_t)nb * n));
     MS_TRY(d_tds_off_.resize((size_t)nb * (nbins + 1)));
-    if (d_tab_.n < (size_t)nb * n * kTabStride) MS_TRY(d_tab_.resize((size_t)nb * n * kTabStride));
     // (copies from pageable memory return once the data is staged, so the
     // host vectors may go out of scope when this returns)
     MS_TRY(cudaMemcpyAsync(d_tdsx_.p, hx.data(), sizeof(float) * hx.size(), cudaMemcpyHostToDevice, stream_));
@@ -1596,20 +1603,7 @@ class Engine {
                               d_tdsz_.p + (size_t)k * n, n, box_, nz, idx, scr, stream_));
       launches += 8;
     }
-    const int tile = std::min(std::max(pot_tile_, 0), potential_tiles_separable() - 1);
-    for (int it = 1; it <= S; ++it) {
-      PotArgs a = pot_args(POT_CONVENTIONAL, it, d_fpstack_.p + (size_t)(it - 1) * N);
-      a.atoms = d_tds_atoms_.p;
-      a.off = d_tds_off_.p;
-      a.b_atoms = n;
-      a.b_off = nbins + 1;
-      a.b_tab = (long long)n * kTabStride;
-      a.b_V = (long long)S * N;
-      MS_TRY(launch_potential(a, POT_CONVENTIONAL, stream_, tile, true, nb));
-      launches += 2;
-    }
-    last_pot_sum_ = 2;
-    return MS_OK;
+    return separable_stack(S, d_fpstack_.p, N, nb, d_tds_atoms_.p, d_tds_off_.p, n, nbins + 1);
   }
 
   // ---- frozen-phonon series (the GUI's pass loop, MainWindow.xaml.cs:353-402) ----
@@ -1768,8 +1762,12 @@ class Engine {
         if (int rc = tune_pot_tile()) return rc;
       // device time of the stack (ms_get_last_device_ms)
       MS_TRY(cudaEventRecord(ev0_, stream_));
-      for (int it = 1; it <= S; ++it)
-        if (int rc = potential_slice(kind, it, d_stack_.p + (it - 1) * N)) return rc;
+      if (kind == POT_CONVENTIONAL && separable_ok()) {
+        if (int rc = separable_stack(S, d_stack_.p, N, 1)) return rc;
+      } else {
+        for (int it = 1; it <= S; ++it)
+          if (int rc = potential_slice(kind, it, d_stack_.p + (it - 1) * N)) return rc;
+      }
       MS_TRY(cudaEventRecord(ev1_, stream_));
       MS_TRY(cudaStreamSynchronize(stream_));
       MS_TRY(cudaEventElapsedTime(&last_device_ms_, ev0_, ev1_));
@@ -2640,6 +2638,46 @@ class Engine {
     return MS_OK;
   }
 
+  // Separable potentials of slices 1..S into out + (it - 1) * N (and, for a
+  // batch of nb indices set up as in tds_potential_batch, instance k at
+  // out + k * S * N), two table buffers deep: the tables of slice it + 1 are
+  // built on the side stream while slice it's potential runs on the handle's
+  // stream.  Event order: tables(it) after potential(it - 2), which read the
+  // same buffer; potential(it) after tables(it).  The side stream joins the
+  // handle's stream through the last potential's dependence on its tables.
+  int separable_stack(int S, float* out, size_t N, int nb, const float4* atoms = nullptr, const int* off = nullptr,
+                      long long b_atoms = 0, long long b_off = 0) {
+    if (pot_tile_ < 0 && !capturing_)
+      if (int rc = tune_pot_tile()) return rc;
+    const int tile = std::min(std::max(pot_tile_, 0), potential_tiles_separable() - 1);
+    const size_t per = (size_t)nb * natoms_ * kTabStride;  // one buffer
+    if (d_tab_.n < 2 * per) MS_TRY(d_tab_.resize(2 * per));
+    MS_TRY(cudaEventRecord(ev_fork_, stream_));
+    MS_TRY(cudaStreamWaitEvent(side_, ev_fork_, 0));
+    for (int it = 1; it <= S; ++it) {
+      const int buf = it & 1;
+      PotArgs a = pot_args(POT_CONVENTIONAL, it, out + (size_t)(it - 1) * N);
+      a.tab = d_tab_.p + buf * per;
+      if (atoms) {
+        a.atoms = atoms;
+        a.off = off;
+        a.b_atoms = b_atoms;
+        a.b_off = b_off;
+        a.b_tab = (long long)natoms_ * kTabStride;
+        a.b_V = (long long)S * N;
+      }
+      if (it >= 3) MS_TRY(cudaStreamWaitEvent(side_, ev_pix_[buf], 0));
+      MS_TRY(launch_atom_tables(a, side_, nb));
+      MS_TRY(cudaEventRecord(ev_tab_[buf], side_));
+      MS_TRY(cudaStreamWaitEvent(stream_, ev_tab_[buf], 0));
+      MS_TRY(launch_potential_from_tables(a, stream_, tile, nb));
+      MS_TRY(cudaEventRecord(ev_pix_[buf], stream_));
+      launches += 2;
+    }
+    last_pot_sum_ = 2;
+    return MS_OK;
+  }
+
   // Whether element row r's Gaussian expansion holds for the loaded table:
   // checked once per row in FP64, with the kernel's FP32-rounded exponents and
   // weights, against vatom (U.cu:160-193) on 0.25 <= r <= 2.2365 A.
@@ -2808,6 +2846,8 @@ class Engine {
   // state
   int device_;
   cudaStream_t stream_ = nullptr;
+  cudaStream_t side_ = nullptr;
+  cudaEvent_t ev_tab_[2] = {nullptr, nullptr}, ev_pix_[2] = {nullptr, nullptr}, ev_fork_ = nullptr;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
   bool force_plain_ = false, full_table_ = false;
   int pot_mode_ = 0;
