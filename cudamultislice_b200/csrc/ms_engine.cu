@@ -2409,7 +2409,8 @@ class Engine {
     domain_ = 0;
     fd_state_ = false;
     have_waves_ = true;
-    prop_dz_ = -1.0f;
+    // (the propagator tables depend on dz, the wavelength and the grid only:
+    // they stay valid across re-initialisations, keyed by prop_dz_)
     return MS_OK;
   }
 
