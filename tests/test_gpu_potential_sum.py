@@ -113,3 +113,44 @@ def test_separable_is_default_and_forced_mode_errors(engine_cls):
     with pytest.raises(Exception):
         eng.SetPotentialSum(3)
     eng.close()
+
+
+def test_parameter_file_without_expansion_falls_back(engine_cls, oracle_mod, tmp_path):
+    """A parameterisation whose rows the compiled-in expansions do not match
+    (carbon's Lorentzian amplitudes scaled by 1.01) takes the per-sub-plane sum
+    for specimens holding that element, keeps the separable one for the
+    others, and refuses the separable sum when it is forced."""
+    from cudamultislice_b200 import structures as S
+
+    P = np.loadtxt(FPARAMS)
+    P[5, 0:6:2] *= 1.01
+    path = tmp_path / "fparams_modified.dat"
+    np.savetxt(path, P)
+    carbon = S.amorphous_carbon(size=(10.0, 10.0, 8.0), seed=4)
+    eng = engine_cls()
+    orc = oracle_mod.OracleSimulation()
+    for s in (eng, orc):
+        Z, x, y, z = carbon
+        s.SetAtoms(Z, x, y, z)
+        s.UploadBinnedAtoms()
+        s.GetParameterisation(str(path))
+        s.ApplyMicroscopeParameters(200.0, -500.0, 0.0, 0.0, 1e7, 0.1, 30.0, 20.0)
+        s.SetCalculationVariables(0.1, -500.0, 128, 128, s.GetSizeX(), s.GetSizeY(), s.GetSizeZ(), 2.0, 2.0)
+        s.PreCalculateFrequencies()
+        s.InitialiseWavefunctions(2.0)
+    assert eng.PotentialSum()[1] == 1
+    v = eng.PotentialSlice(0, 3)
+    assert eng.PotentialSum()[0] == 1
+    ref = orc.PotentialConventional(3)
+    assert np.linalg.norm(v - ref) / np.linalg.norm(ref) < TOL_SEP
+    eng.SetPotentialSum(2)
+    with pytest.raises(Exception):
+        eng.PotentialSlice(0, 3)
+    eng.close()
+    orc.close()
+    # silicon is unaffected by the carbon row
+    eng = engine_cls()
+    _setup(eng, S.silicon_110(1, 1, 2), 64, 0.1, 1.92)
+    eng.GetParameterisation(str(path))
+    assert eng.PotentialSum()[1] == 2
+    eng.close()
