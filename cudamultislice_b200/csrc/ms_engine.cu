@@ -275,21 +275,21 @@ class Engine {
     hy_.assign(y, y + n);
     hz_.assign(z, z + n);
     // bounding box as LoadAtomFile (U.cu:1326-1355): extreme atoms, +-2 A in FP32
-    size_t mx = 0, mnx = 0, my = 0, mny = 0, mz = 0, mnz = 0;
-    for (size_t i = 1; i < hx_.size(); ++i) {
-      if (hx_[i] > hx_[mx]) mx = i;
-      if (hy_[i] > hy_[my]) my = i;
-      if (hz_[i] > hz_[mz]) mz = i;
-      if (hx_[i] < hx_[mnx]) mnx = i;
-      if (hy_[i] < hy_[mny]) mny = i;
-      if (hz_[i] < hz_[mnz]) mnz = i;
+    float x1 = hx_[0], x0 = hx_[0], y1 = hy_[0], y0 = hy_[0], z1 = hz_[0], z0 = hz_[0];
+    for (int i = 1; i < n; ++i) {
+      x1 = std::max(x1, hx_[i]);
+      x0 = std::min(x0, hx_[i]);
+      y1 = std::max(y1, hy_[i]);
+      y0 = std::min(y0, hy_[i]);
+      z1 = std::max(z1, hz_[i]);
+      z0 = std::min(z0, hz_[i]);
     }
-    box_.MaxX = hx_[mx] + 2;
-    box_.MinX = hx_[mnx] - 2;
-    box_.MaxY = hy_[my] + 2;
-    box_.MinY = hy_[mny] - 2;
-    box_.MaxZ = hz_[mz] + 2;
-    box_.MinZ = hz_[mnz] - 2;
+    box_.MaxX = x1 + 2;
+    box_.MinX = x0 - 2;
+    box_.MaxY = y1 + 2;
+    box_.MinY = y0 - 2;
+    box_.MaxZ = z1 + 2;
+    box_.MinZ = z0 - 2;
     have_atoms_ = true;
     have_index_ = false;
     stack_valid_ = false;
