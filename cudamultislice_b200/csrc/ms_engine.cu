@@ -143,6 +143,8 @@ class Engine {
     for (cudaEvent_t* e : {&ev_tab_[0], &ev_tab_[1], &ev_pix_[0], &ev_pix_[1], &ev_fork_})
       MS_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     MS_TRY(d_loop_sync_.resize(2));
+    MS_TRY(d_pass_err_.resize(1));
+    MS_TRY(cudaMemsetAsync(d_pass_err_.p, 0, sizeof(int), stream_));
     MS_TRY(cudaHostAlloc((void**)&h_loop_err_, sizeof(unsigned int), cudaHostAllocDefault));
     *h_loop_err_ = 0;
     return MS_OK;
@@ -892,6 +894,7 @@ class Engine {
       MS_TRY(cudaMemcpyAsync(ew_.data(), d_psi_.p, N * sizeof(float2), cudaMemcpyDeviceToHost, stream_));
     }
     MS_TRY(cudaStreamSynchronize(stream_));
+    if (int rc = check_pass_err()) return rc;
     float mn = INFINITY, mx = -INFINITY;
     for (const float2& v : ew_) {
       const float a = std::sqrt(v.x * v.x + v.y * v.y);
@@ -925,7 +928,7 @@ class Engine {
     if (int rc = ensure_real()) return rc;
     MS_TRY(cudaMemcpyAsync(dst, d_psi_.p, sizeof(float2) * nx_ * ny_, cudaMemcpyDeviceToHost, stream_));
     MS_TRY(cudaStreamSynchronize(stream_));
-    return MS_OK;
+    return check_pass_err();
   }
 
   int alloc_tds() {
@@ -1837,6 +1840,8 @@ class Engine {
     MS_TRY(cudaStreamSynchronize(stream_));
     MS_TRY(cudaEventElapsedTime(&last_device_ms_, ev0_, ev1_));
     if (loop && use_fused() && *h_loop_err_ != 0) return loop_timeout_fail();
+    if (!loop && use_fused())
+      if (int rc = check_pass_err()) return rc;
     if (nslices) *nslices = S;
     return MS_OK;
   }
@@ -1983,6 +1988,7 @@ class Engine {
       MS_TRY(cudaMemcpyAsync(h_loop_err_, d_loop_sync_.p + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, stream_));
     MS_TRY(cudaStreamSynchronize(stream_));
     if (loop && *h_loop_err_ != 0) return loop_timeout_fail();
+    if (int rc = check_pass_err()) return rc;
     MS_TRY(cudaEventElapsedTime(total_ms, ev0_, ev1_));
     if (!row_ms || !col_ms) return MS_OK;  // no per-pass breakdown requested
     *row_ms = *col_ms = 0.0f;
@@ -2021,6 +2027,7 @@ class Engine {
       for (auto& e : ev)
         if (e) cudaEventDestroy(e);
       if (rc != MS_OK) return rc;
+      if (int rc2 = check_pass_err()) return rc2;
     }
     return MS_OK;
   }
@@ -2268,7 +2275,7 @@ class Engine {
     MS_TRY(cudaEventElapsedTime(&ms, ev0_, ev1_));
     launches += reps + 2;
     *us = 1000.0f * ms / (float)reps;
-    return MS_OK;
+    return check_pass_err();
   }
 
   // Checkpoint stride when none is set: every wave stored (no recomputation)
@@ -2567,7 +2574,19 @@ class Engine {
     b.in = in; b.out = out; b.tw = d_twy_[variant].p; b.px = d_px_.p; b.py = d_py_.p;
     b.kx = d_kx_.p; b.ky = d_ky_.p; b.kmax = kmax_; b.nx = nx_; b.ny = ny_; b.scale = 1.0f;
     band_limit_thresholds(kmax_, &b.k2_lt, &b.k2_le);
+    b.err = d_pass_err_.p;  // (long propagation columns: tensor-copy staging, see check_pass_err)
     return b;
+  }
+  // The column pass's tensor-copy waits are bounded: one that ran out set the
+  // error word (its columns were left as they were).  Checked where the
+  // handle synchronises after such passes (whole runs, timing, read-outs).
+  int check_pass_err() {
+    int h = 0;
+    MS_TRY(cudaMemcpyAsync(&h, d_pass_err_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    MS_TRY(cudaStreamSynchronize(stream_));
+    if (h == 0) return MS_OK;
+    MS_TRY(cudaMemsetAsync(d_pass_err_.p, 0, sizeof(int), stream_));
+    return fail(MS_ERR_CUDA, "a column pass's tensor-copy wait ran out (bounded at one second)");
   }
   // Row / column pass launchers with the plan tuned for `batch` instances.
   cudaError_t pass_a(PassAArgs a, int flags, int batch = 1) {
@@ -2968,6 +2987,7 @@ class Engine {
          *fd_graph_psim_end_ = nullptr;
   // persistent slice loop: barrier state [count, error], pinned error copy
   DevBuf<unsigned int> d_loop_sync_;
+  DevBuf<int> d_pass_err_;  // error word of the column pass's tensor-copy waits
   unsigned int* h_loop_err_ = nullptr;
   int loop_grid_ = 0, loop_grid_n_ = 0, loop_v_ = 0, forced_loop_ = -1, loop_tuned_for_ = -2;
   bool loop_off_ = false;

@@ -23,6 +23,33 @@ bool supported_length(int n) { return n >= 64 && n <= 4096 && (n & (n - 1)) == 0
 
 bool fused_supported(int nx, int ny) { return supported_length(nx) && supported_length(ny); }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link to
+// the driver library), looked up once.
+bool wave_tensor_map(CUtensorMap* m, const float2* base, int nx, int ny, int cb) {
+  using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                              const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static Encode encode = []() -> Encode {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return reinterpret_cast<Encode>(fn);
+  }();
+  if (!encode || ((uintptr_t)base & 15) || nx <= 0 || ny <= 0 || ((size_t)nx * sizeof(float2)) % 16 ||
+      (2 * cb * (int)sizeof(float)) % 16 || ny % kTmaRows)
+    return false;
+  // the wave as floats: 2 nx per row, ny rows; boxes of 2 cb floats x 256 rows
+  const cuuint64_t dims[2] = {(cuuint64_t)2 * nx, (cuuint64_t)ny};
+  const cuuint64_t strides[1] = {(cuuint64_t)nx * sizeof(float2)};
+  const cuuint32_t box[2] = {(cuuint32_t)(2 * cb), (cuuint32_t)kTmaRows};
+  const cuuint32_t elem[2] = {1, 1};
+  return encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float2*>(base), dims, strides, box, elem,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 void band_limit_thresholds(float kmax, float* k2_lt, float* k2_le) {
   auto first = [](float m, bool strict) {
     // smallest x >= 0 with sqrtf(x) >= m (strict: > m); sqrtf is monotone

@@ -98,6 +98,10 @@ struct PassBArgs {
   int accumulate;      // B_CTF_ADJ: add to out instead of storing
   int nx, ny;
   long long batch_stride_wave;
+  // columns of 2048 and 4096 points, propagation, one instance: when set, the
+  // column pass stages its columns through shared memory with tensor copies
+  // (k_pass_b_tma), and a wait for them that runs out sets this word
+  int* err;
 };
 
 // The smallest FP32 k^2 with sqrt_rn(k^2) >= kmax (k2_lt) and with

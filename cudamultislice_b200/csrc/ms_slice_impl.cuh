@@ -1,6 +1,8 @@
 // ms_slice_impl.cuh -- templates of the fused slice passes, instantiated per
 // line length in ms_slice_n*.cu (see ms_slice.cuh for the scheme).
 #pragma once
+#include <cuda.h>
+#include <stdint.h>
 #include <cmath>
 #include <mutex>
 
@@ -559,9 +561,166 @@ cudaError_t run_a(const PassAArgs& a, int batch, cudaStream_t s) {
   return launch_pdl(kernel, dim3(a.ny / lines, batch), lines * PL::P, smem, s, a);
 }
 
+// ---------------------------------------------------------------------------
+// Column pass for long columns (2048 and 4096 points) with tensor-copy
+// staging.  A CTA's CB columns are CB adjacent complex values of every row: a
+// warp's direct loads of them touch 32/CB rows each, and at these sizes the
+// L1's request rate, not HBM, bounded the pass.  Here one thread issues
+// 2-D tensor copies of [256 rows x CB columns] boxes into shared memory, the
+// threads take their points from there (a warp reads 256 contiguous bytes),
+// and the results leave the same way: written to shared memory in row order,
+// then stored by tensor copies.  The staging buffer doubles as the FFT's
+// exchange slots once every thread holds its points.
+// ---------------------------------------------------------------------------
+constexpr int kTmaRows = 256;  // rows per box (the tensor-copy box limit)
+
+MS_D unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+// Exchange slot length for CB interleaved columns (as col_slot: slots 16/CB
+// points apart mod 16).
+template <class PL, int CB>
+__host__ __device__ constexpr int tma_col_slot() {
+  return ((PL::N + PL::N / PL::R1 + 15) / 16) * 16 + 16 / CB;
+}
+template <class PL, int CB>
+__global__ void __launch_bounds__(CB * PL::P, CB == 2 ? 2 : 1)
+    k_pass_b_tma(PassBArgs a, const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout) {
+  constexpr int NY = PL::N, E = PL::E, P = PL::P, LS = tma_col_slot<PL, CB>();
+  constexpr int GS = CB * P;
+  static_assert(NY % kTmaRows == 0 && (2 * CB * 4) % 16 == 0, "boxes of 256 rows, 16-byte rows");
+  constexpr unsigned kBytes = (unsigned)(NY * CB * sizeof(float2));
+  extern __shared__ __align__(1024) float2 smem_tma[];
+  __shared__ __align__(8) unsigned long long mbar;
+  float2* stage = smem_tma;  // [NY][CB], then the exchange slots
+  const int c0 = blockIdx.x * CB;
+  const int cl = threadIdx.x % CB, t = threadIdx.x / CB;
+  const int col = c0 + cl;
+  float2* sm = smem_tma + cl * LS;
+  const unsigned bar = smem_u32(&mbar);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  pdl_launch_dependents();
+  pdl_wait();
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kBytes) : "memory");
+#pragma unroll 1
+    for (int k = 0; k < NY / kTmaRows; ++k) {
+      const unsigned dst = smem_u32(stage + (size_t)k * kTmaRows * CB);
+      asm volatile(
+          "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+              dst),
+          "l"(&tin), "r"(2 * c0), "r"(k * kTmaRows), "r"(bar)
+          : "memory");
+    }
+  }
+  // bounded wait for the tiles (one second of %globaltimer); a wait that runs
+  // out sets the error word and leaves this CTA's columns as they were
+  bool ok = true;
+  {
+    unsigned long long t0, tn;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    for (;;) {
+      unsigned done;
+      asm volatile(
+          "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+          : "=r"(done)
+          : "r"(bar)
+          : "memory");
+      if (done) break;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(tn));
+      if (tn - t0 > 1000000000ull) {
+        ok = false;
+        break;
+      }
+    }
+  }
+  if (!__syncthreads_and(ok)) {
+    if (threadIdx.x == 0) {
+      atomicExch(a.err, 1);
+      // give copies still in flight a bounded time to land before exiting
+      unsigned long long t0, tn;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+      for (;;) {
+        unsigned done;
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(bar)
+            : "memory");
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(tn));
+        if (done || tn - t0 > 1000000000ull) break;
+      }
+    }
+    __syncthreads();
+    return;
+  }
+  // this thread's E points of its column, rows t + P j
+  float2 v[E];
+#pragma unroll
+  for (int j = 0; j < E; ++j) v[j] = stage[(size_t)(t + P * j) * CB + cl];
+  __syncthreads();  // (the staging buffer becomes the exchange slots)
+
+#pragma unroll 1
+  for (int it = 0; it < 2; ++it) {
+    fft::line_fft<fft::PaddedPlan<PL>, GS>(v, sm, t, a.tw);
+    if (it == 0) col_mid<PL, B_PROPAGATE>(v, a, a.ky, a.py, col, t, 0);
+    fft::conj_all(v);
+  }
+  __syncthreads();  // (every exchange done: the buffer is the staging area again)
+#pragma unroll
+  for (int j = 0; j < E; ++j) stage[(size_t)(t + P * j) * CB + cl] = v[j];
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll 1
+    for (int k = 0; k < NY / kTmaRows; ++k) {
+      const unsigned src = smem_u32(stage + (size_t)k * kTmaRows * CB);
+      asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(&tout),
+                   "r"(2 * c0), "r"(k * kTmaRows), "r"(src)
+                   : "memory");
+    }
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");  // (the writes, not only the reads)
+  }
+}
+
+// 2-D tensor map of a wave [ny][nx] complex (as 2 nx floats per row) for
+// boxes of [256 rows x cb columns]; false if the driver entry point is missing
+// or the encoding fails.
+bool wave_tensor_map(CUtensorMap* m, const float2* base, int nx, int ny, int cb);
+
 template <class PL, int MODE>
 cudaError_t run_b(const PassBArgs& a, int batch, cudaStream_t s) {
   constexpr int CB = cols_per_cta<PL>();
+  constexpr int TCB = 2;  // columns per CTA of the staged pass (two CTAs per SM)
+  if constexpr (MODE == B_PROPAGATE && PL::N >= 2048 && TCB * PL::P <= 1024) {
+    if (a.err && batch == 1 && a.nx % TCB == 0 && a.ny == PL::N &&
+        ((uintptr_t)a.in % 16) == 0 && ((uintptr_t)a.out % 16) == 0 && ((size_t)a.nx * sizeof(float2)) % 16 == 0) {
+      CUtensorMap tin, tout;
+      if (wave_tensor_map(&tin, a.in, a.nx, a.ny, TCB) && wave_tensor_map(&tout, a.out, a.nx, a.ny, TCB)) {
+        const size_t stage = (size_t)PL::N * TCB * sizeof(float2);
+        const size_t slots = (size_t)TCB * tma_col_slot<PL, TCB>() * sizeof(float2);
+        const size_t smem = stage > slots ? stage : slots;
+        auto kernel = k_pass_b_tma<PL, TCB>;
+        static unsigned long long done = 0;
+        if (cudaError_t e = set_smem_once(done, kernel, smem)) return e;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(a.nx / TCB, 1);
+        cfg.blockDim = dim3(TCB * PL::P);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelEx(&cfg, kernel, a, tin, tout);
+      }
+    }
+  }
   const size_t smem = (size_t)CB * col_slot<PL>() * sizeof(float2) +
                       (col_stages_ky<PL, MODE>() ? (size_t)(PL::N + 1) / 2 * sizeof(float2) : 0) +
                       (col_stages_py<PL, MODE>() ? (size_t)PL::N * sizeof(float2) : 0);

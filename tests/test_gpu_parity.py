@@ -538,6 +538,32 @@ def test_non_square_grid(engine_cls, oracle_mod, shape, path):
     assert rel_l2(eng.Image(), orc.SimulateImage()) < TOL
 
 
+# ---------------------------------------------------------------- long columns (tensor-copy staging)
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("shape", [(256, 2048), (512, 4096), (2048, 2048)])
+def test_long_column_propagation(engine_cls, oracle_mod, shape, variant):
+    """Columns of 2048 and 4096 points: the propagation pass stages its
+    columns through shared memory with 2-D tensor copies.  Every FFT plan
+    variant, three slices, against the FP64 oracle."""
+    nx, ny = shape
+    Z, x, y, z = sto(2, 1)
+    eng = engine_cls()
+    eng.SetFFTPlan(variant)
+    orc = oracle_mod.OracleSimulation()
+    for s in (eng, orc):
+        s.SetAtoms(Z, x, y, z)
+        s.UploadBinnedAtoms()
+        s.GetParameterisation(FPARAMS)
+        s.ApplyMicroscopeParameters(200.0, -300.0, 0.0, 0.0, 1e7, 0.1, 30.0, 20.0)
+        s.SetCalculationVariables(0.02, -300.0, nx, ny, s.GetSizeX(), s.GetSizeY(), s.GetSizeZ(), 2.0, 2.0)
+        s.PreCalculateFrequencies()
+        s.InitialiseWavefunctions(1.9525)
+    for i in range(1, 4):
+        eng.MultisliceStepConventional(i)
+        orc.MultisliceStepConventional(i)
+    assert rel_l2(eng.ExitWave(), orc.Wave()) < TOL, (shape, variant)
+
+
 # ---------------------------------------------------------------- errors of the newer entry points
 def test_new_entry_point_errors(engine_cls, oracle_mod, tmp_path):
     from cudamultislice_b200 import MultisliceError, stem_raster_concurrent
