@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <functional>
 #include <memory>
 #include <new>
 #include <sstream>
@@ -120,9 +121,10 @@ class Engine {
     if (have_plan_) cufftDestroy(plan_);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
-    for (cudaEvent_t e : {ev_tab_[0], ev_tab_[1], ev_pix_[0], ev_pix_[1], ev_fork_})
+    for (cudaEvent_t e : {ev_tab_[0], ev_tab_[1], ev_pix_[0], ev_pix_[1], ev_fork_, ev_fork2_, ev_join_})
       if (e) cudaEventDestroy(e);
     if (side_) cudaStreamDestroy(side_);
+    if (pass_) cudaStreamDestroy(pass_);
     if (stream_) cudaStreamDestroy(stream_);
   }
 
@@ -140,7 +142,8 @@ class Engine {
     // the side stream of the potential stack (tables of the next slice while
     // the current slice's potential runs) and its ordering events
     MS_TRY(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
-    for (cudaEvent_t* e : {&ev_tab_[0], &ev_tab_[1], &ev_pix_[0], &ev_pix_[1], &ev_fork_})
+    MS_TRY(cudaStreamCreateWithFlags(&pass_, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&ev_tab_[0], &ev_tab_[1], &ev_pix_[0], &ev_pix_[1], &ev_fork_, &ev_fork2_, &ev_join_})
       MS_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     MS_TRY(d_loop_sync_.resize(2));
     MS_TRY(d_pass_err_.resize(1));
@@ -210,6 +213,10 @@ class Engine {
         stack_valid_ = false;
         fd_stack_valid_ = false;
         invalidate_graph();
+        return MS_OK;
+      case MS_OPT_BUILD_OVERLAP:
+        if (value != 0 && value != 1) return fail(MS_ERR_INVALID, "build overlap must be 0 or 1");
+        overlap_build_ = value == 1;
         return MS_OK;
       case MS_OPT_LOOP_WAIT_TEST:
         if (value < 0) return fail(MS_ERR_INVALID, "test arrivals must be >= 0");
@@ -1783,9 +1790,52 @@ class Engine {
     return MS_OK;
   }
 
+  // A whole conventional run whose potential stack must first be built:
+  // slice i's transmission and propagation (the fused passes, on the pass
+  // stream) run while the potentials of the next slices are built (on the
+  // handle's stream, tables on the side stream); the stack is kept for later
+  // runs, which replay the persistent loop.  Device time of the whole, build
+  // included, in last_device_ms_.
+  int run_conventional_streamed(int S, int* nslices) {
+    if (int rc = require_potential_inputs()) return rc;
+    if (int rc = ensure_prop_tables(convdz_)) return rc;
+    plan_for(1);  // (tuning synchronises: before the streams fork)
+    if (pot_tile_ < 0)
+      if (int rc = tune_pot_tile()) return rc;
+    const size_t N = (size_t)nx_ * ny_;
+    MS_TRY(d_stack_.resize(N * S));
+    MS_TRY(cudaEventRecord(ev0_, stream_));
+    MS_TRY(cudaEventRecord(ev_fork2_, stream_));
+    MS_TRY(cudaStreamWaitEvent(pass_, ev_fork2_, 0));
+    int rc = separable_stack(S, d_stack_.p, N, 1, nullptr, nullptr, 0, 0, [&](int it, cudaEvent_t done) -> int {
+      MS_TRY(cudaStreamWaitEvent(pass_, done, 0));
+      launches += 2;
+      return enqueue_fused_step(d_stack_.p + (size_t)(it - 1) * N, it == 1, pass_);
+    });
+    // join the pass stream (also on failure, so that the handle's stream
+    // orders after everything enqueued)
+    MS_TRY(cudaEventRecord(ev_join_, pass_));
+    MS_TRY(cudaStreamWaitEvent(stream_, ev_join_, 0));
+    if (rc != MS_OK) return rc;
+    MS_TRY(cudaEventRecord(ev1_, stream_));
+    MS_TRY(cudaStreamSynchronize(stream_));
+    MS_TRY(cudaEventElapsedTime(&last_device_ms_, ev0_, ev1_));
+    if (int rc2 = check_pass_err()) return rc2;
+    nstack_ = S;
+    stack_valid_ = true;
+    tstack_valid_ = false;
+    domain_ = 1;
+    if (nslices) *nslices = S;
+    return MS_OK;
+  }
+
   int run_conventional(int* nslices) {
     if (!have_waves_) return fail(MS_ERR_STATE, "wavefunctions not initialised");
     int S = 0;
+    if (use_fused() && pot_mode_ == 0 && overlap_build_ && have_index_ && have_fp_ && have_freq_) {
+      if (int rc = get_slices(true, &S)) return rc;
+      if (S >= 1 && (!stack_valid_ || nstack_ != S) && separable_ok()) return run_conventional_streamed(S, nslices);
+    }
     if (int rc = build_stack(&S)) return rc;
     if (int rc = ensure_prop_tables(convdz_)) return rc;
     const bool loop = use_loop();
@@ -2589,29 +2639,29 @@ class Engine {
     return fail(MS_ERR_CUDA, "a column pass's tensor-copy wait ran out (bounded at one second)");
   }
   // Row / column pass launchers with the plan tuned for `batch` instances.
-  cudaError_t pass_a(PassAArgs a, int flags, int batch = 1) {
+  cudaError_t pass_a(PassAArgs a, int flags, int batch = 1, cudaStream_t s = nullptr) {
     const int v = plan_for(batch).row;
     a.tw = d_twx_[v].p;
-    return launch_pass_a(a, v, flags, batch, stream_);
+    return launch_pass_a(a, v, flags, batch, s ? s : stream_);
   }
-  cudaError_t pass_b(PassBArgs b, int mode, int batch = 1) {
+  cudaError_t pass_b(PassBArgs b, int mode, int batch = 1, cudaStream_t s = nullptr) {
     const int v = plan_for(batch).col;
     b.tw = d_twy_[v].p;
-    return launch_pass_b(b, v, mode, batch, stream_);
+    return launch_pass_b(b, v, mode, batch, s ? s : stream_);
   }
 
   // Enqueue one fused conventional step on the stream (no host sync, no
   // allocation or copy: safe inside stream capture once the propagator
   // tables exist).
-  int enqueue_fused_step(const float* V, bool first) {
+  int enqueue_fused_step(const float* V, bool first, cudaStream_t s = nullptr) {
     fd_state_ = false;
     // iteration 1 starts from the initial wave (real space); later ones from
     // the current wave in whichever domain it is held
     PassAArgs a = passa_args(first ? d_psi0_.p : d_psi_.p, d_psi_.p, 0);
     a.V = V;
     const int fl = (first || domain_ == 0) ? (A_MULT_T | A_FWD) : (A_INV | A_MULT_T | A_FWD);
-    MS_TRY(pass_a(a, fl, 1));
-    MS_TRY(pass_b(passb_args(d_psi_.p, d_psi_.p, 0), B_PROPAGATE, 1));
+    MS_TRY(pass_a(a, fl, 1, s));
+    MS_TRY(pass_b(passb_args(d_psi_.p, d_psi_.p, 0), B_PROPAGATE, 1, s));
     domain_ = 1;
     return MS_OK;
   }
@@ -2665,7 +2715,8 @@ class Engine {
   // same buffer; potential(it) after tables(it).  The side stream joins the
   // handle's stream through the last potential's dependence on its tables.
   int separable_stack(int S, float* out, size_t N, int nb, const float4* atoms = nullptr, const int* off = nullptr,
-                      long long b_atoms = 0, long long b_off = 0) {
+                      long long b_atoms = 0, long long b_off = 0,
+                      const std::function<int(int, cudaEvent_t)>& after_slice = nullptr) {
     if (pot_tile_ < 0 && !capturing_)
       if (int rc = tune_pot_tile()) return rc;
     const int tile = std::min(std::max(pot_tile_, 0), potential_tiles_separable() - 1);
@@ -2692,6 +2743,8 @@ class Engine {
       MS_TRY(launch_potential_from_tables(a, stream_, tile, nb));
       MS_TRY(cudaEventRecord(ev_pix_[buf], stream_));
       launches += 2;
+      if (after_slice)
+        if (int rc = after_slice(it, ev_pix_[buf])) return rc;
     }
     last_pot_sum_ = 2;
     return MS_OK;
@@ -2896,7 +2949,10 @@ class Engine {
   int device_;
   cudaStream_t stream_ = nullptr;
   cudaStream_t side_ = nullptr;
+  cudaStream_t pass_ = nullptr;  // slice passes overlapping the stack build (run_conventional_streamed)
   cudaEvent_t ev_tab_[2] = {nullptr, nullptr}, ev_pix_[2] = {nullptr, nullptr}, ev_fork_ = nullptr;
+  cudaEvent_t ev_fork2_ = nullptr, ev_join_ = nullptr;
+  bool overlap_build_ = true;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
   bool force_plain_ = false, full_table_ = false;
   int pot_mode_ = 0;

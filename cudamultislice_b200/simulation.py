@@ -116,6 +116,11 @@ class ManagedMultisliceSimulation:
         """Conventional potential kernel tile: -1 tuned (default), 0/1/2 = 32x8, 16x16, 64x4 pixels."""
         self._chk(self._L.ms_set_option(self._h, 9, int(tile)))
 
+    def SetBuildOverlap(self, on: bool):
+        """RunConventional with a stack to build: overlap each slice's passes
+        with the next slices' potentials (True, the default) or build first."""
+        self._chk(self._L.ms_set_option(self._h, 11, 1 if on else 0))
+
     def SetPotentialSum(self, mode: int):
         """Conventional potential's sub-plane sum: 0 separable where it applies
         (default), 1 per (pixel, atom, sub-plane), 2 separable or an error."""

@@ -94,7 +94,7 @@ enum {
                                per grid (default); per-sub-plane kernel 0, 1, 2 = 32 x 8,
                                16 x 16, 64 x 4 pixels; separable kernel 0..3 = 16 x 32,
                                32 x 16 (two pixels per thread), 16 x 64, 32 x 32 (four) */
-  MS_OPT_POTENTIAL_SUM = 10 /* how the conventional potential sums an atom's 20 sub-planes
+  MS_OPT_POTENTIAL_SUM = 10, /* how the conventional potential sums an atom's 20 sub-planes
                                (binnedAtomPKernel3, U.cu:582-653): 0 = separable where it
                                applies (default), else per sub-plane; 1 = per (pixel, atom,
                                sub-plane), vatom evaluated term by term; 2 = separable, or
@@ -103,6 +103,12 @@ enum {
                                to 2e-7 of v on 0.25..2.2365 A), so that an atom's sub-plane
                                sum costs 12 exponentials per pixel; the same sub-planes pass
                                the reference's FP32 cut-off test as term by term. */
+  MS_OPT_BUILD_OVERLAP = 11 /* ms_run_conventional when the potential stack must be built:
+                               1 = run each slice's fused passes on a second stream while the
+                               next slices' potentials are built (default; separable
+                               potential, fused path); 0 = build the stack, then run the
+                               slices.  Runs over a resident stack replay the persistent
+                               loop either way. */
 };
 
 /* ---- lifecycle ---- */

@@ -215,6 +215,37 @@ def test_exit_wave_c1_srtio3_256(engine_cls, oracle_mod):
     assert rel_l2(eng.Image(), img) < TOL
 
 
+@pytest.mark.parametrize("n", [128, 512, 1024])
+def test_run_with_build_overlap(engine_cls, oracle_mod, n):
+    """A run whose potential stack must be built overlaps each slice's passes
+    with the next slices' potentials (default); it equals the build-first run
+    and the oracle, and leaves the stack resident: later runs replay the
+    persistent loop (one launch on 512^2 and 1024^2 once the loop variant is
+    tuned, in the first of them)."""
+    atoms = sto(4, 6)
+    ps = 3.905 * 4 / n
+    waves = {}
+    for overlap in (True, False):
+        eng, orc = make_pair(engine_cls, oracle_mod, atoms, n, ps)
+        eng.SetBuildOverlap(overlap)
+        S = eng.RunConventional()
+        waves[overlap] = eng.ExitWave()
+        if overlap:
+            psi = orc.run_conventional()
+            assert S == orc.GetSlices(True)
+            assert rel_l2(waves[True], psi) < TOL
+            for rep in range(2):
+                eng.InitialiseWavefunctions(1.9525)
+                l0 = eng.LaunchCount()
+                eng.RunConventional()
+                if n >= 512 and rep == 1:
+                    assert eng.LaunchCount() - l0 == 1
+                assert rel_l2(eng.ExitWave(), psi) < TOL
+        eng.close()
+        orc.close()
+    assert rel_l2(waves[True], waves[False]) < 3e-6
+
+
 def test_run_equals_step_loop(engine_cls, oracle_mod):
     eng, _ = make_pair(engine_cls, oracle_mod, sto(2, 5), 256, 0.05)
     S = eng.GetSlices(True)

@@ -23,10 +23,19 @@ def rel_l2(a, b):
 
 @pytest.fixture(scope="module")
 def engine_cls():
+    """Engines that build the potential stack before the slices, so that the
+    first RunConventional runs the persistent loop too (by default a run with
+    a stack to build overlaps the build with per-pass slice steps)."""
     from cudamultislice_b200 import ManagedMultisliceSimulation, build
 
     build.build(verbose=False)
-    return ManagedMultisliceSimulation
+
+    def make(*args, **kw):
+        e = ManagedMultisliceSimulation(*args, **kw)
+        e.SetBuildOverlap(False)
+        return e
+
+    return make
 
 
 def setup(s, atoms, n, ps, kV=200.0, df=-500.0, stem=False):
