@@ -855,7 +855,8 @@ def main():
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(psi.nbytes),
                 "note": "host clock around the synchronous C-ABI calls: atoms in from pinned host memory, "
-                        "binning, potential stack (100 slices), slice loop, exit wave out to pinned host memory"},
+                        "binning, potential stack (100 slices) built while each built slice is stepped on a second stream, "
+                        "exit wave out to pinned host memory"},
     }
 
     if rank == 0:  # secondary legs: one GPU, after the collective timing

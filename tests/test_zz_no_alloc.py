@@ -97,3 +97,49 @@ def test_noalloc_refuses_oversized_requests():
         rc = L.ms_build_atom_index_noalloc(fake, fake, fake, fake, 10, b.ctypes.data_as(C.c_void_p), fake, fake,
                                            1 << 22, C.byref(nz), None)
         assert rc == 1, bad
+
+
+def test_noalloc_index_in_graph_capture():
+    """The entry point enqueues into a CUDA graph: after one warm-up call (which
+    looks up the scratch array's device address outside any capture), a call
+    captured on a non-default stream records the index build, and each replay
+    of the graph rebuilds the index of ms_upload_binned_atoms bit for bit."""
+    import torch
+    from cudamultislice_b200 import _lib, structures
+
+    L = _lib.lib()
+    atoms = structures.random_atoms(20000, size=(31.0, 29.0, 40.0), Zs=(6, 8, 38), seed=7)
+    _noalloc_index(L, atoms)  # warm-up, outside capture
+    want = _reference_index(atoms)
+    Z, x, y, z = atoms
+    n = len(Z)
+    box = _box(x, y, z)
+    nz = int(np.ceil(box[4] - box[5]))
+    nz += nz == 0
+    dev = torch.device("cuda", 0)
+    dZ = torch.from_numpy(np.ascontiguousarray(Z, np.int32)).to(dev)
+    dx, dy, dzz = (torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(dev) for a in (x, y, z))
+    d_atoms = torch.zeros(4 * n, dtype=torch.float32, device=dev)
+    d_off = torch.zeros(nz * 2500 + 1, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+    stream = torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    nz_out = C.c_int(-1)
+    with torch.cuda.graph(graph, stream=stream):
+        rc = L.ms_build_atom_index_noalloc(dZ.data_ptr(), dx.data_ptr(), dy.data_ptr(), dzz.data_ptr(), n,
+                                           box.ctypes.data_as(C.c_void_p), d_atoms.data_ptr(), d_off.data_ptr(),
+                                           d_off.numel(), C.byref(nz_out), C.c_void_p(stream.cuda_stream))
+    assert rc == 0, L.ms_last_error(None).decode()
+    assert nz_out.value == nz
+    for _ in range(2):  # the captured work, not the capture, fills the buffers
+        d_off.fill_(-7)
+        d_atoms.zero_()
+        graph.replay()
+        torch.cuda.synchronize()
+        at = d_atoms.cpu().numpy().reshape(n, 4)
+        got = (d_off.cpu().numpy(), at[:, 3].copy().view(np.int32), at[:, 0].copy(), at[:, 1].copy(),
+               at[:, 2].copy())
+        for g, w in zip(got, want):
+            assert g.dtype == w.dtype and g.shape == w.shape
+            assert np.array_equal(g, w)
+    del graph
