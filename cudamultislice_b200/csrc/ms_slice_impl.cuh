@@ -576,6 +576,56 @@ constexpr int kTmaRows = 256;  // rows per box (the tensor-copy box limit)
 
 MS_D unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
+// Waits for the phase of the mbarrier at shared address bar with the given
+// parity to complete, for at most one second of %globaltimer; false if the
+// wait ran out.
+MS_D bool mbar_wait_bounded(unsigned bar, unsigned parity) {
+  unsigned long long t0, tn;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+  for (;;) {
+    unsigned done;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(tn));
+    if (tn - t0 > 1000000000ull) return false;
+  }
+}
+
+// Tensor copies of CB adjacent columns (all NY rows, boxes of 256 rows) from
+// the wave into dst, completing on the mbarrier at bar (one thread).
+template <int NY, int CB>
+MS_D void tma_load_columns(const CUtensorMap* tin, float2* dst, int c0, unsigned bar) {
+  constexpr unsigned kBytes = (unsigned)(NY * CB * sizeof(float2));
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kBytes) : "memory");
+#pragma unroll 1
+  for (int k = 0; k < NY / kTmaRows; ++k) {
+    const unsigned d = smem_u32(dst + (size_t)k * kTmaRows * CB);
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            d),
+        "l"(tin), "r"(2 * c0), "r"(k * kTmaRows), "r"(bar)
+        : "memory");
+  }
+}
+
+// Tensor copies of CB adjacent columns from src back to the wave, committed as
+// one bulk group (one thread).
+template <int NY, int CB>
+MS_D void tma_store_columns(const CUtensorMap* tout, const float2* src, int c0) {
+#pragma unroll 1
+  for (int k = 0; k < NY / kTmaRows; ++k) {
+    const unsigned sa = smem_u32(src + (size_t)k * kTmaRows * CB);
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(tout),
+                 "r"(2 * c0), "r"(k * kTmaRows), "r"(sa)
+                 : "memory");
+  }
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
 // Exchange slot length for CB interleaved columns (as col_slot: slots 16/CB
 // points apart mod 16).
 template <class PL, int CB>
@@ -588,7 +638,6 @@ __global__ void __launch_bounds__(CB * PL::P, CB == 2 ? 2 : 1)
   constexpr int NY = PL::N, E = PL::E, P = PL::P, LS = tma_col_slot<PL, CB>();
   constexpr int GS = CB * P;
   static_assert(NY % kTmaRows == 0 && (2 * CB * 4) % 16 == 0, "boxes of 256 rows, 16-byte rows");
-  constexpr unsigned kBytes = (unsigned)(NY * CB * sizeof(float2));
   extern __shared__ __align__(1024) float2 smem_tma[];
   __shared__ __align__(8) unsigned long long mbar;
   float2* stage = smem_tma;  // [NY][CB], then the exchange slots
@@ -604,55 +653,14 @@ __global__ void __launch_bounds__(CB * PL::P, CB == 2 ? 2 : 1)
   __syncthreads();
   pdl_launch_dependents();
   pdl_wait();
-  if (threadIdx.x == 0) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kBytes) : "memory");
-#pragma unroll 1
-    for (int k = 0; k < NY / kTmaRows; ++k) {
-      const unsigned dst = smem_u32(stage + (size_t)k * kTmaRows * CB);
-      asm volatile(
-          "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-              dst),
-          "l"(&tin), "r"(2 * c0), "r"(k * kTmaRows), "r"(bar)
-          : "memory");
-    }
-  }
+  if (threadIdx.x == 0) tma_load_columns<NY, CB>(&tin, stage, c0, bar);
   // bounded wait for the tiles (one second of %globaltimer); a wait that runs
   // out sets the error word and leaves this CTA's columns as they were
-  bool ok = true;
-  {
-    unsigned long long t0, tn;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
-    for (;;) {
-      unsigned done;
-      asm volatile(
-          "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
-          : "=r"(done)
-          : "r"(bar)
-          : "memory");
-      if (done) break;
-      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(tn));
-      if (tn - t0 > 1000000000ull) {
-        ok = false;
-        break;
-      }
-    }
-  }
+  const bool ok = mbar_wait_bounded(bar, 0);
   if (!__syncthreads_and(ok)) {
     if (threadIdx.x == 0) {
       atomicExch(a.err, 1);
-      // give copies still in flight a bounded time to land before exiting
-      unsigned long long t0, tn;
-      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
-      for (;;) {
-        unsigned done;
-        asm volatile(
-            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
-            : "=r"(done)
-            : "r"(bar)
-            : "memory");
-        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(tn));
-        if (done || tn - t0 > 1000000000ull) break;
-      }
+      mbar_wait_bounded(bar, 0);  // copies still in flight: a bounded time to land
     }
     __syncthreads();
     return;
@@ -675,14 +683,7 @@ __global__ void __launch_bounds__(CB * PL::P, CB == 2 ? 2 : 1)
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   __syncthreads();
   if (threadIdx.x == 0) {
-#pragma unroll 1
-    for (int k = 0; k < NY / kTmaRows; ++k) {
-      const unsigned src = smem_u32(stage + (size_t)k * kTmaRows * CB);
-      asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(&tout),
-                   "r"(2 * c0), "r"(k * kTmaRows), "r"(src)
-                   : "memory");
-    }
-    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    tma_store_columns<NY, CB>(&tout, stage, c0);
     asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");  // (the writes, not only the reads)
   }
 }
@@ -701,6 +702,9 @@ cudaError_t run_b(const PassBArgs& a, int batch, cudaStream_t s) {
         ((uintptr_t)a.in % 16) == 0 && ((uintptr_t)a.out % 16) == 0 && ((size_t)a.nx * sizeof(float2)) % 16 == 0) {
       CUtensorMap tin, tout;
       if (wave_tensor_map(&tin, a.in, a.nx, a.ny, TCB) && wave_tensor_map(&tout, a.out, a.nx, a.ny, TCB)) {
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
         const size_t stage = (size_t)PL::N * TCB * sizeof(float2);
         const size_t slots = (size_t)TCB * tma_col_slot<PL, TCB>() * sizeof(float2);
         const size_t smem = stage > slots ? stage : slots;
@@ -712,9 +716,6 @@ cudaError_t run_b(const PassBArgs& a, int batch, cudaStream_t s) {
         cfg.blockDim = dim3(TCB * PL::P);
         cfg.dynamicSmemBytes = smem;
         cfg.stream = s;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-        attr[0].val.programmaticStreamSerializationAllowed = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         return cudaLaunchKernelEx(&cfg, kernel, a, tin, tout);
