@@ -121,9 +121,10 @@ class Engine {
     if (have_plan_) cufftDestroy(plan_);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
-    for (cudaEvent_t e : {ev_tab_[0], ev_tab_[1], ev_pix_[0], ev_pix_[1], ev_fork_, ev_fork2_, ev_join_})
+    for (cudaEvent_t e : {ev_tab_[0], ev_tab_[1], ev_pix_[0], ev_pix_[1], ev_fork_, ev_fork2_, ev_join_, ev_pjoin_})
       if (e) cudaEventDestroy(e);
     if (side_) cudaStreamDestroy(side_);
+    if (pix2_) cudaStreamDestroy(pix2_);
     if (pass_) cudaStreamDestroy(pass_);
     if (stream_) cudaStreamDestroy(stream_);
   }
@@ -142,8 +143,10 @@ class Engine {
     // the side stream of the potential stack (tables of the next slice while
     // the current slice's potential runs) and its ordering events
     MS_TRY(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+    MS_TRY(cudaStreamCreateWithFlags(&pix2_, cudaStreamNonBlocking));
     MS_TRY(cudaStreamCreateWithFlags(&pass_, cudaStreamNonBlocking));
-    for (cudaEvent_t* e : {&ev_tab_[0], &ev_tab_[1], &ev_pix_[0], &ev_pix_[1], &ev_fork_, &ev_fork2_, &ev_join_})
+    for (cudaEvent_t* e : {&ev_tab_[0], &ev_tab_[1], &ev_pix_[0], &ev_pix_[1], &ev_fork_, &ev_fork2_, &ev_join_,
+                           &ev_pjoin_})
       MS_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     MS_TRY(d_loop_sync_.resize(2));
     MS_TRY(d_pass_err_.resize(1));
@@ -2724,29 +2727,47 @@ class Engine {
     if (d_tab_.n < 2 * per) MS_TRY(d_tab_.resize(2 * per));
     MS_TRY(cudaEventRecord(ev_fork_, stream_));
     MS_TRY(cudaStreamWaitEvent(side_, ev_fork_, 0));
-    for (int it = 1; it <= S; ++it) {
-      const int buf = it & 1;
-      PotArgs a = pot_args(POT_CONVENTIONAL, it, out + (size_t)(it - 1) * N);
-      a.tab = d_tab_.p + buf * per;
-      if (atoms) {
-        a.atoms = atoms;
-        a.off = off;
-        a.b_atoms = b_atoms;
-        a.b_off = b_off;
-        a.b_tab = (long long)natoms_ * kTabStride;
-        a.b_V = (long long)S * N;
-      }
-      if (it >= 3) MS_TRY(cudaStreamWaitEvent(side_, ev_pix_[buf], 0));
-      MS_TRY(launch_atom_tables(a, side_, nb));
-      MS_TRY(cudaEventRecord(ev_tab_[buf], side_));
-      MS_TRY(cudaStreamWaitEvent(stream_, ev_tab_[buf], 0));
-      MS_TRY(launch_potential_from_tables(a, stream_, tile, nb));
-      MS_TRY(cudaEventRecord(ev_pix_[buf], stream_));
-      launches += 2;
-      if (after_slice)
-        if (int rc = after_slice(it, ev_pix_[buf])) return rc;
-    }
+    MS_TRY(cudaStreamWaitEvent(pix2_, ev_fork_, 0));
+    int rc = MS_OK;
+    for (int it = 1; it <= S && rc == MS_OK; ++it)
+      rc = separable_slice(it, out, N, nb, per, tile, atoms, off, b_atoms, b_off, S, after_slice);
+    // join the even slices' stream (also on failure, so that the handle's
+    // stream orders after everything enqueued)
+    MS_TRY(cudaEventRecord(ev_pjoin_, pix2_));
+    MS_TRY(cudaStreamWaitEvent(stream_, ev_pjoin_, 0));
+    if (rc != MS_OK) return rc;
     last_pot_sum_ = 2;
+    return MS_OK;
+  }
+  // One slice of separable_stack: its atom tables on the side stream (into
+  // table buffer it & 1, once the potential of slice it - 2, which read that
+  // buffer, is done), then its potential, odd slices on the handle's stream
+  // and even ones on pix2_: consecutive slices are independent, and on two
+  // streams the last CTAs of one overlap the first of the next.
+  int separable_slice(int it, float* out, size_t N, int nb, size_t per, int tile, const float4* atoms,
+                      const int* off, long long b_atoms, long long b_off, int S,
+                      const std::function<int(int, cudaEvent_t)>& after_slice) {
+    const int buf = it & 1;
+    cudaStream_t ps = (it & 1) ? stream_ : pix2_;
+    PotArgs a = pot_args(POT_CONVENTIONAL, it, out + (size_t)(it - 1) * N);
+    a.tab = d_tab_.p + buf * per;
+    if (atoms) {
+      a.atoms = atoms;
+      a.off = off;
+      a.b_atoms = b_atoms;
+      a.b_off = b_off;
+      a.b_tab = (long long)natoms_ * kTabStride;
+      a.b_V = (long long)S * N;
+    }
+    if (it >= 3) MS_TRY(cudaStreamWaitEvent(side_, ev_pix_[buf], 0));
+    MS_TRY(launch_atom_tables(a, side_, nb));
+    MS_TRY(cudaEventRecord(ev_tab_[buf], side_));
+    MS_TRY(cudaStreamWaitEvent(ps, ev_tab_[buf], 0));
+    MS_TRY(launch_potential_from_tables(a, ps, tile, nb));
+    MS_TRY(cudaEventRecord(ev_pix_[buf], ps));
+    launches += 2;
+    if (after_slice)
+      if (int rc = after_slice(it, ev_pix_[buf])) return rc;
     return MS_OK;
   }
 
@@ -2949,9 +2970,10 @@ class Engine {
   int device_;
   cudaStream_t stream_ = nullptr;
   cudaStream_t side_ = nullptr;
+  cudaStream_t pix2_ = nullptr;  // potentials of the even slices of a separable stack
   cudaStream_t pass_ = nullptr;  // slice passes overlapping the stack build (run_conventional_streamed)
   cudaEvent_t ev_tab_[2] = {nullptr, nullptr}, ev_pix_[2] = {nullptr, nullptr}, ev_fork_ = nullptr;
-  cudaEvent_t ev_fork2_ = nullptr, ev_join_ = nullptr;
+  cudaEvent_t ev_fork2_ = nullptr, ev_join_ = nullptr, ev_pjoin_ = nullptr;
   bool overlap_build_ = true;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
   bool force_plain_ = false, full_table_ = false;

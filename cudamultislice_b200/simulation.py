@@ -113,7 +113,8 @@ class ManagedMultisliceSimulation:
         return v.value, c.value, g.value
 
     def SetPotentialTile(self, tile: int):
-        """Conventional potential kernel tile: -1 tuned (default), 0/1/2 = 32x8, 16x16, 64x4 pixels."""
+        """Conventional potential kernel tile: -1 tuned (default); separable kernel
+        0..3 = 16x32, 32x16, 16x64, 32x32 pixels, per sub-plane 0..2 = 32x8, 16x16, 64x4."""
         self._chk(self._L.ms_set_option(self._h, 9, int(tile)))
 
     def SetBuildOverlap(self, on: bool):
