@@ -121,10 +121,14 @@ class Engine {
     if (have_plan_) cufftDestroy(plan_);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
-    for (cudaEvent_t e : {ev_tab_[0], ev_tab_[1], ev_pix_[0], ev_pix_[1], ev_fork_, ev_fork2_, ev_join_, ev_pjoin_})
+    for (int k = 0; k < kPixStreams; ++k)
+      for (cudaEvent_t e : {ev_tab_[k], ev_pix_[k], ev_pjoin_[k]})
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : {ev_fork_, ev_fork2_, ev_join_})
       if (e) cudaEventDestroy(e);
     if (side_) cudaStreamDestroy(side_);
-    if (pix2_) cudaStreamDestroy(pix2_);
+    for (int k = 1; k < kPixStreams; ++k)
+      if (pix_[k]) cudaStreamDestroy(pix_[k]);
     if (pass_) cudaStreamDestroy(pass_);
     if (stream_) cudaStreamDestroy(stream_);
   }
@@ -143,10 +147,13 @@ class Engine {
     // the side stream of the potential stack (tables of the next slice while
     // the current slice's potential runs) and its ordering events
     MS_TRY(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
-    MS_TRY(cudaStreamCreateWithFlags(&pix2_, cudaStreamNonBlocking));
+    pix_[0] = stream_;
+    for (int k = 1; k < kPixStreams; ++k) MS_TRY(cudaStreamCreateWithFlags(&pix_[k], cudaStreamNonBlocking));
     MS_TRY(cudaStreamCreateWithFlags(&pass_, cudaStreamNonBlocking));
-    for (cudaEvent_t* e : {&ev_tab_[0], &ev_tab_[1], &ev_pix_[0], &ev_pix_[1], &ev_fork_, &ev_fork2_, &ev_join_,
-                           &ev_pjoin_})
+    for (int k = 0; k < kPixStreams; ++k)
+      for (cudaEvent_t* e : {&ev_tab_[k], &ev_pix_[k], &ev_pjoin_[k]})
+        MS_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    for (cudaEvent_t* e : {&ev_fork_, &ev_fork2_, &ev_join_})
       MS_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     MS_TRY(d_loop_sync_.resize(2));
     MS_TRY(d_pass_err_.resize(1));
@@ -1814,7 +1821,7 @@ class Engine {
       MS_TRY(cudaStreamWaitEvent(pass_, done, 0));
       launches += 2;
       return enqueue_fused_step(d_stack_.p + (size_t)(it - 1) * N, it == 1, pass_);
-    });
+    }, 2);
     // join the pass stream (also on failure, so that the handle's stream
     // orders after everything enqueued)
     MS_TRY(cudaEventRecord(ev_join_, pass_));
@@ -2712,43 +2719,49 @@ class Engine {
 
   // Separable potentials of slices 1..S into out + (it - 1) * N (and, for a
   // batch of nb indices set up as in tds_potential_batch, instance k at
-  // out + k * S * N), two table buffers deep: the tables of slice it + 1 are
-  // built on the side stream while slice it's potential runs on the handle's
-  // stream.  Event order: tables(it) after potential(it - 2), which read the
-  // same buffer; potential(it) after tables(it).  The side stream joins the
-  // handle's stream through the last potential's dependence on its tables.
+  // out + k * S * N), npix table buffers deep: the tables of the next slices
+  // are built on the side stream while earlier slices' potentials run.  Slice
+  // it's potential runs on pixel stream it % npix (stream 0 is the handle's):
+  // consecutive slices are independent, and on several streams the last CTAs
+  // of one launch overlap the first of the next (three streams for a stack
+  // alone; two when slice passes run beside the build, which a third
+  // stream's potentials would crowd out).  Event order: tables(it) after
+  // potential(it - npix), which read the same buffer; potential(it) after
+  // tables(it).  The side stream joins the handle's stream through the last
+  // potentials' dependence on their tables.
   int separable_stack(int S, float* out, size_t N, int nb, const float4* atoms = nullptr, const int* off = nullptr,
                       long long b_atoms = 0, long long b_off = 0,
-                      const std::function<int(int, cudaEvent_t)>& after_slice = nullptr) {
+                      const std::function<int(int, cudaEvent_t)>& after_slice = nullptr, int npix = kPixStreams) {
+    npix = std::min(std::max(npix, 1), kPixStreams);
     if (pot_tile_ < 0 && !capturing_)
       if (int rc = tune_pot_tile()) return rc;
     const int tile = std::min(std::max(pot_tile_, 0), potential_tiles_separable() - 1);
     const size_t per = (size_t)nb * natoms_ * kTabStride;  // one buffer
-    if (d_tab_.n < 2 * per) MS_TRY(d_tab_.resize(2 * per));
+    if (d_tab_.n < npix * per) MS_TRY(d_tab_.resize(npix * per));
     MS_TRY(cudaEventRecord(ev_fork_, stream_));
     MS_TRY(cudaStreamWaitEvent(side_, ev_fork_, 0));
-    MS_TRY(cudaStreamWaitEvent(pix2_, ev_fork_, 0));
+    for (int k = 1; k < npix; ++k) MS_TRY(cudaStreamWaitEvent(pix_[k], ev_fork_, 0));
     int rc = MS_OK;
     for (int it = 1; it <= S && rc == MS_OK; ++it)
-      rc = separable_slice(it, out, N, nb, per, tile, atoms, off, b_atoms, b_off, S, after_slice);
-    // join the even slices' stream (also on failure, so that the handle's
+      rc = separable_slice(it, out, N, nb, per, tile, atoms, off, b_atoms, b_off, S, after_slice, npix);
+    // join the other pixel streams (also on failure, so that the handle's
     // stream orders after everything enqueued)
-    MS_TRY(cudaEventRecord(ev_pjoin_, pix2_));
-    MS_TRY(cudaStreamWaitEvent(stream_, ev_pjoin_, 0));
+    for (int k = 1; k < npix; ++k) {
+      MS_TRY(cudaEventRecord(ev_pjoin_[k], pix_[k]));
+      MS_TRY(cudaStreamWaitEvent(stream_, ev_pjoin_[k], 0));
+    }
     if (rc != MS_OK) return rc;
     last_pot_sum_ = 2;
     return MS_OK;
   }
   // One slice of separable_stack: its atom tables on the side stream (into
-  // table buffer it & 1, once the potential of slice it - 2, which read that
-  // buffer, is done), then its potential, odd slices on the handle's stream
-  // and even ones on pix2_: consecutive slices are independent, and on two
-  // streams the last CTAs of one overlap the first of the next.
+  // table buffer it % npix, once the potential of slice it - npix, which read
+  // that buffer, is done), then its potential on pixel stream it % npix.
   int separable_slice(int it, float* out, size_t N, int nb, size_t per, int tile, const float4* atoms,
                       const int* off, long long b_atoms, long long b_off, int S,
-                      const std::function<int(int, cudaEvent_t)>& after_slice) {
-    const int buf = it & 1;
-    cudaStream_t ps = (it & 1) ? stream_ : pix2_;
+                      const std::function<int(int, cudaEvent_t)>& after_slice, int npix) {
+    const int buf = it % npix;
+    cudaStream_t ps = pix_[buf];
     PotArgs a = pot_args(POT_CONVENTIONAL, it, out + (size_t)(it - 1) * N);
     a.tab = d_tab_.p + buf * per;
     if (atoms) {
@@ -2759,7 +2772,7 @@ class Engine {
       a.b_tab = (long long)natoms_ * kTabStride;
       a.b_V = (long long)S * N;
     }
-    if (it >= 3) MS_TRY(cudaStreamWaitEvent(side_, ev_pix_[buf], 0));
+    if (it > npix) MS_TRY(cudaStreamWaitEvent(side_, ev_pix_[buf], 0));
     MS_TRY(launch_atom_tables(a, side_, nb));
     MS_TRY(cudaEventRecord(ev_tab_[buf], side_));
     MS_TRY(cudaStreamWaitEvent(ps, ev_tab_[buf], 0));
@@ -2970,10 +2983,12 @@ class Engine {
   int device_;
   cudaStream_t stream_ = nullptr;
   cudaStream_t side_ = nullptr;
-  cudaStream_t pix2_ = nullptr;  // potentials of the even slices of a separable stack
+  // pixel streams of a separable stack (0: the handle's stream)
+  static constexpr int kPixStreams = 3;
+  cudaStream_t pix_[kPixStreams] = {};
   cudaStream_t pass_ = nullptr;  // slice passes overlapping the stack build (run_conventional_streamed)
-  cudaEvent_t ev_tab_[2] = {nullptr, nullptr}, ev_pix_[2] = {nullptr, nullptr}, ev_fork_ = nullptr;
-  cudaEvent_t ev_fork2_ = nullptr, ev_join_ = nullptr, ev_pjoin_ = nullptr;
+  cudaEvent_t ev_tab_[kPixStreams] = {}, ev_pix_[kPixStreams] = {}, ev_pjoin_[kPixStreams] = {};
+  cudaEvent_t ev_fork_ = nullptr, ev_fork2_ = nullptr, ev_join_ = nullptr;
   bool overlap_build_ = true;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
   bool force_plain_ = false, full_table_ = false;
