@@ -146,10 +146,15 @@ class Engine {
     MS_TRY(cudaEventCreate(&ev1_));
     // the side stream of the potential stack (tables of the next slice while
     // the current slice's potential runs) and its ordering events
-    MS_TRY(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+    // (the side stream's tables and the pass stream's slice steps are short
+    // launches on the critical path: their CTAs are scheduled ahead of the
+    // pixel streams' potentials)
+    int prio_lo = 0, prio_hi = 0;
+    MS_TRY(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    MS_TRY(cudaStreamCreateWithPriority(&side_, cudaStreamNonBlocking, prio_hi));
     pix_[0] = stream_;
     for (int k = 1; k < kPixStreams; ++k) MS_TRY(cudaStreamCreateWithFlags(&pix_[k], cudaStreamNonBlocking));
-    MS_TRY(cudaStreamCreateWithFlags(&pass_, cudaStreamNonBlocking));
+    MS_TRY(cudaStreamCreateWithPriority(&pass_, cudaStreamNonBlocking, prio_hi));
     for (int k = 0; k < kPixStreams; ++k)
       for (cudaEvent_t* e : {&ev_tab_[k], &ev_pix_[k], &ev_pjoin_[k]})
         MS_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
@@ -1821,7 +1826,7 @@ class Engine {
       MS_TRY(cudaStreamWaitEvent(pass_, done, 0));
       launches += 2;
       return enqueue_fused_step(d_stack_.p + (size_t)(it - 1) * N, it == 1, pass_);
-    }, 2);
+    });
     // join the pass stream (also on failure, so that the handle's stream
     // orders after everything enqueued)
     MS_TRY(cudaEventRecord(ev_join_, pass_));
@@ -2723,9 +2728,9 @@ class Engine {
   // are built on the side stream while earlier slices' potentials run.  Slice
   // it's potential runs on pixel stream it % npix (stream 0 is the handle's):
   // consecutive slices are independent, and on several streams the last CTAs
-  // of one launch overlap the first of the next (three streams for a stack
-  // alone; two when slice passes run beside the build, which a third
-  // stream's potentials would crowd out).  Event order: tables(it) after
+  // of one launch overlap the first of the next.  The tables' side stream has
+  // the higher priority, so the next slices' tables are not queued behind
+  // potential CTAs.  Event order: tables(it) after
   // potential(it - npix), which read the same buffer; potential(it) after
   // tables(it).  The side stream joins the handle's stream through the last
   // potentials' dependence on their tables.

@@ -247,9 +247,8 @@ def test_run_with_build_overlap(engine_cls, oracle_mod, n):
 
 
 def test_stack_builds_bit_identical(engine_cls, oracle_mod):
-    """The potential stack's slices are built on several streams (three for a
-    stack alone, two in a run with a stack to build, beside the slice passes on
-    another).  With one FFT plan forced (the same per-pass kernels everywhere),
+    """The potential stack's slices are built on three streams (in a run with
+    a stack to build, beside the slice passes on another).  With one FFT plan forced (the same per-pass kernels everywhere),
     the step-by-step run (one slice potential at a time on the handle's
     stream), the overlapped run, the build-first run and the overlapped run
     after re-uploading the atoms give bit-identical exit waves."""
