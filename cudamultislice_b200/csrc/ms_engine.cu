@@ -124,7 +124,7 @@ class Engine {
     for (int k = 0; k < kPixStreams; ++k)
       for (cudaEvent_t e : {ev_tab_[k], ev_pix_[k], ev_pjoin_[k]})
         if (e) cudaEventDestroy(e);
-    for (cudaEvent_t e : {ev_fork_, ev_fork2_, ev_join_})
+    for (cudaEvent_t e : {ev_fork_, ev_fork2_, ev_join_, ev_dv_, ev_adj_[0], ev_adj_[1]})
       if (e) cudaEventDestroy(e);
     if (side_) cudaStreamDestroy(side_);
     for (int k = 1; k < kPixStreams; ++k)
@@ -158,7 +158,7 @@ class Engine {
     for (int k = 0; k < kPixStreams; ++k)
       for (cudaEvent_t* e : {&ev_tab_[k], &ev_pix_[k], &ev_pjoin_[k]})
         MS_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
-    for (cudaEvent_t* e : {&ev_fork_, &ev_fork2_, &ev_join_})
+    for (cudaEvent_t* e : {&ev_fork_, &ev_fork2_, &ev_join_, &ev_dv_, &ev_adj_[0], &ev_adj_[1]})
       MS_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     MS_TRY(d_loop_sync_.resize(2));
     MS_TRY(d_pass_err_.resize(1));
@@ -2166,7 +2166,7 @@ class Engine {
       MS_TRY(d_U_.resize(N));
       MS_TRY(d_ck_.resize(N * std::max(nck - 1, 1)));
       MS_TRY(d_seg_.resize(N * K));
-      MS_TRY(d_dV_.resize(dLdV ? N * S : N));
+      MS_TRY(d_dV_.resize(dLdV ? N * S : 2 * N));
       if (dLdxy) {
         MS_TRY(d_dxy_.resize(2 * (size_t)natoms_));
         if (int rc = zbin_starts()) return rc;
@@ -2256,7 +2256,10 @@ class Engine {
           PassAArgs a = passa_args(d_G_.p, d_G_.p, 0);
           a.V = d_stack_.p + (size_t)(n - 1) * N;
           a.in2 = d_seg_.p + (size_t)(n - 1 - c) * N;
-          float* dV = dLdV ? d_dV_.p + (size_t)(n - 1) * N : d_dV_.p;
+          // (without dLdV kept per slice: two buffers, slice n in n & 1, free
+          // again once slice n + 2's atom-position adjoint has read it)
+          float* dV = dLdV ? d_dV_.p + (size_t)(n - 1) * N : d_dV_.p + (size_t)(n & 1) * N;
+          if (!dLdV && dLdxy) MS_TRY(cudaStreamWaitEvent(stream_, ev_adj_[n & 1], 0));
           a.out_f = dV;
           a.scale = 1.0f / (float)nx_;
           MS_TRY(pass_a(a, A_INV | A_ADJ | A_FWD, 1));
@@ -2265,10 +2268,19 @@ class Engine {
             const PotArgs pa = pot_args(POT_CONVENTIONAL, n, nullptr);
             const int a0 = hzoff_[pa.kt], a1 = hzoff_[pa.kb + 1];
             const bool sep = separable_ok();
-            MS_TRY(launch_potential_adjoint(pa, dV, d_idx_.p, a0, a1, d_dxy_.p, stream_, sep));
+            // on a second stream: the next slices' adjoint passes do not wait
+            // for it (it reads dV and adds into dL/dxy only)
+            MS_TRY(cudaEventRecord(ev_dv_, stream_));
+            MS_TRY(cudaStreamWaitEvent(pix_[1], ev_dv_, 0));
+            MS_TRY(launch_potential_adjoint(pa, dV, d_idx_.p, a0, a1, d_dxy_.p, pix_[1], sep));
+            MS_TRY(cudaEventRecord(ev_adj_[n & 1], pix_[1]));
             launches += sep ? 2 : 1;
           }
         }
+      }
+      if (dLdxy) {
+        MS_TRY(cudaEventRecord(ev_join_, pix_[1]));
+        MS_TRY(cudaStreamWaitEvent(stream_, ev_join_, 0));
       }
     }
     MS_TRY(cudaEventRecord(ev1_, stream_));
@@ -2994,6 +3006,7 @@ class Engine {
   cudaStream_t pass_ = nullptr;  // slice passes overlapping the stack build (run_conventional_streamed)
   cudaEvent_t ev_tab_[kPixStreams] = {}, ev_pix_[kPixStreams] = {}, ev_pjoin_[kPixStreams] = {};
   cudaEvent_t ev_fork_ = nullptr, ev_fork2_ = nullptr, ev_join_ = nullptr;
+  cudaEvent_t ev_dv_ = nullptr, ev_adj_[2] = {};  // focal-series gradient: dV ready, dV buffer read
   bool overlap_build_ = true;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
   bool force_plain_ = false, full_table_ = false;
