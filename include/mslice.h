@@ -250,7 +250,10 @@ ms_status ms_get_grid(ms_sim* sim, int* nx, int* ny);
 
 /* ---- whole-run entry points (new) ---- */
 /* Builds the potentials of slices 1..S into a device-resident stack (device
- * time of a build that ran in ms_get_last_device_ms). */
+ * time of a build that ran in ms_get_last_device_ms).  The separable
+ * potential's slices run on three streams of the handle (atom tables on a
+ * fourth, at the highest stream priority); the call returns once the stack
+ * is complete, and the result does not depend on the stream order. */
 ms_status ms_build_potential_stack(ms_sim* sim, int* nslices);
 /* Runs conventional slices 1..S from the initial wave (replayed as one
  * captured CUDA graph: on square 256, 512 and 1024 grids a single persistent
