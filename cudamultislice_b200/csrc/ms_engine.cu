@@ -2175,6 +2175,10 @@ class Engine {
     invalidate_graph();  // the sweep below leaves d_psi_ at psi_S
     MS_TRY(cudaMemcpyAsync(d_T_.p, targets, sizeof(float) * N * nd, cudaMemcpyHostToDevice, stream_));
     MS_TRY(cudaMemsetAsync(d_loss_.p, 0, sizeof(double), stream_));
+    // (after any atom-position adjoint still on the second pixel stream, which
+    // an earlier call that failed part-way may have left unjoined)
+    MS_TRY(cudaEventRecord(ev_join_, pix_[1]));
+    MS_TRY(cudaStreamWaitEvent(stream_, ev_join_, 0));
     if (grad && dLdxy) MS_TRY(cudaMemsetAsync(d_dxy_.p, 0, sizeof(double) * 2 * natoms_, stream_));
     // timed from here: the potential stack (when the atoms changed), the sweeps
     MS_TRY(cudaEventRecord(ev0_, stream_));
